@@ -1,0 +1,237 @@
+"""ctypes binding of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+The oracle is a plain-C FP64 restatement of pmlib3d's single-rank path
+(``oracle/pmoracle.c``).  Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU
+baseline leg of ``bench.py`` may import this module; the product library never
+does.
+
+Arrays use the reference's Fortran layouts flattened in C order of the reversed
+shape: a mesh ``(3, nx', ny', nz')`` is a NumPy array of shape ``(nz', ny', nx', 3)``;
+particles ``(3, np)`` are ``(np, 3)``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libpmoracle.so")
+
+
+class Patch(C.Structure):
+    """class_patch, source/pmlib_patch.f:15-27."""
+
+    _fields_ = [
+        ("xmin", C.c_double * 3),
+        ("xmax", C.c_double * 3),
+        ("dx", C.c_double * 3),
+        ("ncell", C.c_int * 3),
+        ("bound_cond", C.c_int * 3),
+        ("nghost", C.c_int),
+        ("fft_seq", C.c_int * 3),
+    ]
+
+
+class Topo(C.Structure):
+    """class_topology, source/pmlib_topology.f:15-30 (one subdomain)."""
+
+    _fields_ = [
+        ("xmin", C.c_double * 3),
+        ("xmax", C.c_double * 3),
+        ("dx", C.c_double * 3),
+        ("ncell", C.c_int * 3),
+        ("nghost", C.c_int * 6),
+        ("bound_cond", C.c_int * 6),
+        ("npart", C.c_int),
+    ]
+
+
+class Params(C.Structure):
+    """Module globals of source/pmlib_parameters.f:54-59 read by the path."""
+
+    _fields_ = [
+        ("poisson_order", C.c_int),
+        ("poisson_kernel", C.c_int),
+        ("regularisation_radius", C.c_double),
+        ("interpolation_order", C.c_int),
+    ]
+
+
+_lib = None
+
+
+def build() -> None:
+    """Compile the oracle with its Makefile (gcc, -O2 -ffp-contract=off)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int)
+        L.pmo_set_threads.argtypes = [C.c_int]
+        L.pmo_parameters_check.argtypes = [C.POINTER(Params)]
+        L.pmo_patch_adjust.argtypes = [C.POINTER(Patch)]
+        L.pmo_topology_cuboid.argtypes = [C.POINTER(Patch), C.c_int, C.POINTER(Topo)]
+        L.pmo_remesh.argtypes = [C.POINTER(Topo), dp, dp, dp, C.c_void_p, C.c_double, C.c_double,
+                                 C.c_int, C.c_int, dp, dp, dp, dp, ip]
+        L.pmo_interp_particle_mesh.argtypes = [C.POINTER(Topo), C.c_int, dp, dp, C.c_int, C.c_int,
+                                               dp, C.c_int, C.c_int, C.c_int]
+        L.pmo_interp_mesh_particle.argtypes = [C.POINTER(Topo), C.c_int, dp, dp, dp, C.c_int]
+        L.pmo_fft_line.argtypes = [dp, dp, C.c_int]
+        L.pmo_ifft_line.argtypes = [dp, dp, C.c_int]
+        L.pmo_kernel_dims.argtypes = [C.POINTER(Patch), C.POINTER(Params), ip, ip]
+        L.pmo_poisson_setup.argtypes = [C.POINTER(Patch), C.POINTER(Params), dp]
+        L.pmo_poisson_kernel_real.argtypes = [C.POINTER(Patch), C.POINTER(Params), dp]
+        L.pmo_poisson_solve.argtypes = [C.POINTER(Patch), C.POINTER(Topo), C.POINTER(Params), dp,
+                                        dp, dp, dp, C.c_int, C.c_int, C.c_int]
+        L.pmo_regularise.argtypes = [C.POINTER(Patch), C.POINTER(Topo), dp, C.c_int, C.c_int,
+                                     C.c_double]
+        L.pmo_si.argtypes = [C.c_double]
+        L.pmo_si.restype = C.c_double
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def set_threads(n: int) -> None:
+    lib().pmo_set_threads(int(n))
+
+
+def make_patch(xmin, xmax, dx, bound_cond=(0, 0, 0), nghost=4, ncell=None, fft_seq=(1, 2, 3)):
+    p = Patch()
+    for d in range(3):
+        p.xmin[d] = xmin[d]
+        p.xmax[d] = xmax[d]
+        p.dx[d] = dx[d]
+        p.bound_cond[d] = bound_cond[d]
+        p.fft_seq[d] = fft_seq[d]
+        p.ncell[d] = ncell[d] if ncell is not None else int(round((xmax[d] - xmin[d]) / dx[d]))
+    p.nghost = nghost
+    return p
+
+
+def make_params(order=6, kernel=1, radius=2.0, interp=3):
+    q = Params()
+    q.poisson_order = order
+    q.poisson_kernel = kernel
+    q.regularisation_radius = radius
+    q.interpolation_order = interp
+    return q
+
+
+def parameters_check(par) -> int:
+    return lib().pmo_parameters_check(C.byref(par))
+
+
+def patch_adjust(patch) -> int:
+    return lib().pmo_patch_adjust(C.byref(patch))
+
+
+def topology_cuboid(patch, interp_order=3):
+    t = Topo()
+    ierr = lib().pmo_topology_cuboid(C.byref(patch), interp_order, C.byref(t))
+    return ierr, t
+
+
+def topo_shape(t, nvar=3):
+    """NumPy shape (nz', ny', nx', nvar) of a mesh on topology t (ghosts included)."""
+    ext = [t.ncell[d] + t.nghost[2 * d] + t.nghost[2 * d + 1] for d in range(3)]
+    return (ext[2], ext[1], ext[0], nvar)
+
+
+def remesh(t, mvort, mdvort=None, mvel=None, mask=None, min_vort=0.0, min_dvort=0.0,
+           incl_ghost=False):
+    n = C.c_int(0)
+    L = lib()
+    mk = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    mkp = None if mk is None else mk.ctypes.data_as(C.c_void_p)
+    L.pmo_remesh(C.byref(t), _p(mvort), _p(mdvort), _p(mvel), mkp, min_vort, min_dvort,
+                 int(incl_ghost), 0, None, None, None, None, C.byref(n))
+    npart = n.value
+    pos = np.zeros((npart, 3))
+    pv = np.zeros((npart, 3))
+    pdv = np.zeros((npart, 3))
+    pvel = np.zeros((npart, 3))
+    ierr = L.pmo_remesh(C.byref(t), _p(mvort), _p(mdvort), _p(mvel), mkp, min_vort, min_dvort,
+                        int(incl_ghost), npart, _p(pos), _p(pv), _p(pdv), _p(pvel), C.byref(n))
+    return ierr, pos, pv, pdv, pvel
+
+
+def interp_particle_mesh(t, order, xpart, part, mesh, clear=True, clear_ghost=False):
+    nvar = part.shape[1]
+    return lib().pmo_interp_particle_mesh(C.byref(t), order, _p(xpart), _p(part), nvar,
+                                          part.shape[0], _p(mesh), mesh.shape[-1], int(clear),
+                                          int(clear_ghost))
+
+
+def interp_mesh_particle(t, order, mesh, pos):
+    out = np.zeros((pos.shape[0], 3))
+    ierr = lib().pmo_interp_mesh_particle(C.byref(t), order, _p(mesh), _p(pos), _p(out),
+                                          pos.shape[0])
+    return ierr, out
+
+
+def fft_line(x, inverse=False):
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    a = x.view(np.float64).copy()
+    o = np.zeros_like(a)
+    f = lib().pmo_ifft_line if inverse else lib().pmo_fft_line
+    f(_p(a), _p(o), x.shape[0])
+    return o.view(np.complex128)
+
+
+def kernel_dims(patch, par):
+    M = (C.c_int * 3)()
+    nk = C.c_int(0)
+    lib().pmo_kernel_dims(C.byref(patch), C.byref(par), M, C.byref(nk))
+    return tuple(M), nk.value
+
+
+def poisson_setup(patch, par):
+    """Returns (ierr, pkernel_fft) with pkernel_fft complex of shape (Mz, My, Mx, ncomp)."""
+    M, nk = kernel_dims(patch, par)
+    buf = np.zeros(2 * nk * M[0] * M[1] * M[2])
+    ierr = lib().pmo_poisson_setup(C.byref(patch), C.byref(par), _p(buf))
+    return ierr, buf.view(np.complex128).reshape(M[2], M[1], M[0], nk)
+
+
+def poisson_kernel_real(patch, par):
+    M, nk = kernel_dims(patch, par)
+    buf = np.zeros(nk * M[0] * M[1] * M[2])
+    ierr = lib().pmo_poisson_kernel_real(C.byref(patch), C.byref(par), _p(buf))
+    return ierr, buf.reshape(M[2], M[1], M[0], nk)
+
+
+def poisson_solve(patch, t, par, pkernel_fft, vort, reg_vort=False, reproj=False,
+                  calc_vecpot=False):
+    """vort is updated in place when reg_vort or reproj; returns (ierr, vel, vecpot)."""
+    vel = np.zeros_like(vort)
+    vecpot = np.zeros_like(vort) if calc_vecpot else None
+    pk = np.ascontiguousarray(pkernel_fft).view(np.float64).reshape(-1)
+    ierr = lib().pmo_poisson_solve(C.byref(patch), C.byref(t), C.byref(par), _p(pk), _p(vort),
+                                   _p(vel), _p(vecpot), int(reg_vort), int(reproj),
+                                   int(calc_vecpot))
+    return ierr, vel, vecpot
+
+
+def regularise(patch, t, mesh, reg_order, filter_width):
+    return lib().pmo_regularise(C.byref(patch), C.byref(t), _p(mesh), mesh.shape[-1], reg_order,
+                                filter_width)
+
+
+def si(x: float) -> float:
+    return lib().pmo_si(float(x))
