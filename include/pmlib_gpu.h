@@ -1,0 +1,159 @@
+/*
+ * pmlib_gpu.h -- C ABI of the B200 implementation of pmlib3d's particle-mesh step.
+ *
+ * Every entry point replaces one Fortran module procedure of pmlib3d (cited below,
+ * paths relative to the pmlib3d project root) and keeps its argument meaning and
+ * error convention: the return value is the reference's `ierr` (0 = success,
+ * -1 = error), and an error prints "[0000](caller) : message" on stdout exactly as
+ * pmlib_write (source/pmlib_write.f:40-48) does.  The same message is available
+ * from pmgpu_last_error().
+ *
+ * Layouts are the reference's Fortran layouts, so a Fortran caller passes C_LOC of
+ * the first element of its arrays:
+ *   mesh      (nvar, 1-nghost(1):ncell(1)+nghost(2), ..., ...)   component fastest
+ *   particles (3, npart)                                          component fastest
+ * Host pointers are copied to and from the GPU inside the call.  The `_dev` entry
+ * points take device pointers and a CUDA stream and copy nothing.
+ *
+ * Precision: the `double` entry points are the FP64 plain path (the drop-in).  The
+ * `_f32` entry points are the FP32 form: deposition, FFTs, spectral multiply and
+ * interpolation in FP32; the Green's function is evaluated in FP64 and stored in FP32.
+ */
+#ifndef PMLIB_GPU_H
+#define PMLIB_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* class_patch, source/pmlib_patch.f:15-27 (level/parent/nsubs are not used by the path) */
+typedef struct {
+  double xmin[3];
+  double xmax[3];
+  double dx[3];
+  int ncell[3];
+  int bound_cond[3]; /* 0 = free (unbounded), 1 = periodic */
+  int nghost;
+  int fft_seq[3];    /* 1-based axis order of the transforms, as set by pmgpu_patch_adjust */
+} pmgpu_patch;
+
+/* class_topology, source/pmlib_topology.f:15-30, for the single subdomain of one GPU */
+typedef struct {
+  double xmin[3];
+  double xmax[3];
+  double dx[3];
+  int ncell[3];
+  int nghost[6];     /* (west, east, south, north, bottom, top) */
+  int bound_cond[6]; /* 0 = exterior free face, 1 = periodic (self-neighbour) face */
+  int npart;
+} pmgpu_topo;
+
+/* the module globals of source/pmlib_parameters.f:54-59 that the path reads */
+typedef struct {
+  int poisson_order;            /* 0, 2, 4, 6, 8, 10 or 100 */
+  int poisson_kernel;           /* 1 (Green's function) or 2 (derivative kernel) */
+  double regularisation_radius; /* epsilon = radius * max(dx) */
+  int interpolation_order;      /* 3 = M4', 4 = M6* */
+} pmgpu_params;
+
+/* Opaque Poisson plan: replaces mesh%pkernel_fft and the pencil topologies that
+ * pmlib_poisson_setup builds.  Holds the Green's function spectrum, the transform
+ * tables and the work buffers on the GPU. */
+typedef struct pmgpu_plan pmgpu_plan;
+
+enum { PMGPU_FP64 = 0, PMGPU_FP32 = 1 };
+
+/* ---- parameters, patch and topology (host-side arithmetic) ---- */
+
+/* source/parameters/pmlib_parameters_check.f:5-105 (kernel, order, radius, interpolation order) */
+int pmgpu_parameters_check(const pmgpu_params *par);
+
+/* source/patch/pmlib_patch_adjust.f:5-166 (free axes grow to a multiple of 16 with ghosts) */
+int pmgpu_patch_adjust(pmgpu_patch *patch);
+
+/* source/topology/pmlib_topology_cuboid.f:5-356 for one subdomain */
+int pmgpu_topology_cuboid(const pmgpu_patch *patch, int interpolation_order, pmgpu_topo *topo);
+
+/* ---- interpolation (source/pmlib_interpolation.f:5-23) ---- */
+
+/* pmlib_interp_particle_mesh, source/interpolation/pmlib_interp_particle_mesh.f:5-22.
+ * Deposits part(nvar, npart) at xpart(3, npart) onto mesh(nvar_mesh, ...) with the
+ * reference's periodic ghost reverse-add.  clear / clear_ghost as in the reference;
+ * without clear the deposit is added to the mesh passed in. */
+int pmgpu_interp_particle_mesh(const pmgpu_topo *topo, const pmgpu_params *par,
+                               const double *xpart, const double *part, int nvar, int npart,
+                               double *mesh, int nvar_mesh, int clear, int clear_ghost);
+int pmgpu_interp_particle_mesh_f32(const pmgpu_topo *topo, const pmgpu_params *par,
+                                   const float *xpart, const float *part, int nvar, int npart,
+                                   float *mesh, int nvar_mesh, int clear, int clear_ghost);
+
+/* pmlib_interp_mesh_particle, source/interpolation/pmlib_interp_mesh_particle.f:5-24.
+ * Interpolates each non-NULL mesh field (3 components each) to the non-NULL particle
+ * array of the same name: vort -> part_vort, dvort -> part_dvort, vel -> part_vel. */
+int pmgpu_interp_mesh_particle(const pmgpu_topo *topo, const pmgpu_params *par,
+                               const double *mesh_vort, const double *mesh_dvort,
+                               const double *mesh_vel, const double *pos, int npart,
+                               double *part_vort, double *part_dvort, double *part_vel);
+int pmgpu_interp_mesh_particle_f32(const pmgpu_topo *topo, const pmgpu_params *par,
+                                   const float *mesh_vort, const float *mesh_dvort,
+                                   const float *mesh_vel, const float *pos, int npart,
+                                   float *part_vort, float *part_dvort, float *part_vel);
+
+/* ---- Poisson solver (source/pmlib_poisson.f:5-30) ---- */
+
+/* pmlib_poisson_setup, source/poisson/pmlib_poisson_setup.f:5-19.  `precision` is
+ * PMGPU_FP64 (plain path) or PMGPU_FP32 (FP32 form).  On success *plan is a new plan. */
+int pmgpu_poisson_setup(const pmgpu_patch *patch, const pmgpu_topo *cuboid,
+                        const pmgpu_params *par, int precision, pmgpu_plan **plan);
+
+/* pmlib_poisson_solve, source/poisson/pmlib_poisson_solve.f:15-34.  vort is the
+ * cuboid vorticity (3, ...) with ghosts; it is overwritten with the regularised
+ * vorticity when reg_vort or reproj is set.  vel receives the velocity; vecpot (may
+ * be NULL) the vector potential when calc_vecpot is set (kernel 1 only). */
+int pmgpu_poisson_solve(pmgpu_plan *plan, double *vort, double *vel, double *vecpot,
+                        int reg_vort, int reproj, int calc_vecpot);
+int pmgpu_poisson_solve_f32(pmgpu_plan *plan, float *vort, float *vel, float *vecpot,
+                            int reg_vort, int reproj, int calc_vecpot);
+
+/* pmlib_regularise, source/regularise/pmlib_regularise.f:5-21: Gaussian-polynomial
+ * spectral filter of order reg_order and width filter_width on a field of nvar <= 3
+ * components, in place. */
+int pmgpu_regularise(pmgpu_plan *plan, double *mesh, int nvar, int reg_order, double filter_width);
+int pmgpu_regularise_f32(pmgpu_plan *plan, float *mesh, int nvar, int reg_order,
+                         double filter_width);
+
+/* replaces the deallocation of mesh%pkernel_fft (source/pmlib_finalise.f:63) */
+void pmgpu_plan_destroy(pmgpu_plan *plan);
+
+/* ---- the whole step: P2M -> unbounded solve + curl -> M2P ----
+ * The caller loop of vortex_codes/vortex_structures/source/main.f:353,397-428,469
+ * with the in-library solver: pmlib_interp_particle_mesh (clear), pmlib_poisson_solve,
+ * pmlib_interp_mesh_particle (vel).  Element type follows the plan's precision.
+ * pmgpu_step copies host arrays in and the velocities out; pmgpu_step_dev works on
+ * device pointers on `stream` (a cudaStream_t, 0 = legacy default stream). */
+int pmgpu_step(pmgpu_plan *plan, const void *pos, const void *part_vort, int npart,
+               void *part_vel);
+int pmgpu_step_dev(pmgpu_plan *plan, const void *d_pos, const void *d_part_vort, int npart,
+                   void *d_part_vel, void *stream);
+
+/* ---- remesh (source/remesh/pmlib_remesh.f:5-28) ----
+ * Two calls, as the Fortran wrapper needs to ALLOCATE between them: the first with
+ * pos == NULL returns the count in *npart; the second fills pos/vort/dvort/vel
+ * (3, npart) in the reference's k-j-i cell order.  mesh_dvort, mesh_vel and mask may
+ * be NULL (flags absent in the reference call). */
+int pmgpu_remesh(const pmgpu_topo *topo, const double *mesh_vort, const double *mesh_dvort,
+                 const double *mesh_vel, const unsigned char *mask, double min_vort,
+                 double min_dvort, int incl_ghost, int max_part, double *pos, double *part_vort,
+                 double *part_dvort, double *part_vel, int *npart);
+
+/* ---- diagnostics ---- */
+const char *pmgpu_last_error(void);
+/* number of this library's kernels launched since the last reset */
+long long pmgpu_launch_count(int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,154 @@
+// green.cuh -- regularised free-space Green's function, evaluated once per grid in
+// FP64 (source/poisson/pmlib_poisson_setup.f:185-1528, level 1).
+//
+// The kernel is sampled on the fully doubled grid centred on r = 0 (the reference's
+// kernel topology, pmlib_topology_kernel.f:109-110) and stored already shifted so
+// that r = 0 sits at index 0 (the fft_shift of pmlib_fft).  Periodic axes add the
+// images at +-1 patch length (:229-256).  The transform of this real, even sequence
+// is real and even in every axis, so the solve keeps one octant of it.
+#pragma once
+
+#include "common.cuh"
+
+namespace pmgpu {
+
+struct GreenParams {
+  int M[3];
+  int bc[3];
+  double dx[3];
+  double xmin[3];  // -(M/2 + 1/2) dx
+  double plen[3];  // image spacing
+  double eps;      // radius * max(dx)
+  double mdx;      // max(dx)
+  int order;
+  int kernel;
+};
+
+// Si(x) = int_0^x sin t / t dt: Maclaurin series for |x| <= 4, otherwise the
+// continued fraction of E1(ix) (Abramowitz & Stegun 5.1.22, modified Lentz).
+__device__ double dev_si(double x) {
+  const double ax = fabs(x);
+  double r;
+  if (ax < 1e-300) return 0.0;
+  if (ax <= 4.0) {
+    double s = 0.0, term = ax;
+    const double x2 = ax * ax;
+    for (int k = 0; k < 60; k++) {
+      const double add = term / (2 * k + 1);
+      s += add;
+      if (fabs(add) < 1e-18 * fabs(s)) break;
+      term *= -x2 / ((2.0 * k + 2.0) * (2.0 * k + 3.0));
+    }
+    r = s;
+  } else {
+    const double tiny = 1e-300;
+    double br = 1.0, bi = ax;
+    double cr = 1.0 / tiny, ci = 0.0;
+    double den = br * br + bi * bi;
+    double dr = br / den, di = -bi / den;
+    double hr = dr, hi = di;
+    for (int i = 1; i < 100000; i++) {
+      const double an = -(double)i * (double)i;
+      br += 2.0;
+      double tr = an * dr + br, ti = an * di + bi;
+      den = tr * tr + ti * ti;
+      dr = tr / den;
+      di = -ti / den;
+      den = cr * cr + ci * ci;
+      const double qr = an * cr / den, qi = -an * ci / den;
+      cr = br + qr;
+      ci = bi + qi;
+      const double delr = cr * dr - ci * di, deli = cr * di + ci * dr;
+      const double nr = hr * delr - hi * deli, ni = hr * deli + hi * delr;
+      hr = nr;
+      hi = ni;
+      if (fabs(delr - 1.0) + fabs(deli) < 1e-16) break;
+    }
+    double sn, cs;
+    sincos(ax, &sn, &cs);
+    r = 0.5 * 3.14159265358979323846 + (hr * (-sn) + hi * cs);
+  }
+  return x < 0 ? -r : r;
+}
+
+// G(r) of kernel 1 for the given order (:245-1460)
+__device__ __forceinline__ double green_k1(const GreenParams &gp, double r) {
+  const double PI = 3.14159265358979323846;
+  const double eps = gp.eps;
+  const double c_1_4pi = 0.25 / PI;
+  const double c_1_sqrt2 = 0.70710678118654752440;
+  const double c_1_sqrt2pi = 1.0 / sqrt(2.0 * PI);
+  const double c_sq2_4pieps = sqrt(2.0) / (4.0 * pow(PI, 1.5) * eps);
+  const int o = gp.order;
+  if (o == 100) {
+    if (r == 0.0) return 1.0 / (2.0 * PI * gp.mdx);
+    return dev_si(PI * r / gp.mdx) / (2.0 * PI * PI * r);
+  }
+  if (r == 0.0) {
+    switch (o) {
+      case 0: return 1.0;
+      case 2: return c_sq2_4pieps;
+      case 4: return 1.5 * c_sq2_4pieps;
+      case 6: return 1.875 * c_sq2_4pieps;
+      case 8: return 2.1875 * c_sq2_4pieps;
+      default: return 2.4609375 * c_sq2_4pieps;
+    }
+  }
+  if (o == 0) return c_1_4pi / r;
+  const double rho = r / eps;
+  const double r2 = rho * rho, r3 = r2 * rho, r5 = r3 * r2, r7 = r5 * r2;
+  const double ex = exp(-0.5 * r2);
+  const double er = erf(c_1_sqrt2 * rho);
+  switch (o) {
+    case 2: return c_1_4pi / r * er;
+    case 4: return c_1_4pi / r * (rho * ex * c_1_sqrt2pi + er);
+    case 6: return c_1_4pi / r * ((1.75 * rho - 0.25 * r3) * ex * c_1_sqrt2pi + er);
+    case 8: return c_1_4pi / r * ((2.375 * rho + (-2.0 / 3.0) * r3 + (1.0 / 24.0) * r5) * ex * c_1_sqrt2pi + er);
+    default:
+      return c_1_4pi / r *
+             ((2.921875 * rho + (-233.0 / 192.0) * r3 + (29.0 / 192.0) * r5 + (-1.0 / 192.0) * r7) * ex *
+                  c_1_sqrt2pi + er);
+  }
+}
+
+// real kernel on the shifted M0 x M1 x M2 grid, x fastest
+__global__ void k_green_real(GreenParams gp, double *__restrict__ gr) {
+  const size_t total = (size_t)gp.M[0] * gp.M[1] * gp.M[2];
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    int s[3];
+    s[0] = (int)(t % gp.M[0]);
+    s[1] = (int)((t / gp.M[0]) % gp.M[1]);
+    s[2] = (int)(t / ((size_t)gp.M[0] * gp.M[1]));
+    double p0[3];
+    for (int e = 0; e < 3; e++) {
+      const int h = gp.M[e] / 2;
+      const int iu = s[e] < h ? s[e] + h + 1 : s[e] - h + 1;  // unshifted 1-based index
+      p0[e] = gp.xmin[e] + ((double)(iu - 1) + 0.5) * gp.dx[e];
+    }
+    double acc = 0.0;
+    for (int kk = -gp.bc[2]; kk <= gp.bc[2]; kk++)
+      for (int jj = -gp.bc[1]; jj <= gp.bc[1]; jj++)
+        for (int ii = -gp.bc[0]; ii <= gp.bc[0]; ii++) {
+          const double px = p0[0] + gp.plen[0] * (double)ii;
+          const double py = p0[1] + gp.plen[1] * (double)jj;
+          const double pz = p0[2] + gp.plen[2] * (double)kk;
+          acc += green_k1(gp, sqrt(px * px + py * py + pz * pz));
+        }
+    gr[t] = acc;
+  }
+}
+
+// octant of the real spectrum, scaled by dx dy dz / (Mx My Mz), in the plan precision
+template <typename R>
+__global__ void k_green_octant(const double2 *__restrict__ spec, int M1, int H, int gM1, int gM2, double f,
+                               R *__restrict__ out) {
+  const size_t total = (size_t)gM2 * gM1 * H;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int kx = (int)(t % H);
+    const int iy = (int)((t / H) % gM1);
+    const int iz = (int)(t / ((size_t)H * gM1));
+    out[t] = (R)(spec[((size_t)iz * M1 + iy) * H + kx].x * f);
+  }
+}
+
+}  // namespace pmgpu

@@ -1,0 +1,557 @@
+// particles.cuh -- particle binning, stable sort, deterministic M4'/M6* deposition
+// (P2M), mesh-to-particle interpolation (M2P) and remesh.
+//
+// P2M (source/interpolation/pmlib_interp_particle_mesh.f) scatters every particle
+// into its 4^3 (M4') or 6^3 (M6*) stencil with the particle loop in index order.
+// Here particles are binned by the reference's base cell NINT((x - xmin) / dx)
+// (:153-155, bit-exact index arithmetic), sorted by bin with a stable radix sort
+// (ties keep particle order), and every cell then gathers the contributions of the
+// bins whose stencil covers it, in a fixed order: no floating-point atomics, and
+// the same result on every run.
+#pragma once
+
+#include "common.cuh"
+
+namespace pmgpu {
+
+// ------------------------------------------------------------------ geometry
+template <typename R> struct PartGeom {
+  int ext[3];     // cuboid extents including ghosts
+  int lo[3];      // 1-based index of the first cuboid point (1 - nghost_lo)
+  int nint[3];    // interior cells
+  int nglo[3];    // ghosts on the low face
+  int bclo[3], bchi[3];  // face types (0 free, 1 periodic)
+  int blo[3];     // base index of bin 0 along each axis
+  int nb[3];      // bins per axis
+  unsigned nbins; // nb0 nb1 nb2 (the sentinel key of skipped particles)
+  R xmin[3], xmax[3], dx[3], c1dx[3];
+};
+
+template <int W> struct Stencil;
+template <> struct Stencil<4> { static constexpr int off = 1; };  // base-1 .. base+2
+template <> struct Stencil<6> { static constexpr int off = 2; };  // base-2 .. base+3
+
+// NINT((x - xmin) * (1/dx)): the product is not contracted and rounding is half
+// away from zero, as Fortran NINT.
+__device__ __forceinline__ long long base_index(double x, double xmin, double c1dx) {
+  const double t = __dmul_rn(__dsub_rn(x, xmin), c1dx);
+  if (!(fabs(t) < 1.0e15)) return (long long)-4611686018427387904LL;
+  return (long long)round(t);
+}
+__device__ __forceinline__ long long base_index(float x, float xmin, float c1dx) {
+  const float t = __fmul_rn(__fsub_rn(x, xmin), c1dx);
+  if (!(fabsf(t) < 1.0e9f)) return (long long)-4611686018427387904LL;
+  return (long long)roundf(t);
+}
+
+// M4' weights at offsets d+1, d, 1-d, 2-d (interp_particle_mesh.f:201-214)
+template <typename R> __device__ __forceinline__ void weights_m4(R d2, R *a) {
+  const R d1 = d2 + R(1), d3 = R(1) - d2, d4 = R(2) - d2;
+  const R t1 = R(2) - d1, t4 = R(2) - d4;
+  a[0] = R(0.5) * (t1 * t1) * (R(1) - d1);
+  a[1] = R(1) - R(2.5) * (d2 * d2) + R(1.5) * (d2 * d2 * d2);
+  a[2] = R(1) - R(2.5) * (d3 * d3) + R(1.5) * (d3 * d3 * d3);
+  a[3] = R(0.5) * (t4 * t4) * (R(1) - d4);
+}
+// M6* weights (interp_particle_mesh.f:564-602)
+template <typename R> __device__ __forceinline__ void weights_m6(R d3, R *a) {
+  const R c1 = R(-1) / R(24), c2 = R(1) / R(24), c3 = R(-1) / R(12);
+  const R d1 = d3 + R(2), d2 = d3 + R(1), d4 = R(1) - d3, d5 = R(2) - d3, d6 = R(3) - d3;
+  R u;
+  u = d1 - R(3);
+  a[0] = c1 * (d1 - R(2)) * (u * u * u) * (R(5) * d1 - R(8));
+  a[1] = c2 * (d2 - R(1)) * (d2 - R(2)) * (R(25) * (d2 * d2 * d2) - R(114) * (d2 * d2) + R(153) * d2 - R(48));
+  a[2] = c3 * (d3 - R(1)) * (R(25) * (d3 * d3 * d3 * d3) - R(38) * (d3 * d3 * d3) - R(3) * (d3 * d3) + R(12) * d3 + R(12));
+  a[3] = c3 * (d4 - R(1)) * (R(25) * (d4 * d4 * d4 * d4) - R(38) * (d4 * d4 * d4) - R(3) * (d4 * d4) + R(12) * d4 + R(12));
+  a[4] = c2 * (d5 - R(1)) * (d5 - R(2)) * (R(25) * (d5 * d5 * d5) - R(114) * (d5 * d5) + R(153) * d5 - R(48));
+  u = d6 - R(3);
+  a[5] = c1 * (d6 - R(2)) * (u * u * u) * (R(5) * d6 - R(8));
+}
+template <typename R, int W> __device__ __forceinline__ void weights(R d, R *a) {
+  if constexpr (W == 4) weights_m4<R>(d, a); else weights_m6<R>(d, a);
+}
+
+// normalised offset of x from its base cell centre
+template <typename R>
+__device__ __forceinline__ R cell_offset(R x, R xmin, R dx, long long b, R scale) {
+  return (x - xmin - dx * ((R)b - R(0.5))) * scale;
+}
+
+// ------------------------------------------------------------------ binning
+// key = flattened base cell in the bin box; particles whose stencil misses the
+// cuboid, or which lie outside [xmin, xmax] across a periodic face (all weights
+// zeroed, :229-246), get the sentinel key nbins and are skipped by P2M.
+template <typename R, int W>
+__global__ void k_bin(PartGeom<R> g, const R *__restrict__ pos, int n, unsigned *__restrict__ key,
+                      int *__restrict__ val, unsigned *__restrict__ counts) {
+  constexpr int off = Stencil<W>::off;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    bool ok = true;
+    long long bi[3];
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+      const R x = pos[(size_t)3 * p + e];
+      const long long b = base_index(x, g.xmin[e], g.c1dx[e]);
+      const long long first = b - off, last = b - off + W - 1;
+      const int hi = g.lo[e] + g.ext[e] - 1;
+      if (!(last >= g.lo[e] && first <= hi)) ok = false;
+      if (g.bclo[e] != 0 && x < g.xmin[e]) ok = false;
+      if (g.bchi[e] != 0 && x > g.xmax[e]) ok = false;
+      bi[e] = b - g.blo[e];
+    }
+    unsigned k = g.nbins;
+    if (ok) {
+      k = (unsigned)(bi[0] + (long long)g.nb[0] * (bi[1] + (long long)g.nb[1] * bi[2]));
+      atomicAdd(&counts[k], 1u);
+    }
+    key[p] = k;
+    val[p] = p;
+  }
+}
+
+// ------------------------------------------------------------------ scans (exclusive, u32)
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_PER_THREAD = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_PER_THREAD;
+
+__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned *warp_sums, unsigned *total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    unsigned s = lane < nw ? warp_sums[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      unsigned y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < nw) warp_sums[lane] = s;
+    if (lane == nw - 1) *total = s;
+  }
+  __syncthreads();
+  const unsigned before = wid > 0 ? warp_sums[wid - 1] : 0u;
+  const unsigned r = before + x - v;
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const unsigned *__restrict__ in, size_t n,
+                                                              unsigned *__restrict__ part) {
+  __shared__ unsigned ws[32];
+  __shared__ unsigned tot;
+  const size_t base = (size_t)blockIdx.x * SCAN_TILE + (size_t)threadIdx.x * SCAN_PER_THREAD;
+  unsigned s = 0;
+#pragma unroll
+  for (int i = 0; i < SCAN_PER_THREAD; i++)
+    if (base + i < n) s += in[base + i];
+  block_exclusive_scan(s, ws, &tot);
+  if (threadIdx.x == 0) part[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_partials(unsigned *__restrict__ part, int np) {
+  __shared__ unsigned ws[32];
+  __shared__ unsigned tot;
+  const int per = (np + blockDim.x - 1) / blockDim.x;
+  const int b = threadIdx.x * per;
+  unsigned s = 0;
+  for (int i = 0; i < per; i++)
+    if (b + i < np) s += part[b + i];
+  unsigned off = block_exclusive_scan(s, ws, &tot);
+  for (int i = 0; i < per; i++)
+    if (b + i < np) {
+      const unsigned v = part[b + i];
+      part[b + i] = off;
+      off += v;
+    }
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const unsigned *__restrict__ in, size_t n,
+                                                             const unsigned *__restrict__ part,
+                                                             unsigned *__restrict__ out) {
+  __shared__ unsigned ws[32];
+  __shared__ unsigned tot;
+  const size_t base = (size_t)blockIdx.x * SCAN_TILE + (size_t)threadIdx.x * SCAN_PER_THREAD;
+  unsigned v[SCAN_PER_THREAD];
+  unsigned s = 0;
+#pragma unroll
+  for (int i = 0; i < SCAN_PER_THREAD; i++) {
+    v[i] = (base + i < n) ? in[base + i] : 0u;
+    s += v[i];
+  }
+  unsigned off = block_exclusive_scan(s, ws, &tot) + part[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < SCAN_PER_THREAD; i++) {
+    if (base + i < n) out[base + i] = off;
+    off += v[i];
+  }
+}
+
+// ------------------------------------------------------------------ stable LSB radix sort
+constexpr int RADIX_THREADS = 1024;
+constexpr int RADIX_PER_THREAD = 4;
+constexpr int RADIX_TILE = RADIX_THREADS * RADIX_PER_THREAD;
+constexpr int RADIX_MAXBITS = 10;
+
+__global__ void __launch_bounds__(RADIX_THREADS) k_radix_hist(const unsigned *__restrict__ key, int n, int shift,
+                                                              int bits, unsigned *__restrict__ ghist, int nblk) {
+  __shared__ unsigned h[1 << RADIX_MAXBITS];
+  const int nbk = 1 << bits;
+  for (int i = threadIdx.x; i < nbk; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  const int base = blockIdx.x * RADIX_TILE;
+  for (int i = threadIdx.x; i < RADIX_TILE; i += blockDim.x) {
+    const int q = base + i;
+    if (q < n) atomicAdd(&h[(key[q] >> shift) & (nbk - 1)], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nbk; i += blockDim.x) ghist[(size_t)i * nblk + blockIdx.x] = h[i];
+}
+
+// stable scatter: elements keep their order within a digit (tile order, then
+// round, then warp, then lane)
+__global__ void __launch_bounds__(RADIX_THREADS) k_radix_scatter(const unsigned *__restrict__ key_in,
+                                                                 const int *__restrict__ val_in, int n, int shift,
+                                                                 int bits, const unsigned *__restrict__ goff,
+                                                                 int nblk, unsigned *__restrict__ key_out,
+                                                                 int *__restrict__ val_out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nbk = 1 << bits;
+  unsigned short *cnt = reinterpret_cast<unsigned short *>(smem_raw);  // [32][nbk]
+  unsigned *run = reinterpret_cast<unsigned *>(smem_raw + sizeof(unsigned short) * 32 * nbk);
+  unsigned *tot = run + nbk;
+  unsigned *boff = tot + nbk;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int i = threadIdx.x; i < nbk; i += blockDim.x) {
+    run[i] = 0;
+    boff[i] = goff[(size_t)i * nblk + blockIdx.x];
+  }
+  const int base = blockIdx.x * RADIX_TILE;
+  for (int round = 0; round < RADIX_PER_THREAD; round++) {
+    for (int i = threadIdx.x; i < 32 * nbk; i += blockDim.x) cnt[i] = 0;
+    __syncthreads();
+    const int q = base + round * RADIX_THREADS + threadIdx.x;
+    const bool valid = q < n;
+    unsigned k = 0;
+    int d = nbk;  // invalid lanes share a digit nobody uses
+    if (valid) {
+      k = key_in[q];
+      d = (int)((k >> shift) & (unsigned)(nbk - 1));
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const unsigned lt = peers & ((1u << lane) - 1u);
+    const int rank = __popc(lt);
+    if (valid && rank == 0) cnt[wid * nbk + d] = (unsigned short)__popc(peers);
+    __syncthreads();
+    for (int dd = threadIdx.x; dd < nbk; dd += blockDim.x) {
+      unsigned s = 0;
+      for (int w = 0; w < 32; w++) {
+        const unsigned c = cnt[w * nbk + dd];
+        cnt[w * nbk + dd] = (unsigned short)s;
+        s += c;
+      }
+      tot[dd] = s;
+    }
+    __syncthreads();
+    if (valid) {
+      const unsigned dst = boff[d] + run[d] + cnt[wid * nbk + d] + rank;
+      key_out[dst] = k;
+      val_out[dst] = val_in[q];
+    }
+    __syncthreads();
+    for (int dd = threadIdx.x; dd < nbk; dd += blockDim.x) run[dd] += tot[dd];
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ deposition (gather)
+// A CTA owns TX x TY cell columns and a chunk of ZC cell layers, and marches up the
+// bin layers.  For every bin layer it stages the particles of the (TX+W-1) x
+// (TY+W-1) bins that reach its columns in shared memory (weights precomputed), and
+// each thread adds them to a rolling window of W cell layers held in registers.
+// A cell layer is final once the last bin layer that reaches it has been added.
+constexpr int DEP_TX = 32;
+constexpr int DEP_TY = 8;
+
+template <typename R, int W, int NV>
+__global__ void __launch_bounds__(DEP_TX *DEP_TY) k_deposit(PartGeom<R> g, const R *__restrict__ pos,
+                                                            const R *__restrict__ val, int vstride,
+                                                            const unsigned *__restrict__ start,
+                                                            const int *__restrict__ perm, R *__restrict__ mesh,
+                                                            int mstride, int ZC, int cap, int clear_mode) {
+  constexpr int BX = DEP_TX + W - 1, BY = DEP_TY + W - 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *wxs = reinterpret_cast<R *>(smem_raw);  // [W][cap]
+  R *wys = wxs + W * cap;                    // [W][cap]
+  R *wzs = wys + W * cap;                    // [W][cap]
+  R *vs = wzs + W * cap;                     // [NV][cap]
+  int *btab = reinterpret_cast<int *>(vs + NV * cap);  // [BY][BX][2] concatenated ranges
+  int *rowg = btab + 2 * BX * BY;                      // [BY] global start of row
+  int *rowo = rowg + BY;                               // [BY+1] concatenated offset of row
+
+  const int tx = threadIdx.x % DEP_TX, ty = threadIdx.x / DEP_TX;
+  const int x0 = blockIdx.x * DEP_TX, y0 = blockIdx.y * DEP_TY;
+  const int zc0 = blockIdx.z * ZC, zc1 = min(zc0 + ZC, g.ext[2]);
+  const int cx = x0 + tx, cy = y0 + ty;
+  const bool active = cx < g.ext[0] && cy < g.ext[1];
+
+  // acc[s] is cell layer bz - (W - 1) + s while bin layer bz is added; after the
+  // layer acc[0] is final and the window shifts up by one
+  R acc[W][NV];
+#pragma unroll
+  for (int s = 0; s < W; s++)
+#pragma unroll
+    for (int c = 0; c < NV; c++) acc[s][c] = R(0);
+
+  const int bz_end = zc1 + W - 2;  // last bin layer (inclusive)
+  for (int bz = zc0; bz <= bz_end; bz++) {
+    // ---- row ranges of this bin layer
+    if (threadIdx.x < BY) {
+      const int r = threadIdx.x, by = y0 + r;
+      int gs = 0, ge = 0;
+      if (by < g.nb[1] && bz < g.nb[2] && x0 < g.nb[0]) {
+        const unsigned rb = (unsigned)g.nb[0] * ((unsigned)by + (unsigned)g.nb[1] * (unsigned)bz);
+        const int xl = min(x0 + BX, g.nb[0]);
+        gs = (int)start[rb + x0];
+        ge = (int)start[rb + xl];
+      }
+      rowg[r] = gs;
+      rowo[r + 1] = ge - gs;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      rowo[0] = 0;
+      for (int r = 0; r < BY; r++) rowo[r + 1] += rowo[r];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < BX * BY; i += blockDim.x) {
+      const int r = i / BX, bx = i - r * BX;
+      const int by = y0 + r, gx = x0 + bx;
+      int cs = 0, ce = 0;
+      if (by < g.nb[1] && bz < g.nb[2] && gx < g.nb[0]) {
+        const unsigned b = (unsigned)gx + (unsigned)g.nb[0] * ((unsigned)by + (unsigned)g.nb[1] * (unsigned)bz);
+        cs = rowo[r] + ((int)start[b] - rowg[r]);
+        ce = rowo[r] + ((int)start[b + 1] - rowg[r]);
+      }
+      btab[2 * i] = cs;
+      btab[2 * i + 1] = ce;
+    }
+    const int total = rowo[BY];
+    __syncthreads();
+    for (int c0 = 0; c0 < total; c0 += cap) {
+      const int c1 = min(total, c0 + cap);
+      // ---- stage particles [c0, c1) with their weights
+      for (int q = c0 + threadIdx.x; q < c1; q += blockDim.x) {
+        int r = 0;
+        while (r + 1 < BY && rowo[r + 1] <= q) r++;
+        const int gi = rowg[r] + (q - rowo[r]);
+        const int p = perm[gi];
+        const int i = q - c0;
+        R wv[3][W];
+#pragma unroll
+        for (int e = 0; e < 3; e++) {
+          const R x = pos[(size_t)3 * p + e];
+          const long long b = base_index(x, g.xmin[e], g.c1dx[e]);
+          weights<R, W>(cell_offset<R>(x, g.xmin[e], g.dx[e], b, g.c1dx[e]), wv[e]);
+        }
+#pragma unroll
+        for (int s = 0; s < W; s++) {
+          wxs[s * cap + i] = wv[0][s];
+          wys[s * cap + i] = wv[1][s];
+          wzs[s * cap + i] = wv[2][s];
+        }
+#pragma unroll
+        for (int c = 0; c < NV; c++) vs[c * cap + i] = val[(size_t)vstride * p + c];
+      }
+      __syncthreads();
+      if (active) {
+#pragma unroll 1
+        for (int ry = 0; ry < W; ry++) {
+          const int r = ty + ry;      // bin row in the tile
+          const int sy = W - 1 - ry;  // stencil position of this cell row
+#pragma unroll 1
+          for (int rx = 0; rx < W; rx++) {
+            const int sx = W - 1 - rx;
+            const int bi = r * BX + tx + rx;
+            const int lo = max(btab[2 * bi], c0), hi = min(btab[2 * bi + 1], c1);
+            for (int q = lo; q < hi; q++) {
+              const int i = q - c0;
+              const R wxy = wxs[sx * cap + i] * wys[sy * cap + i];
+              R v[NV];
+#pragma unroll
+              for (int c = 0; c < NV; c++) v[c] = vs[c * cap + i];
+#pragma unroll
+              for (int sz = 0; sz < W; sz++) {
+                const R w = wxy * wzs[sz * cap + i];
+#pragma unroll
+                for (int c = 0; c < NV; c++) acc[sz][c] += w * v[c];
+              }
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+    // ---- cell layer bz - (W - 1) is complete
+    const int cz = bz - (W - 1);
+    if (active && cz >= zc0 && cz < zc1) {
+      const size_t m = (((size_t)cz * g.ext[1] + cy) * g.ext[0] + cx) * mstride;
+      const int ii = cx + g.lo[0], jj = cy + g.lo[1], kk = cz + g.lo[2];
+      const bool ghost = ii < 1 || ii > g.nint[0] || jj < 1 || jj > g.nint[1] || kk < 1 || kk > g.nint[2];
+      const bool overwrite = clear_mode == 1 || (clear_mode == 2 && ghost);
+#pragma unroll
+      for (int c = 0; c < NV; c++) mesh[m + c] = overwrite ? acc[0][c] : mesh[m + c] + acc[0][c];
+    }
+#pragma unroll
+    for (int s = 0; s + 1 < W; s++)
+#pragma unroll
+      for (int c = 0; c < NV; c++) acc[s][c] = acc[s + 1][c];
+#pragma unroll
+    for (int c = 0; c < NV; c++) acc[W - 1][c] = R(0);
+  }
+}
+
+// periodic ghost reverse-add of P2M, one axis (pmlib_mesh_map_ghost.f:119-207 with
+// pmlib_comm_unpack.f:269-273): both strips [1-ngl, ngh] and [N-ngl+1, N+ngh]
+// receive the sum of the two, from the values before the exchange.
+template <typename R>
+__global__ void k_ghost_add(R *__restrict__ mesh, int ex, int ey, int ez, int nv, int axis, int N, int ngl,
+                            int ngh) {
+  const int e[3] = {ex, ey, ez};
+  const int S = ngl + ngh;
+  const int o1 = axis == 0 ? 1 : 0, o2 = axis == 2 ? 1 : 2;
+  const long long total = (long long)S * e[o1] * e[o2];
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int s = (int)(t % S);
+    const long long r = t / S;
+    const int a = (int)(r % e[o1]), b = (int)(r / e[o1]);
+    int iw[3], ie[3];
+    iw[o1] = a; iw[o2] = b; iw[axis] = s;
+    ie[o1] = a; ie[o2] = b; ie[axis] = N + s;
+    const size_t mw = (((size_t)iw[2] * ey + iw[1]) * ex + iw[0]) * nv;
+    const size_t me = (((size_t)ie[2] * ey + ie[1]) * ex + ie[0]) * nv;
+    for (int c = 0; c < nv; c++) {
+      const R w = mesh[mw + c], v = mesh[me + c];
+      mesh[me + c] = v + w;
+      mesh[mw + c] = w + v;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ M2P
+// source/interpolation/pmlib_interp_mesh_particle.f:76-409 (M4'), :412-1266 (M6*):
+// stencil indices clamp to the cuboid with zero weight, no particle is skipped, and
+// the M4' branch scales the y and z offsets by 1/dx(1) (:115-116).
+template <typename R, int W>
+__global__ void k_m2p(PartGeom<R> g, const R *__restrict__ pos, const int *__restrict__ order, int n,
+                      const R *__restrict__ f0, const R *__restrict__ f1, const R *__restrict__ f2,
+                      R *__restrict__ o0, R *__restrict__ o1, R *__restrict__ o2) {
+  constexpr int off = Stencil<W>::off;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int p = order ? order[i] : i;
+    R w[3][W];
+    int idx[3][W];
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+      const R x = pos[(size_t)3 * p + e];
+      long long b = base_index(x, g.xmin[e], g.c1dx[e]);
+      const R scale = (W == 4) ? g.c1dx[0] : g.c1dx[e];
+      const long long bc = b < -(1LL << 40) ? 0 : b;
+      weights<R, W>(cell_offset<R>(x, g.xmin[e], g.dx[e], bc, scale), w[e]);
+      const long long hi = g.lo[e] + g.ext[e] - 1;
+#pragma unroll
+      for (int s = 0; s < W; s++) {
+        long long ii = bc - off + s;
+        if (b < -(1LL << 40)) { w[e][s] = R(0); ii = g.lo[e]; }
+        if (ii < g.lo[e]) { w[e][s] = R(0); ii = g.lo[e]; }
+        if (ii > hi) { w[e][s] = R(0); ii = hi; }
+        idx[e][s] = (int)(ii - g.lo[e]);
+      }
+    }
+    const R *fs[3] = {f0, f1, f2};
+    R *os[3] = {o0, o1, o2};
+#pragma unroll
+    for (int f = 0; f < 3; f++) {
+      if (!fs[f]) continue;
+      const R *m = fs[f];
+      R a0 = R(0), a1 = R(0), a2 = R(0);
+#pragma unroll
+      for (int sk = 0; sk < W; sk++)
+#pragma unroll
+        for (int sj = 0; sj < W; sj++) {
+          const size_t rowb = ((size_t)idx[2][sk] * g.ext[1] + idx[1][sj]) * g.ext[0];
+          const R wjk = w[1][sj] * w[2][sk];
+#pragma unroll
+          for (int si = 0; si < W; si++) {
+            const R wt = w[0][si] * wjk;
+            const R *q = m + (rowb + idx[0][si]) * 3;
+            a0 += wt * __ldg(q);
+            a1 += wt * __ldg(q + 1);
+            a2 += wt * __ldg(q + 2);
+          }
+        }
+      os[f][(size_t)3 * p + 0] = a0;
+      os[f][(size_t)3 * p + 1] = a1;
+      os[f][(size_t)3 * p + 2] = a2;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ remesh
+// source/remesh/pmlib_remesh.f:84-226: a particle per kept cell, cells in k-j-i order
+__global__ void k_remesh_flag(PartGeom<double> g, const double *__restrict__ vort,
+                              const double *__restrict__ dvort, const unsigned char *__restrict__ mask,
+                              double min_vort, double min_dvort, int incl_ghost, unsigned *__restrict__ flag) {
+  const size_t total = (size_t)g.ext[0] * g.ext[1] * g.ext[2];
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % g.ext[0]) + g.lo[0];
+    const int j = (int)((t / g.ext[0]) % g.ext[1]) + g.lo[1];
+    const int k = (int)(t / ((size_t)g.ext[0] * g.ext[1])) + g.lo[2];
+    const int ii[3] = {i, j, k};
+    bool place = true;
+    for (int e = 0; e < 3; e++) {
+      const bool in = (ii[e] >= 1 && ii[e] <= g.nint[e]) || (incl_ghost && ii[e] < 1 && g.bclo[e] == 0) ||
+                      (incl_ghost && ii[e] > g.nint[e] && g.bchi[e] == 0);
+      place = place && in;
+    }
+    const double *v = vort + 3 * t;
+    const double s = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    double ds = 0.0;
+    if (dvort) {
+      const double *dv = dvort + 3 * t;
+      ds = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+    }
+    if (place && (s > min_vort || ds > min_dvort)) place = mask ? (mask[t] != 0) : true;
+    else place = false;
+    flag[t] = place ? 1u : 0u;
+  }
+}
+
+__global__ void k_remesh_fill(PartGeom<double> g, const double *__restrict__ vort,
+                              const double *__restrict__ dvort, const double *__restrict__ vel,
+                              const unsigned *__restrict__ flag, const unsigned *__restrict__ slot,
+                              double *__restrict__ pos, double *__restrict__ pv, double *__restrict__ pdv,
+                              double *__restrict__ pvel) {
+  const size_t total = (size_t)g.ext[0] * g.ext[1] * g.ext[2];
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    if (!flag[t]) continue;
+    const int ii[3] = {(int)(t % g.ext[0]) + g.lo[0], (int)((t / g.ext[0]) % g.ext[1]) + g.lo[1],
+                       (int)(t / ((size_t)g.ext[0] * g.ext[1])) + g.lo[2]};
+    const size_t q = 3 * (size_t)slot[t];
+    for (int e = 0; e < 3; e++) {
+      pos[q + e] = g.xmin[e] + ((double)(ii[e] - 1) + 0.5) * g.dx[e];
+      pv[q + e] = vort[3 * t + e];
+      if (pdv) pdv[q + e] = dvort ? dvort[3 * t + e] : 0.0;
+      if (pvel) pvel[q + e] = vel ? vel[3 * t + e] : 0.0;
+    }
+  }
+}
+
+}  // namespace pmgpu

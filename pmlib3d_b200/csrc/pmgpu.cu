@@ -1,0 +1,1144 @@
+// pmgpu.cu -- C ABI of the B200 particle-mesh step (the library's one translation
+// unit: it includes the kernel headers, so no relocatable device code is needed).
+#include "../../include/pmlib_gpu.h"
+
+#include "common.cuh"
+#include "fft.cuh"
+#include "green.cuh"
+#include "particles.cuh"
+#include "solve.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace pmgpu {
+
+long long g_launches = 0;
+
+static char g_err[512] = "";
+static std::mutex g_mu;
+
+// source/pmlib_write.f:40-48 format for rank 0
+void set_error(const char *caller, const char *msg) {
+  snprintf(g_err, sizeof(g_err), "[%04d](%s) : %s", 0, caller, msg);
+  printf("%s\n", g_err);
+  fflush(stdout);
+}
+
+bool cuda_ok(cudaError_t e, const char *caller) {
+  if (e == cudaSuccess) return true;
+  set_error(caller, cudaGetErrorString(e));
+  return false;
+}
+
+#define CK(expr, caller)                         \
+  do {                                           \
+    if (!::pmgpu::cuda_ok((expr), (caller))) {   \
+      return -1;                                 \
+    }                                            \
+  } while (0)
+#define CKL(caller) CK(cudaGetLastError(), caller)
+
+// ------------------------------------------------------------------ per-device tables
+static bool g_dev_ready[128];
+
+static int ensure_device(const char *caller) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev), caller);
+  if (dev >= 0 && dev < 128 && g_dev_ready[dev]) return 0;
+  static float t32[18][17][2];
+  static double t64[18][17][2];
+  const long double twopi = 2.0L * acosl(-1.0L);
+  for (int R = 1; R < 18; R++)
+    for (int m = 0; m < 17; m++) {
+      long double a = (m < R) ? twopi * (long double)m / (long double)R : 0.0L;
+      t64[R][m][0] = (double)cosl(a);
+      t64[R][m][1] = (double)sinl(a);
+      t32[R][m][0] = (float)cosl(a);
+      t32[R][m][1] = (float)sinl(a);
+    }
+  CK(cudaMemcpyToSymbol(c_cs32, t32, sizeof(t32)), caller);
+  CK(cudaMemcpyToSymbol(c_cs64, t64, sizeof(t64)), caller);
+  if (dev >= 0 && dev < 128) g_dev_ready[dev] = true;
+  return 0;
+}
+
+// ------------------------------------------------------------------ device buffers
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes, const char *caller) {
+    if (bytes <= cap && p) return 0;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t b = std::max<size_t>(bytes, 256);
+    CK(cudaMalloc(&p, b), caller);
+    cap = b;
+    return 0;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <typename T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+// ------------------------------------------------------------------ FFT plans
+typedef std::complex<long double> cld;
+
+static bool supported_radix(int r) {
+  return r == 2 || r == 3 || r == 4 || r == 5 || r == 7 || r == 8 || r == 11 || r == 13 || r == 16 || r == 17;
+}
+
+// radices: powers of two as 16, then 8/4/2; the other primes ascending
+static bool make_fft(int n, int extM, FftDesc &d, std::vector<cld> &tw) {
+  if (n < 1) return false;
+  std::vector<int> pf;
+  int m = n;
+  for (int p = 2; (long long)p * p <= m; p++)
+    while (m % p == 0) {
+      pf.push_back(p);
+      m /= p;
+    }
+  if (m > 1) pf.push_back(m);
+  int c2 = (int)std::count(pf.begin(), pf.end(), 2);
+  std::vector<int> rad;
+  while (c2 >= 4) {
+    rad.push_back(16);
+    c2 -= 4;
+  }
+  if (c2 == 3) rad.push_back(8);
+  else if (c2 == 2) rad.push_back(4);
+  else if (c2 == 1) rad.push_back(2);
+  std::vector<int> odd;
+  for (int p : pf)
+    if (p != 2) odd.push_back(p);
+  std::sort(odd.begin(), odd.end());
+  for (int p : odd) rad.push_back(p);
+  if ((int)rad.size() > FFT_MAXPASS) return false;
+  memset(&d, 0, sizeof(d));
+  d.n = n;
+  d.npass = (int)rad.size();
+  const long double twopi = 2.0L * acosl(-1.0L);
+  tw.clear();
+  long long ns = 1;
+  for (int p = 0; p < d.npass; p++) {
+    const int R = rad[p];
+    d.rad[p] = R;
+    d.ns[p] = (int)ns;
+    d.twoff[p] = (int)tw.size();
+    const long long den = ns * R;
+    for (long long k = 0; k < ns; k++)
+      for (int r = 1; r < R; r++) {
+        const long long q = (k * r) % den;
+        const long double a = twopi * (long double)q / (long double)den;
+        tw.push_back(cld(cosl(a), -sinl(a)));
+      }
+    d.rootoff[p] = (int)tw.size();
+    if (!supported_radix(R))
+      for (int q = 0; q < R; q++) {
+        const long double a = twopi * (long double)q / (long double)R;
+        tw.push_back(cld(cosl(a), -sinl(a)));
+      }
+    ns *= R;
+  }
+  d.ntw = (int)tw.size();
+  d.extoff = 0;
+  d.next = 0;
+  if (extM > 0) {
+    d.extoff = (int)tw.size();
+    d.next = extM / 2 + 1;
+    for (int k = 0; k < d.next; k++) {
+      const long double a = twopi * (long double)k / (long double)extM;
+      tw.push_back(cld(cosl(a), -sinl(a)));
+    }
+  }
+  return true;
+}
+
+template <typename R> static int upload_tw(const std::vector<cld> &tw, DevBuf &buf, const char *caller) {
+  typedef typename cplx_t<R>::type C;
+  std::vector<C> h(tw.size() + 1);
+  for (size_t i = 0; i < tw.size(); i++) h[i] = mk((R)tw[i].real(), (R)tw[i].imag());
+  if (buf.ensure(sizeof(C) * h.size(), caller)) return -1;
+  CK(cudaMemcpy(buf.p, h.data(), sizeof(C) * h.size(), cudaMemcpyHostToDevice), caller);
+  return 0;
+}
+
+// lines per CTA for a ping-pong transform of length n with nc components
+static int lines_for(int n, int nc, size_t csize, int ntw) {
+  const size_t budget = 100 * 1024;
+  const size_t twb = (size_t)((ntw + 1) & ~1) * csize;
+  size_t per = 2 * (size_t)nc * n * csize;
+  long long k = (budget > twb) ? (long long)((budget - twb) / per) : 0;
+  if (k < 1) k = 1;
+  if (k > 16) k = 16;
+  return (int)k;
+}
+static size_t fft_smem(int n, int lines, size_t csize, int ntw) {
+  return (size_t)((ntw + 1) & ~1) * csize + 2 * (size_t)lines * n * csize;
+}
+
+}  // namespace pmgpu
+
+using namespace pmgpu;
+
+// ------------------------------------------------------------------ plan object
+struct Geometry {
+  int ext[3], off[3], P[3], M[3], H, N2;
+  int allper;
+};
+
+struct pmgpu_plan {
+  int prec;
+  pmgpu_patch patch;
+  pmgpu_topo topo;
+  pmgpu_params par;
+  Geometry g;
+  FftDesc fx, fy, fz;
+  DevBuf twx, twy, twz;
+  DevBuf kxt, kyt, kzt;
+  DevBuf green;
+  int gM1, gM2;
+  double eps;
+  DevBuf X, Y, Y2, Y3;
+  DevBuf mesh_w, mesh_u, mesh_a, mesh_b;
+  DevBuf h_pos, h_val, h_out;  // device mirrors used by host-pointer calls
+  // particle scratch
+  DevBuf key, val, key2, val2, counts, start, spart, hist;
+  const int *perm;  // sorted order of the last deposit (device)
+  int perm_n;
+  ~pmgpu_plan() {
+    DevBuf *bs[] = {&twx, &twy, &twz, &kxt, &kyt, &kzt, &green, &X, &Y, &Y2, &Y3, &mesh_w, &mesh_u,
+                    &mesh_a, &mesh_b, &h_pos, &h_val, &h_out, &key, &val, &key2, &val2, &counts,
+                    &start, &spart, &hist};
+    for (DevBuf *b : bs) b->release();
+  }
+};
+
+namespace pmgpu {
+
+// particle scratch shared by calls that have no plan
+struct Scratch {
+  DevBuf key, val, key2, val2, counts, start, spart, hist;
+  DevBuf a, b, c, d, e, f, g, h;
+};
+static Scratch &scratch() {
+  static Scratch s;
+  return s;
+}
+
+static size_t mesh_points(const pmgpu_topo *t) {
+  size_t n = 1;
+  for (int d = 0; d < 3; d++) n *= (size_t)(t->ncell[d] + t->nghost[2 * d] + t->nghost[2 * d + 1]);
+  return n;
+}
+
+// ------------------------------------------------------------------ scans
+static int exclusive_scan(const unsigned *in, unsigned *out, size_t n, DevBuf &part, cudaStream_t st,
+                          const char *caller) {
+  const size_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+  if (part.ensure(sizeof(unsigned) * (nb + 1), caller)) return -1;
+  k_scan_reduce<<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, part.as<unsigned>());
+  PM_LAUNCHED();
+  k_scan_partials<<<1, SCAN_THREADS, 0, st>>>(part.as<unsigned>(), (int)nb);
+  PM_LAUNCHED();
+  k_scan_apply<<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, part.as<unsigned>(), out);
+  PM_LAUNCHED();
+  CKL(caller);
+  return 0;
+}
+
+// stable sort of (key, val); returns via *kout/*vout the buffers holding the result
+static int radix_sort(unsigned maxkey, int n, DevBuf &k1, DevBuf &v1, DevBuf &k2, DevBuf &v2, DevBuf &hist,
+                      DevBuf &part, cudaStream_t st, const unsigned **kout, const int **vout,
+                      const char *caller) {
+  int bits = 1;
+  while (bits < 32 && (maxkey >> bits) != 0) bits++;
+  const int passes = (bits + RADIX_MAXBITS - 1) / RADIX_MAXBITS;
+  const int db = (bits + passes - 1) / passes;
+  const int nbk = 1 << db;
+  const int nblk = (n + RADIX_TILE - 1) / RADIX_TILE;
+  if (hist.ensure(sizeof(unsigned) * ((size_t)nbk * nblk + 1), caller)) return -1;
+  unsigned *ka = k1.as<unsigned>(), *kb = k2.as<unsigned>();
+  int *va = v1.as<int>(), *vb = v2.as<int>();
+  const size_t smem = sizeof(unsigned short) * 32 * nbk + sizeof(unsigned) * 3 * nbk;
+  CK(cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), caller);
+  for (int p = 0; p < passes; p++) {
+    const int shift = p * db;
+    k_radix_hist<<<nblk, RADIX_THREADS, 0, st>>>(ka, n, shift, db, hist.as<unsigned>(), nblk);
+    PM_LAUNCHED();
+    if (exclusive_scan(hist.as<unsigned>(), hist.as<unsigned>(), (size_t)nbk * nblk, part, st, caller)) return -1;
+    k_radix_scatter<<<nblk, RADIX_THREADS, smem, st>>>(ka, va, n, shift, db, hist.as<unsigned>(), nblk, kb, vb);
+    PM_LAUNCHED();
+    CKL(caller);
+    std::swap(ka, kb);
+    std::swap(va, vb);
+  }
+  *kout = ka;
+  *vout = va;
+  return 0;
+}
+
+template <typename R> static PartGeom<R> part_geom(const pmgpu_topo *t, int W) {
+  PartGeom<R> g;
+  memset(&g, 0, sizeof(g));
+  unsigned long long nbins = 1;
+  for (int e = 0; e < 3; e++) {
+    g.ext[e] = t->ncell[e] + t->nghost[2 * e] + t->nghost[2 * e + 1];
+    g.lo[e] = 1 - t->nghost[2 * e];
+    g.nint[e] = t->ncell[e];
+    g.nglo[e] = t->nghost[2 * e];
+    g.bclo[e] = t->bound_cond[2 * e];
+    g.bchi[e] = t->bound_cond[2 * e + 1];
+    const int off = (W == 4) ? 1 : 2;
+    g.blo[e] = g.lo[e] - (W - 1 - off);
+    g.nb[e] = g.ext[e] + W - 1;
+    nbins *= (unsigned long long)g.nb[e];
+    g.xmin[e] = (R)t->xmin[e];
+    g.xmax[e] = (R)t->xmax[e];
+    g.dx[e] = (R)t->dx[e];
+    g.c1dx[e] = R(1) / (R)t->dx[e];
+  }
+  g.nbins = (unsigned)nbins;
+  return g;
+}
+
+struct PartScratchRefs {
+  DevBuf *key, *val, *key2, *val2, *counts, *start, *spart, *hist;
+};
+
+// P2M on device arrays.  clear_mode: 0 add, 1 clear, 2 clear ghosts.  On return
+// *perm_out (if given) points at the sorted particle order.
+template <typename R>
+static int run_p2m(const pmgpu_topo *t, int order, const R *pos, const R *val, int nvar, int n, R *mesh,
+                   int nvar_mesh, int clear_mode, PartScratchRefs s, cudaStream_t st, const int **perm_out,
+                   const char *caller) {
+  const int W = (order == 3) ? 4 : 6;
+  PartGeom<R> g = part_geom<R>(t, W);
+  const unsigned long long nb_total = (unsigned long long)g.nb[0] * g.nb[1] * g.nb[2];
+  if (nb_total >= 0xFFFFFFF0ull) {
+    set_error(caller, "Mesh too large for 32-bit bin keys.");
+    return -1;
+  }
+  if (s.key->ensure(sizeof(unsigned) * (size_t)std::max(n, 1), caller) ||
+      s.val->ensure(sizeof(int) * (size_t)std::max(n, 1), caller) ||
+      s.key2->ensure(sizeof(unsigned) * (size_t)std::max(n, 1), caller) ||
+      s.val2->ensure(sizeof(int) * (size_t)std::max(n, 1), caller) ||
+      s.counts->ensure(sizeof(unsigned) * (g.nbins + 1), caller) ||
+      s.start->ensure(sizeof(unsigned) * (g.nbins + 1), caller))
+    return -1;
+  CK(cudaMemsetAsync(s.counts->p, 0, sizeof(unsigned) * (g.nbins + 1), st), caller);
+  const int *perm = nullptr;
+  if (n > 0) {
+    const int nblk = std::min((n + 255) / 256, 148 * 32);
+    if (W == 4) k_bin<R, 4><<<nblk, 256, 0, st>>>(g, pos, n, s.key->as<unsigned>(), s.val->as<int>(), s.counts->as<unsigned>());
+    else k_bin<R, 6><<<nblk, 256, 0, st>>>(g, pos, n, s.key->as<unsigned>(), s.val->as<int>(), s.counts->as<unsigned>());
+    PM_LAUNCHED();
+    CKL(caller);
+  }
+  if (exclusive_scan(s.counts->as<unsigned>(), s.start->as<unsigned>(), (size_t)g.nbins + 1, *s.spart, st, caller))
+    return -1;
+  if (n > 0) {
+    const unsigned *ks;
+    if (radix_sort(g.nbins, n, *s.key, *s.val, *s.key2, *s.val2, *s.hist, *s.spart, st, &ks, &perm, caller))
+      return -1;
+  }
+  // deposition, components in groups of at most three
+  const int zc = (W == 4) ? 32 : 30;
+  dim3 grid((g.ext[0] + DEP_TX - 1) / DEP_TX, (g.ext[1] + DEP_TY - 1) / DEP_TY, (g.ext[2] + zc - 1) / zc);
+  const int BX = DEP_TX + W - 1, BY = DEP_TY + W - 1;
+  for (int c0 = 0; c0 < nvar;) {
+    const int nv = (nvar - c0 >= 3) ? 3 : 1;
+    int cap = (sizeof(R) == 4) ? 1024 : 512;
+    if (W == 6) cap = cap * 3 / 4;
+    const size_t smem = (size_t)cap * (3 * W + nv) * sizeof(R) + sizeof(int) * (2 * BX * BY + 2 * BY + 2);
+    const R *vp = val + c0;
+    R *mp = mesh + c0;
+    const int *pp = perm ? perm : s.val->as<int>();
+#define DEP_CASE(WW, NVV)                                                                                  \
+  if (W == WW && nv == NVV) {                                                                              \
+    CK(cudaFuncSetAttribute(k_deposit<R, WW, NVV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), \
+       caller);                                                                                            \
+    k_deposit<R, WW, NVV><<<grid, DEP_TX * DEP_TY, smem, st>>>(g, pos, vp, nvar, s.start->as<unsigned>(),   \
+                                                                pp, mp, nvar_mesh, zc, cap, clear_mode);    \
+    PM_LAUNCHED();                                                                                         \
+  }
+    DEP_CASE(4, 1) DEP_CASE(4, 3) DEP_CASE(6, 1) DEP_CASE(6, 3)
+#undef DEP_CASE
+    CKL(caller);
+    c0 += nv;
+  }
+  // components beyond nvar in the mesh are left alone; a wider mesh is an error upstream
+  for (int d = 0; d < 3; d++) {
+    if (t->bound_cond[2 * d] == 0 || t->bound_cond[2 * d + 1] == 0) continue;
+    const int S = t->nghost[2 * d] + t->nghost[2 * d + 1];
+    const long long total = (long long)S * g.ext[(d + 1) % 3] * g.ext[(d + 2) % 3];
+    const int nblk = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+    k_ghost_add<R><<<std::max(nblk, 1), 256, 0, st>>>(mesh, g.ext[0], g.ext[1], g.ext[2], nvar_mesh, d,
+                                                       t->ncell[d], t->nghost[2 * d], t->nghost[2 * d + 1]);
+    PM_LAUNCHED();
+    CKL(caller);
+  }
+  if (perm_out) *perm_out = perm;
+  return 0;
+}
+
+template <typename R>
+static int run_m2p(const pmgpu_topo *t, int order, const R *pos, const int *ord, int n, const R *f0, const R *f1,
+                   const R *f2, R *o0, R *o1, R *o2, cudaStream_t st, const char *caller) {
+  if (n <= 0) return 0;
+  const int W = (order == 3) ? 4 : 6;
+  PartGeom<R> g = part_geom<R>(t, W);
+  const int nblk = std::min((n + 127) / 128, 148 * 32);
+  if (W == 4) k_m2p<R, 4><<<nblk, 128, 0, st>>>(g, pos, ord, n, f0, f1, f2, o0, o1, o2);
+  else k_m2p<R, 6><<<nblk, 128, 0, st>>>(g, pos, ord, n, f0, f1, f2, o0, o1, o2);
+  PM_LAUNCHED();
+  CKL(caller);
+  return 0;
+}
+
+// ------------------------------------------------------------------ solve driver
+template <typename R> static SolveGeom<R> solve_geom(const pmgpu_plan *pl) {
+  typedef typename cplx_t<R>::type C;
+  SolveGeom<R> g;
+  memset(&g, 0, sizeof(g));
+  for (int e = 0; e < 3; e++) {
+    g.ext[e] = pl->g.ext[e];
+    g.off[e] = pl->g.off[e];
+    g.P[e] = pl->g.P[e];
+    g.M[e] = pl->g.M[e];
+  }
+  g.H = pl->g.H;
+  g.N2 = pl->g.N2;
+  g.fx = pl->fx;
+  g.fy = pl->fy;
+  g.fz = pl->fz;
+  g.twx = pl->twx.as<C>();
+  g.twy = pl->twy.as<C>();
+  g.twz = pl->twz.as<C>();
+  g.kxt = pl->kxt.as<R>();
+  g.kyt = pl->kyt.as<R>();
+  g.kzt = pl->kzt.as<R>();
+  g.green = pl->green.as<R>();
+  g.gM1 = pl->gM1;
+  g.gM2 = pl->gM2;
+  g.scale = (R)(1.0 / ((double)g.M[0] * (double)g.M[1] * (double)g.M[2]));
+  g.eps2pi = (R)(2.0 * 3.14159265358979323846 * pl->eps);
+  g.order = pl->par.poisson_order;
+  g.allper = pl->g.allper;
+  return g;
+}
+
+template <typename R, int NC>
+static int fwd_xy(SolveGeom<R> &g, const R *in, typename cplx_t<R>::type *X, typename cplx_t<R>::type *Y,
+                  cudaStream_t st, const char *caller, int cs = NC) {
+  typedef typename cplx_t<R>::type C;
+  const int ntwx = g.fx.ntw + g.fx.next;
+  const int RB = lines_for(g.N2, NC, sizeof(C), ntwx);
+  size_t sm = fft_smem(g.N2, NC * RB, sizeof(C), ntwx);
+  CK(cudaFuncSetAttribute(k_xfwd<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+  const int rows = g.P[1] * g.P[2];
+  k_xfwd<R, NC><<<(rows + RB - 1) / RB, 256, sm, st>>>(g, in, X, RB, cs);
+  PM_LAUNCHED();
+  CKL(caller);
+  const int TK = std::min(lines_for(g.M[1], NC, sizeof(C), g.fy.ntw), g.H);
+  sm = fft_smem(g.M[1], NC * TK, sizeof(C), g.fy.ntw);
+  CK(cudaFuncSetAttribute(k_ypass<R, NC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+  dim3 grid((g.H + TK - 1) / TK, g.P[2]);
+  k_ypass<R, NC, false><<<grid, 256, sm, st>>>(g, X, Y, TK, g.P[1], g.M[1]);
+  PM_LAUNCHED();
+  CKL(caller);
+  return 0;
+}
+
+template <typename R, int NC>
+static int zpass(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typename cplx_t<R>::type *out, int mode,
+                 int reproj, int use_zeta, int rows_y, cudaStream_t st, const char *caller) {
+  typedef typename cplx_t<R>::type C;
+  const int TK = std::min(lines_for(g.M[2], NC, sizeof(C), g.fz.ntw), g.H);
+  const size_t sm = fft_smem(g.M[2], NC * TK, sizeof(C), g.fz.ntw);
+  CK(cudaFuncSetAttribute(k_zpass<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+  dim3 grid((g.H + TK - 1) / TK, rows_y);
+  k_zpass<R, NC><<<grid, 256, sm, st>>>(g, in, out, TK, mode, reproj, use_zeta);
+  PM_LAUNCHED();
+  CKL(caller);
+  return 0;
+}
+
+template <typename R, int NC>
+static int inv_yx(SolveGeom<R> &g, const pmgpu_topo *topo, typename cplx_t<R>::type *Y,
+                  typename cplx_t<R>::type *X, R *out, cudaStream_t st, const char *caller, int cs = NC,
+                  bool ghosts = true) {
+  typedef typename cplx_t<R>::type C;
+  const int TK = std::min(lines_for(g.M[1], NC, sizeof(C), g.fy.ntw), g.H);
+  size_t sm = fft_smem(g.M[1], NC * TK, sizeof(C), g.fy.ntw);
+  CK(cudaFuncSetAttribute(k_ypass<R, NC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+  dim3 grid((g.H + TK - 1) / TK, g.P[2]);
+  k_ypass<R, NC, true><<<grid, 256, sm, st>>>(g, Y, X, TK, g.M[1], g.P[1]);
+  PM_LAUNCHED();
+  CKL(caller);
+  const int ntwx = g.fx.ntw + g.fx.next;
+  const int RB = lines_for(g.N2, NC, sizeof(C), ntwx);
+  sm = fft_smem(g.N2, NC * RB, sizeof(C), ntwx);
+  CK(cudaFuncSetAttribute(k_xinv<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+  const int rows = g.P[1] * g.P[2];
+  k_xinv<R, NC><<<(rows + RB - 1) / RB, 256, sm, st>>>(g, X, out, RB, cs);
+  PM_LAUNCHED();
+  CKL(caller);
+  // periodic ghosts (x, then y, then z)
+  for (int d = 0; d < 3 && ghosts; d++) {
+    if (topo->bound_cond[2 * d] == 0 || topo->bound_cond[2 * d + 1] == 0) continue;
+    const int S = topo->nghost[2 * d] + topo->nghost[2 * d + 1];
+    const long long total = (long long)S * g.ext[(d + 1) % 3] * g.ext[(d + 2) % 3];
+    const int nblk = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+    k_ghost_fill<R><<<std::max(nblk, 1), 256, 0, st>>>(out, g.ext[0], g.ext[1], g.ext[2], cs, d, topo->ncell[d],
+                                                        topo->nghost[2 * d], topo->nghost[2 * d + 1]);
+    PM_LAUNCHED();
+    CKL(caller);
+  }
+  return 0;
+}
+
+template <typename R>
+static int run_solve(pmgpu_plan *pl, const R *vort, R *vel, R *vort_out, R *vecpot, int reg_vort, int reproj,
+                     int calc_vecpot, cudaStream_t st, const char *caller) {
+  typedef typename cplx_t<R>::type C;
+  SolveGeom<R> g = solve_geom<R>(pl);
+  const int ifft_vort = reg_vort || reproj;
+  const int ifft_vecpot = calc_vecpot && pl->par.poisson_kernel == 1;
+  const size_t nX = (size_t)g.P[1] * g.P[2] * g.H * 3, nY = (size_t)g.M[1] * g.P[2] * g.H * 3;
+  if (pl->X.ensure(sizeof(C) * nX, caller) || pl->Y.ensure(sizeof(C) * nY, caller)) return -1;
+  if (ifft_vort && pl->Y2.ensure(sizeof(C) * nY, caller)) return -1;
+  if (ifft_vecpot && pl->Y3.ensure(sizeof(C) * nY, caller)) return -1;
+  C *X = pl->X.as<C>(), *Y = pl->Y.as<C>();
+  if (fwd_xy<R, 3>(g, vort, X, Y, st, caller)) return -1;
+  if (ifft_vecpot && zpass<R, 3>(g, Y, pl->Y3.as<C>(), Z_VECPOT, 0, ifft_vort, g.M[1], st, caller)) return -1;
+  if (ifft_vort && zpass<R, 3>(g, Y, pl->Y2.as<C>(), Z_VORT, reproj, 1, g.M[1], st, caller)) return -1;
+  if (zpass<R, 3>(g, Y, Y, Z_VEL, 0, ifft_vort, g.M[1], st, caller)) return -1;
+  if (inv_yx<R, 3>(g, &pl->topo, Y, X, vel, st, caller)) return -1;
+  if (ifft_vort && inv_yx<R, 3>(g, &pl->topo, pl->Y2.as<C>(), X, vort_out, st, caller)) return -1;
+  if (ifft_vecpot && vecpot && inv_yx<R, 3>(g, &pl->topo, pl->Y3.as<C>(), X, vecpot, st, caller)) return -1;
+  return 0;
+}
+
+template <typename R, int NC>
+static int run_regularise_nc(pmgpu_plan *pl, R *mesh, int cs, int reg_order, double fw, cudaStream_t st,
+                             const char *caller) {
+  typedef typename cplx_t<R>::type C;
+  SolveGeom<R> g = solve_geom<R>(pl);
+  g.order = reg_order;
+  g.eps2pi = (R)(2.0 * 3.14159265358979323846 * fw);
+  const size_t nX = (size_t)g.P[1] * g.P[2] * g.H * NC, nY = (size_t)g.M[1] * g.P[2] * g.H * NC;
+  if (pl->X.ensure(sizeof(C) * nX, caller) || pl->Y.ensure(sizeof(C) * nY, caller)) return -1;
+  C *X = pl->X.as<C>(), *Y = pl->Y.as<C>();
+  if (fwd_xy<R, NC>(g, mesh, X, Y, st, caller, cs)) return -1;
+  if (zpass<R, NC>(g, Y, Y, Z_REGULARISE, 0, 1, g.M[1], st, caller)) return -1;
+  return inv_yx<R, NC>(g, &pl->topo, Y, X, mesh, st, caller, cs, false);
+}
+
+// pmlib_regularise on a device mesh of nvar components (ghost fill once at the end)
+template <typename R>
+static int run_regularise(pmgpu_plan *pl, R *mesh, int nvar, int reg_order, double fw, cudaStream_t st,
+                          const char *caller) {
+  if (nvar == 3) {
+    if (run_regularise_nc<R, 3>(pl, mesh, 3, reg_order, fw, st, caller)) return -1;
+  } else {
+    for (int c = 0; c < nvar; c++)
+      if (run_regularise_nc<R, 1>(pl, mesh + c, nvar, reg_order, fw, st, caller)) return -1;
+  }
+  const pmgpu_topo *topo = &pl->topo;
+  for (int d = 0; d < 3; d++) {
+    if (topo->bound_cond[2 * d] == 0 || topo->bound_cond[2 * d + 1] == 0) continue;
+    const int ext[3] = {pl->g.ext[0], pl->g.ext[1], pl->g.ext[2]};
+    const int S = topo->nghost[2 * d] + topo->nghost[2 * d + 1];
+    const long long total = (long long)S * ext[(d + 1) % 3] * ext[(d + 2) % 3];
+    const int nblk = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+    k_ghost_fill<R><<<std::max(nblk, 1), 256, 0, st>>>(mesh, ext[0], ext[1], ext[2], nvar, d, topo->ncell[d],
+                                                        topo->nghost[2 * d], topo->nghost[2 * d + 1]);
+    PM_LAUNCHED();
+    CKL(caller);
+  }
+  return 0;
+}
+
+// ------------------------------------------------------------------ Green's function
+template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller) {
+  const Geometry &G = pl->g;
+  pl->gM1 = G.M[1] / 2 + 1;
+  pl->gM2 = G.M[2] / 2 + 1;
+  if (G.allper) return 0;
+  GreenParams gp;
+  memset(&gp, 0, sizeof(gp));
+  double mdx = 0.0;
+  for (int e = 0; e < 3; e++) {
+    gp.M[e] = G.M[e];
+    gp.bc[e] = pl->patch.bound_cond[e] != 0 ? 1 : 0;
+    gp.dx[e] = pl->patch.dx[e];
+    gp.xmin[e] = -(0.5 * (double)G.M[e] + 0.5) * gp.dx[e];
+    gp.plen[e] = pl->patch.bound_cond[e] == 0 ? gp.dx[e] * (double)(2 * (pl->patch.ncell[e] + 2 * pl->patch.nghost))
+                                              : gp.dx[e] * (double)pl->patch.ncell[e];
+    mdx = std::max(mdx, gp.dx[e]);
+  }
+  gp.mdx = mdx;
+  gp.eps = pl->par.regularisation_radius * mdx;
+  gp.order = pl->par.poisson_order;
+  gp.kernel = pl->par.poisson_kernel;
+  // FP64 transform of the sampled kernel, with FP64 tables of the same lengths
+  SolveGeom<double> gg;
+  memset(&gg, 0, sizeof(gg));
+  for (int e = 0; e < 3; e++) {
+    gg.ext[e] = G.M[e];
+    gg.off[e] = 0;
+    gg.P[e] = G.M[e];
+    gg.M[e] = G.M[e];
+  }
+  gg.H = G.H;
+  gg.N2 = G.N2;
+  std::vector<cld> tw;
+  DevBuf tx, ty, tz, gr, gX, gY;
+  int rc = -1;
+  do {
+    if (!make_fft(G.N2, G.M[0], gg.fx, tw) || upload_tw<double>(tw, tx, caller)) break;
+    if (!make_fft(G.M[1], 0, gg.fy, tw) || upload_tw<double>(tw, ty, caller)) break;
+    if (!make_fft(G.M[2], 0, gg.fz, tw) || upload_tw<double>(tw, tz, caller)) break;
+    gg.twx = tx.as<double2>();
+    gg.twy = ty.as<double2>();
+    gg.twz = tz.as<double2>();
+    const size_t npts = (size_t)G.M[0] * G.M[1] * G.M[2];
+    const size_t nspec = (size_t)G.M[2] * G.M[1] * G.H;
+    if (gr.ensure(sizeof(double) * npts, caller) || gX.ensure(sizeof(double2) * nspec, caller) ||
+        gY.ensure(sizeof(double2) * nspec, caller))
+      break;
+    k_green_real<<<(unsigned)std::min<size_t>((npts + 255) / 256, 148 * 64), 256>>>(gp, gr.as<double>());
+    PM_LAUNCHED();
+    if (!cuda_ok(cudaGetLastError(), caller)) break;
+    if (fwd_xy<double, 1>(gg, gr.as<double>(), gX.as<double2>(), gY.as<double2>(), 0, caller)) break;
+    if (zpass<double, 1>(gg, gY.as<double2>(), gY.as<double2>(), Z_FORWARD, 0, 0, G.M[1], 0, caller)) break;
+    const size_t noct = (size_t)pl->gM2 * pl->gM1 * G.H;
+    if (pl->green.ensure(sizeof(R) * noct, caller)) break;
+    const double f = pl->patch.dx[0] * pl->patch.dx[1] * pl->patch.dx[2] /
+                     ((double)G.M[0] * (double)G.M[1] * (double)G.M[2]);
+    k_green_octant<R><<<(unsigned)std::min<size_t>((noct + 255) / 256, 148 * 64), 256>>>(
+        gY.as<double2>(), G.M[1], G.H, pl->gM1, pl->gM2, f, pl->green.as<R>());
+    PM_LAUNCHED();
+    if (!cuda_ok(cudaGetLastError(), caller)) break;
+    if (!cuda_ok(cudaDeviceSynchronize(), caller)) break;
+    rc = 0;
+  } while (0);
+  tx.release(); ty.release(); tz.release(); gr.release(); gX.release(); gY.release();
+  return rc;
+}
+
+template <typename R> static int upload_wavenumbers(pmgpu_plan *pl, const char *caller) {
+  DevBuf *bufs[3] = {&pl->kxt, &pl->kyt, &pl->kzt};
+  for (int e = 0; e < 3; e++) {
+    const int M = pl->g.M[e];
+    const int cnt = (e == 0) ? pl->g.H : M;
+    const double dx = pl->patch.dx[e];
+    const double dk = 1.0 / ((double)M * dx);  // pmlib_poisson_solve.f:209-224, i_ptc = 0
+    const double ksmp = 1.0 / (2.0 * dx);
+    const double kmin = -ksmp;
+    std::vector<R> h(cnt);
+    for (int i = 0; i < cnt; i++) {
+      const double k = (i + 1 <= M / 2) ? kmin + (double)i * dk + ksmp : kmin + (double)i * dk - ksmp;
+      h[i] = (R)k;
+    }
+    if (bufs[e]->ensure(sizeof(R) * cnt, caller)) return -1;
+    CK(cudaMemcpy(bufs[e]->p, h.data(), sizeof(R) * cnt, cudaMemcpyHostToDevice), caller);
+  }
+  return 0;
+}
+
+template <typename R> static int plan_tables(pmgpu_plan *pl, const char *caller) {
+  std::vector<cld> tw;
+  if (!make_fft(pl->g.N2, pl->g.M[0], pl->fx, tw) || upload_tw<R>(tw, pl->twx, caller)) return -1;
+  if (!make_fft(pl->g.M[1], 0, pl->fy, tw) || upload_tw<R>(tw, pl->twy, caller)) return -1;
+  if (!make_fft(pl->g.M[2], 0, pl->fz, tw) || upload_tw<R>(tw, pl->twz, caller)) return -1;
+  if (upload_wavenumbers<R>(pl, caller)) return -1;
+  return setup_green<R>(pl, caller);
+}
+
+static int check_params(const pmgpu_params *par) {
+  const char *caller = "pmlib_parameters_check";
+  if (!par) {
+    set_error(caller, "parameters missing.");
+    return -1;
+  }
+  if (par->poisson_kernel != 1 && par->poisson_kernel != 2) {
+    set_error(caller, "pmlib_poisson_kernel is incorrectly set.");
+    return -1;
+  }
+  const int o = par->poisson_order;
+  if (o != 0 && o != 2 && o != 4 && o != 6 && o != 8 && o != 10 && o != 100) {
+    set_error(caller, "pmlib_poisson_order is incorrectly set.");
+    return -1;
+  }
+  if (o > 0 && par->regularisation_radius < 1.0) {
+    set_error(caller, "pmlib_regularisation_radius is incorrectly set.");
+    return -1;
+  }
+  if (par->interpolation_order != 3 && par->interpolation_order != 4) {
+    set_error(caller, "pmlib_interpolation_order is incorrectly set.");
+    return -1;
+  }
+  return 0;
+}
+
+static int check_interp(const pmgpu_params *par, const char *caller) {
+  if (!par || (par->interpolation_order != 3 && par->interpolation_order != 4)) {
+    set_error(caller, "Interpolation scheme/order unknown.");
+    return -1;
+  }
+  return 0;
+}
+
+}  // namespace pmgpu
+
+// ====================================================================== C ABI
+// (C linkage comes from the declarations in pmlib_gpu.h)
+
+const char *pmgpu_last_error(void) { return pmgpu::g_err; }
+
+long long pmgpu_launch_count(int reset) {
+  long long v = pmgpu::g_launches;
+  if (reset) pmgpu::g_launches = 0;
+  return v;
+}
+
+int pmgpu_parameters_check(const pmgpu_params *par) { return check_params(par); }
+
+// source/patch/pmlib_patch_adjust.f:34-146
+int pmgpu_patch_adjust(pmgpu_patch *p) {
+  const char *caller = "pmlib_patch_adjust";
+  int extend[3];
+  for (int i = 0; i < 3; i++) {
+    if (p->bound_cond[i] == 0) {
+      const double centre = 0.5 * (p->xmax[i] + p->xmin[i]);
+      int ncell = (int)std::ceil((p->xmax[i] - p->xmin[i]) / p->dx[i]);
+      ncell = ncell + (16 - ((ncell + 2 * p->nghost) % 16));
+      const double half = (double)std::lround(0.5 * (double)ncell);
+      p->xmin[i] = centre - half * p->dx[i];
+      p->xmax[i] = centre + half * p->dx[i];
+      p->ncell[i] = (int)std::lround((p->xmax[i] - p->xmin[i]) / p->dx[i]);
+      if (p->ncell[i] != ncell) {
+        set_error(caller, "Failed to adjust the number of mesh cells");
+        return -1;
+      }
+    } else {
+      p->xmax[i] = p->xmin[i] + p->dx[i] * (double)std::lround((p->xmax[i] - p->xmin[i]) / p->dx[i]);
+      p->ncell[i] = (int)std::lround((p->xmax[i] - p->xmin[i]) / p->dx[i]);
+    }
+  }
+  for (int i = 0; i < 3; i++) extend[i] = p->bound_cond[i] == 0 ? 2 * p->ncell[i] : p->ncell[i];
+  int s[3];
+  if (extend[0] >= extend[1] && extend[0] >= extend[2]) {
+    if (extend[1] >= extend[2]) { s[0] = 1; s[1] = 2; s[2] = 3; } else { s[0] = 1; s[1] = 3; s[2] = 2; }
+  } else if (extend[1] >= extend[0] && extend[1] >= extend[2]) {
+    if (extend[0] >= extend[2]) { s[0] = 2; s[1] = 1; s[2] = 3; } else { s[0] = 2; s[1] = 3; s[2] = 1; }
+  } else if (extend[2] >= extend[0] && extend[2] >= extend[1]) {
+    if (extend[0] >= extend[1]) { s[0] = 3; s[1] = 1; s[2] = 2; } else { s[0] = 3; s[1] = 2; s[2] = 1; }
+  } else {
+    set_error(caller, "Cant figure out fft sequence.");
+    return -1;
+  }
+  for (int i = 0; i < 3; i++) p->fft_seq[i] = s[i];
+  return 0;
+}
+
+// source/topology/pmlib_topology_cuboid.f:225-325 for one subdomain
+int pmgpu_topology_cuboid(const pmgpu_patch *patch, int interpolation_order, pmgpu_topo *t) {
+  const char *caller = "pmlib_topology_cuboid";
+  int nghost_int;
+  if (interpolation_order == 3) nghost_int = 2;
+  else if (interpolation_order == 4) nghost_int = 3;
+  else {
+    set_error(caller, "Can not define number of ghost cells.");
+    return -1;
+  }
+  memset(t, 0, sizeof(*t));
+  for (int d = 0; d < 3; d++) {
+    t->xmin[d] = patch->xmin[d];
+    t->xmax[d] = patch->xmax[d];
+    t->dx[d] = patch->dx[d];
+    t->ncell[d] = patch->ncell[d];
+    for (int s = 0; s < 2; s++) {
+      t->bound_cond[2 * d + s] = patch->bound_cond[d] == 0 ? 0 : 1;
+      t->nghost[2 * d + s] = patch->bound_cond[d] == 0 ? patch->nghost : nghost_int;
+    }
+  }
+  return 0;
+}
+
+// ------------------------------------------------------------------ P2M / M2P (host pointers)
+template <typename R>
+static int p2m_host(const pmgpu_topo *t, const pmgpu_params *par, const R *xpart, const R *part, int nvar,
+                    int npart, R *mesh, int nvar_mesh, int clear, int clear_ghost) {
+  const char *caller = "pmlib_interp_particle_mesh";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (nvar != nvar_mesh) {
+    set_error(caller, "Dimension of interpolation variables does not correspond.");
+    return -1;
+  }
+  if (t->npart != npart) {
+    set_error(caller, "Discrepancy in number of particles");
+    return -1;
+  }
+  if (check_interp(par, caller) || ensure_device(caller)) return -1;
+  Scratch &s = scratch();
+  const size_t nm = mesh_points(t) * (size_t)nvar_mesh;
+  if (s.a.ensure(sizeof(R) * 3 * (size_t)std::max(npart, 1), caller) ||
+      s.b.ensure(sizeof(R) * (size_t)nvar * std::max(npart, 1), caller) || s.c.ensure(sizeof(R) * nm, caller))
+    return -1;
+  if (npart > 0) {
+    CK(cudaMemcpy(s.a.p, xpart, sizeof(R) * 3 * (size_t)npart, cudaMemcpyHostToDevice), caller);
+    CK(cudaMemcpy(s.b.p, part, sizeof(R) * (size_t)nvar * npart, cudaMemcpyHostToDevice), caller);
+  }
+  const int mode = clear ? 1 : (clear_ghost ? 2 : 0);
+  if (mode != 1) CK(cudaMemcpy(s.c.p, mesh, sizeof(R) * nm, cudaMemcpyHostToDevice), caller);
+  PartScratchRefs r{&s.key, &s.val, &s.key2, &s.val2, &s.counts, &s.start, &s.spart, &s.hist};
+  if (run_p2m<R>(t, par->interpolation_order, s.a.as<R>(), s.b.as<R>(), nvar, npart, s.c.as<R>(), nvar_mesh, mode,
+                 r, 0, nullptr, caller))
+    return -1;
+  CK(cudaMemcpy(mesh, s.c.p, sizeof(R) * nm, cudaMemcpyDeviceToHost), caller);
+  return 0;
+}
+
+int pmgpu_interp_particle_mesh(const pmgpu_topo *topo, const pmgpu_params *par, const double *xpart,
+                               const double *part, int nvar, int npart, double *mesh, int nvar_mesh, int clear,
+                               int clear_ghost) {
+  return p2m_host<double>(topo, par, xpart, part, nvar, npart, mesh, nvar_mesh, clear, clear_ghost);
+}
+int pmgpu_interp_particle_mesh_f32(const pmgpu_topo *topo, const pmgpu_params *par, const float *xpart,
+                                   const float *part, int nvar, int npart, float *mesh, int nvar_mesh, int clear,
+                                   int clear_ghost) {
+  return p2m_host<float>(topo, par, xpart, part, nvar, npart, mesh, nvar_mesh, clear, clear_ghost);
+}
+
+template <typename R>
+static int m2p_host(const pmgpu_topo *t, const pmgpu_params *par, const R *mvort, const R *mdvort, const R *mvel,
+                    const R *pos, int npart, R *pv, R *pdv, R *pvel) {
+  const char *caller = "pmlib_interp_mesh_particle";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (check_interp(par, caller) || ensure_device(caller)) return -1;
+  Scratch &s = scratch();
+  const size_t nm = mesh_points(t) * 3;
+  const size_t np3 = 3 * (size_t)std::max(npart, 1);
+  if (s.a.ensure(sizeof(R) * np3, caller)) return -1;
+  const R *fin[3] = {mvort, mdvort, mvel};
+  R *fout[3] = {pv, pdv, pvel};
+  DevBuf *mb[3] = {&s.c, &s.d, &s.e};
+  DevBuf *ob[3] = {&s.f, &s.g, &s.h};
+  const R *df[3] = {nullptr, nullptr, nullptr};
+  R *dof[3] = {nullptr, nullptr, nullptr};
+  for (int f = 0; f < 3; f++) {
+    if (!fin[f] || !fout[f]) continue;
+    if (mb[f]->ensure(sizeof(R) * nm, caller) || ob[f]->ensure(sizeof(R) * np3, caller)) return -1;
+    CK(cudaMemcpy(mb[f]->p, fin[f], sizeof(R) * nm, cudaMemcpyHostToDevice), caller);
+    df[f] = mb[f]->as<R>();
+    dof[f] = ob[f]->as<R>();
+  }
+  if (npart > 0) CK(cudaMemcpy(s.a.p, pos, sizeof(R) * 3 * (size_t)npart, cudaMemcpyHostToDevice), caller);
+  if (run_m2p<R>(t, par->interpolation_order, s.a.as<R>(), nullptr, npart, df[0], df[1], df[2], dof[0], dof[1],
+                 dof[2], 0, caller))
+    return -1;
+  for (int f = 0; f < 3; f++)
+    if (dof[f] && npart > 0)
+      CK(cudaMemcpy(fout[f], dof[f], sizeof(R) * 3 * (size_t)npart, cudaMemcpyDeviceToHost), caller);
+  return 0;
+}
+
+int pmgpu_interp_mesh_particle(const pmgpu_topo *topo, const pmgpu_params *par, const double *mesh_vort,
+                               const double *mesh_dvort, const double *mesh_vel, const double *pos, int npart,
+                               double *part_vort, double *part_dvort, double *part_vel) {
+  return m2p_host<double>(topo, par, mesh_vort, mesh_dvort, mesh_vel, pos, npart, part_vort, part_dvort, part_vel);
+}
+int pmgpu_interp_mesh_particle_f32(const pmgpu_topo *topo, const pmgpu_params *par, const float *mesh_vort,
+                                   const float *mesh_dvort, const float *mesh_vel, const float *pos, int npart,
+                                   float *part_vort, float *part_dvort, float *part_vel) {
+  return m2p_host<float>(topo, par, mesh_vort, mesh_dvort, mesh_vel, pos, npart, part_vort, part_dvort, part_vel);
+}
+
+// ------------------------------------------------------------------ Poisson
+int pmgpu_poisson_setup(const pmgpu_patch *patch, const pmgpu_topo *cuboid, const pmgpu_params *par,
+                        int precision, pmgpu_plan **plan) {
+  const char *caller = "pmlib_poisson_setup";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!plan || !patch || !cuboid) {
+    set_error(caller, "missing argument.");
+    return -1;
+  }
+  *plan = nullptr;
+  if (check_params(par)) return -1;
+  if (precision != PMGPU_FP64 && precision != PMGPU_FP32) {
+    set_error(caller, "precision unknown.");
+    return -1;
+  }
+  if (par->poisson_kernel != 1) {
+    set_error(caller, "Poisson kernel 2 is not available on the GPU path.");
+    return -1;
+  }
+  int seen = 0;
+  for (int i = 0; i < 3; i++) {
+    if (patch->fft_seq[i] < 1 || patch->fft_seq[i] > 3) {
+      set_error(caller, "fft direction unknown.");
+      return -1;
+    }
+    seen |= 1 << patch->fft_seq[i];
+  }
+  if (seen != 0xE) {
+    set_error(caller, "fft direction unknown.");
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  pmgpu_plan *pl = new pmgpu_plan();
+  pl->prec = precision;
+  pl->patch = *patch;
+  pl->topo = *cuboid;
+  pl->par = *par;
+  pl->perm = nullptr;
+  pl->perm_n = 0;
+  double mdx = 0.0;
+  int allper = 1;
+  for (int e = 0; e < 3; e++) {
+    const bool freeax = patch->bound_cond[e] == 0;
+    pl->g.ext[e] = cuboid->ncell[e] + cuboid->nghost[2 * e] + cuboid->nghost[2 * e + 1];
+    pl->g.off[e] = freeax ? 0 : cuboid->nghost[2 * e];
+    pl->g.P[e] = freeax ? pl->g.ext[e] : cuboid->ncell[e];
+    pl->g.M[e] = freeax ? 2 * pl->g.P[e] : pl->g.P[e];
+    if (pl->g.M[e] % 2 != 0 || pl->g.M[e] < 2) {
+      delete pl;
+      set_error("pmlib_fft", "nfft is an odd number.");
+      return -1;
+    }
+    if (freeax) allper = 0;
+    mdx = std::max(mdx, patch->dx[e]);
+  }
+  pl->g.H = pl->g.M[0] / 2 + 1;
+  pl->g.N2 = pl->g.M[0] / 2;
+  pl->g.allper = allper;
+  pl->eps = par->regularisation_radius * mdx;
+  const int rc = (precision == PMGPU_FP64) ? plan_tables<double>(pl, caller) : plan_tables<float>(pl, caller);
+  if (rc) {
+    delete pl;
+    return -1;
+  }
+  *plan = pl;
+  return 0;
+}
+
+void pmgpu_plan_destroy(pmgpu_plan *plan) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  delete plan;
+}
+
+template <typename R>
+static int solve_host(pmgpu_plan *pl, R *vort, R *vel, R *vecpot, int reg_vort, int reproj, int calc_vecpot) {
+  const char *caller = "pmlib_poisson_solve";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!pl) {
+    set_error(caller, "plan missing.");
+    return -1;
+  }
+  if ((pl->prec == PMGPU_FP64) != (sizeof(R) == 8)) {
+    set_error(caller, "plan precision does not match the arrays.");
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  const size_t nm = mesh_points(&pl->topo) * 3;
+  const int ifft_vort = reg_vort || reproj;
+  const int ifft_vecpot = calc_vecpot && pl->par.poisson_kernel == 1 && vecpot;
+  if (pl->mesh_w.ensure(sizeof(R) * nm, caller) || pl->mesh_u.ensure(sizeof(R) * nm, caller)) return -1;
+  if (ifft_vecpot && pl->mesh_a.ensure(sizeof(R) * nm, caller)) return -1;
+  CK(cudaMemcpy(pl->mesh_w.p, vort, sizeof(R) * nm, cudaMemcpyHostToDevice), caller);
+  if (run_solve<R>(pl, pl->mesh_w.as<R>(), pl->mesh_u.as<R>(), pl->mesh_w.as<R>(),
+                   ifft_vecpot ? pl->mesh_a.as<R>() : nullptr, reg_vort, reproj, ifft_vecpot, 0, caller))
+    return -1;
+  CK(cudaMemcpy(vel, pl->mesh_u.p, sizeof(R) * nm, cudaMemcpyDeviceToHost), caller);
+  if (ifft_vort) CK(cudaMemcpy(vort, pl->mesh_w.p, sizeof(R) * nm, cudaMemcpyDeviceToHost), caller);
+  if (ifft_vecpot) CK(cudaMemcpy(vecpot, pl->mesh_a.p, sizeof(R) * nm, cudaMemcpyDeviceToHost), caller);
+  return 0;
+}
+
+int pmgpu_poisson_solve(pmgpu_plan *plan, double *vort, double *vel, double *vecpot, int reg_vort, int reproj,
+                        int calc_vecpot) {
+  return solve_host<double>(plan, vort, vel, vecpot, reg_vort, reproj, calc_vecpot);
+}
+int pmgpu_poisson_solve_f32(pmgpu_plan *plan, float *vort, float *vel, float *vecpot, int reg_vort, int reproj,
+                            int calc_vecpot) {
+  return solve_host<float>(plan, vort, vel, vecpot, reg_vort, reproj, calc_vecpot);
+}
+
+template <typename R>
+static int regularise_host(pmgpu_plan *pl, R *mesh, int nvar, int reg_order, double fw) {
+  const char *caller = "pmlib_regularise";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!pl) {
+    set_error(caller, "plan missing.");
+    return -1;
+  }
+  if ((pl->prec == PMGPU_FP64) != (sizeof(R) == 8)) {
+    set_error(caller, "plan precision does not match the arrays.");
+    return -1;
+  }
+  if (nvar > 3) {
+    set_error(caller, "Cant regularise variables of ndim > 3.");
+    return -1;
+  }
+  if (nvar < 1 || (reg_order != 0 && reg_order != 2 && reg_order != 4 && reg_order != 6 && reg_order != 8 &&
+                   reg_order != 10)) {
+    set_error(caller, "Regularisation order unknown.");
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  const size_t nm = mesh_points(&pl->topo) * nvar;
+  if (pl->mesh_w.ensure(sizeof(R) * nm, caller)) return -1;
+  CK(cudaMemcpy(pl->mesh_w.p, mesh, sizeof(R) * nm, cudaMemcpyHostToDevice), caller);
+  if (run_regularise<R>(pl, pl->mesh_w.as<R>(), nvar, reg_order, fw, 0, caller)) return -1;
+  CK(cudaMemcpy(mesh, pl->mesh_w.p, sizeof(R) * nm, cudaMemcpyDeviceToHost), caller);
+  return 0;
+}
+
+int pmgpu_regularise(pmgpu_plan *plan, double *mesh, int nvar, int reg_order, double filter_width) {
+  return regularise_host<double>(plan, mesh, nvar, reg_order, filter_width);
+}
+int pmgpu_regularise_f32(pmgpu_plan *plan, float *mesh, int nvar, int reg_order, double filter_width) {
+  return regularise_host<float>(plan, mesh, nvar, reg_order, filter_width);
+}
+
+// ------------------------------------------------------------------ the step
+template <typename R>
+static int step_dev(pmgpu_plan *pl, const R *pos, const R *pv, int n, R *pvel, cudaStream_t st) {
+  const char *caller = "pmgpu_step";
+  const size_t nm = mesh_points(&pl->topo) * 3;
+  if (pl->mesh_w.ensure(sizeof(R) * nm, caller) || pl->mesh_u.ensure(sizeof(R) * nm, caller)) return -1;
+  pmgpu_topo t = pl->topo;
+  t.npart = n;
+  PartScratchRefs r{&pl->key, &pl->val, &pl->key2, &pl->val2, &pl->counts, &pl->start, &pl->spart, &pl->hist};
+  const int *perm = nullptr;
+  if (run_p2m<R>(&t, pl->par.interpolation_order, pos, pv, 3, n, pl->mesh_w.as<R>(), 3, 1, r, st, &perm, caller))
+    return -1;
+  if (run_solve<R>(pl, pl->mesh_w.as<R>(), pl->mesh_u.as<R>(), nullptr, nullptr, 0, 0, 0, st, caller)) return -1;
+  if (run_m2p<R>(&t, pl->par.interpolation_order, pos, perm, n, nullptr, nullptr, pl->mesh_u.as<R>(), nullptr,
+                 nullptr, pvel, st, caller))
+    return -1;
+  return 0;
+}
+
+int pmgpu_step_dev(pmgpu_plan *plan, const void *d_pos, const void *d_part_vort, int npart, void *d_part_vel,
+                   void *stream) {
+  const char *caller = "pmgpu_step";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!plan) {
+    set_error(caller, "plan missing.");
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->prec == PMGPU_FP64)
+    return step_dev<double>(plan, (const double *)d_pos, (const double *)d_part_vort, npart, (double *)d_part_vel, st);
+  return step_dev<float>(plan, (const float *)d_pos, (const float *)d_part_vort, npart, (float *)d_part_vel, st);
+}
+
+int pmgpu_step(pmgpu_plan *plan, const void *pos, const void *part_vort, int npart, void *part_vel) {
+  const char *caller = "pmgpu_step";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!plan) {
+    set_error(caller, "plan missing.");
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  const size_t es = plan->prec == PMGPU_FP64 ? 8 : 4;
+  const size_t nb = es * 3 * (size_t)std::max(npart, 1);
+  if (plan->h_pos.ensure(nb, caller) || plan->h_val.ensure(nb, caller) || plan->h_out.ensure(nb, caller)) return -1;
+  cudaStream_t st = 0;
+  if (npart > 0) {
+    CK(cudaMemcpyAsync(plan->h_pos.p, pos, es * 3 * (size_t)npart, cudaMemcpyHostToDevice, st), caller);
+    CK(cudaMemcpyAsync(plan->h_val.p, part_vort, es * 3 * (size_t)npart, cudaMemcpyHostToDevice, st), caller);
+  }
+  int rc;
+  if (plan->prec == PMGPU_FP64)
+    rc = step_dev<double>(plan, plan->h_pos.as<double>(), plan->h_val.as<double>(), npart, plan->h_out.as<double>(), st);
+  else
+    rc = step_dev<float>(plan, plan->h_pos.as<float>(), plan->h_val.as<float>(), npart, plan->h_out.as<float>(), st);
+  if (rc) return -1;
+  if (npart > 0) CK(cudaMemcpyAsync(part_vel, plan->h_out.p, es * 3 * (size_t)npart, cudaMemcpyDeviceToHost, st), caller);
+  CK(cudaStreamSynchronize(st), caller);
+  return 0;
+}
+
+// ------------------------------------------------------------------ remesh
+int pmgpu_remesh(const pmgpu_topo *topo, const double *mesh_vort, const double *mesh_dvort, const double *mesh_vel,
+                 const unsigned char *mask, double min_vort, double min_dvort, int incl_ghost, int max_part,
+                 double *pos, double *part_vort, double *part_dvort, double *part_vel, int *npart) {
+  const char *caller = "pmlib_remesh_particles";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!topo || !mesh_vort || !npart) {
+    set_error(caller, "missing argument.");
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  Scratch &s = scratch();
+  const size_t nc = mesh_points(topo);
+  PartGeom<double> g = part_geom<double>(topo, 4);
+  if (s.c.ensure(sizeof(double) * 3 * nc, caller) || s.counts.ensure(sizeof(unsigned) * (nc + 1), caller) ||
+      s.start.ensure(sizeof(unsigned) * (nc + 1), caller))
+    return -1;
+  CK(cudaMemcpy(s.c.p, mesh_vort, sizeof(double) * 3 * nc, cudaMemcpyHostToDevice), caller);
+  const double *ddv = nullptr, *dvel = nullptr;
+  const unsigned char *dmask = nullptr;
+  if (mesh_dvort) {
+    if (s.d.ensure(sizeof(double) * 3 * nc, caller)) return -1;
+    CK(cudaMemcpy(s.d.p, mesh_dvort, sizeof(double) * 3 * nc, cudaMemcpyHostToDevice), caller);
+    ddv = s.d.as<double>();
+  }
+  if (mesh_vel) {
+    if (s.e.ensure(sizeof(double) * 3 * nc, caller)) return -1;
+    CK(cudaMemcpy(s.e.p, mesh_vel, sizeof(double) * 3 * nc, cudaMemcpyHostToDevice), caller);
+    dvel = s.e.as<double>();
+  }
+  if (mask) {
+    if (s.h.ensure(nc, caller)) return -1;
+    CK(cudaMemcpy(s.h.p, mask, nc, cudaMemcpyHostToDevice), caller);
+    dmask = s.h.as<unsigned char>();
+  }
+  const int nblk = (int)std::min<size_t>((nc + 255) / 256, 148 * 32);
+  CK(cudaMemset(s.counts.p, 0, sizeof(unsigned) * (nc + 1)), caller);
+  k_remesh_flag<<<nblk, 256>>>(g, s.c.as<double>(), ddv, dmask, min_vort, min_dvort, incl_ghost,
+                               s.counts.as<unsigned>());
+  PM_LAUNCHED();
+  CKL(caller);
+  if (exclusive_scan(s.counts.as<unsigned>(), s.start.as<unsigned>(), nc + 1, s.spart, 0, caller)) return -1;
+  unsigned total = 0;
+  CK(cudaMemcpy(&total, s.start.as<unsigned>() + nc, sizeof(unsigned), cudaMemcpyDeviceToHost), caller);
+  *npart = (int)total;
+  if (!pos) return 0;
+  if ((int)total > max_part) {
+    set_error(caller, "particle arrays too small.");
+    return -1;
+  }
+  const size_t np3 = 3 * (size_t)std::max<unsigned>(total, 1);
+  if (s.f.ensure(sizeof(double) * np3 * 4, caller)) return -1;
+  double *dpos = s.f.as<double>(), *dpv = dpos + np3, *dpdv = dpv + np3, *dpvel = dpdv + np3;
+  k_remesh_fill<<<nblk, 256>>>(g, s.c.as<double>(), ddv, dvel, s.counts.as<unsigned>(), s.start.as<unsigned>(),
+                               dpos, dpv, dpdv, dpvel);
+  PM_LAUNCHED();
+  CKL(caller);
+  if (total > 0) {
+    const size_t b = sizeof(double) * 3 * (size_t)total;
+    CK(cudaMemcpy(pos, dpos, b, cudaMemcpyDeviceToHost), caller);
+    if (part_vort) CK(cudaMemcpy(part_vort, dpv, b, cudaMemcpyDeviceToHost), caller);
+    if (part_dvort) CK(cudaMemcpy(part_dvort, dpdv, b, cudaMemcpyDeviceToHost), caller);
+    if (part_vel) CK(cudaMemcpy(part_vel, dpvel, b, cudaMemcpyDeviceToHost), caller);
+  }
+  return 0;
+}
+

@@ -1,0 +1,185 @@
+"""Host-side mirror of pmlib3d's module procedures for the particle-mesh step.
+
+Each function keeps the name, argument meaning and ``ierr`` convention of the
+Fortran procedure it replaces (cited per function) and calls the CUDA library
+through its C ABI.  Arrays are NumPy arrays in the reference's Fortran layouts,
+stored in C order of the reversed shape:
+
+* mesh ``(nvar, 1-g:n+g, ...)``  -> shape ``(nz', ny', nx', nvar)``
+* particles ``(3, npart)``       -> shape ``(npart, 3)``
+
+``float64`` arrays run the FP64 plain path, ``float32`` arrays the FP32 form.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._lib import Params, Patch, Topo, lib
+
+FP64, FP32 = 0, 1
+
+
+def make_patch(xmin, xmax, dx, bound_cond=(0, 0, 0), nghost=4, ncell=None, fft_seq=(1, 2, 3)) -> Patch:
+    """class_patch with the fields a caller sets before pmlib_patch_adjust."""
+    p = Patch()
+    for d in range(3):
+        p.xmin[d], p.xmax[d], p.dx[d] = xmin[d], xmax[d], dx[d]
+        p.bound_cond[d] = bound_cond[d]
+        p.fft_seq[d] = fft_seq[d]
+        p.ncell[d] = ncell[d] if ncell is not None else int(round((xmax[d] - xmin[d]) / dx[d]))
+    p.nghost = nghost
+    return p
+
+
+def make_params(order=6, kernel=1, radius=2.0, interp=3) -> Params:
+    """pmlib_poisson_order / _kernel, pmlib_regularisation_radius, pmlib_interpolation_order."""
+    q = Params()
+    q.poisson_order, q.poisson_kernel = order, kernel
+    q.regularisation_radius, q.interpolation_order = radius, interp
+    return q
+
+
+def last_error() -> str:
+    return lib().pmgpu_last_error().decode()
+
+
+def launch_count(reset: bool = False) -> int:
+    """Kernels this library launched since the last reset."""
+    return int(lib().pmgpu_launch_count(int(reset)))
+
+
+def _ptr(a, dtype):
+    if a is None:
+        return None
+    if a.dtype != dtype or not a.flags.c_contiguous:
+        raise TypeError(f"expected a C-contiguous {np.dtype(dtype).name} array")
+    return a.ctypes.data_as(C.POINTER(C.c_double if dtype == np.float64 else C.c_float))
+
+
+def topo_shape(topo: Topo, nvar: int = 3):
+    """Array shape (nz', ny', nx', nvar) of a mesh on ``topo`` (ghosts included)."""
+    ext = [topo.ncell[d] + topo.nghost[2 * d] + topo.nghost[2 * d + 1] for d in range(3)]
+    return (ext[2], ext[1], ext[0], nvar)
+
+
+# ---------------------------------------------------------------------------
+def pmlib_parameters_check(params: Params) -> int:
+    """source/parameters/pmlib_parameters_check.f:5-105 (the checks the path reads)."""
+    return lib().pmgpu_parameters_check(C.byref(params))
+
+
+def pmlib_patch_adjust(patch: Patch) -> int:
+    """source/patch/pmlib_patch_adjust.f:5-166 (adjusts ``patch`` in place)."""
+    return lib().pmgpu_patch_adjust(C.byref(patch))
+
+
+def pmlib_topology_cuboid(patch: Patch, interpolation_order: int = 3):
+    """source/topology/pmlib_topology_cuboid.f:5-356 for one subdomain -> (ierr, topo)."""
+    t = Topo()
+    ierr = lib().pmgpu_topology_cuboid(C.byref(patch), interpolation_order, C.byref(t))
+    return ierr, t
+
+
+def pmlib_interp_particle_mesh(topo: Topo, params: Params, xpart, part, mesh, clear=False,
+                               clear_ghost=False) -> int:
+    """source/interpolation/pmlib_interp_particle_mesh.f:5-22 (mesh updated in place)."""
+    dt = mesh.dtype
+    f = lib().pmgpu_interp_particle_mesh if dt == np.float64 else lib().pmgpu_interp_particle_mesh_f32
+    return f(C.byref(topo), C.byref(params), _ptr(xpart, dt), _ptr(part, dt), part.shape[-1],
+             part.shape[0], _ptr(mesh, dt), mesh.shape[-1], int(bool(clear)), int(bool(clear_ghost)))
+
+
+def pmlib_interp_mesh_particle(topo: Topo, params: Params, pos, mesh_vort=None, mesh_dvort=None,
+                               mesh_vel=None, part_vort=None, part_dvort=None, part_vel=None) -> int:
+    """source/interpolation/pmlib_interp_mesh_particle.f:5-24: the vort / dvort / vel
+    flags of the reference become the non-None (mesh, particle) pairs."""
+    dt = pos.dtype
+    f = lib().pmgpu_interp_mesh_particle if dt == np.float64 else lib().pmgpu_interp_mesh_particle_f32
+    return f(C.byref(topo), C.byref(params), _ptr(mesh_vort, dt), _ptr(mesh_dvort, dt),
+             _ptr(mesh_vel, dt), _ptr(pos, dt), pos.shape[0], _ptr(part_vort, dt),
+             _ptr(part_dvort, dt), _ptr(part_vel, dt))
+
+
+@dataclass
+class Plan:
+    """Owns a pmgpu_plan (the Green's function spectrum and work buffers on the GPU)."""
+
+    handle: C.c_void_p
+    precision: int
+    topo: Topo
+
+    def close(self):
+        if self.handle:
+            lib().pmgpu_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pmlib_poisson_setup(patch: Patch, topo: Topo, params: Params, precision: int = FP64):
+    """source/poisson/pmlib_poisson_setup.f:5-19 -> (ierr, Plan)."""
+    h = C.c_void_p()
+    ierr = lib().pmgpu_poisson_setup(C.byref(patch), C.byref(topo), C.byref(params), precision, C.byref(h))
+    return ierr, (Plan(h, precision, topo) if ierr == 0 else None)
+
+
+def pmlib_poisson_solve(plan: Plan, vort, vel, vecpot=None, reg_vort=False, reproj=False,
+                        calc_vecpot=False) -> int:
+    """source/poisson/pmlib_poisson_solve.f:15-34: vel (and vecpot) written, vort
+    overwritten with the regularised vorticity when reg_vort or reproj."""
+    dt = np.float64 if plan.precision == FP64 else np.float32
+    f = lib().pmgpu_poisson_solve if dt == np.float64 else lib().pmgpu_poisson_solve_f32
+    return f(plan.handle, _ptr(vort, dt), _ptr(vel, dt), _ptr(vecpot, dt), int(bool(reg_vort)),
+             int(bool(reproj)), int(bool(calc_vecpot)))
+
+
+def pmlib_regularise(plan: Plan, mesh, reg_order: int, filter_width: float) -> int:
+    """source/regularise/pmlib_regularise.f:5-21 (mesh filtered in place)."""
+    dt = np.float64 if plan.precision == FP64 else np.float32
+    f = lib().pmgpu_regularise if dt == np.float64 else lib().pmgpu_regularise_f32
+    return f(plan.handle, _ptr(mesh, dt), mesh.shape[-1], reg_order, float(filter_width))
+
+
+def pmlib_remesh(topo: Topo, mesh_vort, mesh_dvort=None, mesh_vel=None, mask=None, min_vort=0.0,
+                 min_dvort=0.0, incl_ghost=False):
+    """source/remesh/pmlib_remesh.f:5-28 -> (ierr, pos, vort, dvort, vel), particles in
+    the reference's k-j-i cell order."""
+    L = lib()
+    n = C.c_int(0)
+    mk = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    mp = None if mk is None else mk.ctypes.data_as(C.c_void_p)
+    d = np.float64
+    ierr = L.pmgpu_remesh(C.byref(topo), _ptr(mesh_vort, d), _ptr(mesh_dvort, d), _ptr(mesh_vel, d), mp,
+                          min_vort, min_dvort, int(bool(incl_ghost)), 0, None, None, None, None, C.byref(n))
+    if ierr:
+        return ierr, None, None, None, None
+    npart = n.value
+    pos, pv, pdv, pvel = (np.zeros((npart, 3)) for _ in range(4))
+    ierr = L.pmgpu_remesh(C.byref(topo), _ptr(mesh_vort, d), _ptr(mesh_dvort, d), _ptr(mesh_vel, d), mp,
+                          min_vort, min_dvort, int(bool(incl_ghost)), npart, _ptr(pos, d), _ptr(pv, d),
+                          _ptr(pdv, d), _ptr(pvel, d), C.byref(n))
+    topo.npart = npart
+    return ierr, pos, pv, pdv, pvel
+
+
+def step(plan: Plan, pos, part_vort, part_vel) -> int:
+    """One vortex step through host arrays: P2M (clear), unbounded solve and curl,
+    M2P of the velocity into ``part_vel``."""
+    dt = np.float64 if plan.precision == FP64 else np.float32
+    for a in (pos, part_vort, part_vel):
+        _ptr(a, dt)
+    return lib().pmgpu_step(plan.handle, pos.ctypes.data, part_vort.ctypes.data, pos.shape[0],
+                            part_vel.ctypes.data)
+
+
+def step_dev(plan: Plan, d_pos: int, d_part_vort: int, npart: int, d_part_vel: int, stream: int = 0) -> int:
+    """The same step on device pointers (e.g. ``tensor.data_ptr()``) on a CUDA stream."""
+    return lib().pmgpu_step_dev(plan.handle, C.c_void_p(d_pos), C.c_void_p(d_part_vort), int(npart),
+                                C.c_void_p(d_part_vel), C.c_void_p(stream))

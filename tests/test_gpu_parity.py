@@ -1,0 +1,248 @@
+"""GPU parity: every entry point of the C ABI against the CPU oracle on the same
+seeded inputs.  FP64 plain path: relative L2 <= 1e-12 (the bar of the north star;
+the FFT summation order differs from the Glassman FFT, ~1e-15).  FP32 form:
+relative L2 <= 1e-5 against the FP64 oracle."""
+import copy
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from oracle import validation as V
+from pmlib3d_b200 import pmlib as P
+from tests.helpers import gaussian_field, jittered_particles, rel_l2, setup_pair
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 1e-5
+
+CASES = [
+    # (name, xmin, xmax, dx, bc, nghost)
+    ("fff", (-1, -1, -1), (1, 1, 1), (0.125, 0.125, 0.125), (0, 0, 0), 4),
+    ("fff-noncubic", (-1, -0.8, -0.5), (1, 0.8, 0.5), (0.1, 0.1, 0.0625), (0, 0, 0), 4),
+    ("ppf", (-1, -1, -0.5), (1, 1, 0.5), (0.125, 0.125, 0.0625), (1, 1, 0), 4),
+    ("pff", (0, -1, -1), (2, 1, 1), (0.125, 0.125, 0.125), (1, 0, 0), 3),
+    ("fpf", (-1, 0, -1), (1, 1.5, 1), (0.125, 0.125, 0.125), (0, 1, 0), 4),
+    ("ppp", (0, 0, 0), (1, 1, 2), (1 / 16, 1 / 16, 1 / 16), (1, 1, 1), 4),
+]
+
+
+def oracle_solve(po, to, qo, w, **kw):
+    ierr, pk = O.poisson_setup(po, qo)
+    assert ierr == 0
+    v = w.copy()
+    ierr, vel, vp = O.poisson_solve(po, to, qo, pk, v, **kw)
+    assert ierr == 0
+    return vel, v, vp
+
+
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", CASES)
+@pytest.mark.parametrize("order", [6, 2])
+def test_solve_fp64(name, xmin, xmax, dx, bc, ng, order):
+    po, to, qo, pg, tg, qg = setup_pair(xmin, xmax, dx, bc, ng, interp=3, order=order)
+    w = gaussian_field(to, seed=1, noise=0.01)
+    vel_o, _, _ = oracle_solve(po, to, qo, w)
+    ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP64)
+    assert ierr == 0, P.last_error()
+    vel = np.zeros_like(w)
+    wg = w.copy()
+    assert P.pmlib_poisson_solve(plan, wg, vel) == 0
+    assert np.array_equal(wg, w)  # vorticity untouched without reg_vort / reproj
+    assert rel_l2(vel, vel_o) < TOL64, rel_l2(vel, vel_o)
+
+
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", [CASES[0], CASES[2], CASES[5]])
+def test_solve_flags_fp64(name, xmin, xmax, dx, bc, ng):
+    """reg_vort + reproj + calc_vecpot outputs (pmlib_poisson_solve.f:309-385)."""
+    po, to, qo, pg, tg, qg = setup_pair(xmin, xmax, dx, bc, ng, interp=3, order=10)
+    w = gaussian_field(to, seed=2, noise=0.02)
+    for reg, rep in ((1, 0), (0, 1), (1, 1)):
+        vel_o, vort_o, vp_o = oracle_solve(po, to, qo, w, reg_vort=bool(reg), reproj=bool(rep), calc_vecpot=True)
+        ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP64)
+        assert ierr == 0
+        vel = np.zeros_like(w)
+        vp = np.zeros_like(w)
+        wg = w.copy()
+        assert P.pmlib_poisson_solve(plan, wg, vel, vp, reg_vort=reg, reproj=rep, calc_vecpot=True) == 0
+        assert rel_l2(vel, vel_o) < TOL64
+        assert rel_l2(wg, vort_o) < TOL64
+        assert rel_l2(vp, vp_o) < TOL64
+
+
+@pytest.mark.parametrize("order", [0, 4, 8, 100])
+def test_solve_orders_fp64(order):
+    po, to, qo, pg, tg, qg = setup_pair((-1, -1, -1), (1, 1, 1), (0.125,) * 3, (0, 0, 0), 4, order=order)
+    w = gaussian_field(to, seed=3)
+    vel_o, _, _ = oracle_solve(po, to, qo, w)
+    ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP64)
+    assert ierr == 0
+    vel = np.zeros_like(w)
+    assert P.pmlib_poisson_solve(plan, w.copy(), vel) == 0
+    assert rel_l2(vel, vel_o) < (TOL64 if order != 100 else 1e-11)
+
+
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", [CASES[0], CASES[2], CASES[3]])
+def test_solve_fp32(name, xmin, xmax, dx, bc, ng):
+    po, to, qo, pg, tg, qg = setup_pair(xmin, xmax, dx, bc, ng, interp=3, order=6)
+    w = gaussian_field(to, seed=4, noise=0.01)
+    vel_o, _, _ = oracle_solve(po, to, qo, w)
+    ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP32)
+    assert ierr == 0
+    vel = np.zeros(w.shape, np.float32)
+    assert P.pmlib_poisson_solve(plan, w.astype(np.float32), vel) == 0
+    assert rel_l2(vel, vel_o) < TOL32, rel_l2(vel, vel_o)
+
+
+def test_mixedbc_convergence_pin_on_gpu():
+    """The GPU FP64 solve reproduces validation/mixedbc__/convergence.dat (h = 1/16, 1/32)."""
+    def gpu_solver(patch, t, par, vort, reg_vort=True, calc_vecpot=False):
+        pg = P.make_patch(list(patch.xmin), list(patch.xmax), list(patch.dx), nghost=patch.nghost,
+                          ncell=list(patch.ncell))
+        ierr, tg = P.pmlib_topology_cuboid(pg, par.interpolation_order)
+        qg = P.make_params(order=par.poisson_order, kernel=1, radius=par.regularisation_radius,
+                           interp=par.interpolation_order)
+        ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP64)
+        assert ierr == 0
+        vel = np.zeros_like(vort)
+        vp = np.zeros_like(vort)
+        assert P.pmlib_poisson_solve(plan, vort.copy(), vel, vp, reg_vort=reg_vort, calc_vecpot=calc_vecpot) == 0
+        return vel
+    r = V.run_validation("mixedbc", solver=gpu_solver, resolutions=(16, 32))
+    for (dx, e), (pdx, pe) in zip(r, V.MIXEDBC_PINS):
+        assert abs(e - pe) / pe < 1e-9, (e, pe)
+
+
+@pytest.mark.parametrize("nvar,order", [(1, 0), (2, 6), (3, 10), (3, 2)])
+def test_regularise(nvar, order):
+    po, to, qo, pg, tg, qg = setup_pair((-1, -1, -0.5), (1, 1, 0.5), (0.125, 0.125, 0.0625), (1, 0, 0), 4)
+    w = gaussian_field(to, seed=5, noise=0.05)[..., :nvar].copy()
+    wo = w.copy()
+    assert O.regularise(po, to, wo, order, 0.15) == 0
+    ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP64)
+    wg = w.copy()
+    assert P.pmlib_regularise(plan, wg, order, 0.15) == 0
+    assert rel_l2(wg, wo) < TOL64
+
+
+P2M_CASES = [CASES[0], CASES[1], CASES[2], CASES[3], CASES[5]]
+
+
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", P2M_CASES)
+@pytest.mark.parametrize("interp", [3, 4])
+def test_p2m_fp64(name, xmin, xmax, dx, bc, ng, interp):
+    po, to, qo, pg, tg, qg = setup_pair(xmin, xmax, dx, bc, ng, interp=interp)
+    pos, val = jittered_particles(to, seed=7, jitter=0.45, incl_ghost=True)
+    # a few particles outside the domain exercise the skip / clamp rules
+    pos[:5] += np.array([3.0, 0.0, 0.0]) * np.array([to.dx[0], 0, 0])
+    pos[5:10] -= np.array([0.0, 2.6, 0.0]) * np.array([0, to.dx[1], 0])
+    to.npart = tg.npart = pos.shape[0]
+    mo = np.zeros(O.topo_shape(to))
+    assert O.interp_particle_mesh(to, interp, pos, val, mo) == 0
+    mg = np.full(P.topo_shape(tg), 7.0)
+    assert P.pmlib_interp_particle_mesh(tg, qg, pos, val, mg, clear=True) == 0
+    assert rel_l2(mg, mo) < 1e-13, rel_l2(mg, mo)
+    # deterministic: bit-identical on a second run
+    mg2 = np.zeros(P.topo_shape(tg))
+    assert P.pmlib_interp_particle_mesh(tg, qg, pos, val, mg2, clear=True) == 0
+    assert np.array_equal(mg, mg2)
+
+
+def test_p2m_accumulate_and_clear_ghost():
+    po, to, qo, pg, tg, qg = setup_pair(*CASES[2][1:])
+    pos, val = jittered_particles(to, seed=8)
+    to.npart = tg.npart = pos.shape[0]
+    base = np.random.default_rng(1).standard_normal(O.topo_shape(to))
+    for clear, cg in ((False, False), (False, True)):
+        mo = base.copy()
+        assert O.interp_particle_mesh(to, 3, pos, val, mo, clear=clear, clear_ghost=cg) == 0
+        mg = base.copy()
+        assert P.pmlib_interp_particle_mesh(tg, qg, pos, val, mg, clear=clear, clear_ghost=cg) == 0
+        assert rel_l2(mg, mo) < 1e-13
+
+
+def test_p2m_errors(capfd):
+    po, to, qo, pg, tg, qg = setup_pair(*CASES[0][1:])
+    pos, val = jittered_particles(to, seed=9)
+    tg.npart = pos.shape[0] + 1
+    assert P.pmlib_interp_particle_mesh(tg, qg, pos, val, np.zeros(P.topo_shape(tg)), clear=True) == -1
+    assert "Discrepancy in number of particles" in capfd.readouterr().out
+    tg.npart = pos.shape[0]
+    assert P.pmlib_interp_particle_mesh(tg, qg, pos, val, np.zeros(P.topo_shape(tg, 2)), clear=True) == -1
+    assert "Dimension of interpolation variables does not correspond." in P.last_error()
+
+
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", [CASES[0], CASES[1], CASES[2]])
+@pytest.mark.parametrize("interp", [3, 4])
+def test_m2p_fp64(name, xmin, xmax, dx, bc, ng, interp):
+    po, to, qo, pg, tg, qg = setup_pair(xmin, xmax, dx, bc, ng, interp=interp)
+    pos, _ = jittered_particles(to, seed=10, jitter=0.45, incl_ghost=True)
+    pos[:7] += 5 * to.dx[0]
+    field = gaussian_field(to, seed=11, noise=0.1)
+    ierr, out_o = O.interp_mesh_particle(to, interp, field, pos)
+    assert ierr == 0
+    out = np.zeros_like(pos)
+    assert P.pmlib_interp_mesh_particle(tg, qg, pos, mesh_vel=field, part_vel=out) == 0
+    assert rel_l2(out, out_o) < 1e-14
+
+
+def test_m2p_fp32():
+    po, to, qo, pg, tg, qg = setup_pair(*CASES[0][1:])
+    pos, _ = jittered_particles(to, seed=12)
+    field = gaussian_field(to, seed=13)
+    ierr, out_o = O.interp_mesh_particle(to, 3, field, pos)
+    out = np.zeros(pos.shape, np.float32)
+    assert P.pmlib_interp_mesh_particle(tg, qg, pos.astype(np.float32), mesh_vel=field.astype(np.float32),
+                                        part_vel=out) == 0
+    assert rel_l2(out, out_o) < TOL32
+
+
+def test_remesh_matches_oracle():
+    po, to, qo, pg, tg, qg = setup_pair(*CASES[2][1:])
+    w = gaussian_field(to, seed=14)
+    dv = 0.1 * gaussian_field(to, seed=15)
+    for incl in (False, True):
+        ro = O.remesh(to, w, dv, None, None, 0.05, 0.01, incl)
+        rg = P.pmlib_remesh(tg, w, dv, None, None, 0.05, 0.01, incl)
+        assert ro[0] == rg[0] == 0
+        for a, b in zip(ro[1:4], rg[1:4]):
+            assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", [CASES[0], CASES[2]])
+def test_step_fp64_and_fp32(name, xmin, xmax, dx, bc, ng):
+    """P2M (clear) -> unbounded solve + curl -> M2P of the velocity."""
+    po, to, qo, pg, tg, qg = setup_pair(xmin, xmax, dx, bc, ng, interp=3, order=6)
+    pos, val = jittered_particles(to, seed=16)
+    to.npart = pos.shape[0]
+    mo = np.zeros(O.topo_shape(to))
+    assert O.interp_particle_mesh(to, 3, pos, val, mo) == 0
+    vel_o, _, _ = oracle_solve(po, to, qo, mo)
+    ierr, up_o = O.interp_mesh_particle(to, 3, vel_o, pos)
+    ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP64)
+    up = np.zeros_like(pos)
+    assert P.step(plan, pos, val, up) == 0
+    assert rel_l2(up, up_o) < TOL64
+    ierr, plan32 = P.pmlib_poisson_setup(pg, tg, qg, P.FP32)
+    up32 = np.zeros(pos.shape, np.float32)
+    assert P.step(plan32, pos.astype(np.float32), val.astype(np.float32), up32) == 0
+    assert rel_l2(up32, up_o) < TOL32
+
+
+def test_fft_lengths_with_generic_radix():
+    """Periodic axes of any even length, including large prime factors (2 x 23, 2 x 37)."""
+    po, to, qo, pg, tg, qg = setup_pair((0, 0, -0.5), (46 / 32, 74 / 32, 0.5), (1 / 32,) * 3, (1, 1, 0), 4)
+    w = gaussian_field(to, seed=17)
+    vel_o, _, _ = oracle_solve(po, to, qo, w)
+    ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP64)
+    assert ierr == 0
+    vel = np.zeros_like(w)
+    assert P.pmlib_poisson_solve(plan, w.copy(), vel) == 0
+    assert rel_l2(vel, vel_o) < TOL64
+
+
+def test_odd_periodic_length_rejected():
+    po, to, qo, pg, tg, qg = setup_pair((0, 0, 0), (1, 1, 1), (1 / 15, 1 / 16, 1 / 16), (1, 1, 1), 4)
+    ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP64)
+    assert ierr == -1
+    assert "nfft is an odd number." in P.last_error()

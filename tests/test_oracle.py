@@ -1,0 +1,108 @@
+"""The CPU oracle against the reference's own golden data and known-answer properties."""
+import copy
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from oracle import validation as V
+from tests.helpers import jittered_particles, rel_l2
+
+
+def test_mixedbc_pin_coarse():
+    """validation/mixedbc__/convergence.dat:1-2 (order 10, fff, [-1,1]^3)."""
+    r = V.run_validation("mixedbc", resolutions=(16, 32))
+    for (dx, e), (pdx, pe) in zip(r, V.MIXEDBC_PINS[:2]):
+        assert dx == pdx
+        assert abs(e - pe) / pe < 1e-9, (e, pe)
+
+
+@pytest.mark.slow
+def test_mixedbc_pin_fine():
+    """validation/mixedbc__/convergence.dat:1-3 including h = 1/64 (patch grows as in the program)."""
+    r = V.run_validation("mixedbc")
+    for (dx, e), (pdx, pe) in zip(r, V.MIXEDBC_PINS):
+        assert dx == pdx
+        assert abs(e - pe) / pe < 1e-9, (e, pe)
+
+
+def test_poisson_pin_rate():
+    """validation/poisson/convergence.dat is not reproduced by the committed poisson.f (order 6
+    gives ~2e-2); the spectral order-100 kernel gives its magnitude and super-convergence."""
+    import oracle.validation as VV
+    par = O.make_params(order=100, kernel=1, radius=2.0, interp=4)
+    patch = O.make_patch((-0.5, -1, -1), (0.5, 1, 1), (1.0, 1.0, 1.0), nghost=4)
+    errs = []
+    for nx in (32, 64):
+        for d in range(3):
+            patch.dx[d] = 1.0 / nx
+        assert O.patch_adjust(patch) == 0
+        ierr, t = O.topology_cuboid(patch, 4)
+        vel = VV.oracle_solver(copy.copy(patch), t, par, VV.ring_vorticity(*VV.cell_centres(t)))
+        g, n = [t.nghost[0], t.nghost[2], t.nghost[4]], [t.ncell[0], t.ncell[1], t.ncell[2]]
+        vi = vel[g[2]:g[2] + n[2], g[1]:g[1] + n[1], g[0]:g[0] + n[0]]
+        ua = VV.ring_velocity(*VV.cell_centres(t, ghosts=False))
+        errs.append(rel_l2(vi, ua))
+    for e, (_, pe) in zip(errs, V.POISSON_PINS):
+        assert 0.5 < e / pe < 2.0, (e, pe)
+    assert errs[0] / errs[1] > 1000  # spectral convergence, as in the pin (7.9e3)
+
+
+def test_glassman_matches_dft():
+    rng = np.random.default_rng(3)
+    for n in (2, 6, 16, 30, 96, 144, 160):
+        x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        assert np.allclose(O.fft_line(x), np.fft.fft(x), rtol=0, atol=1e-12 * np.abs(x).sum())
+        assert np.allclose(O.fft_line(x, inverse=True), np.fft.ifft(x) * n, rtol=0, atol=1e-12 * np.abs(x).sum())
+
+
+@pytest.mark.parametrize("order", [3, 4])
+def test_p2m_conserves_and_m2p_reproduces_linear(order):
+    """Partition of unity (sum of deposited vorticity == sum on particles away from the
+    free boundary) and exact reproduction of linear fields by M2P."""
+    po = O.make_patch((-1, -1, -1), (1, 1, 1), (0.125,) * 3, nghost=4)
+    ierr, t = O.topology_cuboid(po, order)
+    pos, val = jittered_particles(t, seed=1)
+    t.npart = pos.shape[0]
+    mesh = np.zeros(O.topo_shape(t))
+    assert O.interp_particle_mesh(t, order, pos, val, mesh) == 0
+    assert abs(mesh.sum() - val.sum()) < 1e-10 * np.abs(val).sum()
+    ext = O.topo_shape(t)
+    axes = [t.xmin[d] + (np.arange(1 - t.nghost[2 * d], t.ncell[d] + t.nghost[2 * d + 1] + 1) - 0.5) * t.dx[d]
+            for d in range(3)]
+    z, y, x = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
+    lin = np.ascontiguousarray(np.stack([1 + 2 * x - y, 0.5 * z + x, 3 * y - z + 0.25], -1))
+    ierr, out = O.interp_mesh_particle(t, order, lin, pos)
+    px, py, pz = pos[:, 0], pos[:, 1], pos[:, 2]
+    if order == 4:  # M6* uses the correct spacing; M4' has the reference's 1/dx(1) quirk (cubic cells here)
+        pass
+    exact = np.stack([1 + 2 * px - py, 0.5 * pz + px, 3 * py - pz + 0.25], -1)
+    assert np.abs(out - exact).max() < 1e-12
+
+
+def test_remesh_then_p2m_m2p_identity_at_centres():
+    """Particles at cell centres (pmlib_remesh output): M4' weights are (0, 1, 0, 0), so
+    P2M followed by M2P returns the particle values exactly."""
+    po = O.make_patch((-1, -1, -1), (1, 1, 1), (0.25,) * 3, nghost=4)
+    ierr, t = O.topology_cuboid(po, 3)
+    rng = np.random.default_rng(5)
+    mv = np.zeros(O.topo_shape(t))
+    g = 4
+    mv[g:-g, g:-g, g:-g] = rng.standard_normal(mv[g:-g, g:-g, g:-g].shape)
+    ierr, pos, pv, pdv, pvel = O.remesh(t, mv, min_vort=0.0)
+    assert ierr == 0
+    t.npart = pos.shape[0]
+    mesh = np.zeros(O.topo_shape(t))
+    assert O.interp_particle_mesh(t, 3, pos, pv, mesh) == 0
+    ierr, back = O.interp_mesh_particle(t, 3, mesh, pos)
+    assert np.array_equal(back, pv)
+
+
+def test_si_function():
+    from math import pi
+    # Si(inf) = pi/2; Si small x ~ x; a few tabulated values (A&S table 5.1)
+    assert abs(O.si(1e-8) - 1e-8) < 1e-20
+    assert abs(O.si(1.0) - 0.946083070367183) < 1e-14
+    assert abs(O.si(5.0) - 1.549931244944674) < 1e-14
+    assert abs(O.si(10.0) - 1.658347594218874) < 1e-14
+    assert abs(O.si(200.0) - pi / 2) < 1e-2
