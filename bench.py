@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Benchmark of the particle-mesh vortex step (M4' P2M -> unbounded FFT Poisson solve
+with the 6th-order regularised Green's function and spectral curl -> M4' M2P).
+
+Workload (default ``rings256``): 256^3 cells on [-1,1]^3, free on all axes, two
+coaxial vortex rings + 1 % noise, 16.7 M particles (seeded synthetic data).  The
+headline is the FP32 form's steps/s with inputs resident in HBM; beside it the FP64
+plain path is timed on the same inputs and the FP32 velocities are compared with it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs one independent replica per GPU (a single grid does not shard: the path
+has no exchange step), launched by torch.distributed.run; the value is the steps of
+all ranks divided by the slowest rank's device time.  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "256^3 vortex steps/s (FP32 form; FP64 plain path and rel-L2 alongside)"
+L2_NOTE = "inputs and intermediates larger than the 126 MB L2 (no flush)"
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ CPU oracle (baseline / reference arm)
+def oracle_setup(w, threads):
+    from oracle import oracle as O
+    O.set_threads(threads)
+    O.set_sample(1.0)
+    po = O.make_patch(w.xmin, w.xmax, w.dx, bound_cond=w.bound_cond, nghost=w.nghost)
+    ierr, t = O.topology_cuboid(po, w.interp)
+    t.npart = w.npart
+    par = O.make_params(order=w.order, kernel=1, radius=w.radius, interp=w.interp)
+    ierr, pk = O.poisson_setup(po, par)
+    assert ierr == 0
+    return O, po, t, par, pk
+
+
+def oracle_step(O, po, t, par, pk, w, frac):
+    O.set_sample(frac)
+    mesh = np.zeros(O.topo_shape(t))
+    t0 = time.perf_counter()
+    O.interp_particle_mesh(t, w.interp, w.pos, w.vort, mesh)
+    ierr, vel, _ = O.poisson_solve(po, t, par, pk, mesh)
+    ierr, up = O.interp_mesh_particle(t, w.interp, vel, w.pos)
+    dt = time.perf_counter() - t0
+    O.set_sample(1.0)
+    return dt
+
+
+def pick_fraction(O, po, t, par, pk, w, target_s):
+    """Fraction of the particles and FFT lines whose oracle step takes about target_s."""
+    f0 = 1.0 / 64
+    dt = oracle_step(O, po, t, par, pk, w, f0)
+    f = min(1.0, f0 * target_s / max(dt, 1e-3))
+    return f, dt / f0
+
+
+def run_reference(args):
+    """--impl reference: the reference's algorithm on the host cores.  The Fortran/MPI
+    reference cannot be built on these machines (no gfortran, MPI or FFTW), so this
+    times the C restatement of its plain path (oracle/), with all host threads, each
+    step a uniform sample of the full-size workload."""
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    from pmlib3d_b200 import workloads as Wl
+    w = Wl.make(args.config)
+    threads = os.cpu_count() or 1
+    O, po, t, par, pk = oracle_setup(w, threads)
+    budget = 150.0  # seconds for the whole run
+    f, full = pick_fraction(O, po, t, par, pk, w, budget / max(1, args.steps + args.warmup))
+    for _ in range(args.warmup):
+        oracle_step(O, po, t, par, pk, w, f)
+    tot = 0.0
+    for _ in range(args.steps):
+        tot += oracle_step(O, po, t, par, pk, w, f)
+    value = args.steps * f / tot
+    sample = (f"each step: oracle P2M + solve + M2P over the first {f:.4f} of the particles and of the "
+              f"FFT lines of the full {w.n}^3 workload (a full step ~{full:.1f} s on {threads} threads)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Philox)",
+            "config": {"workload": f"{w.name}: {w.n}^3 fff, two coaxial rings + 1% noise, {w.npart} particles, "
+                                   f"order 6, eps = 2h, M4'", "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ GPU arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="rings256")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    from pmlib3d_b200 import pmlib as P
+    from pmlib3d_b200 import workloads as Wl
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    w = Wl.make(args.config)
+    n = w.npart
+    patch = P.make_patch(w.xmin, w.xmax, w.dx, bound_cond=w.bound_cond, nghost=w.nghost)
+    ierr, topo = P.pmlib_topology_cuboid(patch, w.interp)
+    params = P.make_params(order=w.order, kernel=1, radius=w.radius, interp=w.interp)
+    ierr32, plan32 = P.pmlib_poisson_setup(patch, topo, params, P.FP32)
+    ierr64, plan64 = P.pmlib_poisson_setup(patch, topo, params, P.FP64)
+    assert ierr32 == 0 and ierr64 == 0, P.last_error()
+
+    dev = torch.device("cuda", local)
+    pos64 = torch.from_numpy(w.pos).to(dev)
+    vort64 = torch.from_numpy(w.vort).to(dev)
+    pos32, vort32 = pos64.float().contiguous(), vort64.float().contiguous()
+    vel32 = torch.empty_like(pos32)
+    vel64 = torch.empty_like(pos64)
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    def step(plan, pos, vort, vel):
+        rc = P.step_dev(plan, pos.data_ptr(), vort.data_ptr(), n, vel.data_ptr(), sptr)
+        if rc != 0:
+            raise RuntimeError(P.last_error())
+
+    def timed(plan, pos, vort, vel, steps, warmup, sample_clocks=False):
+        for _ in range(warmup):
+            step(plan, pos, vort, vel)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        clk = ClockSampler(local) if sample_clocks else None
+        if clk:
+            clk.start()
+        P.launch_count(reset=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step(plan, pos, vort, vel)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = P.launch_count()
+        barrier()
+        torch.cuda.synchronize()
+        clocks = clk.stop() if clk else None
+        ms = e0.elapsed_time(e1)
+        return max_over_ranks(ms), launches, clocks
+
+    # ---- headline: FP32 form, inputs resident in HBM
+    ms32, launches32, clocks = timed(plan32, pos32, vort32, vel32, args.steps, args.warmup, sample_clocks=True)
+    value = world * args.steps / (ms32 / 1000.0)
+    # ---- FP64 plain path on the same inputs
+    k64 = max(3, args.steps // 2)
+    ms64, _, _ = timed(plan64, pos64, vort64, vel64, k64, args.warmup)
+    value64 = world * k64 / (ms64 / 1000.0)
+    # ---- FP32 against FP64 on the last step
+    d = (vel32.double() - vel64)
+    rel_l2 = float(torch.sqrt((d * d).sum() / (vel64 * vel64).sum()).item())
+    max_err = float((d.abs().max() / vel64.abs().max()).item())
+
+    # ---- per-kernel device times (events around every launch) for the roofline
+    P.timing_reset()
+    P.timing_enable(True)
+    nprof = 3
+    for _ in range(nprof):
+        step(plan32, pos32, vort32, vel32)
+    torch.cuda.synchronize()
+    P.timing_enable(False)
+    kt = P.timing_read()
+    mb = Wl.model_bytes(w.n, w.nghost, 4, n)
+    kernels = {}
+    for k, (kms, cnt) in kt.items():
+        if cnt == 0:
+            continue
+        kernels[k] = {"ms_per_step": kms / nprof, "launches_per_step": cnt / nprof}
+        if k in mb:
+            kernels[k]["model_bytes_per_launch"] = mb[k]
+            kernels[k]["achieved_gbs"] = mb[k] / (kms / cnt / 1e3) / 1e9
+    modeled = {k: v for k, v in kernels.items() if "model_bytes_per_launch" in v}
+    dom = max(modeled, key=lambda k: modeled[k]["ms_per_step"])
+    peaks = {}
+    pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk_path):
+        peaks = json.load(open(pk_path))
+    peak = peaks.get("hbm_gbs")
+    peak_src = "measured (MEASURED_PEAKS.json hbm_gbs)" if peak else "fallback 6650 GB/s"
+    peak = peak or 6650.0
+    traffic = None
+    tr_path = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(tr_path):
+        traffic = json.load(open(tr_path)).get(args.config, {}).get(dom)
+    achieved = kernels[dom]["achieved_gbs"]
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
+                "algorithmic_bytes_per_launch": mb[dom]}
+
+    # ---- end to end through the C ABI with host buffers (H2D + step + D2H per step)
+    e2e = None
+    if not args.no_e2e:
+        pos_h = torch.from_numpy(w.pos.astype(np.float32)).pin_memory()
+        vort_h = torch.from_numpy(w.vort.astype(np.float32)).pin_memory()
+        vel_h = torch.empty_like(pos_h).pin_memory()
+        pn, vn, un = pos_h.numpy(), vort_h.numpy(), vel_h.numpy()
+        for _ in range(args.warmup):
+            P.step(plan32, pn, vn, un)
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        ke = max(3, args.steps // 2)
+        for _ in range(ke):
+            if P.step(plan32, pn, vn, un) != 0:
+                raise RuntimeError(P.last_error())
+        torch.cuda.synchronize()
+        dt = max_over_ranks(time.perf_counter() - t0)
+        e2e = {"value": world * ke / dt, "unit": "steps/s", "h2d_bytes_per_step": 24 * n,
+               "d2h_bytes_per_step": 12 * n, "api": "pmgpu_step (host pointers, pinned)"}
+
+    # ---- CPU baseline: the oracle on this box's host cores (rank 0, one GPU only)
+    cpu = None
+    if not args.no_cpu_baseline and world == 1 and rank == 0:
+        threads = os.cpu_count() or 1
+        O, po, t, par, pk = oracle_setup(w, threads)
+        f, full = pick_fraction(O, po, t, par, pk, w, 15.0)
+        dt = oracle_step(O, po, t, par, pk, w, f)
+        cpu = {"value": f / dt, "unit": "steps/s", "cores": threads, "kind": "port",
+               "sample": f"oracle (C restatement of the reference's plain FP64 path) P2M + solve + M2P over "
+                         f"the first {f:.4f} of the particles and FFT lines of the full workload, "
+                         f"{dt:.1f} s; steps/s = fraction / time"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox)",
+            "config": {"workload": f"{w.name}: {w.n}^3 cells, free-free-free, two coaxial rings + 1% noise, "
+                                   f"{n} particles, order 6 Green's function, eps = 2h, M4'",
+                       "grid": f"N={w.n}, nghost={w.nghost}, FFT M={2 * (w.n + 2 * w.nghost)}",
+                       "parallelism": f"replicas x{world}", "l2": L2_NOTE},
+            "fp64_plain": {"value": value64, "unit": "steps/s", "ms_per_step": ms64 / k64},
+            "fp32_speedup_vs_fp64": value / value64,
+            "accuracy": {"rel_l2_fp32_vs_fp64": rel_l2, "max_rel_err": max_err},
+            "roofline": roofline, "kernels": kernels, "gpu_launches": launches32,
+            "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    for p in (plan32, plan64):
+        p.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -148,10 +148,16 @@ int pmgpu_remesh(const pmgpu_topo *topo, const double *mesh_vort, const double *
                  double min_dvort, int incl_ghost, int max_part, double *pos, double *part_vort,
                  double *part_dvort, double *part_vel, int *npart);
 
-/* ---- diagnostics ---- */
+/* ---- diagnostics (no counterpart in the reference, which has no timers) ---- */
 const char *pmgpu_last_error(void);
 /* number of this library's kernels launched since the last reset */
 long long pmgpu_launch_count(int reset);
+/* per-kernel-class device timing: when enabled every launch is bracketed by CUDA
+ * events on its own stream.  Classes are numbered 0..n-1; pmgpu_timing_get returns
+ * -1 past the last one. */
+void pmgpu_timing_enable(int on);
+void pmgpu_timing_reset(void);
+int pmgpu_timing_get(int index, const char **name, double *ms_total, long long *launches);
 
 #ifdef __cplusplus
 }

@@ -77,6 +77,7 @@ def lib():
         dp = C.POINTER(C.c_double)
         ip = C.POINTER(C.c_int)
         L.pmo_set_threads.argtypes = [C.c_int]
+        L.pmo_set_sample.argtypes = [C.c_double]
         L.pmo_parameters_check.argtypes = [C.POINTER(Params)]
         L.pmo_patch_adjust.argtypes = [C.POINTER(Patch)]
         L.pmo_topology_cuboid.argtypes = [C.POINTER(Patch), C.c_int, C.POINTER(Topo)]
@@ -109,6 +110,11 @@ def _p(a):
 
 def set_threads(n: int) -> None:
     lib().pmo_set_threads(int(n))
+
+
+def set_sample(frac: float) -> None:
+    """Timing aid: run only this fraction of the particles and FFT lines (1.0 = all)."""
+    lib().pmo_set_sample(float(frac))
 
 
 def make_patch(xmin, xmax, dx, bound_cond=(0, 0, 0), nghost=4, ncell=None, fft_seq=(1, 2, 3)):

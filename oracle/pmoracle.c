@@ -22,6 +22,17 @@ static int g_threads = 1;
 void pmo_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
 int pmo_get_threads(void) { return g_threads; }
 
+/* Work sampling for timing only: with a fraction f < 1 the particle loops run over
+ * the first f of the particles and every FFT pass / line loop over the first f of
+ * its lines, so a run costs about f of a full step.  Results are then partial. */
+static double g_frac = 1.0;
+void pmo_set_sample(double f) { g_frac = (f > 0.0 && f < 1.0) ? f : 1.0; }
+static int sampled(int n) {
+  if (g_frac >= 1.0) return n;
+  int m = (int)((double)n * g_frac);
+  return m < 1 ? (n > 0 ? 1 : 0) : m;
+}
+
 /* source/pmlib_write.f:40-48, rank 0 format "[0000](caller) : msg" */
 static void pm_write(const char *caller, const char *msg) {
   printf("[%04d](%s) : %s\n", 0, caller, msg);
@@ -301,47 +312,67 @@ int pmo_interp_particle_mesh(const pmo_topo *t, int order, const double *xpart,
   double c_1_d[3];
   for (int e = 0; e < 3; e++) c_1_d[e] = 1.0 / t->dx[e];
 
-  for (int p = 0; p < npart; p++) {
-    const double *x = xpart + (size_t)3 * p;
-    int base[3], idx[3][6];
-    double w[3][6];
-    for (int e = 0; e < 3; e++) base[e] = nint((x[e] - t->xmin[e]) * c_1_d[e]);
-    int inside = 1;
-    for (int e = 0; e < 3; e++) {
-      int first = base[e] - off, last = base[e] - off + W - 1;
-      if (!(last >= lo[e] && first <= hi[e])) inside = 0;
-    }
-    if (!inside) continue;
-    for (int e = 0; e < 3; e++) {
-      double d = (x[e] - t->xmin[e] - t->dx[e] * ((double)base[e] - 0.5)) * c_1_d[e];
-      if (order == 3) w_m4(d, w[e]); else w_m6(d, w[e]);
-      for (int s = 0; s < W; s++) idx[e][s] = base[e] - off + s;
-    }
-    /* cancel stencils not supported by the mesh (:219-397), axis by axis in the
-     * reference's order; an out-of-domain particle on an interior/periodic face
-     * zeroes all weights */
-    for (int e = 0; e < 3; e++) {
-      if (bc[2 * e] == 0) {
-        for (int s = 0; s < W; s++)
-          if (idx[e][s] < lo[e]) { w[e][s] = 0.0; idx[e][s] = lo[e]; }
-      } else if (x[e] < t->xmin[e]) {
-        for (int s = 0; s < W; s++) { w[0][s] = 0.0; w[1][s] = 0.0; w[2][s] = 0.0; idx[e][s] = lo[e]; }
+  /* Threads own disjoint z-slabs of the mesh and each visits the particles in index
+   * order, so every cell receives its contributions in the serial order and the
+   * result is bit-identical to the single-threaded loop. */
+  const int np_run = sampled(npart);
+  int nth = g_threads;
+#pragma omp parallel num_threads(nth)
+  {
+    int tid = 0, nt = 1;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+    nt = omp_get_num_threads();
+#endif
+    const int nz = hi[2] - lo[2] + 1;
+    const int kb = lo[2] + (int)((long long)nz * tid / nt);
+    const int ke = lo[2] + (int)((long long)nz * (tid + 1) / nt) - 1;
+    for (int p = 0; p < np_run; p++) {
+      const double *x = xpart + (size_t)3 * p;
+      int base[3], idx[3][6];
+      double w[3][6];
+      for (int e = 0; e < 3; e++) base[e] = nint((x[e] - t->xmin[e]) * c_1_d[e]);
+      /* cheap slab test before the full stencil work */
+      if (base[2] - off + W - 1 < kb || base[2] - off > ke) continue;
+      int inside = 1;
+      for (int e = 0; e < 3; e++) {
+        int first = base[e] - off, last = base[e] - off + W - 1;
+        if (!(last >= lo[e] && first <= hi[e])) inside = 0;
       }
-      if (bc[2 * e + 1] == 0) {
-        for (int s = 0; s < W; s++)
-          if (idx[e][s] > hi[e]) { w[e][s] = 0.0; idx[e][s] = hi[e]; }
-      } else if (x[e] > t->xmax[e]) {
-        for (int s = 0; s < W; s++) { w[0][s] = 0.0; w[1][s] = 0.0; w[2][s] = 0.0; idx[e][s] = hi[e]; }
+      if (!inside) continue;
+      for (int e = 0; e < 3; e++) {
+        double d = (x[e] - t->xmin[e] - t->dx[e] * ((double)base[e] - 0.5)) * c_1_d[e];
+        if (order == 3) w_m4(d, w[e]); else w_m6(d, w[e]);
+        for (int s = 0; s < W; s++) idx[e][s] = base[e] - off + s;
       }
-    }
-    const double *v = part + (size_t)nvar * p;
-    for (int sk = 0; sk < W; sk++)
-      for (int sj = 0; sj < W; sj++)
-        for (int si = 0; si < W; si++) {
-          double wt = w[0][si] * w[1][sj] * w[2][sk];
-          size_t m = midx(t, nvar, 0, idx[0][si], idx[1][sj], idx[2][sk]);
-          for (int c = 0; c < nvar; c++) mesh[m + c] = mesh[m + c] + wt * v[c];
+      /* cancel stencils not supported by the mesh (:219-397), axis by axis in the
+       * reference's order; an out-of-domain particle on an interior/periodic face
+       * zeroes all weights */
+      for (int e = 0; e < 3; e++) {
+        if (bc[2 * e] == 0) {
+          for (int s = 0; s < W; s++)
+            if (idx[e][s] < lo[e]) { w[e][s] = 0.0; idx[e][s] = lo[e]; }
+        } else if (x[e] < t->xmin[e]) {
+          for (int s = 0; s < W; s++) { w[0][s] = 0.0; w[1][s] = 0.0; w[2][s] = 0.0; idx[e][s] = lo[e]; }
         }
+        if (bc[2 * e + 1] == 0) {
+          for (int s = 0; s < W; s++)
+            if (idx[e][s] > hi[e]) { w[e][s] = 0.0; idx[e][s] = hi[e]; }
+        } else if (x[e] > t->xmax[e]) {
+          for (int s = 0; s < W; s++) { w[0][s] = 0.0; w[1][s] = 0.0; w[2][s] = 0.0; idx[e][s] = hi[e]; }
+        }
+      }
+      const double *v = part + (size_t)nvar * p;
+      for (int sk = 0; sk < W; sk++) {
+        if (idx[2][sk] < kb || idx[2][sk] > ke) continue;
+        for (int sj = 0; sj < W; sj++)
+          for (int si = 0; si < W; si++) {
+            double wt = w[0][si] * w[1][sj] * w[2][sk];
+            size_t m = midx(t, nvar, 0, idx[0][si], idx[1][sj], idx[2][sk]);
+            for (int c = 0; c < nvar; c++) mesh[m + c] = mesh[m + c] + wt * v[c];
+          }
+      }
+    }
   }
   /* :1128-1134 ghost reverse-add per axis x, y, z */
   for (int d = 0; d < 3; d++) ghost_add_axis(t, mesh, nvar, d);
@@ -365,8 +396,9 @@ int pmo_interp_mesh_particle(const pmo_topo *t, int order, const double *mesh,
   double c_1_d[3];
   for (int e = 0; e < 3; e++) c_1_d[e] = 1.0 / t->dx[e];
   int nth = g_threads;
+  const int np_run = sampled(npart);
 #pragma omp parallel for schedule(static) num_threads(nth)
-  for (int p = 0; p < npart; p++) {
+  for (int p = 0; p < np_run; p++) {
     const double *x = pos + (size_t)3 * p;
     int idx[3][6];
     double w[3][6];
@@ -492,7 +524,10 @@ static cbox cb_map(cbox *src, const int lo[3], const int n[3]) {
     int e1 = src->lo[d] + src->n[d], e2 = lo[d] + n[d];
     z[d] = (e1 < e2 ? e1 : e2);
   }
-  for (int k = a[2]; k < z[2]; k++)
+  const int kend = a[2] + sampled(z[2] - a[2] > 0 ? z[2] - a[2] : 0);
+  int nth = g_threads;
+#pragma omp parallel for schedule(static) num_threads(nth)
+  for (int k = a[2]; k < kend; k++)
     for (int j = a[1]; j < z[1]; j++)
       for (int i = a[0]; i < z[0]; i++) {
         size_t s = cb_idx(src, 0, i - src->lo[0], j - src->lo[1], k - src->lo[2]);
@@ -515,7 +550,7 @@ static int cb_fft_axis(cbox *b, int ax, int inverse, int shift, const char *call
   if (ax >= 1) stride *= b->n[0];
   if (ax >= 2) stride *= b->n[1];
   int o1 = (ax == 0) ? 1 : 0, o2 = (ax == 2) ? 1 : 2;
-  int nlines = b->n[o1] * b->n[o2] * b->nv;
+  int nlines = sampled(b->n[o1] * b->n[o2] * b->nv);
   int nth = g_threads;
 #pragma omp parallel num_threads(nth)
   {
@@ -912,7 +947,7 @@ int pmo_poisson_solve(const pmo_patch *pa, const pmo_topo *cub, const pmo_params
 
   int nout = 3 + (ifft_vort ? 3 : 0) + (ifft_vecpot ? 3 : 0);
   cbox out = cb_alloc(lo3, n3, nout); /* vel (0..2), vort (3..5), vecpot (6..8) */
-  int nlines = n3[o1] * n3[o2];
+  int nlines = sampled(n3[o1] * n3[o2]);
   int nth = g_threads;
 #pragma omp parallel num_threads(nth)
   {

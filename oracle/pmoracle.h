@@ -49,6 +49,8 @@ typedef struct {
 } pmo_params;
 
 void pmo_set_threads(int n);
+/* timing aid: run only a fraction f of the particles and FFT lines (results partial) */
+void pmo_set_sample(double f);
 int pmo_get_threads(void);
 
 int pmo_parameters_check(const pmo_params *par);

@@ -17,6 +17,7 @@ EXPORTS = (
     "pmgpu_poisson_setup", "pmgpu_poisson_solve", "pmgpu_poisson_solve_f32",
     "pmgpu_regularise", "pmgpu_regularise_f32", "pmgpu_plan_destroy",
     "pmgpu_step", "pmgpu_step_dev", "pmgpu_remesh", "pmgpu_last_error", "pmgpu_launch_count",
+    "pmgpu_timing_enable", "pmgpu_timing_reset", "pmgpu_timing_get",
 )
 
 
@@ -76,12 +77,17 @@ def lib():
         "pmgpu_remesh": [TP, dp, dp, dp, vp, C.c_double, C.c_double, C.c_int, C.c_int, dp, dp, dp, dp, ip],
         "pmgpu_last_error": [],
         "pmgpu_launch_count": [C.c_int],
+        "pmgpu_timing_enable": [C.c_int],
+        "pmgpu_timing_reset": [],
+        "pmgpu_timing_get": [C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(C.c_longlong)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
         f.argtypes = args
         f.restype = C.c_int
     L.pmgpu_plan_destroy.restype = None
+    L.pmgpu_timing_enable.restype = None
+    L.pmgpu_timing_reset.restype = None
     L.pmgpu_last_error.restype = C.c_char_p
     L.pmgpu_launch_count.restype = C.c_longlong
     _lib = L

@@ -21,6 +21,53 @@ namespace pmgpu {
 
 long long g_launches = 0;
 
+// ------------------------------------------------------------------ per-kernel timing
+// When enabled, every launch of the library is bracketed by CUDA events on its
+// stream; pmgpu_timing_get sums the elapsed times per kernel class.
+enum KClass { KC_BIN, KC_SCAN, KC_RHIST, KC_RSCAT, KC_DEPOSIT, KC_GADD, KC_XFWD, KC_YFWD, KC_ZPASS, KC_YINV,
+              KC_XINV, KC_GFILL, KC_M2P, KC_OTHER, KC_N };
+static const char *kc_names[KC_N] = {"bin", "scan", "radix_hist", "radix_scatter", "deposit", "ghost_add",
+                                     "x_fwd", "y_fwd", "z_pass", "y_inv", "x_inv", "ghost_fill", "m2p", "other"};
+static bool g_timing = false;
+struct PendingEv {
+  int cls;
+  cudaEvent_t a, b;
+};
+static std::vector<PendingEv> g_pending;
+static double g_kms[KC_N];
+static long long g_kn[KC_N];
+
+struct KTimer {
+  int cls;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr, b = nullptr;
+  KTimer(int c, cudaStream_t s) : cls(c), st(s) {
+    if (g_timing) {
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      cudaEventRecord(a, st);
+    }
+  }
+  ~KTimer() {
+    if (g_timing && a) {
+      cudaEventRecord(b, st);
+      g_pending.push_back({cls, a, b});
+    }
+  }
+};
+static void timing_collect() {
+  for (auto &p : g_pending) {
+    float ms = 0.f;
+    cudaEventSynchronize(p.b);
+    cudaEventElapsedTime(&ms, p.a, p.b);
+    g_kms[p.cls] += ms;
+    g_kn[p.cls] += 1;
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+  }
+  g_pending.clear();
+}
+
 static char g_err[512] = "";
 static std::mutex g_mu;
 
@@ -247,11 +294,11 @@ static int exclusive_scan(const unsigned *in, unsigned *out, size_t n, DevBuf &p
                           const char *caller) {
   const size_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
   if (part.ensure(sizeof(unsigned) * (nb + 1), caller)) return -1;
-  k_scan_reduce<<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, part.as<unsigned>());
+  { KTimer kt_(KC_SCAN, st); k_scan_reduce<<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, part.as<unsigned>()); }
   PM_LAUNCHED();
-  k_scan_partials<<<1, SCAN_THREADS, 0, st>>>(part.as<unsigned>(), (int)nb);
+  { KTimer kt_(KC_SCAN, st); k_scan_partials<<<1, SCAN_THREADS, 0, st>>>(part.as<unsigned>(), (int)nb); }
   PM_LAUNCHED();
-  k_scan_apply<<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, part.as<unsigned>(), out);
+  { KTimer kt_(KC_SCAN, st); k_scan_apply<<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, part.as<unsigned>(), out); }
   PM_LAUNCHED();
   CKL(caller);
   return 0;
@@ -274,10 +321,10 @@ static int radix_sort(unsigned maxkey, int n, DevBuf &k1, DevBuf &v1, DevBuf &k2
   CK(cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), caller);
   for (int p = 0; p < passes; p++) {
     const int shift = p * db;
-    k_radix_hist<<<nblk, RADIX_THREADS, 0, st>>>(ka, n, shift, db, hist.as<unsigned>(), nblk);
+    { KTimer kt_(KC_RHIST, st); k_radix_hist<<<nblk, RADIX_THREADS, 0, st>>>(ka, n, shift, db, hist.as<unsigned>(), nblk); }
     PM_LAUNCHED();
     if (exclusive_scan(hist.as<unsigned>(), hist.as<unsigned>(), (size_t)nbk * nblk, part, st, caller)) return -1;
-    k_radix_scatter<<<nblk, RADIX_THREADS, smem, st>>>(ka, va, n, shift, db, hist.as<unsigned>(), nblk, kb, vb);
+    { KTimer kt_(KC_RSCAT, st); k_radix_scatter<<<nblk, RADIX_THREADS, smem, st>>>(ka, va, n, shift, db, hist.as<unsigned>(), nblk, kb, vb); }
     PM_LAUNCHED();
     CKL(caller);
     std::swap(ka, kb);
@@ -340,8 +387,8 @@ static int run_p2m(const pmgpu_topo *t, int order, const R *pos, const R *val, i
   const int *perm = nullptr;
   if (n > 0) {
     const int nblk = std::min((n + 255) / 256, 148 * 32);
-    if (W == 4) k_bin<R, 4><<<nblk, 256, 0, st>>>(g, pos, n, s.key->as<unsigned>(), s.val->as<int>(), s.counts->as<unsigned>());
-    else k_bin<R, 6><<<nblk, 256, 0, st>>>(g, pos, n, s.key->as<unsigned>(), s.val->as<int>(), s.counts->as<unsigned>());
+    if (W == 4) { KTimer kt_(KC_BIN, st); k_bin<R, 4><<<nblk, 256, 0, st>>>(g, pos, n, s.key->as<unsigned>(), s.val->as<int>(), s.counts->as<unsigned>()); }
+    else { KTimer kt_(KC_BIN, st); k_bin<R, 6><<<nblk, 256, 0, st>>>(g, pos, n, s.key->as<unsigned>(), s.val->as<int>(), s.counts->as<unsigned>()); }
     PM_LAUNCHED();
     CKL(caller);
   }
@@ -368,6 +415,7 @@ static int run_p2m(const pmgpu_topo *t, int order, const R *pos, const R *val, i
   if (W == WW && nv == NVV) {                                                                              \
     CK(cudaFuncSetAttribute(k_deposit<R, WW, NVV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), \
        caller);                                                                                            \
+    KTimer kt_(KC_DEPOSIT, st);                                                                            \
     k_deposit<R, WW, NVV><<<grid, DEP_TX * DEP_TY, smem, st>>>(g, pos, vp, nvar, s.start->as<unsigned>(),   \
                                                                 pp, mp, nvar_mesh, zc, cap, clear_mode);    \
     PM_LAUNCHED();                                                                                         \
@@ -383,8 +431,8 @@ static int run_p2m(const pmgpu_topo *t, int order, const R *pos, const R *val, i
     const int S = t->nghost[2 * d] + t->nghost[2 * d + 1];
     const long long total = (long long)S * g.ext[(d + 1) % 3] * g.ext[(d + 2) % 3];
     const int nblk = (int)std::min<long long>((total + 255) / 256, 148 * 16);
-    k_ghost_add<R><<<std::max(nblk, 1), 256, 0, st>>>(mesh, g.ext[0], g.ext[1], g.ext[2], nvar_mesh, d,
-                                                       t->ncell[d], t->nghost[2 * d], t->nghost[2 * d + 1]);
+    { KTimer kt_(KC_GADD, 0); k_ghost_add<R><<<std::max(nblk, 1), 256, 0, st>>>(mesh, g.ext[0], g.ext[1], g.ext[2], nvar_mesh, d,
+                                                       t->ncell[d], t->nghost[2 * d], t->nghost[2 * d + 1]); }
     PM_LAUNCHED();
     CKL(caller);
   }
@@ -399,8 +447,8 @@ static int run_m2p(const pmgpu_topo *t, int order, const R *pos, const int *ord,
   const int W = (order == 3) ? 4 : 6;
   PartGeom<R> g = part_geom<R>(t, W);
   const int nblk = std::min((n + 127) / 128, 148 * 32);
-  if (W == 4) k_m2p<R, 4><<<nblk, 128, 0, st>>>(g, pos, ord, n, f0, f1, f2, o0, o1, o2);
-  else k_m2p<R, 6><<<nblk, 128, 0, st>>>(g, pos, ord, n, f0, f1, f2, o0, o1, o2);
+  if (W == 4) { KTimer kt_(KC_M2P, st); k_m2p<R, 4><<<nblk, 128, 0, st>>>(g, pos, ord, n, f0, f1, f2, o0, o1, o2); }
+  else { KTimer kt_(KC_M2P, st); k_m2p<R, 6><<<nblk, 128, 0, st>>>(g, pos, ord, n, f0, f1, f2, o0, o1, o2); }
   PM_LAUNCHED();
   CKL(caller);
   return 0;
@@ -447,14 +495,14 @@ static int fwd_xy(SolveGeom<R> &g, const R *in, typename cplx_t<R>::type *X, typ
   size_t sm = fft_smem(g.N2, NC * RB, sizeof(C), ntwx);
   CK(cudaFuncSetAttribute(k_xfwd<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
   const int rows = g.P[1] * g.P[2];
-  k_xfwd<R, NC><<<(rows + RB - 1) / RB, 256, sm, st>>>(g, in, X, RB, cs);
+  { KTimer kt_(KC_XFWD, st); k_xfwd<R, NC><<<(rows + RB - 1) / RB, 256, sm, st>>>(g, in, X, RB, cs); }
   PM_LAUNCHED();
   CKL(caller);
   const int TK = std::min(lines_for(g.M[1], NC, sizeof(C), g.fy.ntw), g.H);
   sm = fft_smem(g.M[1], NC * TK, sizeof(C), g.fy.ntw);
   CK(cudaFuncSetAttribute(k_ypass<R, NC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
   dim3 grid((g.H + TK - 1) / TK, g.P[2]);
-  k_ypass<R, NC, false><<<grid, 256, sm, st>>>(g, X, Y, TK, g.P[1], g.M[1]);
+  { KTimer kt_(KC_YFWD, st); k_ypass<R, NC, false><<<grid, 256, sm, st>>>(g, X, Y, TK, g.P[1], g.M[1]); }
   PM_LAUNCHED();
   CKL(caller);
   return 0;
@@ -468,7 +516,7 @@ static int zpass(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typename c
   const size_t sm = fft_smem(g.M[2], NC * TK, sizeof(C), g.fz.ntw);
   CK(cudaFuncSetAttribute(k_zpass<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
   dim3 grid((g.H + TK - 1) / TK, rows_y);
-  k_zpass<R, NC><<<grid, 256, sm, st>>>(g, in, out, TK, mode, reproj, use_zeta);
+  { KTimer kt_(KC_ZPASS, st); k_zpass<R, NC><<<grid, 256, sm, st>>>(g, in, out, TK, mode, reproj, use_zeta); }
   PM_LAUNCHED();
   CKL(caller);
   return 0;
@@ -483,7 +531,7 @@ static int inv_yx(SolveGeom<R> &g, const pmgpu_topo *topo, typename cplx_t<R>::t
   size_t sm = fft_smem(g.M[1], NC * TK, sizeof(C), g.fy.ntw);
   CK(cudaFuncSetAttribute(k_ypass<R, NC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
   dim3 grid((g.H + TK - 1) / TK, g.P[2]);
-  k_ypass<R, NC, true><<<grid, 256, sm, st>>>(g, Y, X, TK, g.M[1], g.P[1]);
+  { KTimer kt_(KC_YINV, st); k_ypass<R, NC, true><<<grid, 256, sm, st>>>(g, Y, X, TK, g.M[1], g.P[1]); }
   PM_LAUNCHED();
   CKL(caller);
   const int ntwx = g.fx.ntw + g.fx.next;
@@ -491,7 +539,7 @@ static int inv_yx(SolveGeom<R> &g, const pmgpu_topo *topo, typename cplx_t<R>::t
   sm = fft_smem(g.N2, NC * RB, sizeof(C), ntwx);
   CK(cudaFuncSetAttribute(k_xinv<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
   const int rows = g.P[1] * g.P[2];
-  k_xinv<R, NC><<<(rows + RB - 1) / RB, 256, sm, st>>>(g, X, out, RB, cs);
+  { KTimer kt_(KC_XINV, st); k_xinv<R, NC><<<(rows + RB - 1) / RB, 256, sm, st>>>(g, X, out, RB, cs); }
   PM_LAUNCHED();
   CKL(caller);
   // periodic ghosts (x, then y, then z)
@@ -500,8 +548,8 @@ static int inv_yx(SolveGeom<R> &g, const pmgpu_topo *topo, typename cplx_t<R>::t
     const int S = topo->nghost[2 * d] + topo->nghost[2 * d + 1];
     const long long total = (long long)S * g.ext[(d + 1) % 3] * g.ext[(d + 2) % 3];
     const int nblk = (int)std::min<long long>((total + 255) / 256, 148 * 16);
-    k_ghost_fill<R><<<std::max(nblk, 1), 256, 0, st>>>(out, g.ext[0], g.ext[1], g.ext[2], cs, d, topo->ncell[d],
-                                                        topo->nghost[2 * d], topo->nghost[2 * d + 1]);
+    { KTimer kt_(KC_GFILL, 0); k_ghost_fill<R><<<std::max(nblk, 1), 256, 0, st>>>(out, g.ext[0], g.ext[1], g.ext[2], cs, d, topo->ncell[d],
+                                                        topo->nghost[2 * d], topo->nghost[2 * d + 1]); }
     PM_LAUNCHED();
     CKL(caller);
   }
@@ -562,8 +610,8 @@ static int run_regularise(pmgpu_plan *pl, R *mesh, int nvar, int reg_order, doub
     const int S = topo->nghost[2 * d] + topo->nghost[2 * d + 1];
     const long long total = (long long)S * ext[(d + 1) % 3] * ext[(d + 2) % 3];
     const int nblk = (int)std::min<long long>((total + 255) / 256, 148 * 16);
-    k_ghost_fill<R><<<std::max(nblk, 1), 256, 0, st>>>(mesh, ext[0], ext[1], ext[2], nvar, d, topo->ncell[d],
-                                                        topo->nghost[2 * d], topo->nghost[2 * d + 1]);
+    { KTimer kt_(KC_GFILL, 0); k_ghost_fill<R><<<std::max(nblk, 1), 256, 0, st>>>(mesh, ext[0], ext[1], ext[2], nvar, d, topo->ncell[d],
+                                                        topo->nghost[2 * d], topo->nghost[2 * d + 1]); }
     PM_LAUNCHED();
     CKL(caller);
   }
@@ -715,6 +763,31 @@ long long pmgpu_launch_count(int reset) {
 }
 
 int pmgpu_parameters_check(const pmgpu_params *par) { return check_params(par); }
+
+void pmgpu_timing_enable(int on) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  timing_collect();
+  g_timing = on != 0;
+}
+
+void pmgpu_timing_reset(void) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  timing_collect();
+  for (int i = 0; i < KC_N; i++) {
+    g_kms[i] = 0.0;
+    g_kn[i] = 0;
+  }
+}
+
+int pmgpu_timing_get(int index, const char **name, double *ms_total, long long *launches) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  timing_collect();
+  if (index < 0 || index >= KC_N) return -1;
+  if (name) *name = kc_names[index];
+  if (ms_total) *ms_total = g_kms[index];
+  if (launches) *launches = g_kn[index];
+  return 0;
+}
 
 // source/patch/pmlib_patch_adjust.f:34-146
 int pmgpu_patch_adjust(pmgpu_patch *p) {

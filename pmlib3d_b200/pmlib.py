@@ -51,6 +51,28 @@ def launch_count(reset: bool = False) -> int:
     return int(lib().pmgpu_launch_count(int(reset)))
 
 
+def timing_enable(on: bool = True) -> None:
+    """Bracket every library launch with CUDA events (for per-kernel device times)."""
+    lib().pmgpu_timing_enable(int(on))
+
+
+def timing_reset() -> None:
+    lib().pmgpu_timing_reset()
+
+
+def timing_read() -> dict:
+    """{kernel class: (total ms, launches)} accumulated since the last reset."""
+    out = {}
+    i = 0
+    while True:
+        name, ms, n = C.c_char_p(), C.c_double(), C.c_longlong()
+        if lib().pmgpu_timing_get(i, C.byref(name), C.byref(ms), C.byref(n)) != 0:
+            break
+        out[name.value.decode()] = (ms.value, n.value)
+        i += 1
+    return out
+
+
 def _ptr(a, dtype):
     if a is None:
         return None

@@ -1,0 +1,122 @@
+"""Seeded synthetic workloads of the particle-mesh vortex step.
+
+The reference publishes no benchmark data set; these generators stand in for its
+configurations with their shapes and value distributions:
+
+* ``ring64``  : 64^3 cells, h = 2/64 on [-1,1]^3, free on all axes, one vortex ring
+  (R = 0.5, sigma = 0.1), omega_theta = exp(-(d/sigma)^2) cut at 4 sigma, where d is
+  the distance to the ring centre line.
+* ``rings256``: 256^3 cells on [-1,1]^3 (free), two coaxial rings (R = 0.5,
+  sigma = 0.08) at x = -+0.2 with opposite circulation, plus 1 % Gaussian noise on
+  omega.  16.7 M particles.
+* ``rings128``: the same field on 128^3 cells (a scaling and test point).
+
+Particles sit one per interior cell centre in pmlib_remesh order (k-j-i, x fastest;
+source/remesh/pmlib_remesh.f:151-226), jittered by U(-0.1 h, 0.1 h) per axis.  The
+grid is given explicitly (no pmlib_patch_adjust): N' = N + 2 nghost, M = 2 N'.
+Random numbers come from NumPy's counter-based Philox generator with the seed
+20261203 + a config id, so every machine produces the same bytes.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+SEED = 20261203
+
+
+@dataclass
+class Workload:
+    name: str
+    n: int                 # cells per axis
+    xmin: tuple
+    xmax: tuple
+    dx: tuple
+    bound_cond: tuple
+    nghost: int
+    order: int             # Poisson kernel order
+    radius: float          # regularisation radius (epsilon = radius * h)
+    interp: int            # 3 = M4'
+    pos: np.ndarray        # (np, 3) float64
+    vort: np.ndarray       # (np, 3) float64
+
+    @property
+    def npart(self) -> int:
+        return self.pos.shape[0]
+
+
+def _ring_vorticity(pos, x0, R, sigma, sign):
+    """omega = sign * exp(-(d/sigma)^2) e_theta around the x axis, zero beyond 4 sigma."""
+    x = pos[:, 0] - x0
+    y, z = pos[:, 1], pos[:, 2]
+    rho = np.sqrt(y * y + z * z)
+    d = np.sqrt((rho - R) ** 2 + x * x)
+    w = np.where(d < 4.0 * sigma, sign * np.exp(-(d / sigma) ** 2), 0.0)
+    rs = np.where(rho > 0, rho, 1.0)
+    out = np.zeros_like(pos)
+    out[:, 1] = -w * z / rs
+    out[:, 2] = w * y / rs
+    return out
+
+
+def _lattice(n, xmin, h, rng, jitter=0.1):
+    c = xmin + (np.arange(n, dtype=np.float64) + 0.5) * h
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    pos = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=-1)
+    pos += rng.uniform(-jitter * h, jitter * h, size=pos.shape)
+    return pos
+
+
+def make(name: str) -> Workload:
+    if name == "ring64":
+        n, cid = 64, 0
+        rng = np.random.Generator(np.random.Philox(SEED + cid))
+        h = 2.0 / n
+        pos = _lattice(n, -1.0, h, rng)
+        vort = _ring_vorticity(pos, 0.0, 0.5, 0.1, 1.0)
+    elif name in ("rings256", "rings128"):
+        n = 256 if name == "rings256" else 128
+        cid = 1
+        rng = np.random.Generator(np.random.Philox(SEED + cid))
+        h = 2.0 / n
+        pos = _lattice(n, -1.0, h, rng)
+        vort = _ring_vorticity(pos, -0.2, 0.5, 0.08, 1.0) + _ring_vorticity(pos, 0.2, 0.5, 0.08, -1.0)
+        vort += 0.01 * np.abs(vort).max() * rng.standard_normal(vort.shape)
+    else:
+        raise ValueError(f"unknown workload {name}")
+    return Workload(name=name, n=n, xmin=(-1.0,) * 3, xmax=(1.0,) * 3, dx=(h,) * 3, bound_cond=(0, 0, 0),
+                    nghost=4, order=6, radius=2.0, interp=3, pos=np.ascontiguousarray(pos),
+                    vort=np.ascontiguousarray(vort))
+
+
+def model_bytes(n: int, nghost: int = 4, w: int = 4, npart: int | None = None) -> dict:
+    """Algorithmic bytes of one step on an n^3 free grid (5-pass out-of-core FFT model,
+    half spectrum along x, half-spectrum Green's function read once):
+
+      V = N'^3, X = H N'^2, Y = H M N', c = 2 w
+      B_solve = 3wV + 3cX + 3cX + 3cY + 3cY + w H M M + 3cY + 3cY + 3cX + 3cX + 3wV
+      B_P2M = 6 w np + 3 w V ;  B_M2P = 3 w np + 3 w V + 3 w np
+    Per pass: x_fwd 3wV + 3cX, y_fwd 3cX + 3cY, z_pass 6cY + wHMM, y_inv 3cY + 3cX,
+    x_inv 3cX + 3wV.
+    """
+    npr = n + 2 * nghost
+    M = 2 * npr
+    H = M // 2 + 1
+    c = 2 * w
+    npart = n ** 3 if npart is None else npart
+    V = npr ** 3
+    X = H * npr * npr
+    Y = H * M * npr
+    passes = {
+        "x_fwd": 3 * w * V + 3 * c * X,
+        "y_fwd": 3 * c * X + 3 * c * Y,
+        "z_pass": 6 * c * Y + w * H * M * M,
+        "y_inv": 3 * c * Y + 3 * c * X,
+        "x_inv": 3 * c * X + 3 * w * V,
+        "deposit": 6 * w * npart + 3 * w * V,
+        "m2p": 6 * w * npart + 3 * w * V,
+    }
+    passes["solve"] = sum(passes[k] for k in ("x_fwd", "y_fwd", "z_pass", "y_inv", "x_inv"))
+    passes["step"] = passes["solve"] + passes["deposit"] + passes["m2p"]
+    return passes
