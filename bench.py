@@ -165,6 +165,10 @@ def main():
     ap.add_argument("--config", default="rings256")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--mode", default="full", choices=["full", "profile"],
+                    help="profile: only the FP32 warm-up and timed steps (for ncu captures)")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"],
+                    help="precision of --mode profile")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -237,6 +241,20 @@ def main():
         clocks = clk.stop() if clk else None
         ms = e0.elapsed_time(e1)
         return max_over_ranks(ms), launches, clocks
+
+    if args.mode == "profile":
+        if args.precision == "fp32":
+            ms, launches, _ = timed(plan32, pos32, vort32, vel32, args.steps, args.warmup)
+        else:
+            ms, launches, _ = timed(plan64, pos64, vort64, vel64, args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps({"mode": "profile", "precision": args.precision, "config": args.config,
+                              "ms_per_step": ms / args.steps, "gpu_launches": launches}), flush=True)
+        for p in (plan32, plan64):
+            p.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
 
     # ---- headline: FP32 form, inputs resident in HBM
     ms32, launches32, clocks = timed(plan32, pos32, vort32, vel32, args.steps, args.warmup, sample_clocks=True)

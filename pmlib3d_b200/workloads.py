@@ -9,7 +9,8 @@ configurations with their shapes and value distributions:
 * ``rings256``: 256^3 cells on [-1,1]^3 (free), two coaxial rings (R = 0.5,
   sigma = 0.08) at x = -+0.2 with opposite circulation, plus 1 % Gaussian noise on
   omega.  16.7 M particles.
-* ``rings128``: the same field on 128^3 cells (a scaling and test point).
+* ``rings128`` / ``rings192``: the same field on 128^3 / 192^3 cells (scaling,
+  test and profiling points).
 
 Particles sit one per interior cell centre in pmlib_remesh order (k-j-i, x fastest;
 source/remesh/pmlib_remesh.f:151-226), jittered by U(-0.1 h, 0.1 h) per axis.  The
@@ -75,8 +76,8 @@ def make(name: str) -> Workload:
         h = 2.0 / n
         pos = _lattice(n, -1.0, h, rng)
         vort = _ring_vorticity(pos, 0.0, 0.5, 0.1, 1.0)
-    elif name in ("rings256", "rings128"):
-        n = 256 if name == "rings256" else 128
+    elif name in ("rings256", "rings128", "rings192"):
+        n = {"rings256": 256, "rings128": 128, "rings192": 192}[name]
         cid = 1
         rng = np.random.Generator(np.random.Philox(SEED + cid))
         h = 2.0 / n
