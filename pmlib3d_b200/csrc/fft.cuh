@@ -154,91 +154,180 @@ template <int R, bool INV, typename C> __device__ __forceinline__ void dft(C *v)
   }
 }
 
-// one Stockham pass of radix R over L interleaved lines
-template <int R, bool INV, typename C>
-__device__ __noinline__ void stockham_pass(const C *__restrict__ src, C *__restrict__ dst, int L,
-                                              int n, int ns, const C *__restrict__ tw) {
-  const int nr = n / R;
-  const int total = L * nr;
-  for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    const int j = t / L;
-    const int l = t - j * L;
-    const int k = j % ns;
-    C v[R];
-#pragma unroll
-    for (int r = 0; r < R; r++) v[r] = src[(j + r * nr) * L + l];
-    if (ns > 1) {
-      const C *w = tw + k * (R - 1) - 1;
-#pragma unroll
-      for (int r = 1; r < R; r++) v[r] = INV ? cmulc(v[r], w[r]) : cmul(v[r], w[r]);
-    }
-    dft<R, INV>(v);
-    const int base = (j - k) * R + k;
-#pragma unroll
-    for (int r = 0; r < R; r++) dst[(base + r * ns) * L + l] = v[r];
-  }
+// ---------------------------------------------------------------------------
+// Vectorised passes.  Shared-memory buffers hold LG vectors per transform index,
+// a vector being G consecutive lines (FP32: float4 = two complex lines, FP64:
+// double2 = one).  A thread owns one line group g and the butterflies j = jt,
+// jt + JS, ...; the twiddle index k = j mod ns and j - k advance incrementally, so
+// the passes contain no integer division.
+template <typename R> struct Vec;
+template <> struct Vec<float> {
+  typedef float4 V;
+  static constexpr int G = 2;
+};
+template <> struct Vec<double> {
+  typedef double2 V;
+  static constexpr int G = 1;
+};
+
+__device__ __forceinline__ void vsplit(const float4 &v, float2 *a) {
+  a[0] = make_float2(v.x, v.y);
+  a[1] = make_float2(v.z, v.w);
+}
+__device__ __forceinline__ void vsplit(const double2 &v, double2 *a) { a[0] = v; }
+__device__ __forceinline__ float4 vmerge(const float2 *a) { return make_float4(a[0].x, a[0].y, a[1].x, a[1].y); }
+__device__ __forceinline__ double2 vmerge(const double2 *a) { return a[0]; }
+
+struct LineMap {
+  int jt;  // first butterfly of this thread
+  int JS;  // butterfly stride (threads per line group)
+  int g;   // line group, -1 for an idle thread
+};
+
+__device__ __forceinline__ LineMap line_map(int LG) {
+  LineMap m;
+  m.JS = blockDim.x / LG;
+  m.jt = threadIdx.x / LG;
+  m.g = threadIdx.x - m.jt * LG;
+  if (m.jt >= m.JS) m.g = -1;
+  return m;
 }
 
-// generic radix: one output per work item, O(R) terms each
-template <bool INV, typename C>
-__device__ __noinline__ void stockham_generic(const C *__restrict__ src, C *__restrict__ dst,
-                                                 int L, int n, int ns, int R,
-                                                 const C *__restrict__ tw,
-                                                 const C *__restrict__ roots) {
-  const int nr = n / R;
-  const int total = L * n;
-  for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    const int q = t / L;
-    const int l = t - q * L;
-    const int m = q / nr;       // output within the butterfly
-    const int j = q - m * nr;   // butterfly
-    const int k = j % ns;
-    C acc = mk((typename real_of<C>::type)0, (typename real_of<C>::type)0);
-    for (int r = 0; r < R; r++) {
-      C v = src[(j + r * nr) * L + l];
-      if (ns > 1 && r > 0) {
-        C w = tw[k * (R - 1) + r - 1];
-        v = INV ? cmulc(v, w) : cmul(v, w);
+template <int RAD, bool INV, typename R>
+__device__ __forceinline__ void vpass(const typename Vec<R>::V *__restrict__ src, typename Vec<R>::V *__restrict__ dst,
+                                      int LG, int n, int ns, const typename cplx_t<R>::type *__restrict__ tw,
+                                      const LineMap &lm) {
+  typedef typename cplx_t<R>::type C;
+  typedef typename Vec<R>::V V;
+  constexpr int G = Vec<R>::G;
+  if (lm.g < 0) return;
+  const int nr = n / RAD;
+  int j = lm.jt;
+  int k = j % ns;
+  int jmk = j - k;
+  const int JSm = lm.JS % ns;
+  const int JSq = lm.JS - JSm;
+  while (j < nr) {
+    C a[G][RAD];
+#pragma unroll
+    for (int r = 0; r < RAD; r++) {
+      C t[G];
+      vsplit(src[(j + r * nr) * LG + lm.g], t);
+#pragma unroll
+      for (int h = 0; h < G; h++) a[h][r] = t[h];
+    }
+    if (k != 0) {
+      const C *w = tw + k * (RAD - 1) - 1;
+#pragma unroll
+      for (int r = 1; r < RAD; r++) {
+        const C ww = w[r];
+#pragma unroll
+        for (int h = 0; h < G; h++) a[h][r] = INV ? cmulc(a[h][r], ww) : cmul(a[h][r], ww);
       }
-      C w2 = roots[(r * m) % R];
-      acc = cadd(acc, INV ? cmulc(v, w2) : cmul(v, w2));
     }
-    dst[((j - k) * R + k + m * ns) * L + l] = acc;
+#pragma unroll
+    for (int h = 0; h < G; h++) dft<RAD, INV>(a[h]);
+    const int base = jmk * RAD + k;
+#pragma unroll
+    for (int r = 0; r < RAD; r++) {
+      C t[G];
+#pragma unroll
+      for (int h = 0; h < G; h++) t[h] = a[h][r];
+      dst[(base + r * ns) * LG + lm.g] = vmerge(t);
+    }
+    j += lm.JS;
+    k += JSm;
+    jmk += JSq;
+    if (k >= ns) {
+      k -= ns;
+      jmk += ns;
+    }
   }
 }
 
-// Transforms the L lines in buffer a (ping-pong partner b); returns the buffer
-// holding the result.  The radix passes are separate (non-inlined) functions so
-// every kernel shares one compiled copy per precision and direction.  Caller
-// synchronises before (data staged) and after.
-template <bool INV, typename C>
-__device__ __noinline__ C *fft_batch(C *a, C *b, int L, const FftDesc &d, const C *__restrict__ tw) {
+// generic radix (primes without an unrolled kernel): O(RAD^2) per butterfly
+template <bool INV, typename R>
+__device__ __forceinline__ void vpass_generic(const typename Vec<R>::V *__restrict__ src,
+                                              typename Vec<R>::V *__restrict__ dst, int LG, int n, int ns,
+                                              int RAD, const typename cplx_t<R>::type *__restrict__ tw,
+                                              const typename cplx_t<R>::type *__restrict__ roots,
+                                              const LineMap &lm) {
+  typedef typename cplx_t<R>::type C;
+  constexpr int G = Vec<R>::G;
+  if (lm.g < 0) return;
+  const int nr = n / RAD;
+  for (int j = lm.jt; j < nr; j += lm.JS) {
+    const int k = j % ns;
+    const int base = (j - k) * RAD + k;
+    for (int m = 0; m < RAD; m++) {
+      C acc[G];
+#pragma unroll
+      for (int h = 0; h < G; h++) acc[h] = mk(R(0), R(0));
+      for (int r = 0; r < RAD; r++) {
+        C t[G];
+        vsplit(src[(j + r * nr) * LG + lm.g], t);
+        C w2 = roots[(r * m) % RAD];
+        if (k != 0 && r > 0) {
+          const C w = tw[k * (RAD - 1) + r - 1];
+          w2 = cmul(w2, w);
+        }
+#pragma unroll
+        for (int h = 0; h < G; h++) acc[h] = cadd(acc[h], INV ? cmulc(t[h], w2) : cmul(t[h], w2));
+      }
+      dst[(base + m * ns) * LG + lm.g] = vmerge(acc);
+    }
+  }
+}
+
+// Transforms the lines in buffer a (partner b); returns the buffer with the result.
+// The caller synchronises before (data staged); every pass ends with a barrier.
+template <bool INV, typename R>
+__device__ __forceinline__ typename Vec<R>::V *vfft(typename Vec<R>::V *a, typename Vec<R>::V *b, int LG,
+                                                    const FftDesc &d, const typename cplx_t<R>::type *__restrict__ tw,
+                                                    const LineMap &lm) {
+  typedef typename Vec<R>::V V;
   const int np = d.npass, n = d.n;
   for (int p = 0; p < np; p++) {
-    const C *t = tw + d.twoff[p];
+    const typename cplx_t<R>::type *t = tw + d.twoff[p];
     const int ns = d.ns[p];
     switch (d.rad[p]) {
-      case 2: stockham_pass<2, INV>(a, b, L, n, ns, t); break;
-      case 3: stockham_pass<3, INV>(a, b, L, n, ns, t); break;
-      case 4: stockham_pass<4, INV>(a, b, L, n, ns, t); break;
-      case 5: stockham_pass<5, INV>(a, b, L, n, ns, t); break;
-      case 7: stockham_pass<7, INV>(a, b, L, n, ns, t); break;
-      case 8: stockham_pass<8, INV>(a, b, L, n, ns, t); break;
-      case 11: stockham_pass<11, INV>(a, b, L, n, ns, t); break;
-      case 13: stockham_pass<13, INV>(a, b, L, n, ns, t); break;
-      case 16: stockham_pass<16, INV>(a, b, L, n, ns, t); break;
-      case 17: stockham_pass<17, INV>(a, b, L, n, ns, t); break;
-      default:
-        stockham_generic<INV>(a, b, L, n, ns, d.rad[p], t, tw + d.rootoff[p]);
-        break;
+      case 2: vpass<2, INV, R>(a, b, LG, n, ns, t, lm); break;
+      case 3: vpass<3, INV, R>(a, b, LG, n, ns, t, lm); break;
+      case 4: vpass<4, INV, R>(a, b, LG, n, ns, t, lm); break;
+      case 5: vpass<5, INV, R>(a, b, LG, n, ns, t, lm); break;
+      case 7: vpass<7, INV, R>(a, b, LG, n, ns, t, lm); break;
+      case 8: vpass<8, INV, R>(a, b, LG, n, ns, t, lm); break;
+      case 11: vpass<11, INV, R>(a, b, LG, n, ns, t, lm); break;
+      case 13: vpass<13, INV, R>(a, b, LG, n, ns, t, lm); break;
+      case 16: vpass<16, INV, R>(a, b, LG, n, ns, t, lm); break;
+      case 17: vpass<17, INV, R>(a, b, LG, n, ns, t, lm); break;
+      default: vpass_generic<INV, R>(a, b, LG, n, ns, d.rad[p], t, tw + d.rootoff[p], lm); break;
     }
     __syncthreads();
-    C *s = a;
+    V *s = a;
     a = b;
     b = s;
   }
   return a;
 }
+
+// ---------------------------------------------------------------------------
+// asynchronous global -> shared copies (sm_80+ cp.async; completion is waited for
+// with cp.async.wait_group, no spinning)
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // copy a table from global to shared memory (caller synchronises)
 template <typename C>

@@ -140,14 +140,14 @@ __global__ void k_green_real(GreenParams gp, double *__restrict__ gr) {
 
 // octant of the real spectrum, scaled by dx dy dz / (Mx My Mz), in the plan precision
 template <typename R>
-__global__ void k_green_octant(const double2 *__restrict__ spec, int M1, int H, int gM1, int gM2, double f,
+__global__ void k_green_octant(const double2 *__restrict__ spec, int M1, int H, int Hp, int gM1, int gM2, double f,
                                R *__restrict__ out) {
   const size_t total = (size_t)gM2 * gM1 * H;
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
     const int kx = (int)(t % H);
     const int iy = (int)((t / H) % gM1);
     const int iz = (int)(t / ((size_t)H * gM1));
-    out[t] = (R)(spec[((size_t)iz * M1 + iy) * H + kx].x * f);
+    out[t] = (R)(spec[((size_t)iz * M1 + iy) * Hp + kx].x * f);
   }
 }
 

@@ -220,18 +220,48 @@ template <typename R> static int upload_tw(const std::vector<cld> &tw, DevBuf &b
   return 0;
 }
 
-// lines per CTA for a ping-pong transform of length n with nc components
-static int lines_for(int n, int nc, size_t csize, int ntw) {
-  const size_t budget = 100 * 1024;
-  const size_t twb = (size_t)((ntw + 1) & ~1) * csize;
-  size_t per = 2 * (size_t)nc * n * csize;
-  long long k = (budget > twb) ? (long long)((budget - twb) / per) : 0;
-  if (k < 1) k = 1;
-  if (k > 16) k = 16;
-  return (int)k;
+// shared-memory budget of one persistent pass CTA
+constexpr size_t PASS_SMEM_BUDGET = 220 * 1024;
+
+static size_t tw_bytes(int ntw, size_t csize) { return (size_t)((ntw + 7) & ~7) * csize; }
+
+// kx tile of the y / z passes: the largest of 8, 4, 2, 1 whose three buffers fit
+// (FP32 needs an even line count: two lines per 16-byte vector)
+static int pick_tk(int n, int nc, size_t csize, int ntw) {
+  for (int tk = 8; tk >= 1; tk /= 2) {
+    if (csize == 8 && (nc * tk) % 2) continue;
+    if (tw_bytes(ntw, csize) + 3 * (size_t)nc * tk * n * csize <= PASS_SMEM_BUDGET) return tk;
+  }
+  return 0;
 }
-static size_t fft_smem(int n, int lines, size_t csize, int ntw) {
-  return (size_t)((ntw + 1) & ~1) * csize + 2 * (size_t)lines * n * csize;
+static size_t lines_smem(int n, int nc, int tk, size_t csize, int ntw) {
+  return tw_bytes(ntw, csize) + 3 * (size_t)nc * tk * n * csize;
+}
+// rows per tile of the x passes
+static int pick_rb(int n2, int P0, int Hp, int nc, size_t csize, size_t rsize, int ntw, bool inverse) {
+  for (int rb = 8; rb >= 1; rb--) {
+    if (csize == 8 && (nc * rb) % 2) continue;
+    const size_t stage = inverse ? (size_t)rb * Hp * nc * csize : (((size_t)rb * P0 * nc * rsize + 15) / 16) * 16;
+    if (tw_bytes(ntw, csize) + stage + 2 * (size_t)nc * rb * n2 * csize <= PASS_SMEM_BUDGET) return rb;
+  }
+  return 0;
+}
+
+static int g_nsm = 0;
+static int num_sms() {
+  if (g_nsm == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (g_nsm <= 0) g_nsm = 148;
+  }
+  return g_nsm;
+}
+
+template <typename K> static int persistent_grid(K kernel, size_t smem, int ntiles) {
+  int per = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, PASS_THREADS, smem) != cudaSuccess || per < 1) per = 1;
+  return std::max(1, std::min(ntiles, per * num_sms()));
 }
 
 }  // namespace pmgpu
@@ -240,7 +270,7 @@ using namespace pmgpu;
 
 // ------------------------------------------------------------------ plan object
 struct Geometry {
-  int ext[3], off[3], P[3], M[3], H, N2;
+  int ext[3], off[3], P[3], M[3], H, Hp, N2;
   int allper;
 };
 
@@ -466,6 +496,7 @@ template <typename R> static SolveGeom<R> solve_geom(const pmgpu_plan *pl) {
     g.M[e] = pl->g.M[e];
   }
   g.H = pl->g.H;
+  g.Hp = pl->g.Hp;
   g.N2 = pl->g.N2;
   g.fx = pl->fx;
   g.fy = pl->fy;
@@ -487,39 +518,73 @@ template <typename R> static SolveGeom<R> solve_geom(const pmgpu_plan *pl) {
 }
 
 template <typename R, int NC>
-static int fwd_xy(SolveGeom<R> &g, const R *in, typename cplx_t<R>::type *X, typename cplx_t<R>::type *Y,
-                  cudaStream_t st, const char *caller, int cs = NC) {
+static int launch_lines(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typename cplx_t<R>::type *out, int axis,
+                        int lmode, int zmode, int reproj, int use_zeta, int rows_in, int rows_out, long long in_os,
+                        long long in_rs, long long out_os, long long out_rs, int nouter, cudaStream_t st,
+                        const char *caller) {
   typedef typename cplx_t<R>::type C;
-  const int ntwx = g.fx.ntw + g.fx.next;
-  const int RB = lines_for(g.N2, NC, sizeof(C), ntwx);
-  size_t sm = fft_smem(g.N2, NC * RB, sizeof(C), ntwx);
-  CK(cudaFuncSetAttribute(k_xfwd<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
-  const int rows = g.P[1] * g.P[2];
-  { KTimer kt_(KC_XFWD, st); k_xfwd<R, NC><<<(rows + RB - 1) / RB, 256, sm, st>>>(g, in, X, RB, cs); }
-  PM_LAUNCHED();
-  CKL(caller);
-  const int TK = std::min(lines_for(g.M[1], NC, sizeof(C), g.fy.ntw), g.H);
-  sm = fft_smem(g.M[1], NC * TK, sizeof(C), g.fy.ntw);
-  CK(cudaFuncSetAttribute(k_ypass<R, NC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
-  dim3 grid((g.H + TK - 1) / TK, g.P[2]);
-  { KTimer kt_(KC_YFWD, st); k_ypass<R, NC, false><<<grid, 256, sm, st>>>(g, X, Y, TK, g.P[1], g.M[1]); }
+  const int n = g.M[axis];
+  const int ntw = (axis == 1) ? g.fy.ntw : g.fz.ntw;
+  const int TK = pick_tk(n, NC, sizeof(C), ntw);
+  if (TK == 0) {
+    set_error(caller, "FFT length too large for the shared-memory transform.");
+    return -1;
+  }
+  LineTiles lt;
+  lt.n = n;
+  lt.rows_in = rows_in;
+  lt.rows_out = rows_out;
+  lt.in_os = in_os;
+  lt.in_rs = in_rs;
+  lt.out_os = out_os;
+  lt.out_rs = out_rs;
+  lt.nouter = nouter;
+  lt.nkt = g.Hp / TK;
+  lt.TK = TK;
+  const size_t sm = lines_smem(n, NC, TK, sizeof(C), ntw);
+  CK(cudaFuncSetAttribute(k_lines<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+  const int grid = persistent_grid(k_lines<R, NC>, sm, lt.nouter * lt.nkt);
+  k_lines<R, NC><<<grid, PASS_THREADS, sm, st>>>(g, lt, in, out, axis, lmode, zmode, reproj, use_zeta);
   PM_LAUNCHED();
   CKL(caller);
   return 0;
 }
 
 template <typename R, int NC>
-static int zpass(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typename cplx_t<R>::type *out, int mode,
-                 int reproj, int use_zeta, int rows_y, cudaStream_t st, const char *caller) {
+static int fwd_xy(SolveGeom<R> &g, const R *in, typename cplx_t<R>::type *X, typename cplx_t<R>::type *Y,
+                  cudaStream_t st, const char *caller, int cs = NC) {
   typedef typename cplx_t<R>::type C;
-  const int TK = std::min(lines_for(g.M[2], NC, sizeof(C), g.fz.ntw), g.H);
-  const size_t sm = fft_smem(g.M[2], NC * TK, sizeof(C), g.fz.ntw);
-  CK(cudaFuncSetAttribute(k_zpass<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
-  dim3 grid((g.H + TK - 1) / TK, rows_y);
-  { KTimer kt_(KC_ZPASS, st); k_zpass<R, NC><<<grid, 256, sm, st>>>(g, in, out, TK, mode, reproj, use_zeta); }
+  const int ntwx = g.fx.ntw + g.fx.next;
+  const int RB = pick_rb(g.N2, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), ntwx, false);
+  if (RB == 0) {
+    set_error(caller, "FFT length too large for the shared-memory transform.");
+    return -1;
+  }
+  const size_t stage = (((size_t)RB * g.P[0] * NC * sizeof(R) + 15) / 16) * 16;
+  const size_t sm = tw_bytes(ntwx, sizeof(C)) + stage + 2 * (size_t)NC * RB * g.N2 * sizeof(C);
+  const bool vec16 = cs == NC && ((size_t)g.ext[0] * NC * sizeof(R)) % 16 == 0 &&
+                     ((size_t)g.off[0] * NC * sizeof(R)) % 16 == 0 && ((size_t)g.P[0] * NC * sizeof(R)) % 16 == 0;
+  CK(cudaFuncSetAttribute(k_xfwd<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+  const int rows = g.P[1] * g.P[2];
+  const int ntiles = (rows + RB - 1) / RB;
+  { KTimer kt_(KC_XFWD, st);
+    k_xfwd<R, NC><<<persistent_grid(k_xfwd<R, NC>, sm, ntiles), PASS_THREADS, sm, st>>>(g, in, X, RB, cs, vec16 ? 1 : 0); }
   PM_LAUNCHED();
   CKL(caller);
-  return 0;
+  const long long Hp = g.Hp;
+  KTimer kt_(KC_YFWD, st);
+  return launch_lines<R, NC>(g, X, Y, 1, L_FWD, 0, 0, 0, g.P[1], g.M[1], (long long)g.P[1] * Hp, Hp,
+                             (long long)g.M[1] * Hp, Hp, g.P[2], st, caller);
+}
+
+template <typename R, int NC>
+static int zpass(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typename cplx_t<R>::type *out, int mode,
+                 int reproj, int use_zeta, int rows_y, cudaStream_t st, const char *caller) {
+  const long long Hp = g.Hp;
+  const int rows = (mode == Z_FORWARD) ? g.M[2] : g.P[2];
+  KTimer kt_(KC_ZPASS, st);
+  return launch_lines<R, NC>(g, in, out, 2, mode == Z_FORWARD ? L_FWD : L_Z, mode, reproj, use_zeta, rows, rows, Hp,
+                             (long long)g.M[1] * Hp, Hp, (long long)g.M[1] * Hp, rows_y, st, caller);
 }
 
 template <typename R, int NC>
@@ -527,19 +592,25 @@ static int inv_yx(SolveGeom<R> &g, const pmgpu_topo *topo, typename cplx_t<R>::t
                   typename cplx_t<R>::type *X, R *out, cudaStream_t st, const char *caller, int cs = NC,
                   bool ghosts = true) {
   typedef typename cplx_t<R>::type C;
-  const int TK = std::min(lines_for(g.M[1], NC, sizeof(C), g.fy.ntw), g.H);
-  size_t sm = fft_smem(g.M[1], NC * TK, sizeof(C), g.fy.ntw);
-  CK(cudaFuncSetAttribute(k_ypass<R, NC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
-  dim3 grid((g.H + TK - 1) / TK, g.P[2]);
-  { KTimer kt_(KC_YINV, st); k_ypass<R, NC, true><<<grid, 256, sm, st>>>(g, Y, X, TK, g.M[1], g.P[1]); }
-  PM_LAUNCHED();
-  CKL(caller);
+  const long long Hp = g.Hp;
+  {
+    KTimer kt_(KC_YINV, st);
+    if (launch_lines<R, NC>(g, Y, X, 1, L_INV, 0, 0, 0, g.M[1], g.P[1], (long long)g.M[1] * Hp, Hp,
+                            (long long)g.P[1] * Hp, Hp, g.P[2], st, caller))
+      return -1;
+  }
   const int ntwx = g.fx.ntw + g.fx.next;
-  const int RB = lines_for(g.N2, NC, sizeof(C), ntwx);
-  sm = fft_smem(g.N2, NC * RB, sizeof(C), ntwx);
+  const int RB = pick_rb(g.N2, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), ntwx, true);
+  if (RB == 0) {
+    set_error(caller, "FFT length too large for the shared-memory transform.");
+    return -1;
+  }
+  const size_t sm = tw_bytes(ntwx, sizeof(C)) + (size_t)RB * g.Hp * NC * sizeof(C) + 2 * (size_t)NC * RB * g.N2 * sizeof(C);
   CK(cudaFuncSetAttribute(k_xinv<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
   const int rows = g.P[1] * g.P[2];
-  { KTimer kt_(KC_XINV, st); k_xinv<R, NC><<<(rows + RB - 1) / RB, 256, sm, st>>>(g, X, out, RB, cs); }
+  const int ntiles = (rows + RB - 1) / RB;
+  { KTimer kt_(KC_XINV, st);
+    k_xinv<R, NC><<<persistent_grid(k_xinv<R, NC>, sm, ntiles), PASS_THREADS, sm, st>>>(g, X, out, RB, cs); }
   PM_LAUNCHED();
   CKL(caller);
   // periodic ghosts (x, then y, then z)
@@ -548,7 +619,7 @@ static int inv_yx(SolveGeom<R> &g, const pmgpu_topo *topo, typename cplx_t<R>::t
     const int S = topo->nghost[2 * d] + topo->nghost[2 * d + 1];
     const long long total = (long long)S * g.ext[(d + 1) % 3] * g.ext[(d + 2) % 3];
     const int nblk = (int)std::min<long long>((total + 255) / 256, 148 * 16);
-    { KTimer kt_(KC_GFILL, 0); k_ghost_fill<R><<<std::max(nblk, 1), 256, 0, st>>>(out, g.ext[0], g.ext[1], g.ext[2], cs, d, topo->ncell[d],
+    { KTimer kt_(KC_GFILL, st); k_ghost_fill<R><<<std::max(nblk, 1), 256, 0, st>>>(out, g.ext[0], g.ext[1], g.ext[2], cs, d, topo->ncell[d],
                                                         topo->nghost[2 * d], topo->nghost[2 * d + 1]); }
     PM_LAUNCHED();
     CKL(caller);
@@ -563,7 +634,7 @@ static int run_solve(pmgpu_plan *pl, const R *vort, R *vel, R *vort_out, R *vecp
   SolveGeom<R> g = solve_geom<R>(pl);
   const int ifft_vort = reg_vort || reproj;
   const int ifft_vecpot = calc_vecpot && pl->par.poisson_kernel == 1;
-  const size_t nX = (size_t)g.P[1] * g.P[2] * g.H * 3, nY = (size_t)g.M[1] * g.P[2] * g.H * 3;
+  const size_t nX = (size_t)g.P[1] * g.P[2] * g.Hp * 3, nY = (size_t)g.M[1] * g.P[2] * g.Hp * 3;
   if (pl->X.ensure(sizeof(C) * nX, caller) || pl->Y.ensure(sizeof(C) * nY, caller)) return -1;
   if (ifft_vort && pl->Y2.ensure(sizeof(C) * nY, caller)) return -1;
   if (ifft_vecpot && pl->Y3.ensure(sizeof(C) * nY, caller)) return -1;
@@ -585,7 +656,7 @@ static int run_regularise_nc(pmgpu_plan *pl, R *mesh, int cs, int reg_order, dou
   SolveGeom<R> g = solve_geom<R>(pl);
   g.order = reg_order;
   g.eps2pi = (R)(2.0 * 3.14159265358979323846 * fw);
-  const size_t nX = (size_t)g.P[1] * g.P[2] * g.H * NC, nY = (size_t)g.M[1] * g.P[2] * g.H * NC;
+  const size_t nX = (size_t)g.P[1] * g.P[2] * g.Hp * NC, nY = (size_t)g.M[1] * g.P[2] * g.Hp * NC;
   if (pl->X.ensure(sizeof(C) * nX, caller) || pl->Y.ensure(sizeof(C) * nY, caller)) return -1;
   C *X = pl->X.as<C>(), *Y = pl->Y.as<C>();
   if (fwd_xy<R, NC>(g, mesh, X, Y, st, caller, cs)) return -1;
@@ -650,6 +721,7 @@ template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller)
     gg.M[e] = G.M[e];
   }
   gg.H = G.H;
+  gg.Hp = G.Hp;
   gg.N2 = G.N2;
   std::vector<cld> tw;
   DevBuf tx, ty, tz, gr, gX, gY;
@@ -662,7 +734,7 @@ template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller)
     gg.twy = ty.as<double2>();
     gg.twz = tz.as<double2>();
     const size_t npts = (size_t)G.M[0] * G.M[1] * G.M[2];
-    const size_t nspec = (size_t)G.M[2] * G.M[1] * G.H;
+    const size_t nspec = (size_t)G.M[2] * G.M[1] * G.Hp;
     if (gr.ensure(sizeof(double) * npts, caller) || gX.ensure(sizeof(double2) * nspec, caller) ||
         gY.ensure(sizeof(double2) * nspec, caller))
       break;
@@ -676,7 +748,7 @@ template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller)
     const double f = pl->patch.dx[0] * pl->patch.dx[1] * pl->patch.dx[2] /
                      ((double)G.M[0] * (double)G.M[1] * (double)G.M[2]);
     k_green_octant<R><<<(unsigned)std::min<size_t>((noct + 255) / 256, 148 * 64), 256>>>(
-        gY.as<double2>(), G.M[1], G.H, pl->gM1, pl->gM2, f, pl->green.as<R>());
+        gY.as<double2>(), G.M[1], G.H, G.Hp, pl->gM1, pl->gM2, f, pl->green.as<R>());
     PM_LAUNCHED();
     if (!cuda_ok(cudaGetLastError(), caller)) break;
     if (!cuda_ok(cudaDeviceSynchronize(), caller)) break;
@@ -996,6 +1068,7 @@ int pmgpu_poisson_setup(const pmgpu_patch *patch, const pmgpu_topo *cuboid, cons
     mdx = std::max(mdx, patch->dx[e]);
   }
   pl->g.H = pl->g.M[0] / 2 + 1;
+  pl->g.Hp = (pl->g.H + 7) / 8 * 8;
   pl->g.N2 = pl->g.M[0] / 2;
   pl->g.allper = allper;
   pl->eps = par->regularisation_radius * mdx;

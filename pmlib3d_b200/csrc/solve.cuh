@@ -8,6 +8,7 @@
 //
 //   x_fwd : real cuboid -> X[z][y][kx][c], kx < H = Mx/2+1   (R2C, zero-pad fused)
 //   y_fwd : X -> Y[z][ky][kx][c], ky < My                      (C2C, zero-pad fused)
+// (the kx extent of X and Y is padded to Hp, a multiple of 8, for aligned tiles)
 //   z_pass: Y -> Y (or another buffer): pad, FFT, multiply+curl, iFFT, truncate
 //   y_inv : Y -> X (truncate to the pencil extent)
 //   x_inv : X -> real cuboid                                     (C2R, truncate fused)
@@ -31,6 +32,7 @@ template <typename R> struct SolveGeom {
   int P[3];        // pencil extents (free: N + 2 nghost, periodic: N)
   int M[3];        // FFT lengths (free: 2 P, periodic: P)
   int H;           // Mx / 2 + 1
+  int Hp;          // H padded to a multiple of 8 (16-byte aligned tile rows)
   int N2;          // Mx / 2
   FftDesc fx, fy, fz;
   const C *twx, *twy, *twz;
@@ -58,149 +60,126 @@ template <typename R> __device__ __forceinline__ R zeta_filter(int order, R s) {
   return order == 0 ? R(1) : p * e;
 }
 
-// ---------------------------------------------------------------- x forward (R2C)
-template <typename R, int NC>
-__global__ void __launch_bounds__(256, 2) k_xfwd(SolveGeom<R> g, const R *__restrict__ in,
-                                              typename cplx_t<R>::type *__restrict__ X, int RB, int cs) {
-  typedef typename cplx_t<R>::type C;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ FftDesc sd;
-  if (threadIdx.x == 0) sd = g.fx;
-  const int N = g.N2, L = NC * RB;
-  const int ntw = g.fx.ntw + g.fx.next;
-  C *tw = reinterpret_cast<C *>(smem_raw);
-  C *A = tw + ((ntw + 1) & ~1);
-  C *B = A + (size_t)L * N;
-  stage_table(tw, g.twx, ntw);
-  const int nrows = g.P[1] * g.P[2];
-  const int row0 = blockIdx.x * RB;
-  for (int t = threadIdx.x; t < RB * N; t += blockDim.x) {
-    const int rr = t / N, m = t - rr * N;
-    const int row = row0 + rr;
-    R a[NC], b[NC];
-#pragma unroll
-    for (int c = 0; c < NC; c++) { a[c] = R(0); b[c] = R(0); }
-    if (row < nrows) {
-      const int y = row % g.P[1], z = row / g.P[1];
-      const R *src = in + (((size_t)(z + g.off[2]) * g.ext[1] + (y + g.off[1])) * g.ext[0] + g.off[0]) * cs;
-      const int x0 = 2 * m, x1 = 2 * m + 1;
-      if (x0 < g.P[0]) {
-#pragma unroll
-        for (int c = 0; c < NC; c++) a[c] = src[(size_t)x0 * cs + c];
-      }
-      if (x1 < g.P[0]) {
-#pragma unroll
-        for (int c = 0; c < NC; c++) b[c] = src[(size_t)x1 * cs + c];
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < NC; c++) A[m * L + rr * NC + c] = mk(a[c], b[c]);
-  }
-  __syncthreads();
-  C *Z = fft_batch<false>(A, B, L, sd, tw);
-  const C *W = tw + g.fx.extoff;  // exp(-2 pi i k / Mx), k < H
-  for (int t = threadIdx.x; t < RB * g.H; t += blockDim.x) {
-    const int rr = t / g.H, k = t - rr * g.H;
-    const int row = row0 + rr;
-    if (row >= nrows) continue;
-    const int kk = (k == N) ? 0 : k;
-    const int km = (k == 0 || k == N) ? 0 : N - k;
-    const C w = W[k];
-#pragma unroll
-    for (int c = 0; c < NC; c++) {
-      const C zk = Z[kk * L + rr * NC + c];
-      const C zn = cconj(Z[km * L + rr * NC + c]);
-      const C a = cadd(zk, zn), bb = csub(zk, zn);
-      const C wb = cmul(w, bb);
-      // X[k] = (a - i W^k b) / 2
-      X[((size_t)row * g.H + k) * NC + c] = mk(R(0.5) * (a.x + wb.y), R(0.5) * (a.y - wb.x));
-    }
+// ---------------------------------------------------------------- common tile machinery
+// All passes are persistent: a CTA loops over tiles, and while it transforms tile i
+// the rows of tile i+1 stream into a staging buffer with cp.async.  Buffers: S
+// (staging), A and B (ping-pong); the first pass reads S, later passes alternate A/B.
+constexpr int PASS_THREADS = 512;
+
+template <bool INV, typename R>
+__device__ __forceinline__ void vpass_any(const typename Vec<R>::V *src, typename Vec<R>::V *dst, int LG,
+                                          const FftDesc &d, int p, const typename cplx_t<R>::type *tw,
+                                          const LineMap &lm) {
+  const typename cplx_t<R>::type *t = tw + d.twoff[p];
+  const int ns = d.ns[p], n = d.n;
+  switch (d.rad[p]) {
+    case 2: vpass<2, INV, R>(src, dst, LG, n, ns, t, lm); break;
+    case 3: vpass<3, INV, R>(src, dst, LG, n, ns, t, lm); break;
+    case 4: vpass<4, INV, R>(src, dst, LG, n, ns, t, lm); break;
+    case 5: vpass<5, INV, R>(src, dst, LG, n, ns, t, lm); break;
+    case 7: vpass<7, INV, R>(src, dst, LG, n, ns, t, lm); break;
+    case 8: vpass<8, INV, R>(src, dst, LG, n, ns, t, lm); break;
+    case 11: vpass<11, INV, R>(src, dst, LG, n, ns, t, lm); break;
+    case 13: vpass<13, INV, R>(src, dst, LG, n, ns, t, lm); break;
+    case 16: vpass<16, INV, R>(src, dst, LG, n, ns, t, lm); break;
+    case 17: vpass<17, INV, R>(src, dst, LG, n, ns, t, lm); break;
+    default: vpass_generic<INV, R>(src, dst, LG, n, ns, d.rad[p], t, tw + d.rootoff[p], lm); break;
   }
 }
 
-// ---------------------------------------------------------------- y forward / inverse
-// lines along y for a tile of TK consecutive kx at one z; IN has `rows_in` rows,
-// the transform length is M1, OUT receives `rows_out` rows.
-template <typename R, int NC, bool INV>
-__global__ void __launch_bounds__(256, 2) k_ypass(SolveGeom<R> g, const typename cplx_t<R>::type *__restrict__ in,
-                                               typename cplx_t<R>::type *__restrict__ out, int TK,
-                                               int rows_in, int rows_out) {
-  typedef typename cplx_t<R>::type C;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ FftDesc sd;
-  if (threadIdx.x == 0) sd = g.fy;
-  const int N = g.M[1], L = NC * TK;
-  const int ntw = g.fy.ntw;
-  C *tw = reinterpret_cast<C *>(smem_raw);
-  C *A = tw + ((ntw + 1) & ~1);
-  C *B = A + (size_t)L * N;
-  stage_table(tw, g.twy, ntw);
-  const int k0 = blockIdx.x * TK, z = blockIdx.y;
-  const int nk = min(TK, g.H - k0), Lv = NC * nk;
-  const C zero = mk(R(0), R(0));
-  for (int t = threadIdx.x; t < N * L; t += blockDim.x) {
-    const int y = t / L, l = t - y * L;
-    C v = zero;
-    if (y < rows_in && l < Lv) v = in[(((size_t)z * rows_in + y) * g.H + k0) * NC + l];
-    A[t] = v;
+// A transform that reads `first` (S or A) and ping-pongs between A and B; `hook`
+// runs once after the first pass has finished reading `first` (the prefetch point).
+template <bool INV, typename R, typename Hook>
+__device__ __forceinline__ typename Vec<R>::V *vfft_chain(typename Vec<R>::V *first, typename Vec<R>::V *A,
+                                                          typename Vec<R>::V *B, int LG, const FftDesc &d,
+                                                          const typename cplx_t<R>::type *tw, const LineMap &lm,
+                                                          Hook hook) {
+  typedef typename Vec<R>::V V;
+  V *src = first, *dst = (first == A) ? B : A;
+  for (int p = 0; p < d.npass; p++) {
+    vpass_any<INV, R>(src, dst, LG, d, p, tw, lm);
+    __syncthreads();
+    if (p == 0) hook();
+    V *nsrc = dst;
+    V *ndst = (dst == A) ? B : A;
+    src = nsrc;
+    dst = ndst;
   }
-  __syncthreads();
-  C *res = fft_batch<INV>(A, B, L, sd, tw);
-  for (int t = threadIdx.x; t < rows_out * L; t += blockDim.x) {
-    const int y = t / L, l = t - y * L;
-    if (l < Lv) out[(((size_t)z * rows_out + y) * g.H + k0) * NC + l] = res[t];
-  }
+  if (d.npass == 0) hook();
+  return src;
 }
 
-// ---------------------------------------------------------------- z pass (fused)
+struct NoHook {
+  __device__ void operator()() const {}
+};
+
+// ---------------------------------------------------------------- y and z passes
+// Tile t = (outer o, kx-tile kt): L = NC * TK lines of n points.  Row r of the tile
+// starts at complex offset ((o * os + kt * TK) + r * rs) * NC and holds L complex.
+struct LineTiles {
+  int n;          // transform length
+  int rows_in;    // rows read (the rest is zero padding)
+  int rows_out;   // rows written (truncation)
+  long long in_os, in_rs, out_os, out_rs;
+  int nouter, nkt, TK;
+};
+
+enum LMode { L_FWD = 0, L_INV = 1, L_Z = 2 };
+
+template <typename R>
+__device__ __forceinline__ void tile_rows_load(typename cplx_t<R>::type *S, const typename cplx_t<R>::type *in,
+                                               long long base, long long rs, int nrows, int L, int NC) {
+  // 16-byte chunks; rows are 16-byte aligned (kx padded to a multiple of 8)
+  const int cpr = (L * (int)sizeof(typename cplx_t<R>::type)) / 16;
+  const int rsub = threadIdx.x / cpr, c = threadIdx.x - rsub * cpr;
+  const int RS = blockDim.x / cpr;
+  if (rsub >= RS) return;
+  const char *src = reinterpret_cast<const char *>(in + base * NC);
+  char *dst = reinterpret_cast<char *>(S);
+  const size_t rowb = (size_t)L * sizeof(typename cplx_t<R>::type);
+  const size_t strideb = (size_t)rs * NC * sizeof(typename cplx_t<R>::type);
+  for (int r = rsub; r < nrows; r += RS) cp_async16(dst + r * rowb + c * 16, src + r * strideb + c * 16);
+}
+
+template <typename R>
+__device__ __forceinline__ void tile_rows_store(typename cplx_t<R>::type *out, const typename cplx_t<R>::type *Rb,
+                                                long long base, long long rs, int nrows, int L, int NC) {
+  const int cpr = (L * (int)sizeof(typename cplx_t<R>::type)) / 16;
+  const int rsub = threadIdx.x / cpr, c = threadIdx.x - rsub * cpr;
+  const int RS = blockDim.x / cpr;
+  if (rsub >= RS) return;
+  char *dst = reinterpret_cast<char *>(out + base * NC);
+  const char *src = reinterpret_cast<const char *>(Rb);
+  const size_t rowb = (size_t)L * sizeof(typename cplx_t<R>::type);
+  const size_t strideb = (size_t)rs * NC * sizeof(typename cplx_t<R>::type);
+  for (int r = rsub; r < nrows; r += RS)
+    *reinterpret_cast<float4 *>(dst + r * strideb + c * 16) = *reinterpret_cast<const float4 *>(src + r * rowb + c * 16);
+}
+
+// z-pass spectral multiply of one tile held in buffer V (complex view C)
 template <typename R, int NC>
-__global__ void __launch_bounds__(256, 2) k_zpass(SolveGeom<R> g, const typename cplx_t<R>::type *in,
-                                               typename cplx_t<R>::type *out, int TK,
-                                               int mode, int reproj, int use_zeta) {
+__device__ __forceinline__ void z_multiply(const SolveGeom<R> &g, typename cplx_t<R>::type *Cb, int L, int TK, int k0,
+                                           int y, int zmode, int reproj, int use_zeta) {
   typedef typename cplx_t<R>::type C;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ FftDesc sd;
-  if (threadIdx.x == 0) sd = g.fz;
-  const int N = g.M[2], L = NC * TK;
-  const int ntw = g.fz.ntw;
-  C *tw = reinterpret_cast<C *>(smem_raw);
-  C *A = tw + ((ntw + 1) & ~1);
-  C *B = A + (size_t)L * N;
-  stage_table(tw, g.twz, ntw);
-  const int k0 = blockIdx.x * TK, y = blockIdx.y;
-  const int nk = min(TK, g.H - k0), Lv = NC * nk;
-  const int M1 = g.M[1];
-  const int rows_in = (mode == Z_FORWARD) ? g.M[2] : g.P[2];
-  const C zero = mk(R(0), R(0));
-  for (int t = threadIdx.x; t < N * L; t += blockDim.x) {
-    const int z = t / L, l = t - z * L;
-    C v = zero;
-    if (z < rows_in && l < Lv) v = in[(((size_t)z * M1 + y) * g.H + k0) * NC + l];
-    A[t] = v;
-  }
-  __syncthreads();
-  C *res = fft_batch<false>(A, B, L, sd, tw);
-  if (mode == Z_FORWARD) {
-    for (int t = threadIdx.x; t < N * L; t += blockDim.x) {
-      const int z = t / L, l = t - z * L;
-      if (l < Lv) out[(((size_t)z * M1 + y) * g.H + k0) * NC + l] = res[t];
-    }
-    return;
-  }
-  C *other = (res == A) ? B : A;
   const R twopi = R(6.283185307179586476925286766559);
+  const int N = g.M[2];
   const R ky = g.kyt[y];
   const R kyc = (2 * y == g.M[1]) ? R(0) : ky;  // Nyquist component dropped in the curl
+  const int iy = min(y, g.M[1] - y);
   for (int t = threadIdx.x; t < N * TK; t += blockDim.x) {
     const int z = t / TK, kk = t - z * TK;
-    if (kk >= nk) continue;
     const int kx_i = k0 + kk;
+    C *v = Cb + z * L + kk * NC;
+    if (kx_i >= g.H) {
+#pragma unroll
+      for (int c = 0; c < NC; c++) v[c] = mk(R(0), R(0));
+      continue;
+    }
     const R kx = g.kxt[kx_i], kz = g.kzt[z];
     const R kxc = (2 * kx_i == g.M[0]) ? R(0) : kx;
     const R kzc = (2 * z == g.M[2]) ? R(0) : kz;
-    C *v = res + z * L + kk * NC;
     const R kmag = kx * kx + ky * ky + kz * kz;
-    if (mode == Z_REGULARISE) {
+    if (zmode == Z_REGULARISE) {
       const R zt = zeta_filter<R>(g.order, g.eps2pi * sqrt(kmag)) * g.scale;
 #pragma unroll
       for (int c = 0; c < NC; c++) v[c] = cscale(v[c], zt);
@@ -213,12 +192,11 @@ __global__ void __launch_bounds__(256, 2) k_zpass(SolveGeom<R> g, const typename
       if (g.allper) {
         G = (kmag > R(0)) ? zt / (twopi * twopi * kmag) * g.scale : R(0);
       } else {
-        const int iy = min(y, g.M[1] - y), iz = min(z, g.M[2] - z);
+        const int iz = min(z, g.M[2] - z);
         G = g.green[((size_t)iz * g.gM1 + iy) * g.H + kx_i];
       }
       const C w1 = v[0], w2 = v[1], w3 = v[2];
-      if (mode == Z_VEL) {
-        // u = G 2 pi i (k x w)
+      if (zmode == Z_VEL) {
         const C c1 = csub(cscale(w3, kyc), cscale(w2, kzc));
         const C c2 = csub(cscale(w1, kzc), cscale(w3, kxc));
         const C c3 = csub(cscale(w2, kxc), cscale(w1, kyc));
@@ -226,7 +204,7 @@ __global__ void __launch_bounds__(256, 2) k_zpass(SolveGeom<R> g, const typename
         v[0] = mk(-f * c1.y, f * c1.x);
         v[1] = mk(-f * c2.y, f * c2.x);
         v[2] = mk(-f * c3.y, f * c3.x);
-      } else if (mode == Z_VECPOT) {
+      } else if (zmode == Z_VECPOT) {
         v[0] = cscale(w1, G);
         v[1] = cscale(w2, G);
         v[2] = cscale(w3, G);
@@ -247,68 +225,257 @@ __global__ void __launch_bounds__(256, 2) k_zpass(SolveGeom<R> g, const typename
       }
     }
   }
-  // padding lines (kk >= nk) stay zero through the multiply
-  __syncthreads();
-  C *res2 = fft_batch<true>(res, other, L, sd, tw);
-  for (int t = threadIdx.x; t < g.P[2] * L; t += blockDim.x) {
-    const int z = t / L, l = t - z * L;
-    if (l < Lv) out[(((size_t)z * M1 + y) * g.H + k0) * NC + l] = res2[t];
+}
+
+// lines along y (lmode L_FWD / L_INV) or the fused z pass (L_Z, or L_FWD along z
+// for the Green's function transform).  axis: 1 = y, 2 = z.
+template <typename R, int NC>
+__global__ void __launch_bounds__(PASS_THREADS, 1) k_lines(SolveGeom<R> g, LineTiles lt,
+                                                            const typename cplx_t<R>::type *in,
+                                                            typename cplx_t<R>::type *out, int axis, int lmode,
+                                                            int zmode, int reproj, int use_zeta) {
+  typedef typename cplx_t<R>::type C;
+  typedef typename Vec<R>::V V;
+  constexpr int G = Vec<R>::G;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ FftDesc sd;
+  if (threadIdx.x == 0) sd = (axis == 1) ? g.fy : g.fz;
+  const FftDesc &dsrc = (axis == 1) ? g.fy : g.fz;
+  const int ntw = dsrc.ntw;
+  C *tw = reinterpret_cast<C *>(smem_raw);
+  const int N = lt.n, TK = lt.TK, L = NC * TK, LG = L / G;
+  V *S = reinterpret_cast<V *>(tw + ((ntw + 7) & ~7));
+  V *A = S + (size_t)LG * N;
+  V *B = A + (size_t)LG * N;
+  stage_table(tw, axis == 1 ? g.twy : g.twz, ntw);
+  {
+    C *Sc = reinterpret_cast<C *>(S);
+    for (int i = threadIdx.x; i < L * N; i += blockDim.x) Sc[i] = mk(R(0), R(0));
   }
+  __syncthreads();
+  const LineMap lm = line_map(LG);
+  const int ntiles = lt.nouter * lt.nkt;
+  auto load = [&](int tile) {
+    const int o = tile / lt.nkt, kt = tile - o * lt.nkt;
+    tile_rows_load<R>(reinterpret_cast<C *>(S), in, o * lt.in_os + (long long)kt * TK, lt.in_rs, lt.rows_in, L, NC);
+    cp_async_commit();
+  };
+  int tile = blockIdx.x;
+  if (tile < ntiles) load(tile);
+  for (; tile < ntiles; tile += gridDim.x) {
+    cp_async_wait_all();
+    __syncthreads();
+    const int next = tile + gridDim.x;
+    auto hook = [&]() {
+      if (next < ntiles) load(next);
+    };
+    const int o = tile / lt.nkt, kt = tile - o * lt.nkt;
+    V *res;
+    if (lmode == L_INV) {
+      res = vfft_chain<true, R>(S, A, B, LG, sd, tw, lm, hook);
+    } else {
+      res = vfft_chain<false, R>(S, A, B, LG, sd, tw, lm, hook);
+      if (lmode == L_Z) {
+        z_multiply<R, NC>(g, reinterpret_cast<C *>(res), L, TK, kt * TK, o, zmode, reproj, use_zeta);
+        __syncthreads();
+        res = vfft_chain<true, R>(res, A, B, LG, sd, tw, lm, NoHook());
+      }
+    }
+    tile_rows_store<R>(out, reinterpret_cast<C *>(res), o * lt.out_os + (long long)kt * TK, lt.out_rs, lt.rows_out,
+                       L, NC);
+    __syncthreads();
+  }
+  cp_async_wait_all();
+}
+
+// ---------------------------------------------------------------- x forward (R2C)
+// RB rows per tile, L = NC RB real lines packed as N = Mx/2 complex points
+// (z[m] = x[2m] + i x[2m+1]); the Mx-point spectrum X[k], k < H follows from Z[k]
+// and Z[N-k].  Rows of the real cuboid are staged raw in S.
+template <typename R, int NC>
+__global__ void __launch_bounds__(PASS_THREADS, 1) k_xfwd(SolveGeom<R> g, const R *__restrict__ in,
+                                                           typename cplx_t<R>::type *__restrict__ X, int RB, int cs,
+                                                           int vec16) {
+  typedef typename cplx_t<R>::type C;
+  typedef typename Vec<R>::V V;
+  constexpr int G = Vec<R>::G;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ FftDesc sd;
+  if (threadIdx.x == 0) sd = g.fx;
+  const int ntw = g.fx.ntw + g.fx.next;
+  C *tw = reinterpret_cast<C *>(smem_raw);
+  const int N = g.N2, L = NC * RB, LG = L / G;
+  const int P0 = g.P[0];
+  const size_t sreal = (size_t)RB * P0 * NC;  // staged reals
+  const size_t sS = ((sreal * sizeof(R) + 15) / 16) * 16 / sizeof(V);
+  V *S = reinterpret_cast<V *>(tw + ((ntw + 7) & ~7));
+  V *A = S + sS;
+  V *B = A + (size_t)LG * N;
+  stage_table(tw, g.twx, ntw);
+  const LineMap lm = line_map(LG);
+  const int nrows = g.P[1] * g.P[2];
+  const int ntiles = (nrows + RB - 1) / RB;
+  R *Sr = reinterpret_cast<R *>(S);
+  auto load = [&](int tile) {
+    const int row0 = tile * RB;
+    for (int rr = 0; rr < RB; rr++) {
+      const int row = row0 + rr;
+      if (row >= nrows) break;
+      const int y = row % g.P[1], z = row / g.P[1];
+      const R *src = in + (((size_t)(z + g.off[2]) * g.ext[1] + (y + g.off[1])) * g.ext[0] + g.off[0]) * cs;
+      R *dst = Sr + (size_t)rr * P0 * NC;
+      if (vec16) {
+        const int nch = (P0 * NC * (int)sizeof(R)) / 16;
+        for (int c = threadIdx.x; c < nch; c += blockDim.x)
+          cp_async16(reinterpret_cast<char *>(dst) + 16 * c, reinterpret_cast<const char *>(src) + 16 * c);
+      } else {
+        for (int e = threadIdx.x; e < P0 * NC; e += blockDim.x) {
+          const int x = e / NC, c = e - x * NC;
+          if (sizeof(R) == 8) cp_async8(dst + e, src + (size_t)x * cs + c);
+          else cp_async4(dst + e, src + (size_t)x * cs + c);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  int tile = blockIdx.x;
+  if (tile < ntiles) load(tile);
+  for (; tile < ntiles; tile += gridDim.x) {
+    cp_async_wait_all();
+    __syncthreads();
+    const int row0 = tile * RB;
+    // pack the staged reals into complex lines
+    C *Ac = reinterpret_cast<C *>(A);
+    for (int t = threadIdx.x; t < RB * N; t += blockDim.x) {
+      const int rr = t / N, m = t - rr * N;
+      const R *xr = Sr + (size_t)rr * P0 * NC;
+      const int x0 = 2 * m, x1 = 2 * m + 1;
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        const R a = (x0 < P0 && row0 + rr < nrows) ? xr[x0 * NC + c] : R(0);
+        const R b = (x1 < P0 && row0 + rr < nrows) ? xr[x1 * NC + c] : R(0);
+        Ac[m * L + rr * NC + c] = mk(a, b);
+      }
+    }
+    __syncthreads();
+    const int next = tile + gridDim.x;
+    if (next < ntiles) load(next);
+    V *res = vfft_chain<false, R>(A, A, B, LG, sd, tw, lm, NoHook());
+    const C *Z = reinterpret_cast<const C *>(res);
+    const C *W = tw + sd.extoff;  // exp(-2 pi i k / Mx), k < H
+    for (int t = threadIdx.x; t < RB * g.Hp; t += blockDim.x) {
+      const int rr = t / g.Hp, k = t - rr * g.Hp;
+      const int row = row0 + rr;
+      if (row >= nrows) continue;
+      C o[NC];
+      if (k < g.H) {
+        const int kk = (k == N) ? 0 : k;
+        const int km = (k == 0 || k == N) ? 0 : N - k;
+        const C w = W[k];
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          const C zk = Z[kk * L + rr * NC + c];
+          const C zn = cconj(Z[km * L + rr * NC + c]);
+          const C a = cadd(zk, zn), bb = csub(zk, zn);
+          const C wb = cmul(w, bb);
+          o[c] = mk(R(0.5) * (a.x + wb.y), R(0.5) * (a.y - wb.x));  // (a - i W^k b) / 2
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < NC; c++) o[c] = mk(R(0), R(0));
+      }
+#pragma unroll
+      for (int c = 0; c < NC; c++) X[((size_t)row * g.Hp + k) * NC + c] = o[c];
+    }
+    __syncthreads();
+  }
+  cp_async_wait_all();
 }
 
 // ---------------------------------------------------------------- x inverse (C2R)
 template <typename R, int NC>
-__global__ void __launch_bounds__(256, 2) k_xinv(SolveGeom<R> g, const typename cplx_t<R>::type *__restrict__ X,
-                                              R *__restrict__ outp, int RB, int cs) {
+__global__ void __launch_bounds__(PASS_THREADS, 1) k_xinv(SolveGeom<R> g, const typename cplx_t<R>::type *__restrict__ X,
+                                                           R *__restrict__ outp, int RB, int cs) {
   typedef typename cplx_t<R>::type C;
+  typedef typename Vec<R>::V V;
+  constexpr int G = Vec<R>::G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ FftDesc sd;
   if (threadIdx.x == 0) sd = g.fx;
-  const int N = g.N2, L = NC * RB;
   const int ntw = g.fx.ntw + g.fx.next;
   C *tw = reinterpret_cast<C *>(smem_raw);
-  C *A = tw + ((ntw + 1) & ~1);
-  C *B = A + (size_t)L * N;
+  const int N = g.N2, L = NC * RB, LG = L / G;
+  const size_t rowc = (size_t)g.Hp * NC;  // complex per X row
+  const size_t sS = (RB * rowc * sizeof(C)) / sizeof(V);
+  V *S = reinterpret_cast<V *>(tw + ((ntw + 7) & ~7));
+  V *A = S + sS;
+  V *B = A + (size_t)LG * N;
   stage_table(tw, g.twx, ntw);
-  __syncthreads();
-  const C *W = tw + g.fx.extoff;
+  const LineMap lm = line_map(LG);
   const int nrows = g.P[1] * g.P[2];
-  const int row0 = blockIdx.x * RB;
-  for (int t = threadIdx.x; t < RB * N; t += blockDim.x) {
-    const int rr = t / N, m = t - rr * N;
-    const int row = row0 + rr;
-    const C w = cconj(W[m]);
+  const int ntiles = (nrows + RB - 1) / RB;
+  C *Sc = reinterpret_cast<C *>(S);
+  auto load = [&](int tile) {
+    const int row0 = tile * RB;
+    const int nr = min(RB, nrows - row0);
+    const size_t nch = (size_t)nr * rowc * sizeof(C) / 16;
+    const char *src = reinterpret_cast<const char *>(X + (size_t)row0 * rowc);
+    for (size_t c = threadIdx.x; c < nch; c += blockDim.x)
+      cp_async16(reinterpret_cast<char *>(Sc) + 16 * c, src + 16 * c);
+    cp_async_commit();
+  };
+  int tile = blockIdx.x;
+  if (tile < ntiles) load(tile);
+  for (; tile < ntiles; tile += gridDim.x) {
+    cp_async_wait_all();
+    __syncthreads();
+    const int row0 = tile * RB;
+    const C *W = tw + sd.extoff;
+    C *Ac = reinterpret_cast<C *>(A);
+    for (int t = threadIdx.x; t < RB * N; t += blockDim.x) {
+      const int rr = t / N, m = t - rr * N;
+      const C w = cconj(W[m]);
+      const bool ok = row0 + rr < nrows;
 #pragma unroll
-    for (int c = 0; c < NC; c++) {
-      C z = mk(R(0), R(0));
-      if (row < nrows) {
-        C xm = X[((size_t)row * g.H + m) * NC + c];
-        C xn = X[((size_t)row * g.H + (N - m)) * NC + c];
-        if (m == 0) { xm.y = R(0); xn.y = R(0); }  // DC and Nyquist are real
-        const C a = cadd(xm, cconj(xn));
-        const C b = csub(xm, cconj(xn));
-        const C wb = cmul(w, b);
-        z = mk(a.x - wb.y, a.y + wb.x);  // a + i W^{-m} b
+      for (int c = 0; c < NC; c++) {
+        C z = mk(R(0), R(0));
+        if (ok) {
+          C xm = Sc[rr * rowc + (size_t)m * NC + c];
+          C xn = Sc[rr * rowc + (size_t)(N - m) * NC + c];
+          if (m == 0) {
+            xm.y = R(0);
+            xn.y = R(0);
+          }  // DC and Nyquist are real
+          const C a = cadd(xm, cconj(xn));
+          const C b = csub(xm, cconj(xn));
+          const C wb = cmul(w, b);
+          z = mk(a.x - wb.y, a.y + wb.x);  // a + i W^{-m} b
+        }
+        Ac[m * L + rr * NC + c] = z;
       }
-      A[m * L + rr * NC + c] = z;
     }
-  }
-  __syncthreads();
-  C *res = fft_batch<true>(A, B, L, sd, tw);
-  for (int t = threadIdx.x; t < RB * N; t += blockDim.x) {
-    const int rr = t / N, m = t - rr * N;
-    const int row = row0 + rr;
-    if (row >= nrows) continue;
-    const int y = row % g.P[1], z = row / g.P[1];
-    R *dst = outp + (((size_t)(z + g.off[2]) * g.ext[1] + (y + g.off[1])) * g.ext[0] + g.off[0]) * cs;
-    const int x0 = 2 * m, x1 = 2 * m + 1;
+    __syncthreads();
+    const int next = tile + gridDim.x;
+    if (next < ntiles) load(next);
+    V *res = vfft_chain<true, R>(A, A, B, LG, sd, tw, lm, NoHook());
+    const C *Rc = reinterpret_cast<const C *>(res);
+    for (int t = threadIdx.x; t < RB * N; t += blockDim.x) {
+      const int rr = t / N, m = t - rr * N;
+      const int row = row0 + rr;
+      if (row >= nrows) continue;
+      const int y = row % g.P[1], z = row / g.P[1];
+      R *dst = outp + (((size_t)(z + g.off[2]) * g.ext[1] + (y + g.off[1])) * g.ext[0] + g.off[0]) * cs;
+      const int x0 = 2 * m, x1 = 2 * m + 1;
 #pragma unroll
-    for (int c = 0; c < NC; c++) {
-      const C v = res[m * L + rr * NC + c];
-      if (x0 < g.P[0]) dst[(size_t)x0 * cs + c] = v.x;
-      if (x1 < g.P[0]) dst[(size_t)x1 * cs + c] = v.y;
+      for (int c = 0; c < NC; c++) {
+        const C v = Rc[m * L + rr * NC + c];
+        if (x0 < g.P[0]) dst[(size_t)x0 * cs + c] = v.x;
+        if (x1 < g.P[0]) dst[(size_t)x1 * cs + c] = v.y;
+      }
     }
+    __syncthreads();
   }
+  cp_async_wait_all();
 }
 
 // ---------------------------------------------------------------- periodic ghosts
