@@ -148,6 +148,23 @@ int pmgpu_remesh(const pmgpu_topo *topo, const double *mesh_vort, const double *
                  double min_dvort, int incl_ghost, int max_part, double *pos, double *part_vort,
                  double *part_dvort, double *part_vel, int *npart);
 
+/* ---- allocation-free deposition (no counterpart in the reference) ----
+ * For callers that cannot allocate device memory while they run, e.g. a host
+ * program that reserved the GPU's memory up front for its own pool, or a loop that
+ * must not risk the implicit synchronisation of cudaMalloc / cudaFree.  Same
+ * arguments and result as pmgpu_interp_particle_mesh (FP64), but every array is a
+ * device pointer and the work runs on `stream`; the call allocates nothing.  Its
+ * scratch is one static device array of about 8.6 MB that every GPU loading the
+ * library holds until the process exits; a call is limited to 262144 particles and
+ * 524288 bins ((nx'+3)(ny'+3)(nz'+3) for M4', +5 per axis for M6*; larger inputs are
+ * rejected with ierr = -1).  The first call on a device looks up the array's device
+ * address, so make it before any CUDA stream capture.  All calls share the array:
+ * calls that overlap on the GPU (different streams or threads) race. */
+int pmgpu_interp_particle_mesh_noalloc(const pmgpu_topo *topo, const pmgpu_params *par,
+                                       const double *d_xpart, const double *d_part, int nvar,
+                                       int npart, double *d_mesh, int nvar_mesh, int clear,
+                                       int clear_ghost, void *stream);
+
 /* ---- diagnostics (no counterpart in the reference, which has no timers) ---- */
 const char *pmgpu_last_error(void);
 /* number of this library's kernels launched since the last reset */

@@ -120,8 +120,13 @@ static int ensure_device(const char *caller) {
 struct DevBuf {
   void *p = nullptr;
   size_t cap = 0;
+  bool fixed = false;  // a view of preallocated memory: never allocates or frees
   int ensure(size_t bytes, const char *caller) {
     if (bytes <= cap && p) return 0;
+    if (fixed) {
+      set_error(caller, "scratch size exceeds the fixed device scratch area.");
+      return -1;
+    }
     if (p) cudaFree(p);
     p = nullptr;
     cap = 0;
@@ -131,7 +136,7 @@ struct DevBuf {
     return 0;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p && !fixed) cudaFree(p);
     p = nullptr;
     cap = 0;
   }
@@ -1288,3 +1293,97 @@ int pmgpu_remesh(const pmgpu_topo *topo, const double *mesh_vort, const double *
   return 0;
 }
 
+
+// ------------------------------------------------------------------ allocation-free P2M
+// Some callers cannot allocate device memory while they run: a host program that
+// reserved the GPU's memory up front (a fixed-budget pool or another runtime owning
+// the allocator), or a loop that must not risk the implicit synchronisation and
+// failure modes of cudaMalloc / cudaFree.  This variant of the deposition keeps all
+// of its scratch (bin keys, particle order, bin counts and starts, sort histograms)
+// in one static device array that the library reserves when it is loaded on a GPU,
+// and takes only device pointers from the caller.
+namespace pmgpu {
+constexpr size_t NOALLOC_MAX_PART = size_t(1) << 18;  // particles per call
+constexpr size_t NOALLOC_MAX_BINS = size_t(1) << 19;  // (nx' + 3)(ny' + 3)(nz' + 3) for M4'
+constexpr size_t NA_PART_BYTES = NOALLOC_MAX_PART * 4;
+constexpr size_t NA_BIN_BYTES = (NOALLOC_MAX_BINS + 256) * 4;
+constexpr size_t NA_HIST_BYTES = (65536 + 256) * 4;  // 1024 digits x 64 sort tiles, + 1
+constexpr size_t NA_SPART_BYTES = size_t(1) << 12;
+constexpr size_t NOALLOC_BYTES = 4 * NA_PART_BYTES + 2 * NA_BIN_BYTES + NA_HIST_BYTES + NA_SPART_BYTES;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+static void *g_noalloc_addr[128];
+}  // namespace pmgpu
+
+int pmgpu_interp_particle_mesh_noalloc(const pmgpu_topo *topo, const pmgpu_params *par, const double *d_xpart,
+                                       const double *d_part, int nvar, int npart, double *d_mesh, int nvar_mesh,
+                                       int clear, int clear_ghost, void *stream) {
+  const char *caller = "pmlib_interp_particle_mesh";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!topo) {
+    set_error(caller, "missing argument.");
+    return -1;
+  }
+  if (nvar != nvar_mesh) {
+    set_error(caller, "Dimension of interpolation variables does not correspond.");
+    return -1;
+  }
+  if (topo->npart != npart) {
+    set_error(caller, "Discrepancy in number of particles");
+    return -1;
+  }
+  if (check_interp(par, caller)) return -1;
+  const int W = par->interpolation_order == 3 ? 4 : 6;
+  unsigned long long nbins = 1;
+  for (int e = 0; e < 3; e++)
+    nbins *= (unsigned long long)(topo->ncell[e] + topo->nghost[2 * e] + topo->nghost[2 * e + 1] + W - 1);
+  if (npart < 0 || (size_t)npart > NOALLOC_MAX_PART || nbins > NOALLOC_MAX_BINS) {
+    char msg[200];
+    snprintf(msg, sizeof(msg),
+             "allocation-free deposition is limited to %zu particles and %zu bins (got %d particles, %llu bins).",
+             (size_t)NOALLOC_MAX_PART, (size_t)NOALLOC_MAX_BINS, npart, nbins);
+    set_error(caller, msg);
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  int dev = 0;
+  CK(cudaGetDevice(&dev), caller);
+  if (dev < 0 || dev >= 128) {
+    set_error(caller, "device index out of range.");
+    return -1;
+  }
+  if (!g_noalloc_addr[dev]) {
+    // once per device, with that device current: the host-side symbol is only a
+    // stand-in, the kernels need the device address of the array
+    void *ptr = nullptr;
+    CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch), caller);
+    g_noalloc_addr[dev] = ptr;
+  }
+  unsigned char *base = reinterpret_cast<unsigned char *>(g_noalloc_addr[dev]);
+  DevBuf key, val, key2, val2, counts, start, spart, hist;
+  DevBuf *views[] = {&key, &val, &key2, &val2};
+  size_t off = 0;
+  for (DevBuf *v : views) {
+    v->p = base + off;
+    v->cap = NA_PART_BYTES;
+    v->fixed = true;
+    off += NA_PART_BYTES;
+  }
+  DevBuf *bviews[] = {&counts, &start};
+  for (DevBuf *v : bviews) {
+    v->p = base + off;
+    v->cap = NA_BIN_BYTES;
+    v->fixed = true;
+    off += NA_BIN_BYTES;
+  }
+  hist.p = base + off;
+  hist.cap = NA_HIST_BYTES;
+  hist.fixed = true;
+  off += NA_HIST_BYTES;
+  spart.p = base + off;
+  spart.cap = NA_SPART_BYTES;
+  spart.fixed = true;
+  PartScratchRefs r{&key, &val, &key2, &val2, &counts, &start, &spart, &hist};
+  const int mode = clear ? 1 : (clear_ghost ? 2 : 0);
+  return run_p2m<double>(topo, par->interpolation_order, d_xpart, d_part, nvar, npart, d_mesh, nvar_mesh, mode, r,
+                         (cudaStream_t)stream, nullptr, caller);
+}

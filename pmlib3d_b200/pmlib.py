@@ -191,6 +191,19 @@ def pmlib_remesh(topo: Topo, mesh_vort, mesh_dvort=None, mesh_vel=None, mask=Non
     return ierr, pos, pv, pdv, pvel
 
 
+def pmlib_interp_particle_mesh_noalloc(topo: Topo, params: Params, d_xpart: int, d_part: int, nvar: int,
+                                       npart: int, d_mesh: int, nvar_mesh: int, clear=False, clear_ghost=False,
+                                       stream: int = 0) -> int:
+    """FP64 deposition on device pointers that allocates nothing: for callers that
+    cannot allocate device memory while they run.  Its scratch is a fixed static
+    device array (at most 262144 particles and 524288 bins per call); calls that
+    overlap on the GPU share it and race."""
+    return lib().pmgpu_interp_particle_mesh_noalloc(C.byref(topo), C.byref(params), C.c_void_p(d_xpart),
+                                                    C.c_void_p(d_part), int(nvar), int(npart), C.c_void_p(d_mesh),
+                                                    int(nvar_mesh), int(bool(clear)), int(bool(clear_ghost)),
+                                                    C.c_void_p(stream))
+
+
 def step(plan: Plan, pos, part_vort, part_vel) -> int:
     """One vortex step through host arrays: P2M (clear), unbounded solve and curl,
     M2P of the velocity into ``part_vel``."""
