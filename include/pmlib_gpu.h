@@ -148,6 +148,12 @@ int pmgpu_remesh(const pmgpu_topo *topo, const double *mesh_vort, const double *
                  double min_dvort, int incl_ghost, int max_part, double *pos, double *part_vort,
                  double *part_dvort, double *part_vel, int *npart);
 
+/* Selects the line-FFT engine of plans created afterwards (no counterpart in the
+ * reference): 0 = in-place register passes wherever the y / z lengths factor into
+ * radices up to 17 (default), 1 = out-of-place Stockham passes everywhere.  Both give
+ * the same results to round-off; returns the previous setting. */
+int pmgpu_fft_engine(int engine);
+
 /* ---- allocation-free deposition (no counterpart in the reference) ----
  * For callers that cannot allocate device memory while they run, e.g. a host
  * program that reserved the GPU's memory up front for its own pool, or a loop that

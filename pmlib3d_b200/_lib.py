@@ -18,7 +18,7 @@ EXPORTS = (
     "pmgpu_regularise", "pmgpu_regularise_f32", "pmgpu_plan_destroy",
     "pmgpu_step", "pmgpu_step_dev", "pmgpu_remesh", "pmgpu_last_error", "pmgpu_launch_count",
     "pmgpu_timing_enable", "pmgpu_timing_reset", "pmgpu_timing_get",
-    "pmgpu_interp_particle_mesh_noalloc",
+    "pmgpu_interp_particle_mesh_noalloc", "pmgpu_fft_engine",
 )
 
 
@@ -82,6 +82,7 @@ def lib():
         "pmgpu_timing_reset": [],
         "pmgpu_timing_get": [C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(C.c_longlong)],
         "pmgpu_interp_particle_mesh_noalloc": [TP, QP, vp, vp, C.c_int, C.c_int, vp, C.c_int, C.c_int, C.c_int, vp],
+        "pmgpu_fft_engine": [C.c_int],
     }
     for name, args in sig.items():
         f = getattr(L, name)

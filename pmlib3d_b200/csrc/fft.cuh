@@ -32,10 +32,10 @@ struct FftDesc {
   int next;                  // entries of the extra table
 };
 
-// (cos, sin)(2 pi m / R) for R <= 17, m < R; filled once per device by the host
-// (the library is a single translation unit, so these are defined here)
-__constant__ float c_cs32[18][17][2];
-__constant__ double c_cs64[18][17][2];
+// (cos, sin)(2 pi m / R) for R <= 17, m < R; every translation unit that runs the
+// transforms holds its own copy, filled once per device by the host
+static __constant__ float c_cs32[18][17][2];
+static __constant__ double c_cs64[18][17][2];
 
 template <typename T> __device__ __forceinline__ T cs_c(int R, int m);
 template <typename T> __device__ __forceinline__ T cs_s(int R, int m);
@@ -145,8 +145,16 @@ template <int R, bool INV, typename C> __device__ __forceinline__ void dft(C *v)
     dft2<INV>(v);
   } else if constexpr (R == 4) {
     dft4<INV>(v);
+  } else if constexpr (R == 6) {
+    dft_comp<3, 2, INV>(v);
   } else if constexpr (R == 8) {
     dft_comp<4, 2, INV>(v);
+  } else if constexpr (R == 9) {
+    dft_comp<3, 3, INV>(v);
+  } else if constexpr (R == 10) {
+    dft_comp<5, 2, INV>(v);
+  } else if constexpr (R == 12) {
+    dft_comp<4, 3, INV>(v);
   } else if constexpr (R == 16) {
     dft_comp<4, 4, INV>(v);
   } else {

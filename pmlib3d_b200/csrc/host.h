@@ -1,0 +1,99 @@
+// host.h -- host-side declarations shared by the library's translation units:
+// error reporting, launch accounting and per-kernel timing, and the FFT pass
+// launchers that are compiled in their own units (passes_*.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+#include "../../include/pmlib_gpu.h"
+#include "common.cuh"
+#include "solve.cuh"
+
+namespace pmgpu {
+
+enum KClass { KC_BIN, KC_SCAN, KC_PLACE, KC_FIXUP, KC_DEPOSIT, KC_GADD, KC_XFWD, KC_YFWD, KC_ZPASS, KC_YINV,
+              KC_XINV, KC_GFILL, KC_M2P, KC_OTHER, KC_N };
+
+// brackets one launch with CUDA events on its stream while timing is enabled
+struct KTimer {
+  int cls;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr, b = nullptr;
+  KTimer(int c, cudaStream_t s);
+  ~KTimer();
+};
+
+#define CK(expr, caller)                         \
+  do {                                           \
+    if (!::pmgpu::cuda_ok((expr), (caller))) {   \
+      return -1;                                 \
+    }                                            \
+  } while (0)
+#define CKL(caller) CK(cudaGetLastError(), caller)
+
+int num_sms();
+
+// shared-memory budget of one persistent pass CTA
+constexpr size_t PASS_SMEM_BUDGET = 220 * 1024;
+
+static inline size_t tw_bytes(int ntw, size_t csize) { return (size_t)((ntw + 7) & ~7) * csize; }
+
+// kx tile of the Stockham y / z passes: the largest of 8, 4, 2, 1 whose three
+// buffers fit (FP32 needs an even line count: two lines per 16-byte vector)
+static inline int pick_tk(int n, int nc, size_t csize, int ntw) {
+  for (int tk = 8; tk >= 1; tk /= 2) {
+    if (csize == 8 && (nc * tk) % 2) continue;
+    if (tw_bytes(ntw, csize) + 3 * (size_t)nc * tk * n * csize <= PASS_SMEM_BUDGET) return tk;
+  }
+  return 0;
+}
+static inline size_t lines_smem(int n, int nc, int tk, size_t csize, int ntw) {
+  return tw_bytes(ntw, csize) + 3 * (size_t)nc * tk * n * csize;
+}
+// register engine: twiddles w_n^q + position table + one tile buffer
+static inline size_t reg_smem(int n, int nc, int tk, size_t csize) {
+  return (((size_t)n * csize + 15) & ~(size_t)15) + (((size_t)n * 4 + 15) & ~(size_t)15) + (size_t)nc * tk * n * csize;
+}
+// kx tile of the register engine: two CTAs per SM if possible, else one
+static inline int pick_tk_reg(int n, int nc, size_t csize, int Hp) {
+  for (size_t budget : {(size_t)112 * 1024, PASS_SMEM_BUDGET})
+    for (int tk = 8; tk >= 1; tk /= 2) {
+      if (Hp % tk) continue;
+      if (csize == 8 && (nc * tk) % 2) continue;
+      if (reg_smem(n, nc, tk, csize) <= budget) return tk;
+    }
+  return 0;
+}
+// rows per tile of the x passes
+static inline int pick_rb(int n2, int P0, int Hp, int nc, size_t csize, size_t rsize, int ntw, bool inverse) {
+  for (int rb = 8; rb >= 1; rb--) {
+    if (csize == 8 && (nc * rb) % 2) continue;
+    const size_t stage = inverse ? (size_t)rb * Hp * nc * csize : (((size_t)rb * P0 * nc * rsize + 15) / 16) * 16;
+    if (tw_bytes(ntw, csize) + stage + 2 * (size_t)nc * rb * n2 * csize <= PASS_SMEM_BUDGET) return rb;
+  }
+  return 0;
+}
+
+// ---- FFT passes (passes.cuh, instantiated per precision and component count)
+// x then y forward: real cuboid (component stride cs) -> X -> Y
+template <typename R, int NC>
+int fwd_xy(SolveGeom<R> &g, const R *in, typename cplx_t<R>::type *X, typename cplx_t<R>::type *Y, cudaStream_t st,
+           const char *caller, int cs = NC);
+// z pass on rows_y spectrum rows: Z_VEL / Z_VORT / Z_VECPOT / Z_REGULARISE / Z_FORWARD
+template <typename R, int NC>
+int zpass(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typename cplx_t<R>::type *out, int mode, int reproj,
+          int use_zeta, int rows_y, cudaStream_t st, const char *caller);
+// y then x inverse into the cuboid (periodic ghosts filled when `ghosts`)
+template <typename R, int NC>
+int inv_yx(SolveGeom<R> &g, const pmgpu_topo *topo, typename cplx_t<R>::type *Y, typename cplx_t<R>::type *X, R *out,
+           cudaStream_t st, const char *caller, int cs = NC, bool ghosts = true);
+
+// each pass unit holds its own copy of the DFT constant tables
+int upload_cs_f32_1(const void *t32, const void *t64);
+int upload_cs_f32_3(const void *t32, const void *t64);
+int upload_cs_f64_1(const void *t32, const void *t64);
+int upload_cs_f64_3(const void *t32, const void *t64);
+
+}  // namespace pmgpu

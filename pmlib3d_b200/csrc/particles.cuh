@@ -4,10 +4,11 @@
 // P2M (source/interpolation/pmlib_interp_particle_mesh.f) scatters every particle
 // into its 4^3 (M4') or 6^3 (M6*) stencil with the particle loop in index order.
 // Here particles are binned by the reference's base cell NINT((x - xmin) / dx)
-// (:153-155, bit-exact index arithmetic), sorted by bin with a stable radix sort
-// (ties keep particle order), and every cell then gathers the contributions of the
+// (:153-155, bit-exact index arithmetic), sorted stably by bin (ties keep particle
+// order), and every cell then gathers the contributions of the
 // bins whose stencil covers it, in a fixed order: no floating-point atomics, and
-// the same result on every run.
+// the same result on every run.  The stable order comes from a counting sort: slots
+// within a bin are taken by integer atomics and then put back in particle order.
 #pragma once
 
 #include "common.cuh"
@@ -80,32 +81,157 @@ __device__ __forceinline__ R cell_offset(R x, R xmin, R dx, long long b, R scale
 // ------------------------------------------------------------------ binning
 // key = flattened base cell in the bin box; particles whose stencil misses the
 // cuboid, or which lie outside [xmin, xmax] across a periodic face (all weights
-// zeroed, :229-246), get the sentinel key nbins and are skipped by P2M.
+// zeroed, :229-246), get the sentinel key nbins and are skipped by P2M (they still
+// take a slot, so the sorted order is a permutation of all particles).
+// rank = the particle's provisional slot within its bin: lanes of a warp that share
+// a key take consecutive slots in lane order, one atomic per key and warp.
 template <typename R, int W>
 __global__ void k_bin(PartGeom<R> g, const R *__restrict__ pos, int n, unsigned *__restrict__ key,
-                      int *__restrict__ val, unsigned *__restrict__ counts) {
+                      unsigned *__restrict__ rank, unsigned *__restrict__ counts) {
   constexpr int off = Stencil<W>::off;
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-    bool ok = true;
-    long long bi[3];
+  const int lane = threadIdx.x & 31;
+  const int stride = gridDim.x * blockDim.x;
+  // the loop runs whole warps so that the warp-wide match below sees every lane
+  for (int p0 = blockIdx.x * blockDim.x; p0 < n; p0 += stride) {
+    const int p = p0 + (int)threadIdx.x;
+    const bool valid = p < n;
+    unsigned k = 0xFFFFFFFFu;
+    if (valid) {
+      bool ok = true;
+      long long bi[3];
 #pragma unroll
-    for (int e = 0; e < 3; e++) {
-      const R x = pos[(size_t)3 * p + e];
-      const long long b = base_index(x, g.xmin[e], g.c1dx[e]);
-      const long long first = b - off, last = b - off + W - 1;
-      const int hi = g.lo[e] + g.ext[e] - 1;
-      if (!(last >= g.lo[e] && first <= hi)) ok = false;
-      if (g.bclo[e] != 0 && x < g.xmin[e]) ok = false;
-      if (g.bchi[e] != 0 && x > g.xmax[e]) ok = false;
-      bi[e] = b - g.blo[e];
+      for (int e = 0; e < 3; e++) {
+        const R x = pos[(size_t)3 * p + e];
+        const long long b = base_index(x, g.xmin[e], g.c1dx[e]);
+        const long long first = b - off, last = b - off + W - 1;
+        const int hi = g.lo[e] + g.ext[e] - 1;
+        if (!(last >= g.lo[e] && first <= hi)) ok = false;
+        if (g.bclo[e] != 0 && x < g.xmin[e]) ok = false;
+        if (g.bchi[e] != 0 && x > g.xmax[e]) ok = false;
+        bi[e] = b - g.blo[e];
+      }
+      k = g.nbins;
+      if (ok) k = (unsigned)(bi[0] + (long long)g.nb[0] * (bi[1] + (long long)g.nb[1] * bi[2]));
     }
-    unsigned k = g.nbins;
-    if (ok) {
-      k = (unsigned)(bi[0] + (long long)g.nb[0] * (bi[1] + (long long)g.nb[1] * bi[2]));
-      atomicAdd(&counts[k], 1u);
+    const unsigned peers = __match_any_sync(0xffffffffu, k);
+    const int leader = __ffs(peers) - 1;
+    unsigned base = 0;
+    if (valid && lane == leader) base = atomicAdd(&counts[k], (unsigned)__popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (valid) {
+      key[p] = k;
+      rank[p] = base + (unsigned)__popc(peers & ((1u << lane) - 1u));
     }
-    key[p] = k;
-    val[p] = p;
+  }
+}
+
+// order[start[key] + rank] = p
+__global__ void k_place(const unsigned *__restrict__ key, const unsigned *__restrict__ rank, int n,
+                        const unsigned *__restrict__ start, int *__restrict__ order) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+    order[start[key[p]] + rank[p]] = p;
+}
+
+// Slots within a bin were taken in atomic order; restore ascending particle index
+// so the sorted order is the stable one.  Bins of up to FIX_SMALL particles are
+// sorted in place by one thread; larger bins go to an overflow list (ovf[0] =
+// count, ovf[1..] = bins) for k_fixup_big.  The sentinel bin is not needed in order.
+constexpr int FIX_SMALL = 32;
+__global__ void k_fixup_small(const unsigned *__restrict__ start, unsigned nbins, int *__restrict__ order,
+                              unsigned *__restrict__ ovf) {
+  for (unsigned b = blockIdx.x * blockDim.x + threadIdx.x; b < nbins; b += gridDim.x * blockDim.x) {
+    const unsigned s = start[b], e = start[b + 1];
+    const unsigned k = e - s;
+    if (k < 2) continue;
+    if (k > (unsigned)FIX_SMALL) {
+      const unsigned i = atomicAdd(&ovf[0], 1u);
+      ovf[1 + i] = b;
+      continue;
+    }
+    int *o = order + s;
+    for (unsigned i = 1; i < k; i++) {
+      const int v = o[i];
+      unsigned j = i;
+      while (j > 0 && o[j - 1] > v) {
+        o[j] = o[j - 1];
+        j--;
+      }
+      o[j] = v;
+    }
+  }
+}
+
+// One CTA sorts one overflow bin at a time: runs of FIX_CHUNK ids by a bitonic sort
+// in shared memory, then merge-path merges of doubling runs through `tmp` (same
+// offsets as `order`).  Ids in a bin are distinct, so the order is unique.
+constexpr int FIX_THREADS = 1024;
+constexpr int FIX_CHUNK = 4096;
+__global__ void __launch_bounds__(FIX_THREADS) k_fixup_big(const unsigned *__restrict__ start,
+                                                           const unsigned *__restrict__ ovf, int *__restrict__ order,
+                                                           int *__restrict__ tmp) {
+  __shared__ int sh[FIX_CHUNK];
+  const unsigned nov = ovf[0];
+  for (unsigned ib = blockIdx.x; ib < nov; ib += gridDim.x) {
+    const unsigned b = ovf[1 + ib];
+    const unsigned s = start[b];
+    const int k = (int)(start[b + 1] - s);
+    // 1. sort chunks in shared memory
+    for (int c0 = 0; c0 < k; c0 += FIX_CHUNK) {
+      const int m = min(FIX_CHUNK, k - c0);
+      int P = 1;
+      while (P < m) P <<= 1;
+      for (int i = threadIdx.x; i < P; i += blockDim.x) sh[i] = i < m ? order[s + c0 + i] : 0x7FFFFFFF;
+      __syncthreads();
+      for (int sz = 2; sz <= P; sz <<= 1)
+        for (int st = sz >> 1; st > 0; st >>= 1) {
+          for (int i = threadIdx.x; i < P; i += blockDim.x) {
+            const int j = i ^ st;
+            if (j > i) {
+              const bool up = (i & sz) == 0;
+              const int a = sh[i], c = sh[j];
+              if ((a > c) == up) {
+                sh[i] = c;
+                sh[j] = a;
+              }
+            }
+          }
+          __syncthreads();
+        }
+      for (int i = threadIdx.x; i < m; i += blockDim.x) order[s + c0 + i] = sh[i];
+      __syncthreads();
+    }
+    // 2. merge runs of width w into 2w, ping-pong between order and tmp
+    int *src = order + s, *dst = tmp + s;
+    for (int w = FIX_CHUNK; w < k; w <<= 1) {
+      for (int a0 = 0; a0 < k; a0 += 2 * w) {
+        const int na = min(w, k - a0), nb = max(0, min(w, k - a0 - w));
+        const int *A = src + a0, *B = src + a0 + na;
+        const int m = na + nb;
+        const int per = (m + blockDim.x - 1) / blockDim.x;
+        const int d0 = min(m, (int)threadIdx.x * per), d1 = min(m, d0 + per);
+        if (d0 < d1) {
+          // merge path: i elements from A and d0 - i from B precede diagonal d0
+          int lo = max(0, d0 - nb), hi = min(d0, na);
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (A[mid] < B[d0 - mid - 1]) lo = mid + 1;
+            else hi = mid;
+          }
+          int i = lo, j = d0 - lo;
+          for (int d = d0; d < d1; d++) {
+            if (j >= nb || (i < na && A[i] < B[j])) dst[a0 + d] = A[i++];
+            else dst[a0 + d] = B[j++];
+          }
+        }
+      }
+      __syncthreads();
+      int *t = src;
+      src = dst;
+      dst = t;
+    }
+    if (src != order + s)
+      for (int i = threadIdx.x; i < k; i += blockDim.x) order[s + i] = src[i];
+    __syncthreads();
   }
 }
 
@@ -190,83 +316,6 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const unsigned *__r
   for (int i = 0; i < SCAN_PER_THREAD; i++) {
     if (base + i < n) out[base + i] = off;
     off += v[i];
-  }
-}
-
-// ------------------------------------------------------------------ stable LSB radix sort
-constexpr int RADIX_THREADS = 1024;
-constexpr int RADIX_PER_THREAD = 4;
-constexpr int RADIX_TILE = RADIX_THREADS * RADIX_PER_THREAD;
-constexpr int RADIX_MAXBITS = 10;
-
-__global__ void __launch_bounds__(RADIX_THREADS) k_radix_hist(const unsigned *__restrict__ key, int n, int shift,
-                                                              int bits, unsigned *__restrict__ ghist, int nblk) {
-  __shared__ unsigned h[1 << RADIX_MAXBITS];
-  const int nbk = 1 << bits;
-  for (int i = threadIdx.x; i < nbk; i += blockDim.x) h[i] = 0;
-  __syncthreads();
-  const int base = blockIdx.x * RADIX_TILE;
-  for (int i = threadIdx.x; i < RADIX_TILE; i += blockDim.x) {
-    const int q = base + i;
-    if (q < n) atomicAdd(&h[(key[q] >> shift) & (nbk - 1)], 1u);
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < nbk; i += blockDim.x) ghist[(size_t)i * nblk + blockIdx.x] = h[i];
-}
-
-// stable scatter: elements keep their order within a digit (tile order, then
-// round, then warp, then lane)
-__global__ void __launch_bounds__(RADIX_THREADS) k_radix_scatter(const unsigned *__restrict__ key_in,
-                                                                 const int *__restrict__ val_in, int n, int shift,
-                                                                 int bits, const unsigned *__restrict__ goff,
-                                                                 int nblk, unsigned *__restrict__ key_out,
-                                                                 int *__restrict__ val_out) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int nbk = 1 << bits;
-  unsigned short *cnt = reinterpret_cast<unsigned short *>(smem_raw);  // [32][nbk]
-  unsigned *run = reinterpret_cast<unsigned *>(smem_raw + sizeof(unsigned short) * 32 * nbk);
-  unsigned *tot = run + nbk;
-  unsigned *boff = tot + nbk;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int i = threadIdx.x; i < nbk; i += blockDim.x) {
-    run[i] = 0;
-    boff[i] = goff[(size_t)i * nblk + blockIdx.x];
-  }
-  const int base = blockIdx.x * RADIX_TILE;
-  for (int round = 0; round < RADIX_PER_THREAD; round++) {
-    for (int i = threadIdx.x; i < 32 * nbk; i += blockDim.x) cnt[i] = 0;
-    __syncthreads();
-    const int q = base + round * RADIX_THREADS + threadIdx.x;
-    const bool valid = q < n;
-    unsigned k = 0;
-    int d = nbk;  // invalid lanes share a digit nobody uses
-    if (valid) {
-      k = key_in[q];
-      d = (int)((k >> shift) & (unsigned)(nbk - 1));
-    }
-    const unsigned peers = __match_any_sync(0xffffffffu, d);
-    const unsigned lt = peers & ((1u << lane) - 1u);
-    const int rank = __popc(lt);
-    if (valid && rank == 0) cnt[wid * nbk + d] = (unsigned short)__popc(peers);
-    __syncthreads();
-    for (int dd = threadIdx.x; dd < nbk; dd += blockDim.x) {
-      unsigned s = 0;
-      for (int w = 0; w < 32; w++) {
-        const unsigned c = cnt[w * nbk + dd];
-        cnt[w * nbk + dd] = (unsigned short)s;
-        s += c;
-      }
-      tot[dd] = s;
-    }
-    __syncthreads();
-    if (valid) {
-      const unsigned dst = boff[d] + run[d] + cnt[wid * nbk + d] + rank;
-      key_out[dst] = k;
-      val_out[dst] = val_in[q];
-    }
-    __syncthreads();
-    for (int dd = threadIdx.x; dd < nbk; dd += blockDim.x) run[dd] += tot[dd];
-    __syncthreads();
   }
 }
 

@@ -1,10 +1,13 @@
-// pmgpu.cu -- C ABI of the B200 particle-mesh step (the library's one translation
-// unit: it includes the kernel headers, so no relocatable device code is needed).
+// pmgpu.cu -- C ABI of the B200 particle-mesh step: plans, particle kernels,
+// Green's function set-up and the solve drivers.  The FFT pass kernels and their
+// launchers are compiled in the passes_*.cu units (no relocatable device code:
+// every unit registers its own kernels).
 #include "../../include/pmlib_gpu.h"
 
 #include "common.cuh"
 #include "fft.cuh"
 #include "green.cuh"
+#include "host.h"
 #include "particles.cuh"
 #include "solve.cuh"
 
@@ -24,9 +27,7 @@ long long g_launches = 0;
 // ------------------------------------------------------------------ per-kernel timing
 // When enabled, every launch of the library is bracketed by CUDA events on its
 // stream; pmgpu_timing_get sums the elapsed times per kernel class.
-enum KClass { KC_BIN, KC_SCAN, KC_RHIST, KC_RSCAT, KC_DEPOSIT, KC_GADD, KC_XFWD, KC_YFWD, KC_ZPASS, KC_YINV,
-              KC_XINV, KC_GFILL, KC_M2P, KC_OTHER, KC_N };
-static const char *kc_names[KC_N] = {"bin", "scan", "radix_hist", "radix_scatter", "deposit", "ghost_add",
+static const char *kc_names[KC_N] = {"bin", "scan", "place", "fixup", "deposit", "ghost_add",
                                      "x_fwd", "y_fwd", "z_pass", "y_inv", "x_inv", "ghost_fill", "m2p", "other"};
 static bool g_timing = false;
 struct PendingEv {
@@ -37,24 +38,19 @@ static std::vector<PendingEv> g_pending;
 static double g_kms[KC_N];
 static long long g_kn[KC_N];
 
-struct KTimer {
-  int cls;
-  cudaStream_t st;
-  cudaEvent_t a = nullptr, b = nullptr;
-  KTimer(int c, cudaStream_t s) : cls(c), st(s) {
-    if (g_timing) {
-      cudaEventCreate(&a);
-      cudaEventCreate(&b);
-      cudaEventRecord(a, st);
-    }
+KTimer::KTimer(int c, cudaStream_t s) : cls(c), st(s) {
+  if (g_timing) {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, st);
   }
-  ~KTimer() {
-    if (g_timing && a) {
-      cudaEventRecord(b, st);
-      g_pending.push_back({cls, a, b});
-    }
+}
+KTimer::~KTimer() {
+  if (g_timing && a) {
+    cudaEventRecord(b, st);
+    g_pending.push_back({cls, a, b});
   }
-};
+}
 static void timing_collect() {
   for (auto &p : g_pending) {
     float ms = 0.f;
@@ -84,16 +80,10 @@ bool cuda_ok(cudaError_t e, const char *caller) {
   return false;
 }
 
-#define CK(expr, caller)                         \
-  do {                                           \
-    if (!::pmgpu::cuda_ok((expr), (caller))) {   \
-      return -1;                                 \
-    }                                            \
-  } while (0)
-#define CKL(caller) CK(cudaGetLastError(), caller)
-
 // ------------------------------------------------------------------ per-device tables
 static bool g_dev_ready[128];
+// plans made while set use the out-of-place Stockham passes along y and z only
+static int g_force_stockham = 0;
 
 static int ensure_device(const char *caller) {
   int dev = 0;
@@ -110,8 +100,11 @@ static int ensure_device(const char *caller) {
       t32[R][m][0] = (float)cosl(a);
       t32[R][m][1] = (float)sinl(a);
     }
-  CK(cudaMemcpyToSymbol(c_cs32, t32, sizeof(t32)), caller);
-  CK(cudaMemcpyToSymbol(c_cs64, t64, sizeof(t64)), caller);
+  if (upload_cs_f32_1(t32, t64) || upload_cs_f32_3(t32, t64) || upload_cs_f64_1(t32, t64) ||
+      upload_cs_f64_3(t32, t64)) {
+    set_error(caller, "could not upload the DFT constant tables.");
+    return -1;
+  }
   if (dev >= 0 && dev < 128) g_dev_ready[dev] = true;
   return 0;
 }
@@ -225,35 +218,100 @@ template <typename R> static int upload_tw(const std::vector<cld> &tw, DevBuf &b
   return 0;
 }
 
-// shared-memory budget of one persistent pass CTA
-constexpr size_t PASS_SMEM_BUDGET = 220 * 1024;
-
-static size_t tw_bytes(int ntw, size_t csize) { return (size_t)((ntw + 7) & ~7) * csize; }
-
-// kx tile of the y / z passes: the largest of 8, 4, 2, 1 whose three buffers fit
-// (FP32 needs an even line count: two lines per 16-byte vector)
-static int pick_tk(int n, int nc, size_t csize, int ntw) {
-  for (int tk = 8; tk >= 1; tk /= 2) {
-    if (csize == 8 && (nc * tk) % 2) continue;
-    if (tw_bytes(ntw, csize) + 3 * (size_t)nc * tk * n * csize <= PASS_SMEM_BUDGET) return tk;
+// ------------------------------------------------------------------ register-engine plans
+// Factor n into at most three register radices; the score models per-point work
+// (a shared-memory round trip + twiddles per phase, plus the DFT of the radix).
+static double radix_cost(int r) {
+  switch (r) {
+    case 2: return 1.0;
+    case 3: return 1.3;
+    case 4: return 1.1;
+    case 5: return 1.7;
+    case 6: return 1.4;
+    case 7: return 2.3;
+    case 8: return 1.2;
+    case 9: return 1.7;
+    case 10: return 1.6;
+    case 11: return 3.2;
+    case 12: return 1.5;
+    case 13: return 3.6;
+    case 16: return 1.3;
+    case 17: return 4.4;
+    default: return 1e9;
   }
-  return 0;
 }
-static size_t lines_smem(int n, int nc, int tk, size_t csize, int ntw) {
-  return tw_bytes(ntw, csize) + 3 * (size_t)nc * tk * n * csize;
-}
-// rows per tile of the x passes
-static int pick_rb(int n2, int P0, int Hp, int nc, size_t csize, size_t rsize, int ntw, bool inverse) {
-  for (int rb = 8; rb >= 1; rb--) {
-    if (csize == 8 && (nc * rb) % 2) continue;
-    const size_t stage = inverse ? (size_t)rb * Hp * nc * csize : (((size_t)rb * P0 * nc * rsize + 15) / 16) * 16;
-    if (tw_bytes(ntw, csize) + stage + 2 * (size_t)nc * rb * n2 * csize <= PASS_SMEM_BUDGET) return rb;
+
+static bool make_regplan(int n, RegPlan &pl) {
+  static const int S[] = {16, 17, 13, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2};
+  double best = 1e18;
+  int br[3] = {0, 0, 0}, bnp = 0;
+  auto consider = [&](int np, const int *r) {
+    double c = 0.0;
+    for (int i = 0; i < np; i++) c += 1.5 + radix_cost(r[i]);
+    if (r[0] % 2) c += 0.5;  // the zero half of a padded line is skipped only with an even first radix
+    if (c < best - 1e-9) {
+      best = c;
+      bnp = np;
+      for (int i = 0; i < 3; i++) br[i] = i < np ? r[i] : 0;
+    }
+  };
+  for (int a : S) {
+    if (n % a) continue;
+    const int n1 = n / a;
+    if (n1 == 1) {
+      int r[3] = {a, 0, 0};
+      consider(1, r);
+      continue;
+    }
+    for (int b : S) {
+      if (n1 % b) continue;
+      const int n2 = n1 / b;
+      if (n2 == 1) {
+        int r[3] = {a, b, 0};
+        consider(2, r);
+        continue;
+      }
+      if (reg_radix(n2)) {
+        int r[3] = {a, b, n2};
+        consider(3, r);
+      }
+    }
   }
-  return 0;
+  if (bnp == 0) return false;
+  memset(&pl, 0, sizeof(pl));
+  pl.n = n;
+  pl.np = bnp;
+  int B = n;
+  for (int p = 0; p < bnp; p++) {
+    pl.rad[p] = br[p];
+    pl.blk[p] = B;
+    pl.str[p] = B / br[p];
+    pl.twm[p] = n / B;
+    pl.dstr[p] = make_fastdiv((unsigned)pl.str[p]);
+    B /= br[p];
+  }
+  return true;
+}
+
+// position -> frequency index of the digit-reversed output of a plan
+static std::vector<int> regplan_positions(const RegPlan &pl) {
+  std::vector<int> k(pl.n);
+  for (int q = 0; q < pl.n; q++) {
+    int rem = q, mul = 1, f = 0;
+    for (int p = 0; p < pl.np; p++) {
+      const int sub = pl.blk[p] / pl.rad[p];
+      const int d = rem / sub;
+      rem -= d * sub;
+      f += mul * d;
+      mul *= pl.rad[p];
+    }
+    k[q] = f;
+  }
+  return k;
 }
 
 static int g_nsm = 0;
-static int num_sms() {
+int num_sms() {
   if (g_nsm == 0) {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -261,12 +319,6 @@ static int num_sms() {
     if (g_nsm <= 0) g_nsm = 148;
   }
   return g_nsm;
-}
-
-template <typename K> static int persistent_grid(K kernel, size_t smem, int ntiles) {
-  int per = 1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, PASS_THREADS, smem) != cudaSuccess || per < 1) per = 1;
-  return std::max(1, std::min(ntiles, per * num_sms()));
 }
 
 }  // namespace pmgpu
@@ -292,6 +344,10 @@ struct pmgpu_plan {
   int gM1, gM2;
   double eps;
   DevBuf X, Y, Y2, Y3;
+  // register-engine plans along y and z (in-place, digit-reversed spectra)
+  int ry_ok, rz_ok;
+  RegPlan ry, rz;
+  DevBuf rtwy, rtwz, yk, zk;
   DevBuf mesh_w, mesh_u, mesh_a, mesh_b;
   DevBuf h_pos, h_val, h_out;  // device mirrors used by host-pointer calls
   // particle scratch
@@ -301,7 +357,7 @@ struct pmgpu_plan {
   ~pmgpu_plan() {
     DevBuf *bs[] = {&twx, &twy, &twz, &kxt, &kyt, &kzt, &green, &X, &Y, &Y2, &Y3, &mesh_w, &mesh_u,
                     &mesh_a, &mesh_b, &h_pos, &h_val, &h_out, &key, &val, &key2, &val2, &counts,
-                    &start, &spart, &hist};
+                    &start, &spart, &hist, &rtwy, &rtwz, &yk, &zk};
     for (DevBuf *b : bs) b->release();
   }
 };
@@ -336,37 +392,6 @@ static int exclusive_scan(const unsigned *in, unsigned *out, size_t n, DevBuf &p
   { KTimer kt_(KC_SCAN, st); k_scan_apply<<<(unsigned)nb, SCAN_THREADS, 0, st>>>(in, n, part.as<unsigned>(), out); }
   PM_LAUNCHED();
   CKL(caller);
-  return 0;
-}
-
-// stable sort of (key, val); returns via *kout/*vout the buffers holding the result
-static int radix_sort(unsigned maxkey, int n, DevBuf &k1, DevBuf &v1, DevBuf &k2, DevBuf &v2, DevBuf &hist,
-                      DevBuf &part, cudaStream_t st, const unsigned **kout, const int **vout,
-                      const char *caller) {
-  int bits = 1;
-  while (bits < 32 && (maxkey >> bits) != 0) bits++;
-  const int passes = (bits + RADIX_MAXBITS - 1) / RADIX_MAXBITS;
-  const int db = (bits + passes - 1) / passes;
-  const int nbk = 1 << db;
-  const int nblk = (n + RADIX_TILE - 1) / RADIX_TILE;
-  if (hist.ensure(sizeof(unsigned) * ((size_t)nbk * nblk + 1), caller)) return -1;
-  unsigned *ka = k1.as<unsigned>(), *kb = k2.as<unsigned>();
-  int *va = v1.as<int>(), *vb = v2.as<int>();
-  const size_t smem = sizeof(unsigned short) * 32 * nbk + sizeof(unsigned) * 3 * nbk;
-  CK(cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), caller);
-  for (int p = 0; p < passes; p++) {
-    const int shift = p * db;
-    { KTimer kt_(KC_RHIST, st); k_radix_hist<<<nblk, RADIX_THREADS, 0, st>>>(ka, n, shift, db, hist.as<unsigned>(), nblk); }
-    PM_LAUNCHED();
-    if (exclusive_scan(hist.as<unsigned>(), hist.as<unsigned>(), (size_t)nbk * nblk, part, st, caller)) return -1;
-    { KTimer kt_(KC_RSCAT, st); k_radix_scatter<<<nblk, RADIX_THREADS, smem, st>>>(ka, va, n, shift, db, hist.as<unsigned>(), nblk, kb, vb); }
-    PM_LAUNCHED();
-    CKL(caller);
-    std::swap(ka, kb);
-    std::swap(va, vb);
-  }
-  *kout = ka;
-  *vout = va;
   return 0;
 }
 
@@ -411,28 +436,37 @@ static int run_p2m(const pmgpu_topo *t, int order, const R *pos, const R *val, i
     set_error(caller, "Mesh too large for 32-bit bin keys.");
     return -1;
   }
-  if (s.key->ensure(sizeof(unsigned) * (size_t)std::max(n, 1), caller) ||
-      s.val->ensure(sizeof(int) * (size_t)std::max(n, 1), caller) ||
-      s.key2->ensure(sizeof(unsigned) * (size_t)std::max(n, 1), caller) ||
-      s.val2->ensure(sizeof(int) * (size_t)std::max(n, 1), caller) ||
+  const size_t nn = (size_t)std::max(n, 1);
+  if (s.key->ensure(sizeof(unsigned) * nn, caller) || s.val->ensure(sizeof(unsigned) * nn, caller) ||
+      s.key2->ensure(sizeof(int) * nn, caller) || s.val2->ensure(sizeof(int) * nn, caller) ||
+      s.hist->ensure(sizeof(unsigned) * (nn / (FIX_SMALL + 1) + 2), caller) ||
       s.counts->ensure(sizeof(unsigned) * (g.nbins + 1), caller) ||
       s.start->ensure(sizeof(unsigned) * (g.nbins + 1), caller))
     return -1;
+  // counting sort by bin: provisional slots, bin starts, placement, stable fix-up
   CK(cudaMemsetAsync(s.counts->p, 0, sizeof(unsigned) * (g.nbins + 1), st), caller);
-  const int *perm = nullptr;
+  CK(cudaMemsetAsync(s.hist->p, 0, sizeof(unsigned), st), caller);
+  unsigned *keys = s.key->as<unsigned>(), *ranks = s.val->as<unsigned>();
+  int *perm = s.val2->as<int>();
   if (n > 0) {
     const int nblk = std::min((n + 255) / 256, 148 * 32);
-    if (W == 4) { KTimer kt_(KC_BIN, st); k_bin<R, 4><<<nblk, 256, 0, st>>>(g, pos, n, s.key->as<unsigned>(), s.val->as<int>(), s.counts->as<unsigned>()); }
-    else { KTimer kt_(KC_BIN, st); k_bin<R, 6><<<nblk, 256, 0, st>>>(g, pos, n, s.key->as<unsigned>(), s.val->as<int>(), s.counts->as<unsigned>()); }
+    if (W == 4) { KTimer kt_(KC_BIN, st); k_bin<R, 4><<<nblk, 256, 0, st>>>(g, pos, n, keys, ranks, s.counts->as<unsigned>()); }
+    else { KTimer kt_(KC_BIN, st); k_bin<R, 6><<<nblk, 256, 0, st>>>(g, pos, n, keys, ranks, s.counts->as<unsigned>()); }
     PM_LAUNCHED();
     CKL(caller);
   }
   if (exclusive_scan(s.counts->as<unsigned>(), s.start->as<unsigned>(), (size_t)g.nbins + 1, *s.spart, st, caller))
     return -1;
   if (n > 0) {
-    const unsigned *ks;
-    if (radix_sort(g.nbins, n, *s.key, *s.val, *s.key2, *s.val2, *s.hist, *s.spart, st, &ks, &perm, caller))
-      return -1;
+    const int nblk = std::min((n + 255) / 256, 148 * 32);
+    { KTimer kt_(KC_PLACE, st); k_place<<<nblk, 256, 0, st>>>(keys, ranks, n, s.start->as<unsigned>(), perm); }
+    PM_LAUNCHED();
+    const int nbb = (int)std::min<unsigned>((g.nbins + 255) / 256, 148u * 32u);
+    { KTimer kt_(KC_FIXUP, st); k_fixup_small<<<std::max(nbb, 1), 256, 0, st>>>(s.start->as<unsigned>(), g.nbins, perm, s.hist->as<unsigned>()); }
+    PM_LAUNCHED();
+    { KTimer kt_(KC_FIXUP, st); k_fixup_big<<<num_sms(), FIX_THREADS, 0, st>>>(s.start->as<unsigned>(), s.hist->as<unsigned>(), perm, s.key2->as<int>()); }
+    PM_LAUNCHED();
+    CKL(caller);
   }
   // deposition, components in groups of at most three
   const int zc = (W == 4) ? 32 : 30;
@@ -445,7 +479,7 @@ static int run_p2m(const pmgpu_topo *t, int order, const R *pos, const R *val, i
     const size_t smem = (size_t)cap * (3 * W + nv) * sizeof(R) + sizeof(int) * (2 * BX * BY + 2 * BY + 2);
     const R *vp = val + c0;
     R *mp = mesh + c0;
-    const int *pp = perm ? perm : s.val->as<int>();
+    const int *pp = perm;
 #define DEP_CASE(WW, NVV)                                                                                  \
   if (W == WW && nv == NVV) {                                                                              \
     CK(cudaFuncSetAttribute(k_deposit<R, WW, NVV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), \
@@ -466,7 +500,7 @@ static int run_p2m(const pmgpu_topo *t, int order, const R *pos, const R *val, i
     const int S = t->nghost[2 * d] + t->nghost[2 * d + 1];
     const long long total = (long long)S * g.ext[(d + 1) % 3] * g.ext[(d + 2) % 3];
     const int nblk = (int)std::min<long long>((total + 255) / 256, 148 * 16);
-    { KTimer kt_(KC_GADD, 0); k_ghost_add<R><<<std::max(nblk, 1), 256, 0, st>>>(mesh, g.ext[0], g.ext[1], g.ext[2], nvar_mesh, d,
+    { KTimer kt_(KC_GADD, st); k_ghost_add<R><<<std::max(nblk, 1), 256, 0, st>>>(mesh, g.ext[0], g.ext[1], g.ext[2], nvar_mesh, d,
                                                        t->ncell[d], t->nghost[2 * d], t->nghost[2 * d + 1]); }
     PM_LAUNCHED();
     CKL(caller);
@@ -519,117 +553,15 @@ template <typename R> static SolveGeom<R> solve_geom(const pmgpu_plan *pl) {
   g.eps2pi = (R)(2.0 * 3.14159265358979323846 * pl->eps);
   g.order = pl->par.poisson_order;
   g.allper = pl->g.allper;
+  g.ry_ok = pl->ry_ok;
+  g.rz_ok = pl->rz_ok;
+  g.ry = pl->ry;
+  g.rz = pl->rz;
+  g.rtwy = pl->rtwy.as<C>();
+  g.rtwz = pl->rtwz.as<C>();
+  g.yk = pl->ry_ok ? pl->yk.as<int>() : nullptr;
+  g.zk = pl->rz_ok ? pl->zk.as<int>() : nullptr;
   return g;
-}
-
-template <typename R, int NC>
-static int launch_lines(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typename cplx_t<R>::type *out, int axis,
-                        int lmode, int zmode, int reproj, int use_zeta, int rows_in, int rows_out, long long in_os,
-                        long long in_rs, long long out_os, long long out_rs, int nouter, cudaStream_t st,
-                        const char *caller) {
-  typedef typename cplx_t<R>::type C;
-  const int n = g.M[axis];
-  const int ntw = (axis == 1) ? g.fy.ntw : g.fz.ntw;
-  const int TK = pick_tk(n, NC, sizeof(C), ntw);
-  if (TK == 0) {
-    set_error(caller, "FFT length too large for the shared-memory transform.");
-    return -1;
-  }
-  LineTiles lt;
-  lt.n = n;
-  lt.rows_in = rows_in;
-  lt.rows_out = rows_out;
-  lt.in_os = in_os;
-  lt.in_rs = in_rs;
-  lt.out_os = out_os;
-  lt.out_rs = out_rs;
-  lt.nouter = nouter;
-  lt.nkt = g.Hp / TK;
-  lt.TK = TK;
-  const size_t sm = lines_smem(n, NC, TK, sizeof(C), ntw);
-  CK(cudaFuncSetAttribute(k_lines<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
-  const int grid = persistent_grid(k_lines<R, NC>, sm, lt.nouter * lt.nkt);
-  k_lines<R, NC><<<grid, PASS_THREADS, sm, st>>>(g, lt, in, out, axis, lmode, zmode, reproj, use_zeta);
-  PM_LAUNCHED();
-  CKL(caller);
-  return 0;
-}
-
-template <typename R, int NC>
-static int fwd_xy(SolveGeom<R> &g, const R *in, typename cplx_t<R>::type *X, typename cplx_t<R>::type *Y,
-                  cudaStream_t st, const char *caller, int cs = NC) {
-  typedef typename cplx_t<R>::type C;
-  const int ntwx = g.fx.ntw + g.fx.next;
-  const int RB = pick_rb(g.N2, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), ntwx, false);
-  if (RB == 0) {
-    set_error(caller, "FFT length too large for the shared-memory transform.");
-    return -1;
-  }
-  const size_t stage = (((size_t)RB * g.P[0] * NC * sizeof(R) + 15) / 16) * 16;
-  const size_t sm = tw_bytes(ntwx, sizeof(C)) + stage + 2 * (size_t)NC * RB * g.N2 * sizeof(C);
-  const bool vec16 = cs == NC && ((size_t)g.ext[0] * NC * sizeof(R)) % 16 == 0 &&
-                     ((size_t)g.off[0] * NC * sizeof(R)) % 16 == 0 && ((size_t)g.P[0] * NC * sizeof(R)) % 16 == 0;
-  CK(cudaFuncSetAttribute(k_xfwd<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
-  const int rows = g.P[1] * g.P[2];
-  const int ntiles = (rows + RB - 1) / RB;
-  { KTimer kt_(KC_XFWD, st);
-    k_xfwd<R, NC><<<persistent_grid(k_xfwd<R, NC>, sm, ntiles), PASS_THREADS, sm, st>>>(g, in, X, RB, cs, vec16 ? 1 : 0); }
-  PM_LAUNCHED();
-  CKL(caller);
-  const long long Hp = g.Hp;
-  KTimer kt_(KC_YFWD, st);
-  return launch_lines<R, NC>(g, X, Y, 1, L_FWD, 0, 0, 0, g.P[1], g.M[1], (long long)g.P[1] * Hp, Hp,
-                             (long long)g.M[1] * Hp, Hp, g.P[2], st, caller);
-}
-
-template <typename R, int NC>
-static int zpass(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typename cplx_t<R>::type *out, int mode,
-                 int reproj, int use_zeta, int rows_y, cudaStream_t st, const char *caller) {
-  const long long Hp = g.Hp;
-  const int rows = (mode == Z_FORWARD) ? g.M[2] : g.P[2];
-  KTimer kt_(KC_ZPASS, st);
-  return launch_lines<R, NC>(g, in, out, 2, mode == Z_FORWARD ? L_FWD : L_Z, mode, reproj, use_zeta, rows, rows, Hp,
-                             (long long)g.M[1] * Hp, Hp, (long long)g.M[1] * Hp, rows_y, st, caller);
-}
-
-template <typename R, int NC>
-static int inv_yx(SolveGeom<R> &g, const pmgpu_topo *topo, typename cplx_t<R>::type *Y,
-                  typename cplx_t<R>::type *X, R *out, cudaStream_t st, const char *caller, int cs = NC,
-                  bool ghosts = true) {
-  typedef typename cplx_t<R>::type C;
-  const long long Hp = g.Hp;
-  {
-    KTimer kt_(KC_YINV, st);
-    if (launch_lines<R, NC>(g, Y, X, 1, L_INV, 0, 0, 0, g.M[1], g.P[1], (long long)g.M[1] * Hp, Hp,
-                            (long long)g.P[1] * Hp, Hp, g.P[2], st, caller))
-      return -1;
-  }
-  const int ntwx = g.fx.ntw + g.fx.next;
-  const int RB = pick_rb(g.N2, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), ntwx, true);
-  if (RB == 0) {
-    set_error(caller, "FFT length too large for the shared-memory transform.");
-    return -1;
-  }
-  const size_t sm = tw_bytes(ntwx, sizeof(C)) + (size_t)RB * g.Hp * NC * sizeof(C) + 2 * (size_t)NC * RB * g.N2 * sizeof(C);
-  CK(cudaFuncSetAttribute(k_xinv<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
-  const int rows = g.P[1] * g.P[2];
-  const int ntiles = (rows + RB - 1) / RB;
-  { KTimer kt_(KC_XINV, st);
-    k_xinv<R, NC><<<persistent_grid(k_xinv<R, NC>, sm, ntiles), PASS_THREADS, sm, st>>>(g, X, out, RB, cs); }
-  PM_LAUNCHED();
-  CKL(caller);
-  // periodic ghosts (x, then y, then z)
-  for (int d = 0; d < 3 && ghosts; d++) {
-    if (topo->bound_cond[2 * d] == 0 || topo->bound_cond[2 * d + 1] == 0) continue;
-    const int S = topo->nghost[2 * d] + topo->nghost[2 * d + 1];
-    const long long total = (long long)S * g.ext[(d + 1) % 3] * g.ext[(d + 2) % 3];
-    const int nblk = (int)std::min<long long>((total + 255) / 256, 148 * 16);
-    { KTimer kt_(KC_GFILL, st); k_ghost_fill<R><<<std::max(nblk, 1), 256, 0, st>>>(out, g.ext[0], g.ext[1], g.ext[2], cs, d, topo->ncell[d],
-                                                        topo->nghost[2 * d], topo->nghost[2 * d + 1]); }
-    PM_LAUNCHED();
-    CKL(caller);
-  }
-  return 0;
 }
 
 template <typename R>
@@ -686,7 +618,7 @@ static int run_regularise(pmgpu_plan *pl, R *mesh, int nvar, int reg_order, doub
     const int S = topo->nghost[2 * d] + topo->nghost[2 * d + 1];
     const long long total = (long long)S * ext[(d + 1) % 3] * ext[(d + 2) % 3];
     const int nblk = (int)std::min<long long>((total + 255) / 256, 148 * 16);
-    { KTimer kt_(KC_GFILL, 0); k_ghost_fill<R><<<std::max(nblk, 1), 256, 0, st>>>(mesh, ext[0], ext[1], ext[2], nvar, d, topo->ncell[d],
+    { KTimer kt_(KC_GFILL, st); k_ghost_fill<R><<<std::max(nblk, 1), 256, 0, st>>>(mesh, ext[0], ext[1], ext[2], nvar, d, topo->ncell[d],
                                                         topo->nghost[2 * d], topo->nghost[2 * d + 1]); }
     PM_LAUNCHED();
     CKL(caller);
@@ -783,12 +715,44 @@ template <typename R> static int upload_wavenumbers(pmgpu_plan *pl, const char *
   return 0;
 }
 
+template <typename R> static int reg_tables(pmgpu_plan *pl, const char *caller) {
+  typedef typename cplx_t<R>::type C;
+  pl->ry_ok = pl->rz_ok = 0;
+  if (g_force_stockham) return 0;
+  const long double twopi = 2.0L * acosl(-1.0L);
+  for (int axis = 1; axis <= 2; axis++) {
+    RegPlan rp;
+    const int n = pl->g.M[axis];
+    if (!make_regplan(n, rp)) continue;
+    std::vector<C> tw(n);
+    for (int q = 0; q < n; q++) {
+      const long double a = twopi * (long double)q / (long double)n;
+      tw[q] = mk((R)cosl(a), (R)-sinl(a));
+    }
+    const std::vector<int> kp = regplan_positions(rp);
+    DevBuf &tb = axis == 1 ? pl->rtwy : pl->rtwz;
+    DevBuf &kb = axis == 1 ? pl->yk : pl->zk;
+    if (tb.ensure(sizeof(C) * n, caller) || kb.ensure(sizeof(int) * n, caller)) return -1;
+    CK(cudaMemcpy(tb.p, tw.data(), sizeof(C) * n, cudaMemcpyHostToDevice), caller);
+    CK(cudaMemcpy(kb.p, kp.data(), sizeof(int) * n, cudaMemcpyHostToDevice), caller);
+    if (axis == 1) {
+      pl->ry = rp;
+      pl->ry_ok = 1;
+    } else {
+      pl->rz = rp;
+      pl->rz_ok = 1;
+    }
+  }
+  return 0;
+}
+
 template <typename R> static int plan_tables(pmgpu_plan *pl, const char *caller) {
   std::vector<cld> tw;
   if (!make_fft(pl->g.N2, pl->g.M[0], pl->fx, tw) || upload_tw<R>(tw, pl->twx, caller)) return -1;
   if (!make_fft(pl->g.M[1], 0, pl->fy, tw) || upload_tw<R>(tw, pl->twy, caller)) return -1;
   if (!make_fft(pl->g.M[2], 0, pl->fz, tw) || upload_tw<R>(tw, pl->twz, caller)) return -1;
   if (upload_wavenumbers<R>(pl, caller)) return -1;
+  if (reg_tables<R>(pl, caller)) return -1;
   return setup_green<R>(pl, caller);
 }
 
@@ -1386,4 +1350,11 @@ int pmgpu_interp_particle_mesh_noalloc(const pmgpu_topo *topo, const pmgpu_param
   const int mode = clear ? 1 : (clear_ghost ? 2 : 0);
   return run_p2m<double>(topo, par->interpolation_order, d_xpart, d_part, nvar, npart, d_mesh, nvar_mesh, mode, r,
                          (cudaStream_t)stream, nullptr, caller);
+}
+
+int pmgpu_fft_engine(int engine) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int old = g_force_stockham;
+  g_force_stockham = engine == 1 ? 1 : 0;
+  return old;
 }

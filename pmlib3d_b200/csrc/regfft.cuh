@@ -1,0 +1,219 @@
+// regfft.cuh -- in-place, register-blocked line FFTs for the solve passes.
+//
+// A line of length n = R0 R1 ... (at most three phases, radices up to 17) is
+// transformed in place in shared memory:
+//
+//   forward (decimation in frequency): phase p works on blocks of B_p points with
+//   stride s_p = B_p / R_p.  Butterfly (block beta, offset r) reads the R_p points
+//   beta B_p + r + s_p j, takes their R_p-point DFT in registers, multiplies output k
+//   by w_{B_p}^{r k} (skipped in the last phase, where s = 1) and writes it back to
+//   beta B_p + r + s_p k.  The result is in digit-reversed order: position
+//   p = k0 B_1 + k1 B_2 + k2 holds frequency k0 + R0 (k1 + R1 k2).
+//   inverse (decimation in time): the same phases in reverse order with conjugate
+//   twiddles applied before the inverse DFT; digit-reversed input, natural output.
+//
+// The first forward phase can read its points straight from global memory (points
+// beyond the row count are the zero padding and are not read), and the last
+// inverse phase can write straight to global memory (rows beyond the row count are
+// the truncation and are not written), so padding and truncation cost no traffic.
+// Consumers of a digit-reversed spectrum index it through a position -> frequency
+// table.  Lines are held as vectors of G lines (FP32: float4 = two complex lines;
+// FP64: double2 = one) interleaved by position: vector g of position q sits at
+// buf[q * LG + g], so consecutive threads touch consecutive 16-byte vectors.
+// Twiddles come from one table of w_n^q, q < n, built in long double on the host.
+#pragma once
+
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace pmgpu {
+
+// u / d for u < 2^31 by multiply-high (Granlund-Montgomery): l = ceil(log2 d),
+// m = floor(2^32 (2^l - d) / d) + 1, q = (umulhi(u, m) + u) >> l
+struct FastDiv {
+  unsigned d, m, l;
+};
+static inline FastDiv make_fastdiv(unsigned d) {
+  FastDiv f;
+  f.d = d;
+  unsigned l = 0;
+  while ((1ull << l) < d) l++;
+  f.l = l;
+  f.m = (unsigned)((((1ull << l) - d) << 32) / d + 1);
+  return f;
+}
+__host__ __device__ __forceinline__ unsigned fdiv(unsigned u, const FastDiv &f) {
+#ifdef __CUDA_ARCH__
+  return (__umulhi(u, f.m) + u) >> f.l;
+#else
+  return (unsigned)((((unsigned long long)u * f.m) >> 32) + u) >> f.l;
+#endif
+}
+
+constexpr int RP_MAX = 3;
+struct RegPlan {
+  int n, np;
+  int rad[RP_MAX];  // radix of each phase, outermost first
+  int blk[RP_MAX];  // block size B_p = n / (R_0 ... R_{p-1})
+  int str[RP_MAX];  // stride s_p = B_p / R_p
+  int twm[RP_MAX];  // n / B_p: w_{B_p}^q = w_n^{twm q}
+  FastDiv dstr[RP_MAX];
+};
+
+// radices with a register DFT
+__host__ __device__ constexpr bool reg_radix(int r) {
+  return r == 2 || r == 3 || r == 4 || r == 5 || r == 6 || r == 7 || r == 8 || r == 9 || r == 10 || r == 11 ||
+         r == 12 || r == 13 || r == 16 || r == 17;
+}
+
+// where a phase reads from / writes to
+struct PhaseGlobal {
+  const void *in;          // tile base (complex), row = position
+  void *out;
+  long long rs_in, rs_out; // row strides in complex elements
+  int rows_in;             // rows present in `in` (the rest is zero)
+  int rows_out;            // rows wanted in `out`
+};
+
+template <typename R> __device__ __forceinline__ typename Vec<R>::V ldg_vec(const typename Vec<R>::V *p);
+template <> __device__ __forceinline__ float4 ldg_vec<float>(const float4 *p) { return __ldg(p); }
+template <> __device__ __forceinline__ double2 ldg_vec<double>(const double2 *p) { return __ldg(p); }
+
+template <typename R> __device__ __forceinline__ typename Vec<R>::V zero_vec();
+template <> __device__ __forceinline__ float4 zero_vec<float>() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+template <> __device__ __forceinline__ double2 zero_vec<double>() { return make_double2(0.0, 0.0); }
+
+// One phase over a tile of LG line vectors.  gsrc / gdst: read from / write to
+// global memory instead of `buf`.  twid: the phase carries twiddles.
+template <int RAD, bool INV, typename R>
+__device__ __forceinline__ void rphase(const RegPlan &pl, int p, typename Vec<R>::V *buf, int LG, const FastDiv &dLG,
+                                       const typename cplx_t<R>::type *__restrict__ tw, bool gsrc, bool gdst,
+                                       bool twid, const PhaseGlobal &gl) {
+  typedef typename cplx_t<R>::type C;
+  typedef typename Vec<R>::V V;
+  constexpr int G = Vec<R>::G;
+  const int s = pl.str[p], B = pl.blk[p], tm = pl.twm[p];
+  const unsigned total = (unsigned)(pl.n / RAD) * (unsigned)LG;
+  const V *gin = reinterpret_cast<const V *>(gl.in);
+  V *gout = reinterpret_cast<V *>(gl.out);
+  const long long vri = gl.rs_in / G, vro = gl.rs_out / G;  // row strides in vectors
+  for (unsigned u = threadIdx.x; u < total; u += blockDim.x) {
+    const unsigned b = fdiv(u, dLG);
+    const int g = (int)(u - b * (unsigned)LG);
+    const unsigned beta = fdiv(b, pl.dstr[p]);
+    const int r = (int)(b - beta * (unsigned)s);
+    const int pos0 = (int)beta * B + r;
+    C a[G][RAD];
+    if (gsrc) {
+      const V *src = gin + (long long)pos0 * vri + g;
+#pragma unroll
+      for (int j = 0; j < RAD; j++) {
+        V v = zero_vec<R>();
+        if (pos0 + s * j < gl.rows_in) v = ldg_vec<R>(src + (long long)(s * j) * vri);
+        C t[G];
+        vsplit(v, t);
+#pragma unroll
+        for (int h = 0; h < G; h++) a[h][j] = t[h];
+      }
+    } else {
+      const V *src = buf + pos0 * LG + g;
+#pragma unroll
+      for (int j = 0; j < RAD; j++) {
+        C t[G];
+        vsplit(src[s * j * LG], t);
+#pragma unroll
+        for (int h = 0; h < G; h++) a[h][j] = t[h];
+      }
+    }
+    if (INV && twid) {
+      const int tb = tm * r;
+#pragma unroll
+      for (int j = 1; j < RAD; j++) {
+        const C w = tw[tb * j];
+#pragma unroll
+        for (int h = 0; h < G; h++) a[h][j] = cmulc(a[h][j], w);
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < G; h++) dft<RAD, INV>(a[h]);
+    if (!INV && twid) {
+      const int tb = tm * r;
+#pragma unroll
+      for (int k = 1; k < RAD; k++) {
+        const C w = tw[tb * k];
+#pragma unroll
+        for (int h = 0; h < G; h++) a[h][k] = cmul(a[h][k], w);
+      }
+    }
+    if (gdst) {
+      V *dst = gout + (long long)pos0 * vro + g;
+#pragma unroll
+      for (int k = 0; k < RAD; k++) {
+        C t[G];
+#pragma unroll
+        for (int h = 0; h < G; h++) t[h] = a[h][k];
+        if (pos0 + s * k < gl.rows_out) dst[(long long)(s * k) * vro] = vmerge(t);
+      }
+    } else {
+      V *dst = buf + pos0 * LG + g;
+#pragma unroll
+      for (int k = 0; k < RAD; k++) {
+        C t[G];
+#pragma unroll
+        for (int h = 0; h < G; h++) t[h] = a[h][k];
+        dst[s * k * LG] = vmerge(t);
+      }
+    }
+  }
+}
+
+template <bool INV, typename R>
+__device__ __forceinline__ void rphase_any(const RegPlan &pl, int p, typename Vec<R>::V *buf, int LG,
+                                           const FastDiv &dLG, const typename cplx_t<R>::type *tw, bool gsrc,
+                                           bool gdst, bool twid, const PhaseGlobal &gl) {
+  switch (pl.rad[p]) {
+    case 2: rphase<2, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
+    case 3: rphase<3, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
+    case 4: rphase<4, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
+    case 5: rphase<5, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
+    case 6: rphase<6, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
+    case 7: rphase<7, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
+    case 8: rphase<8, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
+    case 9: rphase<9, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
+    case 10: rphase<10, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
+    case 11: rphase<11, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
+    case 12: rphase<12, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
+    case 13: rphase<13, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
+    case 16: rphase<16, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
+    case 17: rphase<17, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
+    default: break;  // plans only hold register radices
+  }
+}
+
+// forward transform of a tile: natural-order input (global when gfirst, else buf),
+// digit-reversed output in buf, or in global memory when glast.  The caller
+// synchronises before; every phase but a final global one ends with a barrier.
+template <typename R>
+__device__ __forceinline__ void rfft_fwd(const RegPlan &pl, typename Vec<R>::V *buf, int LG, const FastDiv &dLG,
+                                         const typename cplx_t<R>::type *tw, bool gfirst, bool glast,
+                                         const PhaseGlobal &gl) {
+  for (int p = 0; p < pl.np; p++) {
+    const bool last = p == pl.np - 1;
+    rphase_any<false, R>(pl, p, buf, LG, dLG, tw, gfirst && p == 0, glast && last, !last, gl);
+    __syncthreads();
+  }
+}
+
+// inverse transform: digit-reversed input (global when gfirst, else buf), natural
+// output in buf, or in global memory (rows < rows_out) when glast
+template <typename R>
+__device__ __forceinline__ void rfft_inv(const RegPlan &pl, typename Vec<R>::V *buf, int LG, const FastDiv &dLG,
+                                         const typename cplx_t<R>::type *tw, bool gfirst, bool glast,
+                                         const PhaseGlobal &gl) {
+  for (int p = pl.np - 1; p >= 0; p--) {
+    rphase_any<true, R>(pl, p, buf, LG, dLG, tw, gfirst && p == pl.np - 1, glast && p == 0, p < pl.np - 1, gl);
+    __syncthreads();
+  }
+}
+
+}  // namespace pmgpu

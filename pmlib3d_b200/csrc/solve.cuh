@@ -22,6 +22,7 @@
 
 #include "common.cuh"
 #include "fft.cuh"
+#include "regfft.cuh"
 
 namespace pmgpu {
 
@@ -43,6 +44,12 @@ template <typename R> struct SolveGeom {
   R eps2pi;                  // 2 pi epsilon (filter argument scale)
   int order;                 // filter order (poisson order or reg_order)
   int allper;                // all axes periodic: spectral Green's function
+  // in-place register FFTs along y and z (when the lengths factor into register radices)
+  int ry_ok, rz_ok;
+  RegPlan ry, rz;
+  const C *rtwy, *rtwz;      // w_n^q, q < n
+  const int *yk;             // row of the y spectrum -> ky index (nullptr: natural order)
+  const int *zk;             // position of the z transform -> kz index
 };
 
 enum ZMode { Z_VEL = 0, Z_VORT = 1, Z_VECPOT = 2, Z_REGULARISE = 3, Z_FORWARD = 4 };
@@ -122,6 +129,7 @@ struct LineTiles {
   int rows_out;   // rows written (truncation)
   long long in_os, in_rs, out_os, out_rs;
   int nouter, nkt, TK;
+  FastDiv dLG;    // division by the line vectors per row (register engine)
 };
 
 enum LMode { L_FWD = 0, L_INV = 1, L_Z = 2 };
@@ -159,7 +167,7 @@ __device__ __forceinline__ void tile_rows_store(typename cplx_t<R>::type *out, c
 // z-pass spectral multiply of one tile held in buffer V (complex view C)
 template <typename R, int NC>
 __device__ __forceinline__ void z_multiply(const SolveGeom<R> &g, typename cplx_t<R>::type *Cb, int L, int TK, int k0,
-                                           int y, int zmode, int reproj, int use_zeta) {
+                                           int y, int zmode, int reproj, int use_zeta, const int *zpos) {
   typedef typename cplx_t<R>::type C;
   const R twopi = R(6.283185307179586476925286766559);
   const int N = g.M[2];
@@ -167,9 +175,10 @@ __device__ __forceinline__ void z_multiply(const SolveGeom<R> &g, typename cplx_
   const R kyc = (2 * y == g.M[1]) ? R(0) : ky;  // Nyquist component dropped in the curl
   const int iy = min(y, g.M[1] - y);
   for (int t = threadIdx.x; t < N * TK; t += blockDim.x) {
-    const int z = t / TK, kk = t - z * TK;
+    const int q = t / TK, kk = t - q * TK;
+    const int z = zpos ? zpos[q] : q;
     const int kx_i = k0 + kk;
-    C *v = Cb + z * L + kk * NC;
+    C *v = Cb + q * L + kk * NC;
     if (kx_i >= g.H) {
 #pragma unroll
       for (int c = 0; c < NC; c++) v[c] = mk(R(0), R(0));
@@ -276,7 +285,8 @@ __global__ void __launch_bounds__(PASS_THREADS, 1) k_lines(SolveGeom<R> g, LineT
     } else {
       res = vfft_chain<false, R>(S, A, B, LG, sd, tw, lm, hook);
       if (lmode == L_Z) {
-        z_multiply<R, NC>(g, reinterpret_cast<C *>(res), L, TK, kt * TK, o, zmode, reproj, use_zeta);
+        z_multiply<R, NC>(g, reinterpret_cast<C *>(res), L, TK, kt * TK, g.yk ? g.yk[o] : o, zmode, reproj,
+                          use_zeta, nullptr);
         __syncthreads();
         res = vfft_chain<true, R>(res, A, B, LG, sd, tw, lm, NoHook());
       }
@@ -286,6 +296,61 @@ __global__ void __launch_bounds__(PASS_THREADS, 1) k_lines(SolveGeom<R> g, LineT
     __syncthreads();
   }
   cp_async_wait_all();
+}
+
+// Register-engine version of k_lines (lmode L_FWD along y, L_INV along y, L_Z):
+// one tile buffer per CTA, transformed in place; the first phase reads the rows
+// from global memory (zero padding not read) and the last phase writes them back
+// (truncation not written).  Forward y output rows are stored in digit-reversed
+// order (row -> ky through g.yk); the z pass keeps its spectrum digit-reversed in
+// shared memory (position -> kz through g.zk).  Several CTAs share an SM so that
+// one CTA's loads overlap another's transforms.
+constexpr int RL_THREADS = 256;
+
+template <typename R, int NC>
+__global__ void __launch_bounds__(RL_THREADS, 2) k_rlines(SolveGeom<R> g, LineTiles lt,
+                                                          const typename cplx_t<R>::type *in,
+                                                          typename cplx_t<R>::type *out, int axis, int lmode,
+                                                          int zmode, int reproj, int use_zeta) {
+  typedef typename cplx_t<R>::type C;
+  typedef typename Vec<R>::V V;
+  constexpr int G = Vec<R>::G;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const RegPlan &pl = (axis == 1) ? g.ry : g.rz;
+  const int n = pl.n, TK = lt.TK, L = NC * TK, LG = L / G;
+  C *tw = reinterpret_cast<C *>(smem_raw);
+  int *zpos = reinterpret_cast<int *>(smem_raw + (((size_t)n * sizeof(C) + 15) & ~(size_t)15));
+  V *buf = reinterpret_cast<V *>(smem_raw + (((size_t)n * sizeof(C) + 15) & ~(size_t)15) +
+                                 (((size_t)n * sizeof(int) + 15) & ~(size_t)15));
+  {
+    const C *twg = (axis == 1) ? g.rtwy : g.rtwz;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = twg[i];
+    if (lmode == L_Z)
+      for (int i = threadIdx.x; i < n; i += blockDim.x) zpos[i] = g.zk[i];
+  }
+  __syncthreads();
+  const int ntiles = lt.nouter * lt.nkt;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int o = tile / lt.nkt, kt = tile - o * lt.nkt;
+    PhaseGlobal gl;
+    gl.in = in + (o * lt.in_os + (long long)kt * TK) * NC;
+    gl.out = out + (o * lt.out_os + (long long)kt * TK) * NC;
+    gl.rs_in = lt.in_rs * NC;
+    gl.rs_out = lt.out_rs * NC;
+    gl.rows_in = lt.rows_in;
+    gl.rows_out = lt.rows_out;
+    if (lmode == L_FWD) {
+      rfft_fwd<R>(pl, buf, LG, lt.dLG, tw, true, true, gl);
+    } else if (lmode == L_INV) {
+      rfft_inv<R>(pl, buf, LG, lt.dLG, tw, true, true, gl);
+    } else {
+      rfft_fwd<R>(pl, buf, LG, lt.dLG, tw, true, false, gl);
+      z_multiply<R, NC>(g, reinterpret_cast<C *>(buf), L, TK, kt * TK, g.yk ? g.yk[o] : o, zmode, reproj, use_zeta,
+                        zpos);
+      __syncthreads();
+      rfft_inv<R>(pl, buf, LG, lt.dLG, tw, false, true, gl);
+    }
+  }
 }
 
 // ---------------------------------------------------------------- x forward (R2C)

@@ -204,6 +204,12 @@ def pmlib_interp_particle_mesh_noalloc(topo: Topo, params: Params, d_xpart: int,
                                                     C.c_void_p(stream))
 
 
+def fft_engine(engine: int) -> int:
+    """Line-FFT engine of plans created afterwards: 0 = register passes where the
+    lengths allow (default), 1 = Stockham passes.  Returns the previous setting."""
+    return lib().pmgpu_fft_engine(int(engine))
+
+
 def step(plan: Plan, pos, part_vort, part_vel) -> int:
     """One vortex step through host arrays: P2M (clear), unbounded solve and curl,
     M2P of the velocity into ``part_vel``."""

@@ -94,6 +94,56 @@ def test_solve_fp32(name, xmin, xmax, dx, bc, ng):
     assert rel_l2(vel, vel_o) < TOL32, rel_l2(vel, vel_o)
 
 
+# grids whose y or z FFT length needs three register phases (M = 528 = 16*11*3,
+# 264 = 12*11*2, periodic 240 = 12*10*2) or two with radix 17 / 13 (272, 208)
+LONG_CASES = [
+    ("fff-y528", (-1, -16, -1), (1, 16, 1), (0.125,) * 3, (0, 0, 0), 4),
+    ("fff-z264", (-1, -1, -7.75), (1, 1, 7.75), (0.125,) * 3, (0, 0, 0), 4),
+    ("pff-y240", (0, 0, -1), (2, 30, 1), (0.125,) * 3, (1, 1, 0), 4),
+    ("fff-y272-z208", (-1, -8, -6), (1, 8, 6), (0.125,) * 3, (0, 0, 0), 4),
+]
+
+
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", LONG_CASES)
+@pytest.mark.parametrize("prec", [P.FP64, P.FP32])
+def test_solve_register_phases(name, xmin, xmax, dx, bc, ng, prec):
+    po, to, qo, pg, tg, qg = setup_pair(xmin, xmax, dx, bc, ng, interp=3, order=6)
+    w = gaussian_field(to, seed=8, noise=0.01)
+    vel_o, vort_o, vp_o = oracle_solve(po, to, qo, w, reg_vort=True, calc_vecpot=True)
+    dt = np.float64 if prec == P.FP64 else np.float32
+    ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, prec)
+    assert ierr == 0, P.last_error()
+    vel = np.zeros(w.shape, dt)
+    vp = np.zeros(w.shape, dt)
+    wg = w.astype(dt)
+    assert P.pmlib_poisson_solve(plan, wg, vel, vp, reg_vort=True, calc_vecpot=True) == 0
+    tol = TOL64 if prec == P.FP64 else TOL32
+    assert rel_l2(vel, vel_o) < tol, rel_l2(vel, vel_o)
+    assert rel_l2(wg, vort_o) < tol
+    assert rel_l2(vp, vp_o) < tol
+
+
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", [CASES[0], CASES[1], CASES[2], CASES[5], LONG_CASES[0]])
+@pytest.mark.parametrize("prec", [P.FP64, P.FP32])
+def test_fft_engines_agree(name, xmin, xmax, dx, bc, ng, prec):
+    """The register passes and the Stockham passes give the same solve to round-off."""
+    po, to, qo, pg, tg, qg = setup_pair(xmin, xmax, dx, bc, ng, interp=3, order=6)
+    w = gaussian_field(to, seed=9, noise=0.01)
+    dt = np.float64 if prec == P.FP64 else np.float32
+    outs = []
+    for engine in (1, 0):
+        old = P.fft_engine(engine)
+        try:
+            ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, prec)
+        finally:
+            P.fft_engine(old)
+        assert ierr == 0
+        vel = np.zeros(w.shape, dt)
+        assert P.pmlib_poisson_solve(plan, w.astype(dt), vel) == 0
+        outs.append(vel)
+    assert rel_l2(outs[1], outs[0]) < (1e-14 if prec == P.FP64 else 1e-6), rel_l2(outs[1], outs[0])
+
+
 def test_mixedbc_convergence_pin_on_gpu():
     """The GPU FP64 solve reproduces validation/mixedbc__/convergence.dat (h = 1/16, 1/32)."""
     def gpu_solver(patch, t, par, vort, reg_vort=True, calc_vecpot=False):
@@ -146,6 +196,34 @@ def test_p2m_fp64(name, xmin, xmax, dx, bc, ng, interp):
     mg2 = np.zeros(P.topo_shape(tg))
     assert P.pmlib_interp_particle_mesh(tg, qg, pos, val, mg2, clear=True) == 0
     assert np.array_equal(mg, mg2)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_p2m_crowded_bins(precision):
+    """Collisions: bins holding 2..32 particles (thread fix-up), 100 and 3000 (one
+    shared-memory chunk) and 12000 (chunks + merges), interleaved in index order with
+    an ordinary lattice; same result as the oracle and bit-identical on a rerun."""
+    po, to, qo, pg, tg, qg = setup_pair(*CASES[0][1:])
+    lat, lval = jittered_particles(to, seed=11, jitter=0.3)
+    rng = np.random.default_rng(12)
+    groups = [lat]
+    for cnt, at in ((100, (0.1, 0.2, -0.3)), (12000, (-0.4, 0.05, 0.5)), (3000, (0.7, -0.7, 0.0)), (17, (0.0, 0.0, 0.0))):
+        groups.append(np.asarray(at) + rng.uniform(-0.01, 0.01, (cnt, 3)))
+    pos = np.concatenate(groups)
+    perm = rng.permutation(pos.shape[0])  # crowded particles scattered through the index range
+    pos = np.ascontiguousarray(pos[perm])
+    val = rng.standard_normal(pos.shape)
+    to.npart = tg.npart = pos.shape[0]
+    mo = np.zeros(O.topo_shape(to))
+    assert O.interp_particle_mesh(to, 3, pos, val, mo) == 0
+    dt = np.float64 if precision == "fp64" else np.float32
+    runs = []
+    for _ in range(2):
+        mg = np.zeros(P.topo_shape(tg), dt)
+        assert P.pmlib_interp_particle_mesh(tg, qg, pos.astype(dt), val.astype(dt), mg, clear=True) == 0
+        runs.append(mg)
+    assert rel_l2(runs[0], mo) < (1e-13 if precision == "fp64" else 1e-5), rel_l2(runs[0], mo)
+    assert np.array_equal(runs[0], runs[1])
 
 
 def test_p2m_accumulate_and_clear_ghost():
