@@ -321,28 +321,63 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const unsigned *__r
 
 // ------------------------------------------------------------------ deposition (gather)
 // A CTA owns TX x TY cell columns and a chunk of ZC cell layers, and marches up the
-// bin layers.  For every bin layer it stages the particles of the (TX+W-1) x
-// (TY+W-1) bins that reach its columns in shared memory (weights precomputed), and
-// each thread adds them to a rolling window of W cell layers held in registers.
-// A cell layer is final once the last bin layer that reaches it has been added.
+// bin layers, DEP_LB at a time.  For each batch of bin layers it stages the
+// particles of the (TX+W-1) x (TY+W-1) bins of every layer that reach its columns
+// in shared memory with their weights, and each thread adds them to a rolling
+// window of W + DEP_LB - 1 cell layers held in registers.  The W bins of one bin
+// row that reach a cell column are consecutive in the sorted order, so a thread
+// walks one contiguous range of staged particles per bin row.  Per cell the order
+// is fixed (bin layer, bin row, bin, particle index), so the result is the same on
+// every run.  A cell layer is final once the last bin layer that reaches it has
+// been added.
 constexpr int DEP_TX = 32;
 constexpr int DEP_TY = 8;
+constexpr int DEP_THREADS = DEP_TX * DEP_TY;
+constexpr int DEP_LB = 4;
+
+template <int W> struct WStride { static constexpr int v = W == 4 ? 4 : 8; };
+
+// shared-memory bytes of k_deposit for `cap` staged particles
+template <typename R, int W> __host__ __device__ constexpr size_t deposit_smem(int cap) {
+  return (size_t)cap * (3 * WStride<W>::v + 4) * sizeof(R) + (size_t)cap * sizeof(int) +
+         sizeof(int) * (DEP_LB * (DEP_TY + W - 1) * (DEP_TX + W) + DEP_LB * (DEP_TY + W - 1) + 2);
+}
+
+template <typename R> __device__ __forceinline__ void lds4(const R *p, R *o);
+template <> __device__ __forceinline__ void lds4<float>(const float *p, float *o) {
+  const float4 v = *reinterpret_cast<const float4 *>(p);
+  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+template <> __device__ __forceinline__ void lds4<double>(const double *p, double *o) {
+  const double2 a = *reinterpret_cast<const double2 *>(p), b = *reinterpret_cast<const double2 *>(p + 2);
+  o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+template <typename R> __device__ __forceinline__ void sts4(R *p, R a, R b, R c, R d);
+template <> __device__ __forceinline__ void sts4<float>(float *p, float a, float b, float c, float d) {
+  *reinterpret_cast<float4 *>(p) = make_float4(a, b, c, d);
+}
+template <> __device__ __forceinline__ void sts4<double>(double *p, double a, double b, double c, double d) {
+  *reinterpret_cast<double2 *>(p) = make_double2(a, b);
+  *reinterpret_cast<double2 *>(p + 2) = make_double2(c, d);
+}
 
 template <typename R, int W, int NV>
-__global__ void __launch_bounds__(DEP_TX *DEP_TY) k_deposit(PartGeom<R> g, const R *__restrict__ pos,
-                                                            const R *__restrict__ val, int vstride,
-                                                            const unsigned *__restrict__ start,
-                                                            const int *__restrict__ perm, R *__restrict__ mesh,
-                                                            int mstride, int ZC, int cap, int clear_mode) {
-  constexpr int BX = DEP_TX + W - 1, BY = DEP_TY + W - 1;
+__global__ void __launch_bounds__(DEP_THREADS) k_deposit(PartGeom<R> g, const R *__restrict__ pos,
+                                                         const R *__restrict__ val, int vstride,
+                                                         const unsigned *__restrict__ start,
+                                                         const int *__restrict__ perm, R *__restrict__ mesh,
+                                                         int mstride, int ZC, int cap, int clear_mode) {
+  constexpr int BX = DEP_TX + W - 1, BY = DEP_TY + W - 1, WS = WStride<W>::v;
+  constexpr int NA = W + DEP_LB - 1;   // accumulator layers
+  constexpr int NROW = DEP_LB * BY;    // bin rows of one batch
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R *wxs = reinterpret_cast<R *>(smem_raw);  // [W][cap]
-  R *wys = wxs + W * cap;                    // [W][cap]
-  R *wzs = wys + W * cap;                    // [W][cap]
-  R *vs = wzs + W * cap;                     // [NV][cap]
-  int *btab = reinterpret_cast<int *>(vs + NV * cap);  // [BY][BX][2] concatenated ranges
-  int *rowg = btab + 2 * BX * BY;                      // [BY] global start of row
-  int *rowo = rowg + BY;                               // [BY+1] concatenated offset of row
+  R *wxs = reinterpret_cast<R *>(smem_raw);  // [cap][WS]
+  R *wys = wxs + (size_t)WS * cap;           // [cap][WS]
+  R *wzs = wys + (size_t)WS * cap;           // [cap][WS]
+  R *vs = wzs + (size_t)WS * cap;            // [cap][4]
+  int *sbx = reinterpret_cast<int *>(vs + (size_t)4 * cap);  // [cap] bin x within the tile
+  int *sraw = sbx + cap;                                     // [NROW][BX+1] start of bin (row clamp)
+  int *rowo = sraw + NROW * (BX + 1);                        // [NROW+1] staged offset of each row
 
   const int tx = threadIdx.x % DEP_TX, ty = threadIdx.x / DEP_TX;
   const int x0 = blockIdx.x * DEP_TX, y0 = blockIdx.y * DEP_TY;
@@ -350,96 +385,113 @@ __global__ void __launch_bounds__(DEP_TX *DEP_TY) k_deposit(PartGeom<R> g, const
   const int cx = x0 + tx, cy = y0 + ty;
   const bool active = cx < g.ext[0] && cy < g.ext[1];
 
-  // acc[s] is cell layer bz - (W - 1) + s while bin layer bz is added; after the
-  // layer acc[0] is final and the window shifts up by one
-  R acc[W][NV];
+  // acc[s] is cell layer bz0 - (W - 1) + s while the batch starting at bin layer
+  // bz0 is added; after the batch the first nl layers are final and the window
+  // shifts by nl
+  R acc[NA][NV];
 #pragma unroll
-  for (int s = 0; s < W; s++)
+  for (int s = 0; s < NA; s++)
 #pragma unroll
     for (int c = 0; c < NV; c++) acc[s][c] = R(0);
 
   const int bz_end = zc1 + W - 2;  // last bin layer (inclusive)
-  for (int bz = zc0; bz <= bz_end; bz++) {
-    // ---- row ranges of this bin layer
-    if (threadIdx.x < BY) {
-      const int r = threadIdx.x, by = y0 + r;
-      int gs = 0, ge = 0;
-      if (by < g.nb[1] && bz < g.nb[2] && x0 < g.nb[0]) {
+  for (int bz0 = zc0; bz0 <= bz_end; bz0 += DEP_LB) {
+    const int nl = min(DEP_LB, bz_end - bz0 + 1);
+    // ---- bin starts of the batch's rows (clamped to the row end)
+    for (int i = threadIdx.x; i < NROW * (BX + 1); i += blockDim.x) {
+      const int row = i / (BX + 1), bx = i - row * (BX + 1);
+      const int l = row / BY, r = row - l * BY;
+      const int by = y0 + r, bz = bz0 + l;
+      int v = 0;
+      if (l < nl && by < g.nb[1] && bz < g.nb[2] && x0 < g.nb[0]) {
         const unsigned rb = (unsigned)g.nb[0] * ((unsigned)by + (unsigned)g.nb[1] * (unsigned)bz);
-        const int xl = min(x0 + BX, g.nb[0]);
-        gs = (int)start[rb + x0];
-        ge = (int)start[rb + xl];
+        v = (int)start[rb + (unsigned)min(x0 + bx, g.nb[0])];
       }
-      rowg[r] = gs;
-      rowo[r + 1] = ge - gs;
+      sraw[i] = v;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      rowo[0] = 0;
-      for (int r = 0; r < BY; r++) rowo[r + 1] += rowo[r];
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < BX * BY; i += blockDim.x) {
-      const int r = i / BX, bx = i - r * BX;
-      const int by = y0 + r, gx = x0 + bx;
-      int cs = 0, ce = 0;
-      if (by < g.nb[1] && bz < g.nb[2] && gx < g.nb[0]) {
-        const unsigned b = (unsigned)gx + (unsigned)g.nb[0] * ((unsigned)by + (unsigned)g.nb[1] * (unsigned)bz);
-        cs = rowo[r] + ((int)start[b] - rowg[r]);
-        ce = rowo[r] + ((int)start[b + 1] - rowg[r]);
+    if (threadIdx.x < 32) {
+      // exclusive prefix of the row lengths, two rows per lane (NROW <= 64)
+      const int lane = threadIdx.x;
+      const int r0 = 2 * lane, r1 = 2 * lane + 1;
+      const int l0 = r0 < NROW ? sraw[r0 * (BX + 1) + BX] - sraw[r0 * (BX + 1)] : 0;
+      const int l1 = r1 < NROW ? sraw[r1 * (BX + 1) + BX] - sraw[r1 * (BX + 1)] : 0;
+      int x = l0 + l1;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
       }
-      btab[2 * i] = cs;
-      btab[2 * i + 1] = ce;
+      const int ex = x - l0 - l1;
+      if (r0 <= NROW) rowo[r0] = ex;
+      if (r1 <= NROW) rowo[r1] = ex + l0;
     }
-    const int total = rowo[BY];
     __syncthreads();
+    const int total = rowo[NROW];
     for (int c0 = 0; c0 < total; c0 += cap) {
       const int c1 = min(total, c0 + cap);
       // ---- stage particles [c0, c1) with their weights
       for (int q = c0 + threadIdx.x; q < c1; q += blockDim.x) {
-        int r = 0;
-        while (r + 1 < BY && rowo[r + 1] <= q) r++;
-        const int gi = rowg[r] + (q - rowo[r]);
+        int lo = 0, hi = NROW - 1;  // last row with rowo[row] <= q
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (rowo[mid] <= q) lo = mid;
+          else hi = mid - 1;
+        }
+        const int gi = sraw[lo * (BX + 1)] + (q - rowo[lo]);
         const int p = perm[gi];
         const int i = q - c0;
-        R wv[3][W];
+        R wv[3][WS];
+        long long bxi = 0;
 #pragma unroll
         for (int e = 0; e < 3; e++) {
           const R x = pos[(size_t)3 * p + e];
           const long long b = base_index(x, g.xmin[e], g.c1dx[e]);
+          if (e == 0) bxi = b;
           weights<R, W>(cell_offset<R>(x, g.xmin[e], g.dx[e], b, g.c1dx[e]), wv[e]);
+#pragma unroll
+          for (int t = W; t < WS; t++) wv[e][t] = R(0);
         }
 #pragma unroll
-        for (int s = 0; s < W; s++) {
-          wxs[s * cap + i] = wv[0][s];
-          wys[s * cap + i] = wv[1][s];
-          wzs[s * cap + i] = wv[2][s];
+        for (int t = 0; t < WS; t += 4) {
+          sts4<R>(wxs + i * WS + t, wv[0][t], wv[0][t + 1], wv[0][t + 2], wv[0][t + 3]);
+          sts4<R>(wys + i * WS + t, wv[1][t], wv[1][t + 1], wv[1][t + 2], wv[1][t + 3]);
+          sts4<R>(wzs + i * WS + t, wv[2][t], wv[2][t + 1], wv[2][t + 2], wv[2][t + 3]);
         }
+        R vv[4] = {R(0), R(0), R(0), R(0)};
 #pragma unroll
-        for (int c = 0; c < NV; c++) vs[c * cap + i] = val[(size_t)vstride * p + c];
+        for (int c = 0; c < NV; c++) vv[c] = val[(size_t)vstride * p + c];
+        sts4<R>(vs + i * 4, vv[0], vv[1], vv[2], vv[3]);
+        sbx[i] = (int)(bxi - g.blo[0]) - x0;
       }
       __syncthreads();
       if (active) {
+#pragma unroll
+        for (int l = 0; l < DEP_LB; l++) {
+          if (l < nl) {
 #pragma unroll 1
-        for (int ry = 0; ry < W; ry++) {
-          const int r = ty + ry;      // bin row in the tile
-          const int sy = W - 1 - ry;  // stencil position of this cell row
+            for (int ry = 0; ry < W; ry++) {
+              const int row = l * BY + ty + ry;  // bin row of the batch
+              const int sy = W - 1 - ry;         // stencil position of this cell row
+              const int *sr = sraw + row * (BX + 1);
+              const int b0 = sr[0];
+              const int lo = max(rowo[row] + sr[tx] - b0, c0);
+              const int hi = min(rowo[row] + sr[tx + W] - b0, c1);
 #pragma unroll 1
-          for (int rx = 0; rx < W; rx++) {
-            const int sx = W - 1 - rx;
-            const int bi = r * BX + tx + rx;
-            const int lo = max(btab[2 * bi], c0), hi = min(btab[2 * bi + 1], c1);
-            for (int q = lo; q < hi; q++) {
-              const int i = q - c0;
-              const R wxy = wxs[sx * cap + i] * wys[sy * cap + i];
-              R v[NV];
+              for (int q = lo; q < hi; q++) {
+                const int i = q - c0;
+                const int sx = W - 1 - (sbx[i] - tx);
+                const R wxy = wxs[i * WS + sx] * wys[i * WS + sy];
+                R wz[WS], v[4];
+                lds4<R>(wzs + i * WS, wz);
+                if constexpr (WS == 8) lds4<R>(wzs + i * WS + 4, wz + 4);
+                lds4<R>(vs + i * 4, v);
 #pragma unroll
-              for (int c = 0; c < NV; c++) v[c] = vs[c * cap + i];
+                for (int sz = 0; sz < W; sz++) {
+                  const R w = wxy * wz[sz];
 #pragma unroll
-              for (int sz = 0; sz < W; sz++) {
-                const R w = wxy * wzs[sz * cap + i];
-#pragma unroll
-                for (int c = 0; c < NV; c++) acc[sz][c] += w * v[c];
+                  for (int c = 0; c < NV; c++) acc[l + sz][c] += w * v[c];
+                }
               }
             }
           }
@@ -447,22 +499,25 @@ __global__ void __launch_bounds__(DEP_TX *DEP_TY) k_deposit(PartGeom<R> g, const
       }
       __syncthreads();
     }
-    // ---- cell layer bz - (W - 1) is complete
-    const int cz = bz - (W - 1);
-    if (active && cz >= zc0 && cz < zc1) {
-      const size_t m = (((size_t)cz * g.ext[1] + cy) * g.ext[0] + cx) * mstride;
-      const int ii = cx + g.lo[0], jj = cy + g.lo[1], kk = cz + g.lo[2];
-      const bool ghost = ii < 1 || ii > g.nint[0] || jj < 1 || jj > g.nint[1] || kk < 1 || kk > g.nint[2];
-      const bool overwrite = clear_mode == 1 || (clear_mode == 2 && ghost);
+    // ---- cell layers bz0 - (W - 1) .. + nl - 1 are complete
 #pragma unroll
-      for (int c = 0; c < NV; c++) mesh[m + c] = overwrite ? acc[0][c] : mesh[m + c] + acc[0][c];
+    for (int l = 0; l < DEP_LB; l++) {
+      const int cz = bz0 - (W - 1) + l;
+      if (l < nl && active && cz >= zc0 && cz < zc1) {
+        const size_t m = (((size_t)cz * g.ext[1] + cy) * g.ext[0] + cx) * mstride;
+        const int ii = cx + g.lo[0], jj = cy + g.lo[1], kk = cz + g.lo[2];
+        const bool ghost = ii < 1 || ii > g.nint[0] || jj < 1 || jj > g.nint[1] || kk < 1 || kk > g.nint[2];
+        const bool overwrite = clear_mode == 1 || (clear_mode == 2 && ghost);
+#pragma unroll
+        for (int c = 0; c < NV; c++) mesh[m + c] = overwrite ? acc[l][c] : mesh[m + c] + acc[l][c];
+      }
     }
+    if (nl == DEP_LB) {
 #pragma unroll
-    for (int s = 0; s + 1 < W; s++)
+      for (int s = 0; s < NA; s++)
 #pragma unroll
-      for (int c = 0; c < NV; c++) acc[s][c] = acc[s + 1][c];
-#pragma unroll
-    for (int c = 0; c < NV; c++) acc[W - 1][c] = R(0);
+        for (int c = 0; c < NV; c++) acc[s][c] = (s + DEP_LB < NA) ? acc[s + DEP_LB][c] : R(0);
+    }  // a shorter batch is the last one
   }
 }
 
@@ -498,12 +553,14 @@ __global__ void k_ghost_add(R *__restrict__ mesh, int ex, int ey, int ez, int nv
 // source/interpolation/pmlib_interp_mesh_particle.f:76-409 (M4'), :412-1266 (M6*):
 // stencil indices clamp to the cuboid with zero weight, no particle is skipped, and
 // the M4' branch scales the y and z offsets by 1/dx(1) (:115-116).
+// Particles order[i] for i in [first ? *first : 0, n).
 template <typename R, int W>
 __global__ void k_m2p(PartGeom<R> g, const R *__restrict__ pos, const int *__restrict__ order, int n,
-                      const R *__restrict__ f0, const R *__restrict__ f1, const R *__restrict__ f2,
-                      R *__restrict__ o0, R *__restrict__ o1, R *__restrict__ o2) {
+                      const unsigned *__restrict__ first, const R *__restrict__ f0, const R *__restrict__ f1,
+                      const R *__restrict__ f2, R *__restrict__ o0, R *__restrict__ o1, R *__restrict__ o2) {
   constexpr int off = Stencil<W>::off;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const int i0 = first ? (int)*first : 0;
+  for (int i = i0 + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int p = order ? order[i] : i;
     R w[3][W];
     int idx[3][W];
@@ -550,6 +607,122 @@ __global__ void k_m2p(PartGeom<R> g, const R *__restrict__ pos, const int *__res
       os[f][(size_t)3 * p + 1] = a1;
       os[f][(size_t)3 * p + 2] = a2;
     }
+  }
+}
+
+// M2P over particles sorted by bin (the order of the preceding deposition): a CTA
+// owns TX x TY x TZ bins, stages the cells their stencils reach in shared memory
+// (one 16- or 32-byte vector per cell, zero outside the cuboid, where the weight is
+// zero as well) and interpolates the particles of those bins from there.  The
+// particles of one bin row are one contiguous range of the sorted order.  Same
+// index and weight rules as k_m2p; particles with the sentinel key (outside every
+// bin) are left to k_m2p.
+constexpr int M2P_TX = 32, M2P_TY = 8, M2P_TZ = 4, M2P_THREADS = 256;
+
+template <typename R, int W> __host__ __device__ constexpr size_t m2p_tile_smem() {
+  return (size_t)(M2P_TX + W - 1) * (M2P_TY + W - 1) * (M2P_TZ + W - 1) * 4 * sizeof(R);
+}
+
+template <typename R, int W>
+__global__ void __launch_bounds__(M2P_THREADS) k_m2p_tile(PartGeom<R> g, const R *__restrict__ pos,
+                                                          const unsigned *__restrict__ start,
+                                                          const int *__restrict__ perm, const R *__restrict__ f,
+                                                          R *__restrict__ o) {
+  constexpr int off = Stencil<W>::off;
+  constexpr int CX = M2P_TX + W - 1, CY = M2P_TY + W - 1, CZ = M2P_TZ + W - 1, NR = M2P_TY * M2P_TZ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *cells = reinterpret_cast<R *>(smem_raw);  // [CZ][CY][CX][4]
+  __shared__ int rs[NR + 1], rg[NR];
+  const int x0 = blockIdx.x * M2P_TX, y0 = blockIdx.y * M2P_TY, z0 = blockIdx.z * M2P_TZ;
+  const int cx0 = x0 - (W - 1), cy0 = y0 - (W - 1), cz0 = z0 - (W - 1);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  // ---- stage the cells: one warp per cell row, lanes along the row's 3 CX values
+  {
+    const int xa = max(cx0, 0), xb = min(cx0 + CX, g.ext[0]);  // cells present in the cuboid
+    for (int row = wid; row < CZ * CY; row += nw) {
+      const int yy = row % CY, zz = row / CY;
+      const int cy = cy0 + yy, cz = cz0 + zz;
+      R *dst = cells + (size_t)row * CX * 4;
+      const bool rowin = cy >= 0 && cy < g.ext[1] && cz >= 0 && cz < g.ext[2];
+      const R *src = f + (((size_t)cz * g.ext[1] + cy) * g.ext[0]) * 3;
+      for (int e = lane; e < CX * 3; e += 32) {
+        const int xx = e / 3, c = e - 3 * xx;
+        const int cx = cx0 + xx;
+        R v = R(0);
+        if (rowin && cx >= xa && cx < xb) v = __ldg(src + (size_t)cx * 3 + c);
+        dst[xx * 4 + c] = v;
+      }
+    }
+  }
+  // ---- particle ranges of the bin rows
+  if (threadIdx.x < 32) {
+    int len = 0, gs = 0;
+    if (lane < NR) {
+      const int by = y0 + lane % M2P_TY, bz = z0 + lane / M2P_TY;
+      if (by < g.nb[1] && bz < g.nb[2]) {
+        const unsigned rb = (unsigned)g.nb[0] * ((unsigned)by + (unsigned)g.nb[1] * (unsigned)bz);
+        gs = (int)start[rb + x0];
+        len = (int)start[rb + (unsigned)min(x0 + M2P_TX, g.nb[0])] - gs;
+      }
+      rg[lane] = gs;
+    }
+    int x = len;
+#pragma unroll
+    for (int o2 = 1; o2 < 32; o2 <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o2);
+      if (lane >= o2) x += y;
+    }
+    if (lane < NR) rs[lane] = x - len;
+    if (lane == NR - 1) rs[NR] = x;
+  }
+  __syncthreads();
+  const int total = rs[NR];
+  for (int q = threadIdx.x; q < total; q += blockDim.x) {
+    int lo = 0, hi = NR - 1;  // last row with rs[row] <= q
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (rs[mid] <= q) lo = mid;
+      else hi = mid - 1;
+    }
+    const int p = perm[rg[lo] + (q - rs[lo])];
+    R w[3][W];
+    int tb[3];
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+      const R x = pos[(size_t)3 * p + e];
+      const int b = (int)base_index(x, g.xmin[e], g.c1dx[e]);  // a binned particle has a small index
+      const R scale = (W == 4) ? g.c1dx[0] : g.c1dx[e];
+      weights<R, W>(cell_offset<R>(x, g.xmin[e], g.dx[e], (long long)b, scale), w[e]);
+      const int lo_e = g.lo[e], hi_e = g.lo[e] + g.ext[e] - 1;
+#pragma unroll
+      for (int s2 = 0; s2 < W; s2++) {
+        const int ii = b - off + s2;
+        if (ii < lo_e || ii > hi_e) w[e][s2] = R(0);
+      }
+      // first stencil cell relative to the tile: bin - tile origin
+      tb[e] = b - g.blo[e] - (e == 0 ? x0 : e == 1 ? y0 : z0);
+    }
+    const R *base = cells + ((tb[2] * CY + tb[1]) * CX + tb[0]) * 4;
+    R a0 = R(0), a1 = R(0), a2 = R(0);
+#pragma unroll
+    for (int sk = 0; sk < W; sk++)
+#pragma unroll
+      for (int sj = 0; sj < W; sj++) {
+        const R wjk = w[1][sj] * w[2][sk];
+        const R *row = base + (sk * CY + sj) * CX * 4;
+#pragma unroll
+        for (int si = 0; si < W; si++) {
+          const R wt = w[0][si] * wjk;
+          R v[4];
+          lds4<R>(row + si * 4, v);
+          a0 += wt * v[0];
+          a1 += wt * v[1];
+          a2 += wt * v[2];
+        }
+      }
+    o[(size_t)3 * p + 0] = a0;
+    o[(size_t)3 * p + 1] = a1;
+    o[(size_t)3 * p + 2] = a2;
   }
 }
 

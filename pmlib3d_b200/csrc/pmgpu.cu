@@ -471,12 +471,11 @@ static int run_p2m(const pmgpu_topo *t, int order, const R *pos, const R *val, i
   // deposition, components in groups of at most three
   const int zc = (W == 4) ? 32 : 30;
   dim3 grid((g.ext[0] + DEP_TX - 1) / DEP_TX, (g.ext[1] + DEP_TY - 1) / DEP_TY, (g.ext[2] + zc - 1) / zc);
-  const int BX = DEP_TX + W - 1, BY = DEP_TY + W - 1;
   for (int c0 = 0; c0 < nvar;) {
     const int nv = (nvar - c0 >= 3) ? 3 : 1;
     int cap = (sizeof(R) == 4) ? 1024 : 512;
     if (W == 6) cap = cap * 3 / 4;
-    const size_t smem = (size_t)cap * (3 * W + nv) * sizeof(R) + sizeof(int) * (2 * BX * BY + 2 * BY + 2);
+    const size_t smem = (W == 4) ? deposit_smem<R, 4>(cap) : deposit_smem<R, 6>(cap);
     const R *vp = val + c0;
     R *mp = mesh + c0;
     const int *pp = perm;
@@ -485,7 +484,7 @@ static int run_p2m(const pmgpu_topo *t, int order, const R *pos, const R *val, i
     CK(cudaFuncSetAttribute(k_deposit<R, WW, NVV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), \
        caller);                                                                                            \
     KTimer kt_(KC_DEPOSIT, st);                                                                            \
-    k_deposit<R, WW, NVV><<<grid, DEP_TX * DEP_TY, smem, st>>>(g, pos, vp, nvar, s.start->as<unsigned>(),   \
+    k_deposit<R, WW, NVV><<<grid, DEP_THREADS, smem, st>>>(g, pos, vp, nvar, s.start->as<unsigned>(),      \
                                                                 pp, mp, nvar_mesh, zc, cap, clear_mode);    \
     PM_LAUNCHED();                                                                                         \
   }
@@ -516,11 +515,38 @@ static int run_m2p(const pmgpu_topo *t, int order, const R *pos, const int *ord,
   const int W = (order == 3) ? 4 : 6;
   PartGeom<R> g = part_geom<R>(t, W);
   const int nblk = std::min((n + 127) / 128, 148 * 32);
-  if (W == 4) { KTimer kt_(KC_M2P, st); k_m2p<R, 4><<<nblk, 128, 0, st>>>(g, pos, ord, n, f0, f1, f2, o0, o1, o2); }
-  else { KTimer kt_(KC_M2P, st); k_m2p<R, 6><<<nblk, 128, 0, st>>>(g, pos, ord, n, f0, f1, f2, o0, o1, o2); }
+  if (W == 4) { KTimer kt_(KC_M2P, st); k_m2p<R, 4><<<nblk, 128, 0, st>>>(g, pos, ord, n, nullptr, f0, f1, f2, o0, o1, o2); }
+  else { KTimer kt_(KC_M2P, st); k_m2p<R, 6><<<nblk, 128, 0, st>>>(g, pos, ord, n, nullptr, f0, f1, f2, o0, o1, o2); }
   PM_LAUNCHED();
   CKL(caller);
   return 0;
+}
+
+// M2P of one field for particles already sorted by bin (perm, start of the
+// deposition with the same positions): tiles of bins through shared memory, then
+// the particles outside every bin (the tail of perm) one by one.
+template <typename R, int W>
+static int run_m2p_sorted_w(const pmgpu_topo *t, const R *pos, const unsigned *start, const int *perm, int n,
+                            const R *f, R *o, cudaStream_t st, const char *caller) {
+  PartGeom<R> g = part_geom<R>(t, W);
+  const size_t sm = m2p_tile_smem<R, W>();
+  CK(cudaFuncSetAttribute(k_m2p_tile<R, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+  dim3 grid((g.nb[0] + M2P_TX - 1) / M2P_TX, (g.nb[1] + M2P_TY - 1) / M2P_TY, (g.nb[2] + M2P_TZ - 1) / M2P_TZ);
+  { KTimer kt_(KC_M2P, st); k_m2p_tile<R, W><<<grid, M2P_THREADS, sm, st>>>(g, pos, start, perm, f, o); }
+  PM_LAUNCHED();
+  const int nblk = std::min((n + 127) / 128, 148 * 8);
+  { KTimer kt_(KC_M2P, st);
+    k_m2p<R, W><<<nblk, 128, 0, st>>>(g, pos, perm, n, start + g.nbins, nullptr, nullptr, f, nullptr, nullptr, o); }
+  PM_LAUNCHED();
+  CKL(caller);
+  return 0;
+}
+template <typename R>
+static int run_m2p_sorted(const pmgpu_topo *t, int order, const R *pos, const unsigned *start, const int *perm,
+                          int n, const R *f, R *o, cudaStream_t st, const char *caller) {
+  if (n <= 0) return 0;
+  return order == 3 ? run_m2p_sorted_w<R, 4>(t, pos, start, perm, n, f, o, st, caller)
+                    : run_m2p_sorted_w<R, 6>(t, pos, start, perm, n, f, o, st, caller);
 }
 
 // ------------------------------------------------------------------ solve driver
@@ -1142,8 +1168,8 @@ static int step_dev(pmgpu_plan *pl, const R *pos, const R *pv, int n, R *pvel, c
   if (run_p2m<R>(&t, pl->par.interpolation_order, pos, pv, 3, n, pl->mesh_w.as<R>(), 3, 1, r, st, &perm, caller))
     return -1;
   if (run_solve<R>(pl, pl->mesh_w.as<R>(), pl->mesh_u.as<R>(), nullptr, nullptr, 0, 0, 0, st, caller)) return -1;
-  if (run_m2p<R>(&t, pl->par.interpolation_order, pos, perm, n, nullptr, nullptr, pl->mesh_u.as<R>(), nullptr,
-                 nullptr, pvel, st, caller))
+  if (run_m2p_sorted<R>(&t, pl->par.interpolation_order, pos, pl->start.as<unsigned>(), perm, n,
+                        pl->mesh_u.as<R>(), pvel, st, caller))
     return -1;
   return 0;
 }

@@ -307,6 +307,31 @@ def test_step_fp64_and_fp32(name, xmin, xmax, dx, bc, ng):
     assert rel_l2(up32, up_o) < TOL32
 
 
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", [CASES[0], CASES[2]])
+@pytest.mark.parametrize("interp", [3, 4])
+def test_step_stray_particles(name, xmin, xmax, dx, bc, ng, interp):
+    """Step with particles outside the cuboid, beyond periodic faces and in ghost
+    cells: they are skipped by P2M but still interpolated by M2P."""
+    po, to, qo, pg, tg, qg = setup_pair(xmin, xmax, dx, bc, ng, interp=interp, order=6)
+    pos, val = jittered_particles(to, seed=18, jitter=0.45, incl_ghost=True)
+    rng = np.random.default_rng(19)
+    span = np.array([to.xmax[d] - to.xmin[d] for d in range(3)])
+    lo = np.array([to.xmin[d] for d in range(3)])
+    stray = lo + rng.uniform(-0.3, 1.3, (400, 3)) * span
+    pos = np.ascontiguousarray(np.concatenate([pos, stray])[rng.permutation(pos.shape[0] + 400)])
+    val = np.ascontiguousarray(rng.standard_normal(pos.shape) * 0.1)
+    to.npart = pos.shape[0]
+    mo = np.zeros(O.topo_shape(to))
+    assert O.interp_particle_mesh(to, interp, pos, val, mo) == 0
+    vel_o, _, _ = oracle_solve(po, to, qo, mo)
+    ierr, up_o = O.interp_mesh_particle(to, interp, vel_o, pos)
+    for prec, dt, tol in ((P.FP64, np.float64, TOL64), (P.FP32, np.float32, TOL32)):
+        ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, prec)
+        up = np.zeros(pos.shape, dt)
+        assert P.step(plan, pos.astype(dt), val.astype(dt), up) == 0
+        assert rel_l2(up, up_o) < tol, (prec, rel_l2(up, up_o))
+
+
 def test_fft_lengths_with_generic_radix():
     """Periodic axes of any even length, including large prime factors (2 x 23, 2 x 37)."""
     po, to, qo, pg, tg, qg = setup_pair((0, 0, -0.5), (46 / 32, 74 / 32, 0.5), (1 / 32,) * 3, (1, 1, 0), 4)
