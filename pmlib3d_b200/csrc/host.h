@@ -66,6 +66,26 @@ static inline int pick_tk_reg(int n, int nc, size_t csize, int Hp) {
     }
   return 0;
 }
+// rows per tile of the register-engine x passes (table bytes + staging + buffer),
+// two CTAs per SM if possible
+static inline int pick_rb_reg(int N, int H, int P0, int Hp, int nc, size_t csize, size_t rsize, bool inverse) {
+  const size_t tabs = (((size_t)N * csize + 15) & ~(size_t)15) + (((size_t)H * csize + 15) & ~(size_t)15) +
+                      (((size_t)N * 4 + 15) & ~(size_t)15);
+  for (size_t budget : {(size_t)112 * 1024, PASS_SMEM_BUDGET})
+    for (int rb = 16; rb >= 1; rb--) {
+      if (csize == 8 && (nc * rb) % 2) continue;
+      const size_t stage = inverse ? (size_t)rb * Hp * nc * csize : (((size_t)rb * P0 * nc * rsize + 15) / 16) * 16;
+      if (tabs + stage + (size_t)nc * rb * N * csize <= budget) return rb;
+    }
+  return 0;
+}
+static inline size_t rx_smem(int N, int H, int P0, int Hp, int nc, int rb, size_t csize, size_t rsize, bool inverse) {
+  const size_t tabs = (((size_t)N * csize + 15) & ~(size_t)15) + (((size_t)H * csize + 15) & ~(size_t)15) +
+                      (((size_t)N * 4 + 15) & ~(size_t)15);
+  const size_t stage = inverse ? (size_t)rb * Hp * nc * csize : (((size_t)rb * P0 * nc * rsize + 15) / 16) * 16;
+  return tabs + stage + (size_t)nc * rb * N * csize;
+}
+
 // rows per tile of the x passes
 static inline int pick_rb(int n2, int P0, int Hp, int nc, size_t csize, size_t rsize, int ntw, bool inverse) {
   for (int rb = 8; rb >= 1; rb--) {

@@ -83,6 +83,30 @@ template <typename R, int NC>
 int fwd_xy(SolveGeom<R> &g, const R *in, typename cplx_t<R>::type *X, typename cplx_t<R>::type *Y,
            cudaStream_t st, const char *caller, int cs) {
   typedef typename cplx_t<R>::type C;
+  const bool vec16r = cs == NC && ((size_t)g.ext[0] * NC * sizeof(R)) % 16 == 0 &&
+                      ((size_t)g.off[0] * NC * sizeof(R)) % 16 == 0 && ((size_t)g.P[0] * NC * sizeof(R)) % 16 == 0;
+  if (g.rx_ok) {
+    const int RB = pick_rb_reg(g.N2, g.H, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), false);
+    if (RB > 0) {
+      const size_t sm = rx_smem(g.N2, g.H, g.P[0], g.Hp, NC, RB, sizeof(C), sizeof(R), false);
+      CK(cudaFuncSetAttribute(k_rxfwd<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+      const int rows = g.P[1] * g.P[2];
+      const int ntiles = (rows + RB - 1) / RB;
+      int per = 1;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rxfwd<R, NC>, RL_THREADS, sm) != cudaSuccess || per < 1)
+        per = 1;
+      const int grid = std::max(1, std::min(ntiles, per * num_sms()));
+      { KTimer kt_(KC_XFWD, st);
+        k_rxfwd<R, NC><<<grid, RL_THREADS, sm, st>>>(g, in, X, RB, cs, vec16r ? 1 : 0,
+                                                     make_fastdiv((unsigned)(NC * RB / Vec<R>::G))); }
+      PM_LAUNCHED();
+      CKL(caller);
+      const long long Hp = g.Hp;
+      KTimer kt_(KC_YFWD, st);
+      return launch_lines<R, NC>(g, X, Y, 1, L_FWD, 0, 0, 0, g.P[1], g.M[1], (long long)g.P[1] * Hp, Hp,
+                                 (long long)g.M[1] * Hp, Hp, g.P[2], st, caller);
+    }
+  }
   const int ntwx = g.fx.ntw + g.fx.next;
   const int RB = pick_rb(g.N2, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), ntwx, false);
   if (RB == 0) {
@@ -127,20 +151,36 @@ int inv_yx(SolveGeom<R> &g, const pmgpu_topo *topo, typename cplx_t<R>::type *Y,
                             (long long)g.P[1] * Hp, Hp, g.P[2], st, caller))
       return -1;
   }
-  const int ntwx = g.fx.ntw + g.fx.next;
-  const int RB = pick_rb(g.N2, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), ntwx, true);
-  if (RB == 0) {
-    set_error(caller, "FFT length too large for the shared-memory transform.");
-    return -1;
-  }
-  const size_t sm = tw_bytes(ntwx, sizeof(C)) + (size_t)RB * g.Hp * NC * sizeof(C) + 2 * (size_t)NC * RB * g.N2 * sizeof(C);
-  CK(cudaFuncSetAttribute(k_xinv<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
   const int rows = g.P[1] * g.P[2];
-  const int ntiles = (rows + RB - 1) / RB;
-  { KTimer kt_(KC_XINV, st);
-    k_xinv<R, NC><<<persistent_grid(k_xinv<R, NC>, sm, ntiles), PASS_THREADS, sm, st>>>(g, X, out, RB, cs); }
-  PM_LAUNCHED();
-  CKL(caller);
+  const int RBr = g.rx_ok ? pick_rb_reg(g.N2, g.H, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), true) : 0;
+  if (RBr > 0) {
+    const size_t sm = rx_smem(g.N2, g.H, g.P[0], g.Hp, NC, RBr, sizeof(C), sizeof(R), true);
+    CK(cudaFuncSetAttribute(k_rxinv<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+    const int ntiles = (rows + RBr - 1) / RBr;
+    int per = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rxinv<R, NC>, RL_THREADS, sm) != cudaSuccess || per < 1)
+      per = 1;
+    const int grid = std::max(1, std::min(ntiles, per * num_sms()));
+    { KTimer kt_(KC_XINV, st);
+      k_rxinv<R, NC><<<grid, RL_THREADS, sm, st>>>(g, X, out, RBr, cs, make_fastdiv((unsigned)(NC * RBr / Vec<R>::G))); }
+    PM_LAUNCHED();
+    CKL(caller);
+  } else {
+    const int ntwx = g.fx.ntw + g.fx.next;
+    const int RB = pick_rb(g.N2, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), ntwx, true);
+    if (RB == 0) {
+      set_error(caller, "FFT length too large for the shared-memory transform.");
+      return -1;
+    }
+    const size_t sm =
+        tw_bytes(ntwx, sizeof(C)) + (size_t)RB * g.Hp * NC * sizeof(C) + 2 * (size_t)NC * RB * g.N2 * sizeof(C);
+    CK(cudaFuncSetAttribute(k_xinv<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+    const int ntiles = (rows + RB - 1) / RB;
+    { KTimer kt_(KC_XINV, st);
+      k_xinv<R, NC><<<persistent_grid(k_xinv<R, NC>, sm, ntiles), PASS_THREADS, sm, st>>>(g, X, out, RB, cs); }
+    PM_LAUNCHED();
+    CKL(caller);
+  }
   // periodic ghosts (x, then y, then z)
   for (int d = 0; d < 3 && ghosts; d++) {
     if (topo->bound_cond[2 * d] == 0 || topo->bound_cond[2 * d + 1] == 0) continue;

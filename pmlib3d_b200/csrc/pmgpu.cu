@@ -345,9 +345,9 @@ struct pmgpu_plan {
   double eps;
   DevBuf X, Y, Y2, Y3;
   // register-engine plans along y and z (in-place, digit-reversed spectra)
-  int ry_ok, rz_ok;
-  RegPlan ry, rz;
-  DevBuf rtwy, rtwz, yk, zk;
+  int rx_ok, ry_ok, rz_ok;
+  RegPlan rx, ry, rz;
+  DevBuf rtwx, rtwy, rtwz, yk, zk, rextx, xpos;
   DevBuf mesh_w, mesh_u, mesh_a, mesh_b;
   DevBuf h_pos, h_val, h_out;  // device mirrors used by host-pointer calls
   // particle scratch
@@ -357,7 +357,7 @@ struct pmgpu_plan {
   ~pmgpu_plan() {
     DevBuf *bs[] = {&twx, &twy, &twz, &kxt, &kyt, &kzt, &green, &X, &Y, &Y2, &Y3, &mesh_w, &mesh_u,
                     &mesh_a, &mesh_b, &h_pos, &h_val, &h_out, &key, &val, &key2, &val2, &counts,
-                    &start, &spart, &hist, &rtwy, &rtwz, &yk, &zk};
+                    &start, &spart, &hist, &rtwx, &rtwy, &rtwz, &yk, &zk, &rextx, &xpos};
     for (DevBuf *b : bs) b->release();
   }
 };
@@ -579,6 +579,11 @@ template <typename R> static SolveGeom<R> solve_geom(const pmgpu_plan *pl) {
   g.eps2pi = (R)(2.0 * 3.14159265358979323846 * pl->eps);
   g.order = pl->par.poisson_order;
   g.allper = pl->g.allper;
+  g.rx_ok = pl->rx_ok;
+  g.rx = pl->rx;
+  g.rtwx = pl->rtwx.as<C>();
+  g.rextx = pl->rextx.as<C>();
+  g.xpos = pl->xpos.as<int>();
   g.ry_ok = pl->ry_ok;
   g.rz_ok = pl->rz_ok;
   g.ry = pl->ry;
@@ -743,9 +748,36 @@ template <typename R> static int upload_wavenumbers(pmgpu_plan *pl, const char *
 
 template <typename R> static int reg_tables(pmgpu_plan *pl, const char *caller) {
   typedef typename cplx_t<R>::type C;
-  pl->ry_ok = pl->rz_ok = 0;
+  pl->rx_ok = pl->ry_ok = pl->rz_ok = 0;
   if (g_force_stockham) return 0;
   const long double twopi = 2.0L * acosl(-1.0L);
+  {
+    // x passes: half-length complex transform N = Mx / 2
+    RegPlan rp;
+    const int N = pl->g.N2, H = pl->g.H, Mx = pl->g.M[0];
+    if (make_regplan(N, rp)) {
+      std::vector<C> tw(N), ext(H);
+      for (int q = 0; q < N; q++) {
+        const long double a = twopi * (long double)q / (long double)N;
+        tw[q] = mk((R)cosl(a), (R)-sinl(a));
+      }
+      for (int k = 0; k < H; k++) {
+        const long double a = twopi * (long double)k / (long double)Mx;
+        ext[k] = mk((R)cosl(a), (R)-sinl(a));
+      }
+      const std::vector<int> kp = regplan_positions(rp);
+      std::vector<int> xp(N);
+      for (int q = 0; q < N; q++) xp[kp[q]] = q;
+      if (pl->rtwx.ensure(sizeof(C) * N, caller) || pl->rextx.ensure(sizeof(C) * H, caller) ||
+          pl->xpos.ensure(sizeof(int) * N, caller))
+        return -1;
+      CK(cudaMemcpy(pl->rtwx.p, tw.data(), sizeof(C) * N, cudaMemcpyHostToDevice), caller);
+      CK(cudaMemcpy(pl->rextx.p, ext.data(), sizeof(C) * H, cudaMemcpyHostToDevice), caller);
+      CK(cudaMemcpy(pl->xpos.p, xp.data(), sizeof(int) * N, cudaMemcpyHostToDevice), caller);
+      pl->rx = rp;
+      pl->rx_ok = 1;
+    }
+  }
   for (int axis = 1; axis <= 2; axis++) {
     RegPlan rp;
     const int n = pl->g.M[axis];

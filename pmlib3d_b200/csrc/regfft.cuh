@@ -85,10 +85,12 @@ template <> __device__ __forceinline__ double2 zero_vec<double>() { return make_
 
 // One phase over a tile of LG line vectors.  gsrc / gdst: read from / write to
 // global memory instead of `buf`.  twid: the phase carries twiddles.
+// nz: points at positions >= nz are zero and are not read (the zero padding of
+// the first forward phase; n otherwise)
 template <int RAD, bool INV, typename R>
 __device__ __forceinline__ void rphase(const RegPlan &pl, int p, typename Vec<R>::V *buf, int LG, const FastDiv &dLG,
                                        const typename cplx_t<R>::type *__restrict__ tw, bool gsrc, bool gdst,
-                                       bool twid, const PhaseGlobal &gl) {
+                                       bool twid, const PhaseGlobal &gl, int nz) {
   typedef typename cplx_t<R>::type C;
   typedef typename Vec<R>::V V;
   constexpr int G = Vec<R>::G;
@@ -109,7 +111,7 @@ __device__ __forceinline__ void rphase(const RegPlan &pl, int p, typename Vec<R>
 #pragma unroll
       for (int j = 0; j < RAD; j++) {
         V v = zero_vec<R>();
-        if (pos0 + s * j < gl.rows_in) v = ldg_vec<R>(src + (long long)(s * j) * vri);
+        if (pos0 + s * j < nz) v = ldg_vec<R>(src + (long long)(s * j) * vri);
         C t[G];
         vsplit(v, t);
 #pragma unroll
@@ -117,12 +119,22 @@ __device__ __forceinline__ void rphase(const RegPlan &pl, int p, typename Vec<R>
       }
     } else {
       const V *src = buf + pos0 * LG + g;
+      if (nz >= pl.n) {
 #pragma unroll
-      for (int j = 0; j < RAD; j++) {
-        C t[G];
-        vsplit(src[s * j * LG], t);
+        for (int j = 0; j < RAD; j++) {
+          C t[G];
+          vsplit(src[s * j * LG], t);
 #pragma unroll
-        for (int h = 0; h < G; h++) a[h][j] = t[h];
+          for (int h = 0; h < G; h++) a[h][j] = t[h];
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < RAD; j++) {
+          C t[G];
+          vsplit(pos0 + s * j < nz ? src[s * j * LG] : zero_vec<R>(), t);
+#pragma unroll
+          for (int h = 0; h < G; h++) a[h][j] = t[h];
+        }
       }
     }
     if (INV && twid) {
@@ -170,22 +182,22 @@ __device__ __forceinline__ void rphase(const RegPlan &pl, int p, typename Vec<R>
 template <bool INV, typename R>
 __device__ __forceinline__ void rphase_any(const RegPlan &pl, int p, typename Vec<R>::V *buf, int LG,
                                            const FastDiv &dLG, const typename cplx_t<R>::type *tw, bool gsrc,
-                                           bool gdst, bool twid, const PhaseGlobal &gl) {
+                                           bool gdst, bool twid, const PhaseGlobal &gl, int nz) {
   switch (pl.rad[p]) {
-    case 2: rphase<2, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
-    case 3: rphase<3, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
-    case 4: rphase<4, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
-    case 5: rphase<5, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
-    case 6: rphase<6, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
-    case 7: rphase<7, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
-    case 8: rphase<8, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
-    case 9: rphase<9, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
-    case 10: rphase<10, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
-    case 11: rphase<11, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
-    case 12: rphase<12, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
-    case 13: rphase<13, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
-    case 16: rphase<16, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
-    case 17: rphase<17, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl); break;
+    case 2: rphase<2, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); break;
+    case 3: rphase<3, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); break;
+    case 4: rphase<4, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); break;
+    case 5: rphase<5, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); break;
+    case 6: rphase<6, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); break;
+    case 7: rphase<7, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); break;
+    case 8: rphase<8, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); break;
+    case 9: rphase<9, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); break;
+    case 10: rphase<10, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); break;
+    case 11: rphase<11, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); break;
+    case 12: rphase<12, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); break;
+    case 13: rphase<13, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); break;
+    case 16: rphase<16, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); break;
+    case 17: rphase<17, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); break;
     default: break;  // plans only hold register radices
   }
 }
@@ -193,13 +205,15 @@ __device__ __forceinline__ void rphase_any(const RegPlan &pl, int p, typename Ve
 // forward transform of a tile: natural-order input (global when gfirst, else buf),
 // digit-reversed output in buf, or in global memory when glast.  The caller
 // synchronises before; every phase but a final global one ends with a barrier.
+// nz0: nonzero leading points of an input in buf (the rest is zero padding)
 template <typename R>
 __device__ __forceinline__ void rfft_fwd(const RegPlan &pl, typename Vec<R>::V *buf, int LG, const FastDiv &dLG,
                                          const typename cplx_t<R>::type *tw, bool gfirst, bool glast,
-                                         const PhaseGlobal &gl) {
+                                         const PhaseGlobal &gl, int nz0 = -1) {
   for (int p = 0; p < pl.np; p++) {
     const bool last = p == pl.np - 1;
-    rphase_any<false, R>(pl, p, buf, LG, dLG, tw, gfirst && p == 0, glast && last, !last, gl);
+    const int nz = p > 0 ? pl.n : gfirst ? gl.rows_in : nz0 >= 0 ? nz0 : pl.n;
+    rphase_any<false, R>(pl, p, buf, LG, dLG, tw, gfirst && p == 0, glast && last, !last, gl, nz);
     __syncthreads();
   }
 }
@@ -211,7 +225,8 @@ __device__ __forceinline__ void rfft_inv(const RegPlan &pl, typename Vec<R>::V *
                                          const typename cplx_t<R>::type *tw, bool gfirst, bool glast,
                                          const PhaseGlobal &gl) {
   for (int p = pl.np - 1; p >= 0; p--) {
-    rphase_any<true, R>(pl, p, buf, LG, dLG, tw, gfirst && p == pl.np - 1, glast && p == 0, p < pl.np - 1, gl);
+    const bool gs = gfirst && p == pl.np - 1;
+    rphase_any<true, R>(pl, p, buf, LG, dLG, tw, gs, glast && p == 0, p < pl.np - 1, gl, gs ? gl.rows_in : pl.n);
     __syncthreads();
   }
 }

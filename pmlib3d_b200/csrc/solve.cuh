@@ -45,9 +45,11 @@ template <typename R> struct SolveGeom {
   int order;                 // filter order (poisson order or reg_order)
   int allper;                // all axes periodic: spectral Green's function
   // in-place register FFTs along y and z (when the lengths factor into register radices)
-  int ry_ok, rz_ok;
-  RegPlan ry, rz;
-  const C *rtwy, *rtwz;      // w_n^q, q < n
+  int rx_ok, ry_ok, rz_ok;
+  RegPlan rx, ry, rz;        // rx: the half-length complex transform of the x passes
+  const C *rtwx, *rtwy, *rtwz;  // w_n^q, q < n
+  const C *rextx;            // exp(-2 pi i k / Mx), k < H
+  const int *xpos;           // frequency -> position of the x transform
   const int *yk;             // row of the y spectrum -> ky index (nullptr: natural order)
   const int *zk;             // position of the z transform -> kz index
 };
@@ -351,6 +353,217 @@ __global__ void __launch_bounds__(RL_THREADS, 2) k_rlines(SolveGeom<R> g, LineTi
       rfft_inv<R>(pl, buf, LG, lt.dLG, tw, false, true, gl);
     }
   }
+}
+
+// ---------------------------------------------------------------- x passes, register engine
+// As k_xfwd / k_xinv below (R2C / C2R through a half-length complex transform),
+// with the transform done in place by the register engine: the packed line has
+// its second half zero (not read), and the digit-reversed spectrum is addressed
+// through the frequency -> position table.
+template <typename R, int NC>
+__global__ void __launch_bounds__(RL_THREADS, 2) k_rxfwd(SolveGeom<R> g, const R *__restrict__ in,
+                                                         typename cplx_t<R>::type *__restrict__ X, int RB, int cs,
+                                                         int vec16, FastDiv dLG) {
+  typedef typename cplx_t<R>::type C;
+  typedef typename Vec<R>::V V;
+  constexpr int G = Vec<R>::G;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const RegPlan &pl = g.rx;
+  const int N = pl.n, L = NC * RB, LG = L / G, H = g.H;
+  const int P0 = g.P[0];
+  unsigned char *sp = smem_raw;
+  C *tw = reinterpret_cast<C *>(sp);
+  sp += ((size_t)N * sizeof(C) + 15) & ~(size_t)15;
+  C *ext = reinterpret_cast<C *>(sp);
+  sp += ((size_t)H * sizeof(C) + 15) & ~(size_t)15;
+  int *xpos = reinterpret_cast<int *>(sp);
+  sp += ((size_t)N * sizeof(int) + 15) & ~(size_t)15;
+  R *Sr = reinterpret_cast<R *>(sp);
+  sp += ((size_t)RB * P0 * NC * sizeof(R) + 15) & ~(size_t)15;
+  V *buf = reinterpret_cast<V *>(sp);
+  C *Bc = reinterpret_cast<C *>(buf);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    tw[i] = g.rtwx[i];
+    xpos[i] = g.xpos[i];
+  }
+  for (int i = threadIdx.x; i < H; i += blockDim.x) ext[i] = g.rextx[i];
+  const int nrows = g.P[1] * g.P[2];
+  const int ntiles = (nrows + RB - 1) / RB;
+  const int npk = (P0 + 1) / 2;  // packed points that hold data
+  auto load = [&](int tile) {
+    const int row0 = tile * RB;
+    for (int rr = 0; rr < RB; rr++) {
+      const int row = row0 + rr;
+      if (row >= nrows) break;
+      const int y = row % g.P[1], z = row / g.P[1];
+      const R *src = in + (((size_t)(z + g.off[2]) * g.ext[1] + (y + g.off[1])) * g.ext[0] + g.off[0]) * cs;
+      R *dst = Sr + (size_t)rr * P0 * NC;
+      if (vec16) {
+        const int nch = (P0 * NC * (int)sizeof(R)) / 16;
+        for (int c = threadIdx.x; c < nch; c += blockDim.x)
+          cp_async16(reinterpret_cast<char *>(dst) + 16 * c, reinterpret_cast<const char *>(src) + 16 * c);
+      } else {
+        for (int e = threadIdx.x; e < P0 * NC; e += blockDim.x) {
+          const int x = e / NC, c = e - x * NC;
+          if (sizeof(R) == 8) cp_async8(dst + e, src + (size_t)x * cs + c);
+          else cp_async4(dst + e, src + (size_t)x * cs + c);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  int tile = blockIdx.x;
+  if (tile < ntiles) load(tile);
+  for (; tile < ntiles; tile += gridDim.x) {
+    cp_async_wait_all();
+    __syncthreads();
+    const int row0 = tile * RB;
+    for (int t = threadIdx.x; t < RB * npk; t += blockDim.x) {
+      const int rr = t / npk, m = t - rr * npk;
+      const R *xr = Sr + (size_t)rr * P0 * NC;
+      const int x0 = 2 * m, x1 = 2 * m + 1;
+      const bool ok = row0 + rr < nrows;
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        const R a = ok ? xr[x0 * NC + c] : R(0);
+        const R b = (ok && x1 < P0) ? xr[x1 * NC + c] : R(0);
+        Bc[m * L + rr * NC + c] = mk(a, b);
+      }
+    }
+    __syncthreads();
+    const int next = tile + gridDim.x;
+    if (next < ntiles) load(next);
+    PhaseGlobal gl;
+    gl.in = nullptr;
+    gl.out = nullptr;
+    gl.rs_in = gl.rs_out = 0;
+    gl.rows_in = gl.rows_out = N;
+    rfft_fwd<R>(pl, buf, LG, dLG, tw, false, false, gl, npk);
+    for (int t = threadIdx.x; t < RB * g.Hp; t += blockDim.x) {
+      const int rr = t / g.Hp, k = t - rr * g.Hp;
+      const int row = row0 + rr;
+      if (row >= nrows) continue;
+      C o[NC];
+      if (k < H) {
+        const int kk = (k == N) ? 0 : k;
+        const int km = (k == 0 || k == N) ? 0 : N - k;
+        const int pk = xpos[kk], pm = xpos[km];
+        const C w = ext[k];
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          const C zk = Bc[pk * L + rr * NC + c];
+          const C zn = cconj(Bc[pm * L + rr * NC + c]);
+          const C a = cadd(zk, zn), bb = csub(zk, zn);
+          const C wb = cmul(w, bb);
+          o[c] = mk(R(0.5) * (a.x + wb.y), R(0.5) * (a.y - wb.x));  // (a - i W^k b) / 2
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < NC; c++) o[c] = mk(R(0), R(0));
+      }
+#pragma unroll
+      for (int c = 0; c < NC; c++) X[((size_t)row * g.Hp + k) * NC + c] = o[c];
+    }
+    __syncthreads();
+  }
+  cp_async_wait_all();
+}
+
+template <typename R, int NC>
+__global__ void __launch_bounds__(RL_THREADS, 2) k_rxinv(SolveGeom<R> g,
+                                                         const typename cplx_t<R>::type *__restrict__ X,
+                                                         R *__restrict__ outp, int RB, int cs, FastDiv dLG) {
+  typedef typename cplx_t<R>::type C;
+  typedef typename Vec<R>::V V;
+  constexpr int G = Vec<R>::G;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const RegPlan &pl = g.rx;
+  const int N = pl.n, L = NC * RB, LG = L / G, H = g.H;
+  const size_t rowc = (size_t)g.Hp * NC;  // complex per X row
+  unsigned char *sp = smem_raw;
+  C *tw = reinterpret_cast<C *>(sp);
+  sp += ((size_t)N * sizeof(C) + 15) & ~(size_t)15;
+  C *ext = reinterpret_cast<C *>(sp);
+  sp += ((size_t)H * sizeof(C) + 15) & ~(size_t)15;
+  int *xpos = reinterpret_cast<int *>(sp);
+  sp += ((size_t)N * sizeof(int) + 15) & ~(size_t)15;
+  C *Sc = reinterpret_cast<C *>(sp);
+  sp += (size_t)RB * rowc * sizeof(C);
+  V *buf = reinterpret_cast<V *>(sp);
+  C *Bc = reinterpret_cast<C *>(buf);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    tw[i] = g.rtwx[i];
+    xpos[i] = g.xpos[i];
+  }
+  for (int i = threadIdx.x; i < H; i += blockDim.x) ext[i] = g.rextx[i];
+  const int nrows = g.P[1] * g.P[2];
+  const int ntiles = (nrows + RB - 1) / RB;
+  auto load = [&](int tile) {
+    const int row0 = tile * RB;
+    const int nr = min(RB, nrows - row0);
+    const size_t nch = (size_t)nr * rowc * sizeof(C) / 16;
+    const char *src = reinterpret_cast<const char *>(X + (size_t)row0 * rowc);
+    for (size_t c = threadIdx.x; c < nch; c += blockDim.x)
+      cp_async16(reinterpret_cast<char *>(Sc) + 16 * c, src + 16 * c);
+    cp_async_commit();
+  };
+  int tile = blockIdx.x;
+  if (tile < ntiles) load(tile);
+  for (; tile < ntiles; tile += gridDim.x) {
+    cp_async_wait_all();
+    __syncthreads();
+    const int row0 = tile * RB;
+    for (int t = threadIdx.x; t < RB * N; t += blockDim.x) {
+      const int rr = t / N, m = t - rr * N;
+      const C w = cconj(ext[m]);
+      const bool ok = row0 + rr < nrows;
+      const int pm = xpos[m];
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        C z = mk(R(0), R(0));
+        if (ok) {
+          C xm = Sc[rr * rowc + (size_t)m * NC + c];
+          C xn = Sc[rr * rowc + (size_t)(N - m) * NC + c];
+          if (m == 0) {
+            xm.y = R(0);
+            xn.y = R(0);
+          }  // DC and Nyquist are real
+          const C a = cadd(xm, cconj(xn));
+          const C b = csub(xm, cconj(xn));
+          const C wb = cmul(w, b);
+          z = mk(a.x - wb.y, a.y + wb.x);  // a + i W^{-m} b
+        }
+        Bc[pm * L + rr * NC + c] = z;
+      }
+    }
+    __syncthreads();
+    const int next = tile + gridDim.x;
+    if (next < ntiles) load(next);
+    PhaseGlobal gl;
+    gl.in = nullptr;
+    gl.out = nullptr;
+    gl.rs_in = gl.rs_out = 0;
+    gl.rows_in = gl.rows_out = N;
+    rfft_inv<R>(pl, buf, LG, dLG, tw, false, false, gl);
+    const int P0 = g.P[0];
+    const int nout = (P0 + 1) / 2;
+    for (int t = threadIdx.x; t < RB * nout; t += blockDim.x) {
+      const int rr = t / nout, m = t - rr * nout;
+      const int row = row0 + rr;
+      if (row >= nrows) continue;
+      const int y = row % g.P[1], z = row / g.P[1];
+      R *dst = outp + (((size_t)(z + g.off[2]) * g.ext[1] + (y + g.off[1])) * g.ext[0] + g.off[0]) * cs;
+      const int x0 = 2 * m, x1 = 2 * m + 1;
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        const C v = Bc[m * L + rr * NC + c];
+        dst[(size_t)x0 * cs + c] = v.x;
+        if (x1 < P0) dst[(size_t)x1 * cs + c] = v.y;
+      }
+    }
+    __syncthreads();
+  }
+  cp_async_wait_all();
 }
 
 // ---------------------------------------------------------------- x forward (R2C)
