@@ -52,28 +52,31 @@ static inline int pick_tk(int n, int nc, size_t csize, int ntw) {
 static inline size_t lines_smem(int n, int nc, int tk, size_t csize, int ntw) {
   return tw_bytes(ntw, csize) + 3 * (size_t)nc * tk * n * csize;
 }
-// register engine: twiddles w_n^q + position table + one tile buffer
+// register engine: twiddles w_n^q + position table + wavenumbers + one tile buffer
 static inline size_t reg_smem(int n, int nc, int tk, size_t csize) {
-  return (((size_t)n * csize + 15) & ~(size_t)15) + (((size_t)n * 4 + 15) & ~(size_t)15) + (size_t)nc * tk * n * csize;
+  return (((size_t)n * csize + 15) & ~(size_t)15) + (((size_t)n * 4 + 15) & ~(size_t)15) +
+         (((size_t)n * csize / 2 + 15) & ~(size_t)15) + (size_t)nc * tk * n * csize;
 }
-// kx tile of the register engine: two CTAs per SM if possible, else one
-static inline int pick_tk_reg(int n, int nc, size_t csize, int Hp) {
-  for (size_t budget : {(size_t)112 * 1024, PASS_SMEM_BUDGET})
+// shared memory per CTA that lets the register-engine kernels run as many CTAs per
+// SM as their register budget allows (FP32: 3, FP64: 2; 228 KB per SM)
+static inline size_t reg_budget(size_t rsize) { return rsize == 4 ? (size_t)74 * 1024 : (size_t)112 * 1024; }
+// kx tile of the register engine: within the budget if possible, else one CTA per SM
+static inline int pick_tk_reg(int n, int nc, size_t csize, int Hp, size_t budget1) {
+  for (size_t budget : {budget1, PASS_SMEM_BUDGET})
     for (int tk = 8; tk >= 1; tk /= 2) {
       if (Hp % tk) continue;
-      if (csize == 8 && (nc * tk) % 2) continue;
       if (reg_smem(n, nc, tk, csize) <= budget) return tk;
     }
   return 0;
 }
 // rows per tile of the register-engine x passes (table bytes + staging + buffer),
 // two CTAs per SM if possible
-static inline int pick_rb_reg(int N, int H, int P0, int Hp, int nc, size_t csize, size_t rsize, bool inverse) {
+static inline int pick_rb_reg(int N, int H, int P0, int Hp, int nc, size_t csize, size_t rsize, bool inverse,
+                              size_t budget1) {
   const size_t tabs = (((size_t)N * csize + 15) & ~(size_t)15) + (((size_t)H * csize + 15) & ~(size_t)15) +
                       (((size_t)N * 4 + 15) & ~(size_t)15);
-  for (size_t budget : {(size_t)112 * 1024, PASS_SMEM_BUDGET})
+  for (size_t budget : {budget1, PASS_SMEM_BUDGET})
     for (int rb = 16; rb >= 1; rb--) {
-      if (csize == 8 && (nc * rb) % 2) continue;
       const size_t stage = inverse ? (size_t)rb * Hp * nc * csize : (((size_t)rb * P0 * nc * rsize + 15) / 16) * 16;
       if (tabs + stage + (size_t)nc * rb * N * csize <= budget) return rb;
     }

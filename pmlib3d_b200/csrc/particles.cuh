@@ -636,22 +636,32 @@ __global__ void __launch_bounds__(M2P_THREADS) k_m2p_tile(PartGeom<R> g, const R
   const int x0 = blockIdx.x * M2P_TX, y0 = blockIdx.y * M2P_TY, z0 = blockIdx.z * M2P_TZ;
   const int cx0 = x0 - (W - 1), cy0 = y0 - (W - 1), cz0 = z0 - (W - 1);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  // ---- stage the cells: one warp per cell row, lanes along the row's 3 CX values
+  // ---- stage the cells: one warp per cell row; lane offsets are the same in every row
   {
-    const int xa = max(cx0, 0), xb = min(cx0 + CX, g.ext[0]);  // cells present in the cuboid
+    constexpr int NE = (CX * 3 + 31) / 32;
+    int so[NE], dof[NE];
+    bool ok[NE];
+#pragma unroll
+    for (int k = 0; k < NE; k++) {
+      const int e = lane + 32 * k;
+      const int xx = e / 3, c = e - 3 * xx;
+      const int cx = cx0 + xx;
+      ok[k] = e < CX * 3 && cx >= 0 && cx < g.ext[0];
+      so[k] = cx * 3 + c;
+      dof[k] = e < CX * 3 ? xx * 4 + c : -1;
+    }
     for (int row = wid; row < CZ * CY; row += nw) {
       const int yy = row % CY, zz = row / CY;
       const int cy = cy0 + yy, cz = cz0 + zz;
       R *dst = cells + (size_t)row * CX * 4;
       const bool rowin = cy >= 0 && cy < g.ext[1] && cz >= 0 && cz < g.ext[2];
-      const R *src = f + (((size_t)cz * g.ext[1] + cy) * g.ext[0]) * 3;
-      for (int e = lane; e < CX * 3; e += 32) {
-        const int xx = e / 3, c = e - 3 * xx;
-        const int cx = cx0 + xx;
-        R v = R(0);
-        if (rowin && cx >= xa && cx < xb) v = __ldg(src + (size_t)cx * 3 + c);
-        dst[xx * 4 + c] = v;
-      }
+      const R *src = f + (((size_t)(rowin ? cz : 0) * g.ext[1] + (rowin ? cy : 0)) * g.ext[0]) * 3;
+      R v[NE];
+#pragma unroll
+      for (int k = 0; k < NE; k++) v[k] = (rowin && ok[k]) ? __ldg(src + so[k]) : R(0);
+#pragma unroll
+      for (int k = 0; k < NE; k++)
+        if (dof[k] >= 0) dst[dof[k]] = v[k];
     }
   }
   // ---- particle ranges of the bin rows

@@ -26,7 +26,7 @@ static int launch_lines(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typ
   typedef typename cplx_t<R>::type C;
   const int n = g.M[axis];
   if ((axis == 1 ? g.ry_ok : g.rz_ok) && !(lmode == L_FWD && axis == 2)) {
-    const int TK = pick_tk_reg(n, NC, sizeof(C), g.Hp);
+    const int TK = pick_tk_reg(n, NC, sizeof(C), g.Hp, reg_budget(sizeof(R)));
     if (TK > 0) {
       LineTiles lt;
       lt.n = n;
@@ -39,7 +39,7 @@ static int launch_lines(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typ
       lt.nouter = nouter;
       lt.nkt = g.Hp / TK;
       lt.TK = TK;
-      lt.dLG = make_fastdiv((unsigned)(NC * TK / Vec<R>::G));
+      lt.dLG = make_fastdiv((unsigned)(NC * TK / RVec<R>::G));
       const size_t sm = reg_smem(n, NC, TK, sizeof(C));
       CK(cudaFuncSetAttribute(k_rlines<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
       int per = 1;
@@ -86,7 +86,7 @@ int fwd_xy(SolveGeom<R> &g, const R *in, typename cplx_t<R>::type *X, typename c
   const bool vec16r = cs == NC && ((size_t)g.ext[0] * NC * sizeof(R)) % 16 == 0 &&
                       ((size_t)g.off[0] * NC * sizeof(R)) % 16 == 0 && ((size_t)g.P[0] * NC * sizeof(R)) % 16 == 0;
   if (g.rx_ok) {
-    const int RB = pick_rb_reg(g.N2, g.H, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), false);
+    const int RB = pick_rb_reg(g.N2, g.H, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), false, reg_budget(sizeof(R)));
     if (RB > 0) {
       const size_t sm = rx_smem(g.N2, g.H, g.P[0], g.Hp, NC, RB, sizeof(C), sizeof(R), false);
       CK(cudaFuncSetAttribute(k_rxfwd<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
@@ -98,7 +98,7 @@ int fwd_xy(SolveGeom<R> &g, const R *in, typename cplx_t<R>::type *X, typename c
       const int grid = std::max(1, std::min(ntiles, per * num_sms()));
       { KTimer kt_(KC_XFWD, st);
         k_rxfwd<R, NC><<<grid, RL_THREADS, sm, st>>>(g, in, X, RB, cs, vec16r ? 1 : 0,
-                                                     make_fastdiv((unsigned)(NC * RB / Vec<R>::G))); }
+                                                     make_fastdiv((unsigned)(NC * RB / RVec<R>::G))); }
       PM_LAUNCHED();
       CKL(caller);
       const long long Hp = g.Hp;
@@ -152,7 +152,7 @@ int inv_yx(SolveGeom<R> &g, const pmgpu_topo *topo, typename cplx_t<R>::type *Y,
       return -1;
   }
   const int rows = g.P[1] * g.P[2];
-  const int RBr = g.rx_ok ? pick_rb_reg(g.N2, g.H, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), true) : 0;
+  const int RBr = g.rx_ok ? pick_rb_reg(g.N2, g.H, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), true, reg_budget(sizeof(R))) : 0;
   if (RBr > 0) {
     const size_t sm = rx_smem(g.N2, g.H, g.P[0], g.Hp, NC, RBr, sizeof(C), sizeof(R), true);
     CK(cudaFuncSetAttribute(k_rxinv<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
@@ -162,7 +162,7 @@ int inv_yx(SolveGeom<R> &g, const pmgpu_topo *topo, typename cplx_t<R>::type *Y,
       per = 1;
     const int grid = std::max(1, std::min(ntiles, per * num_sms()));
     { KTimer kt_(KC_XINV, st);
-      k_rxinv<R, NC><<<grid, RL_THREADS, sm, st>>>(g, X, out, RBr, cs, make_fastdiv((unsigned)(NC * RBr / Vec<R>::G))); }
+      k_rxinv<R, NC><<<grid, RL_THREADS, sm, st>>>(g, X, out, RBr, cs, make_fastdiv((unsigned)(NC * RBr / RVec<R>::G))); }
     PM_LAUNCHED();
     CKL(caller);
   } else {

@@ -75,12 +75,26 @@ struct PhaseGlobal {
   int rows_out;            // rows wanted in `out`
 };
 
-template <typename R> __device__ __forceinline__ typename Vec<R>::V ldg_vec(const typename Vec<R>::V *p);
-template <> __device__ __forceinline__ float4 ldg_vec<float>(const float4 *p) { return __ldg(p); }
+// One line per thread and butterfly: the vector is one complex point, so a radix-R
+// butterfly holds R complex values in registers.
+template <typename R> struct RVec {
+  typedef typename cplx_t<R>::type V;
+  static constexpr int G = 1;
+};
+// CTAs per SM the register-engine kernels are compiled for (register budget)
+template <typename R> struct RMinBlocks;
+template <> struct RMinBlocks<float> { static constexpr int v = 3; };
+template <> struct RMinBlocks<double> { static constexpr int v = 2; };
+
+template <typename V> __device__ __forceinline__ void rsplit(const V &v, V *a) { a[0] = v; }
+template <typename V> __device__ __forceinline__ V rmerge(const V *a) { return a[0]; }
+
+template <typename R> __device__ __forceinline__ typename RVec<R>::V ldg_vec(const typename RVec<R>::V *p);
+template <> __device__ __forceinline__ float2 ldg_vec<float>(const float2 *p) { return __ldg(p); }
 template <> __device__ __forceinline__ double2 ldg_vec<double>(const double2 *p) { return __ldg(p); }
 
-template <typename R> __device__ __forceinline__ typename Vec<R>::V zero_vec();
-template <> __device__ __forceinline__ float4 zero_vec<float>() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+template <typename R> __device__ __forceinline__ typename RVec<R>::V zero_vec();
+template <> __device__ __forceinline__ float2 zero_vec<float>() { return make_float2(0.f, 0.f); }
 template <> __device__ __forceinline__ double2 zero_vec<double>() { return make_double2(0.0, 0.0); }
 
 // One phase over a tile of LG line vectors.  gsrc / gdst: read from / write to
@@ -88,12 +102,12 @@ template <> __device__ __forceinline__ double2 zero_vec<double>() { return make_
 // nz: points at positions >= nz are zero and are not read (the zero padding of
 // the first forward phase; n otherwise)
 template <int RAD, bool INV, typename R>
-__device__ __forceinline__ void rphase(const RegPlan &pl, int p, typename Vec<R>::V *buf, int LG, const FastDiv &dLG,
+__device__ __forceinline__ void rphase(const RegPlan &pl, int p, typename RVec<R>::V *buf, int LG, const FastDiv &dLG,
                                        const typename cplx_t<R>::type *__restrict__ tw, bool gsrc, bool gdst,
                                        bool twid, const PhaseGlobal &gl, int nz) {
   typedef typename cplx_t<R>::type C;
-  typedef typename Vec<R>::V V;
-  constexpr int G = Vec<R>::G;
+  typedef typename RVec<R>::V V;
+  constexpr int G = RVec<R>::G;
   const int s = pl.str[p], B = pl.blk[p], tm = pl.twm[p];
   const unsigned total = (unsigned)(pl.n / RAD) * (unsigned)LG;
   const V *gin = reinterpret_cast<const V *>(gl.in);
@@ -113,7 +127,7 @@ __device__ __forceinline__ void rphase(const RegPlan &pl, int p, typename Vec<R>
         V v = zero_vec<R>();
         if (pos0 + s * j < nz) v = ldg_vec<R>(src + (long long)(s * j) * vri);
         C t[G];
-        vsplit(v, t);
+        rsplit(v, t);
 #pragma unroll
         for (int h = 0; h < G; h++) a[h][j] = t[h];
       }
@@ -123,7 +137,7 @@ __device__ __forceinline__ void rphase(const RegPlan &pl, int p, typename Vec<R>
 #pragma unroll
         for (int j = 0; j < RAD; j++) {
           C t[G];
-          vsplit(src[s * j * LG], t);
+          rsplit(src[s * j * LG], t);
 #pragma unroll
           for (int h = 0; h < G; h++) a[h][j] = t[h];
         }
@@ -131,7 +145,7 @@ __device__ __forceinline__ void rphase(const RegPlan &pl, int p, typename Vec<R>
 #pragma unroll
         for (int j = 0; j < RAD; j++) {
           C t[G];
-          vsplit(pos0 + s * j < nz ? src[s * j * LG] : zero_vec<R>(), t);
+          rsplit(pos0 + s * j < nz ? src[s * j * LG] : zero_vec<R>(), t);
 #pragma unroll
           for (int h = 0; h < G; h++) a[h][j] = t[h];
         }
@@ -164,7 +178,7 @@ __device__ __forceinline__ void rphase(const RegPlan &pl, int p, typename Vec<R>
         C t[G];
 #pragma unroll
         for (int h = 0; h < G; h++) t[h] = a[h][k];
-        if (pos0 + s * k < gl.rows_out) dst[(long long)(s * k) * vro] = vmerge(t);
+        if (pos0 + s * k < gl.rows_out) dst[(long long)(s * k) * vro] = rmerge(t);
       }
     } else {
       V *dst = buf + pos0 * LG + g;
@@ -173,14 +187,14 @@ __device__ __forceinline__ void rphase(const RegPlan &pl, int p, typename Vec<R>
         C t[G];
 #pragma unroll
         for (int h = 0; h < G; h++) t[h] = a[h][k];
-        dst[s * k * LG] = vmerge(t);
+        dst[s * k * LG] = rmerge(t);
       }
     }
   }
 }
 
 template <bool INV, typename R>
-__device__ __forceinline__ void rphase_any(const RegPlan &pl, int p, typename Vec<R>::V *buf, int LG,
+__device__ __forceinline__ void rphase_any(const RegPlan &pl, int p, typename RVec<R>::V *buf, int LG,
                                            const FastDiv &dLG, const typename cplx_t<R>::type *tw, bool gsrc,
                                            bool gdst, bool twid, const PhaseGlobal &gl, int nz) {
   switch (pl.rad[p]) {
@@ -207,7 +221,7 @@ __device__ __forceinline__ void rphase_any(const RegPlan &pl, int p, typename Ve
 // synchronises before; every phase but a final global one ends with a barrier.
 // nz0: nonzero leading points of an input in buf (the rest is zero padding)
 template <typename R>
-__device__ __forceinline__ void rfft_fwd(const RegPlan &pl, typename Vec<R>::V *buf, int LG, const FastDiv &dLG,
+__device__ __forceinline__ void rfft_fwd(const RegPlan &pl, typename RVec<R>::V *buf, int LG, const FastDiv &dLG,
                                          const typename cplx_t<R>::type *tw, bool gfirst, bool glast,
                                          const PhaseGlobal &gl, int nz0 = -1) {
   for (int p = 0; p < pl.np; p++) {
@@ -221,7 +235,7 @@ __device__ __forceinline__ void rfft_fwd(const RegPlan &pl, typename Vec<R>::V *
 // inverse transform: digit-reversed input (global when gfirst, else buf), natural
 // output in buf, or in global memory (rows < rows_out) when glast
 template <typename R>
-__device__ __forceinline__ void rfft_inv(const RegPlan &pl, typename Vec<R>::V *buf, int LG, const FastDiv &dLG,
+__device__ __forceinline__ void rfft_inv(const RegPlan &pl, typename RVec<R>::V *buf, int LG, const FastDiv &dLG,
                                          const typename cplx_t<R>::type *tw, bool gfirst, bool glast,
                                          const PhaseGlobal &gl) {
   for (int p = pl.np - 1; p >= 0; p--) {

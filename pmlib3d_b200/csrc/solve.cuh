@@ -166,18 +166,23 @@ __device__ __forceinline__ void tile_rows_store(typename cplx_t<R>::type *out, c
     *reinterpret_cast<float4 *>(dst + r * strideb + c * 16) = *reinterpret_cast<const float4 *>(src + r * rowb + c * 16);
 }
 
-// z-pass spectral multiply of one tile held in buffer V (complex view C)
+// z-pass spectral multiply of one tile held in buffer V (complex view C).
+// zpos: position -> kz index (nullptr: natural order); kzs: kz wavenumbers (shared
+// copy of g.kzt, or nullptr)
 template <typename R, int NC>
 __device__ __forceinline__ void z_multiply(const SolveGeom<R> &g, typename cplx_t<R>::type *Cb, int L, int TK, int k0,
-                                           int y, int zmode, int reproj, int use_zeta, const int *zpos) {
+                                           int y, int zmode, int reproj, int use_zeta, const int *zpos,
+                                           const R *kzs = nullptr) {
   typedef typename cplx_t<R>::type C;
   const R twopi = R(6.283185307179586476925286766559);
   const int N = g.M[2];
   const R ky = g.kyt[y];
   const R kyc = (2 * y == g.M[1]) ? R(0) : ky;  // Nyquist component dropped in the curl
   const int iy = min(y, g.M[1] - y);
+  const int tks = __ffs(TK) - 1;  // TK is a power of two
+  const R *kzt = kzs ? kzs : g.kzt;
   for (int t = threadIdx.x; t < N * TK; t += blockDim.x) {
-    const int q = t / TK, kk = t - q * TK;
+    const int q = t >> tks, kk = t - (q << tks);
     const int z = zpos ? zpos[q] : q;
     const int kx_i = k0 + kk;
     C *v = Cb + q * L + kk * NC;
@@ -186,7 +191,7 @@ __device__ __forceinline__ void z_multiply(const SolveGeom<R> &g, typename cplx_
       for (int c = 0; c < NC; c++) v[c] = mk(R(0), R(0));
       continue;
     }
-    const R kx = g.kxt[kx_i], kz = g.kzt[z];
+    const R kx = g.kxt[kx_i], kz = kzt[z];
     const R kxc = (2 * kx_i == g.M[0]) ? R(0) : kx;
     const R kzc = (2 * z == g.M[2]) ? R(0) : kz;
     const R kmag = kx * kx + ky * ky + kz * kz;
@@ -310,25 +315,28 @@ __global__ void __launch_bounds__(PASS_THREADS, 1) k_lines(SolveGeom<R> g, LineT
 constexpr int RL_THREADS = 256;
 
 template <typename R, int NC>
-__global__ void __launch_bounds__(RL_THREADS, 2) k_rlines(SolveGeom<R> g, LineTiles lt,
+__global__ void __launch_bounds__(RL_THREADS, RMinBlocks<R>::v) k_rlines(SolveGeom<R> g, LineTiles lt,
                                                           const typename cplx_t<R>::type *in,
                                                           typename cplx_t<R>::type *out, int axis, int lmode,
                                                           int zmode, int reproj, int use_zeta) {
   typedef typename cplx_t<R>::type C;
-  typedef typename Vec<R>::V V;
-  constexpr int G = Vec<R>::G;
+  typedef typename RVec<R>::V V;
+  constexpr int G = RVec<R>::G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const RegPlan &pl = (axis == 1) ? g.ry : g.rz;
   const int n = pl.n, TK = lt.TK, L = NC * TK, LG = L / G;
   C *tw = reinterpret_cast<C *>(smem_raw);
   int *zpos = reinterpret_cast<int *>(smem_raw + (((size_t)n * sizeof(C) + 15) & ~(size_t)15));
-  V *buf = reinterpret_cast<V *>(smem_raw + (((size_t)n * sizeof(C) + 15) & ~(size_t)15) +
-                                 (((size_t)n * sizeof(int) + 15) & ~(size_t)15));
+  R *kzs = reinterpret_cast<R *>(reinterpret_cast<unsigned char *>(zpos) + (((size_t)n * sizeof(int) + 15) & ~(size_t)15));
+  V *buf = reinterpret_cast<V *>(reinterpret_cast<unsigned char *>(kzs) + (((size_t)n * sizeof(R) + 15) & ~(size_t)15));
   {
     const C *twg = (axis == 1) ? g.rtwy : g.rtwz;
     for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = twg[i];
     if (lmode == L_Z)
-      for (int i = threadIdx.x; i < n; i += blockDim.x) zpos[i] = g.zk[i];
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        zpos[i] = g.zk[i];
+        kzs[i] = g.kzt[i];
+      }
   }
   __syncthreads();
   const int ntiles = lt.nouter * lt.nkt;
@@ -348,7 +356,7 @@ __global__ void __launch_bounds__(RL_THREADS, 2) k_rlines(SolveGeom<R> g, LineTi
     } else {
       rfft_fwd<R>(pl, buf, LG, lt.dLG, tw, true, false, gl);
       z_multiply<R, NC>(g, reinterpret_cast<C *>(buf), L, TK, kt * TK, g.yk ? g.yk[o] : o, zmode, reproj, use_zeta,
-                        zpos);
+                        zpos, kzs);
       __syncthreads();
       rfft_inv<R>(pl, buf, LG, lt.dLG, tw, false, true, gl);
     }
@@ -361,12 +369,12 @@ __global__ void __launch_bounds__(RL_THREADS, 2) k_rlines(SolveGeom<R> g, LineTi
 // its second half zero (not read), and the digit-reversed spectrum is addressed
 // through the frequency -> position table.
 template <typename R, int NC>
-__global__ void __launch_bounds__(RL_THREADS, 2) k_rxfwd(SolveGeom<R> g, const R *__restrict__ in,
+__global__ void __launch_bounds__(RL_THREADS, RMinBlocks<R>::v) k_rxfwd(SolveGeom<R> g, const R *__restrict__ in,
                                                          typename cplx_t<R>::type *__restrict__ X, int RB, int cs,
                                                          int vec16, FastDiv dLG) {
   typedef typename cplx_t<R>::type C;
-  typedef typename Vec<R>::V V;
-  constexpr int G = Vec<R>::G;
+  typedef typename RVec<R>::V V;
+  constexpr int G = RVec<R>::G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const RegPlan &pl = g.rx;
   const int N = pl.n, L = NC * RB, LG = L / G, H = g.H;
@@ -470,12 +478,12 @@ __global__ void __launch_bounds__(RL_THREADS, 2) k_rxfwd(SolveGeom<R> g, const R
 }
 
 template <typename R, int NC>
-__global__ void __launch_bounds__(RL_THREADS, 2) k_rxinv(SolveGeom<R> g,
+__global__ void __launch_bounds__(RL_THREADS, RMinBlocks<R>::v) k_rxinv(SolveGeom<R> g,
                                                          const typename cplx_t<R>::type *__restrict__ X,
                                                          R *__restrict__ outp, int RB, int cs, FastDiv dLG) {
   typedef typename cplx_t<R>::type C;
-  typedef typename Vec<R>::V V;
-  constexpr int G = Vec<R>::G;
+  typedef typename RVec<R>::V V;
+  constexpr int G = RVec<R>::G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const RegPlan &pl = g.rx;
   const int N = pl.n, L = NC * RB, LG = L / G, H = g.H;
