@@ -117,6 +117,15 @@ int pmgpu_poisson_solve(pmgpu_plan *plan, double *vort, double *vel, double *vec
 int pmgpu_poisson_solve_f32(pmgpu_plan *plan, float *vort, float *vel, float *vecpot,
                             int reg_vort, int reproj, int calc_vecpot);
 
+/* The solve on device arrays (no counterpart in the reference): same flags and
+ * results as pmgpu_poisson_solve, with d_vort / d_vel / d_vecpot device pointers of
+ * the plan's precision in the cuboid layout, queued on `stream` (a cudaStream_t;
+ * NULL = the legacy default stream) without synchronising.  d_vort is updated in
+ * place when reg_vort or reproj is set.  Calls that share a plan share its work
+ * buffers, so they must not overlap on the GPU. */
+int pmgpu_poisson_solve_dev(pmgpu_plan *plan, void *d_vort, void *d_vel, void *d_vecpot,
+                            int reg_vort, int reproj, int calc_vecpot, void *stream);
+
 /* pmlib_regularise, source/regularise/pmlib_regularise.f:5-21: Gaussian-polynomial
  * spectral filter of order reg_order and width filter_width on a field of nvar <= 3
  * components, in place. */
@@ -147,6 +156,23 @@ int pmgpu_remesh(const pmgpu_topo *topo, const double *mesh_vort, const double *
                  const double *mesh_vel, const unsigned char *mask, double min_vort,
                  double min_dvort, int incl_ghost, int max_part, double *pos, double *part_vort,
                  double *part_dvort, double *part_vel, int *npart);
+
+/* ---- batches of independent solves (no counterpart in the reference) ----
+ * A batch holds one plan per patch (patches of any sizes and boundary types, the same
+ * kernel parameters and precision); Green's spectra of identical grids are shared.
+ * pmgpu_batch_solve queues the velocity solve of every patch (d_vort[i] -> d_vel[i],
+ * device arrays in the cuboid layout) on `stream` without synchronising; the solves
+ * overlap on the device.  The first call runs directly and allocates the work
+ * buffers; the next call on a non-default stream captures the batch into a CUDA graph,
+ * which later calls with the same arrays and stream replay. */
+typedef struct pmgpu_batch pmgpu_batch;
+int pmgpu_batch_create(int npatch, const pmgpu_patch *patches, const pmgpu_topo *cuboids,
+                       const pmgpu_params *par, int precision, pmgpu_batch **batch);
+int pmgpu_batch_solve(pmgpu_batch *batch, void *const *d_vort, void *const *d_vel, void *stream);
+int pmgpu_batch_size(const pmgpu_batch *batch);
+/* the plan of patch i (owned by the batch) */
+pmgpu_plan *pmgpu_batch_plan(pmgpu_batch *batch, int i);
+void pmgpu_batch_destroy(pmgpu_batch *batch);
 
 /* Selects the line-FFT engine of plans created afterwards (no counterpart in the
  * reference): 0 = in-place register passes wherever the y / z lengths factor into

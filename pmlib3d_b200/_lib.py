@@ -18,7 +18,8 @@ EXPORTS = (
     "pmgpu_regularise", "pmgpu_regularise_f32", "pmgpu_plan_destroy",
     "pmgpu_step", "pmgpu_step_dev", "pmgpu_remesh", "pmgpu_last_error", "pmgpu_launch_count",
     "pmgpu_timing_enable", "pmgpu_timing_reset", "pmgpu_timing_get",
-    "pmgpu_interp_particle_mesh_noalloc", "pmgpu_fft_engine",
+    "pmgpu_interp_particle_mesh_noalloc", "pmgpu_fft_engine", "pmgpu_poisson_solve_dev",
+    "pmgpu_batch_create", "pmgpu_batch_solve", "pmgpu_batch_size", "pmgpu_batch_plan", "pmgpu_batch_destroy",
 )
 
 
@@ -83,12 +84,20 @@ def lib():
         "pmgpu_timing_get": [C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(C.c_longlong)],
         "pmgpu_interp_particle_mesh_noalloc": [TP, QP, vp, vp, C.c_int, C.c_int, vp, C.c_int, C.c_int, C.c_int, vp],
         "pmgpu_fft_engine": [C.c_int],
+        "pmgpu_poisson_solve_dev": [vp, vp, vp, vp, C.c_int, C.c_int, C.c_int, vp],
+        "pmgpu_batch_create": [C.c_int, PP, TP, QP, C.c_int, C.POINTER(vp)],
+        "pmgpu_batch_solve": [vp, C.POINTER(vp), C.POINTER(vp), vp],
+        "pmgpu_batch_size": [vp],
+        "pmgpu_batch_plan": [vp, C.c_int],
+        "pmgpu_batch_destroy": [vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
         f.argtypes = args
         f.restype = C.c_int
     L.pmgpu_plan_destroy.restype = None
+    L.pmgpu_batch_destroy.restype = None
+    L.pmgpu_batch_plan.restype = vp
     L.pmgpu_timing_enable.restype = None
     L.pmgpu_timing_reset.restype = None
     L.pmgpu_last_error.restype = C.c_char_p

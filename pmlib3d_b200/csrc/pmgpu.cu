@@ -16,6 +16,8 @@
 #include <complex>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -340,7 +342,8 @@ struct pmgpu_plan {
   FftDesc fx, fy, fz;
   DevBuf twx, twy, twz;
   DevBuf kxt, kyt, kzt;
-  DevBuf green;
+  DevBuf green;  // view of green_own (shared between plans of the same grid)
+  std::shared_ptr<DevBuf> green_own;
   int gM1, gM2;
   double eps;
   DevBuf X, Y, Y2, Y3;
@@ -355,7 +358,7 @@ struct pmgpu_plan {
   const int *perm;  // sorted order of the last deposit (device)
   int perm_n;
   ~pmgpu_plan() {
-    DevBuf *bs[] = {&twx, &twy, &twz, &kxt, &kyt, &kzt, &green, &X, &Y, &Y2, &Y3, &mesh_w, &mesh_u,
+    DevBuf *bs[] = {&twx, &twy, &twz, &kxt, &kyt, &kzt, &X, &Y, &Y2, &Y3, &mesh_w, &mesh_u,
                     &mesh_a, &mesh_b, &h_pos, &h_val, &h_out, &key, &val, &key2, &val2, &counts,
                     &start, &spart, &hist, &rtwx, &rtwy, &rtwz, &yk, &zk, &rextx, &xpos};
     for (DevBuf *b : bs) b->release();
@@ -658,11 +661,49 @@ static int run_regularise(pmgpu_plan *pl, R *mesh, int nvar, int reg_order, doub
 }
 
 // ------------------------------------------------------------------ Green's function
+// Spectra are shared by plans of the same grid, kernel parameters, precision and
+// device: the cache holds weak references, a spectrum lives while a plan uses it.
+static std::map<std::string, std::weak_ptr<DevBuf>> g_green_cache;
+
+static std::string green_key(const pmgpu_plan *pl) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  char b[512];
+  const pmgpu_patch &p = pl->patch;
+  snprintf(b, sizeof(b), "%d|%d|%a,%a,%a|%d,%d,%d|%d,%d,%d|%d,%d,%d,%d|%d,%d,%a", dev, pl->prec, p.dx[0], p.dx[1],
+           p.dx[2], pl->g.M[0], pl->g.M[1], pl->g.M[2], p.bound_cond[0], p.bound_cond[1], p.bound_cond[2], p.ncell[0],
+           p.ncell[1], p.ncell[2], p.nghost, pl->par.poisson_order, pl->par.poisson_kernel,
+           pl->par.regularisation_radius);
+  return std::string(b);
+}
+
+static void attach_green(pmgpu_plan *pl, const std::shared_ptr<DevBuf> &sp) {
+  pl->green_own = sp;
+  pl->green.p = sp->p;
+  pl->green.cap = sp->cap;
+  pl->green.fixed = true;
+}
+
 template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller) {
   const Geometry &G = pl->g;
   pl->gM1 = G.M[1] / 2 + 1;
   pl->gM2 = G.M[2] / 2 + 1;
   if (G.allper) return 0;
+  const std::string key = green_key(pl);
+  {
+    auto it = g_green_cache.find(key);
+    if (it != g_green_cache.end()) {
+      if (auto sp = it->second.lock()) {
+        attach_green(pl, sp);
+        return 0;
+      }
+      g_green_cache.erase(it);
+    }
+  }
+  std::shared_ptr<DevBuf> own(new DevBuf(), [](DevBuf *b) {
+    b->release();
+    delete b;
+  });
   GreenParams gp;
   memset(&gp, 0, sizeof(gp));
   double mdx = 0.0;
@@ -712,7 +753,8 @@ template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller)
     if (fwd_xy<double, 1>(gg, gr.as<double>(), gX.as<double2>(), gY.as<double2>(), 0, caller)) break;
     if (zpass<double, 1>(gg, gY.as<double2>(), gY.as<double2>(), Z_FORWARD, 0, 0, G.M[1], 0, caller)) break;
     const size_t noct = (size_t)pl->gM2 * pl->gM1 * G.H;
-    if (pl->green.ensure(sizeof(R) * noct, caller)) break;
+    if (own->ensure(sizeof(R) * noct, caller)) break;
+    attach_green(pl, own);
     const double f = pl->patch.dx[0] * pl->patch.dx[1] * pl->patch.dx[2] /
                      ((double)G.M[0] * (double)G.M[1] * (double)G.M[2]);
     k_green_octant<R><<<(unsigned)std::min<size_t>((noct + 255) / 256, 148 * 64), 256>>>(
@@ -720,6 +762,7 @@ template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller)
     PM_LAUNCHED();
     if (!cuda_ok(cudaGetLastError(), caller)) break;
     if (!cuda_ok(cudaDeviceSynchronize(), caller)) break;
+    g_green_cache[key] = own;
     rc = 0;
   } while (0);
   tx.release(); ty.release(); tz.release(); gr.release(); gX.release(); gY.release();
@@ -1040,10 +1083,9 @@ int pmgpu_interp_mesh_particle_f32(const pmgpu_topo *topo, const pmgpu_params *p
 }
 
 // ------------------------------------------------------------------ Poisson
-int pmgpu_poisson_setup(const pmgpu_patch *patch, const pmgpu_topo *cuboid, const pmgpu_params *par,
-                        int precision, pmgpu_plan **plan) {
-  const char *caller = "pmlib_poisson_setup";
-  std::lock_guard<std::mutex> lk(g_mu);
+// plan creation; the caller holds g_mu
+static int create_plan(const pmgpu_patch *patch, const pmgpu_topo *cuboid, const pmgpu_params *par, int precision,
+                       pmgpu_plan **plan, const char *caller) {
   if (!plan || !patch || !cuboid) {
     set_error(caller, "missing argument.");
     return -1;
@@ -1108,6 +1150,12 @@ int pmgpu_poisson_setup(const pmgpu_patch *patch, const pmgpu_topo *cuboid, cons
   return 0;
 }
 
+int pmgpu_poisson_setup(const pmgpu_patch *patch, const pmgpu_topo *cuboid, const pmgpu_params *par,
+                        int precision, pmgpu_plan **plan) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  return create_plan(patch, cuboid, par, precision, plan, "pmlib_poisson_setup");
+}
+
 void pmgpu_plan_destroy(pmgpu_plan *plan) {
   std::lock_guard<std::mutex> lk(g_mu);
   delete plan;
@@ -1139,6 +1187,24 @@ static int solve_host(pmgpu_plan *pl, R *vort, R *vel, R *vecpot, int reg_vort, 
   if (ifft_vort) CK(cudaMemcpy(vort, pl->mesh_w.p, sizeof(R) * nm, cudaMemcpyDeviceToHost), caller);
   if (ifft_vecpot) CK(cudaMemcpy(vecpot, pl->mesh_a.p, sizeof(R) * nm, cudaMemcpyDeviceToHost), caller);
   return 0;
+}
+
+int pmgpu_poisson_solve_dev(pmgpu_plan *plan, void *d_vort, void *d_vel, void *d_vecpot, int reg_vort, int reproj,
+                            int calc_vecpot, void *stream) {
+  const char *caller = "pmlib_poisson_solve";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!plan || !d_vort || !d_vel) {
+    set_error(caller, "missing argument.");
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  const int vp = calc_vecpot && d_vecpot ? 1 : 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->prec == PMGPU_FP64)
+    return run_solve<double>(plan, (const double *)d_vort, (double *)d_vel, (double *)d_vort, (double *)d_vecpot,
+                             reg_vort, reproj, vp, st, caller);
+  return run_solve<float>(plan, (const float *)d_vort, (float *)d_vel, (float *)d_vort, (float *)d_vecpot, reg_vort,
+                          reproj, vp, st, caller);
 }
 
 int pmgpu_poisson_solve(pmgpu_plan *plan, double *vort, double *vel, double *vecpot, int reg_vort, int reproj,
@@ -1415,4 +1481,166 @@ int pmgpu_fft_engine(int engine) {
   const int old = g_force_stockham;
   g_force_stockham = engine == 1 ? 1 : 0;
   return old;
+}
+
+// ------------------------------------------------------------------ batches of patches
+// Independent solves of patches of uneven sizes and boundary types.  Each patch has
+// its own plan (work buffers; the Green's spectra are shared through the cache when
+// grids coincide).  Patches are spread over a few internal streams, largest first
+// onto the least loaded stream, so small solves overlap on the device; the whole
+// batch is captured once into a CUDA graph and replayed while the caller passes the
+// same arrays on the same stream.
+struct pmgpu_batch {
+  int prec = 0;
+  std::vector<pmgpu_plan *> plans;
+  std::vector<int> lane;  // internal stream of each patch
+  std::vector<cudaStream_t> aux;
+  std::vector<cudaEvent_t> ev;  // [0] fork, [1 + k] join of stream k
+  bool warm = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t gstream = nullptr;
+  std::vector<void *> gptr;  // arrays the graph was captured with
+  ~pmgpu_batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    for (cudaStream_t s : aux) cudaStreamDestroy(s);
+    for (pmgpu_plan *p : plans) delete p;
+  }
+};
+
+namespace pmgpu {
+// queue every patch's solve: fork the internal streams off `st`, join them back
+static int batch_enqueue(pmgpu_batch *b, void *const *d_vort, void *const *d_vel, cudaStream_t st,
+                         const char *caller) {
+  CK(cudaEventRecord(b->ev[0], st), caller);
+  for (cudaStream_t s : b->aux) CK(cudaStreamWaitEvent(s, b->ev[0], 0), caller);
+  for (size_t i = 0; i < b->plans.size(); i++) {
+    pmgpu_plan *pl = b->plans[i];
+    cudaStream_t s = b->aux[b->lane[i]];
+    const int rc = b->prec == PMGPU_FP64
+                       ? run_solve<double>(pl, (const double *)d_vort[i], (double *)d_vel[i], nullptr, nullptr, 0, 0,
+                                           0, s, caller)
+                       : run_solve<float>(pl, (const float *)d_vort[i], (float *)d_vel[i], nullptr, nullptr, 0, 0, 0,
+                                          s, caller);
+    if (rc) return -1;
+  }
+  for (size_t k = 0; k < b->aux.size(); k++) {
+    CK(cudaEventRecord(b->ev[1 + k], b->aux[k]), caller);
+    CK(cudaStreamWaitEvent(st, b->ev[1 + k], 0), caller);
+  }
+  return 0;
+}
+}  // namespace pmgpu
+
+int pmgpu_batch_create(int npatch, const pmgpu_patch *patches, const pmgpu_topo *cuboids,
+                       const pmgpu_params *par, int precision, pmgpu_batch **batch) {
+  const char *caller = "pmgpu_batch_create";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!batch || npatch <= 0 || !patches || !cuboids) {
+    set_error(caller, "missing argument.");
+    return -1;
+  }
+  *batch = nullptr;
+  pmgpu_batch *b = new pmgpu_batch();
+  b->prec = precision;
+  for (int i = 0; i < npatch; i++) {
+    pmgpu_plan *pl = nullptr;
+    if (create_plan(&patches[i], &cuboids[i], par, precision, &pl, caller)) {
+      delete b;
+      return -1;
+    }
+    b->plans.push_back(pl);
+  }
+  const int ns = std::min(npatch, 8);
+  std::vector<int> order(npatch);
+  for (int i = 0; i < npatch; i++) order[i] = i;
+  auto work = [&](int i) {
+    const Geometry &G = b->plans[i]->g;
+    return (double)G.M[0] * G.M[1] * G.M[2];
+  };
+  std::sort(order.begin(), order.end(), [&](int a, int c) { return work(a) > work(c); });
+  std::vector<double> load(ns, 0.0);
+  b->lane.assign(npatch, 0);
+  for (int i : order) {
+    const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    b->lane[i] = k;
+    load[k] += work(i);
+  }
+  b->aux.resize(ns);
+  b->ev.resize(ns + 1);
+  for (int k = 0; k < ns; k++)
+    if (!cuda_ok(cudaStreamCreateWithFlags(&b->aux[k], cudaStreamNonBlocking), caller)) {
+      b->aux.resize(k);
+      delete b;
+      return -1;
+    }
+  for (int k = 0; k <= ns; k++)
+    if (!cuda_ok(cudaEventCreateWithFlags(&b->ev[k], cudaEventDisableTiming), caller)) {
+      b->ev.resize(k);
+      delete b;
+      return -1;
+    }
+  *batch = b;
+  return 0;
+}
+
+int pmgpu_batch_solve(pmgpu_batch *b, void *const *d_vort, void *const *d_vel, void *stream) {
+  const char *caller = "pmgpu_batch_solve";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!b || !d_vort || !d_vel) {
+    set_error(caller, "missing argument.");
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t np = b->plans.size();
+  std::vector<void *> ptrs(d_vort, d_vort + np);
+  ptrs.insert(ptrs.end(), d_vel, d_vel + np);
+  if (b->exec && b->gstream == st && b->gptr == ptrs) {
+    CK(cudaGraphLaunch(b->exec, st), caller);
+    return 0;
+  }
+  if (!b->warm || st == nullptr) {
+    // first call (allocates the work buffers) or the legacy stream: run directly
+    if (batch_enqueue(b, d_vort, d_vel, st, caller)) return -1;
+    b->warm = true;
+    return 0;
+  }
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  if (b->graph) {
+    cudaGraphDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed), caller);
+  const int rc = batch_enqueue(b, d_vort, d_vel, st, caller);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(st, &g);
+  if (rc || e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    if (!rc) cuda_ok(e, caller);
+    return -1;
+  }
+  b->graph = g;
+  CK(cudaGraphInstantiate(&b->exec, g, 0), caller);
+  b->gstream = st;
+  b->gptr = ptrs;
+  CK(cudaGraphLaunch(b->exec, st), caller);
+  return 0;
+}
+
+int pmgpu_batch_size(const pmgpu_batch *b) { return b ? (int)b->plans.size() : 0; }
+
+pmgpu_plan *pmgpu_batch_plan(pmgpu_batch *b, int i) {
+  if (!b || i < 0 || i >= (int)b->plans.size()) return nullptr;
+  return b->plans[i];
+}
+
+void pmgpu_batch_destroy(pmgpu_batch *b) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  delete b;
 }

@@ -131,11 +131,13 @@ class Plan:
 
     handle: C.c_void_p
     precision: int
-    topo: Topo
+    topo: Topo = None
+    owned: bool = True
 
     def close(self):
         if self.handle:
-            lib().pmgpu_plan_destroy(self.handle)
+            if self.owned:
+                lib().pmgpu_plan_destroy(self.handle)
             self.handle = None
 
     def __del__(self):
@@ -202,6 +204,53 @@ def pmlib_interp_particle_mesh_noalloc(topo: Topo, params: Params, d_xpart: int,
                                                     C.c_void_p(d_part), int(nvar), int(npart), C.c_void_p(d_mesh),
                                                     int(nvar_mesh), int(bool(clear)), int(bool(clear_ghost)),
                                                     C.c_void_p(stream))
+
+
+def pmlib_poisson_solve_dev(plan: Plan, d_vort: int, d_vel: int, d_vecpot: int = 0, reg_vort=False, reproj=False,
+                            calc_vecpot=False, stream: int = 0) -> int:
+    """pmlib_poisson_solve on device arrays (pointers of the plan's precision), queued
+    on ``stream`` without synchronising."""
+    return lib().pmgpu_poisson_solve_dev(plan.handle, C.c_void_p(d_vort), C.c_void_p(d_vel),
+                                         C.c_void_p(d_vecpot or None), int(bool(reg_vort)), int(bool(reproj)),
+                                         int(bool(calc_vecpot)), C.c_void_p(stream or None))
+
+
+class Batch:
+    """Independent velocity solves of patches of uneven sizes and boundary types
+    (pmgpu_batch_*): one plan per patch, solves overlapping on the device, replayed
+    from a captured CUDA graph after the first two calls on a stream."""
+
+    def __init__(self, patches, topos, params: Params, precision: int):
+        n = len(patches)
+        pa = (Patch * n)(*patches)
+        ta = (Topo * n)(*topos)
+        h = C.c_void_p()
+        if lib().pmgpu_batch_create(n, pa, ta, C.byref(params), int(precision), C.byref(h)) != 0:
+            raise RuntimeError(last_error())
+        self.handle = h
+        self.n = n
+        self.precision = precision
+
+    def plan(self, i: int) -> "Plan":
+        """A non-owning view of patch i's plan (valid while the batch lives)."""
+        return Plan(C.c_void_p(lib().pmgpu_batch_plan(self.handle, i)), self.precision, None, owned=False)
+
+    def solve(self, d_vort, d_vel, stream: int = 0) -> int:
+        """d_vort[i] -> d_vel[i] for every patch (device pointers)."""
+        vp = C.c_void_p * self.n
+        return lib().pmgpu_batch_solve(self.handle, vp(*[C.c_void_p(x) for x in d_vort]),
+                                       vp(*[C.c_void_p(x) for x in d_vel]), C.c_void_p(stream or None))
+
+    def close(self):
+        if self.handle:
+            lib().pmgpu_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def fft_engine(engine: int) -> int:

@@ -11,6 +11,12 @@ configurations with their shapes and value distributions:
   omega.  16.7 M particles.
 * ``rings128`` / ``rings192``: the same field on 128^3 / 192^3 cells (scaling,
   test and profiling points).
+* ``batched96`` (:func:`batch_specs`): 96 independent patches, cells per axis
+  log-uniform in [32, 192], boundary types drawn from {fff, ppf, pff} (periodic
+  counts rounded to even), h = 1/64, each holding a Gaussian blob
+  exp(-r^2 / (0.2 L)^2) of vorticity along a random axis (L the longest side).  Free
+  axes are then grown by pmlib_patch_adjust, as the reference's programs do, so the
+  transform lengths are multiples of 32.
 
 Particles sit one per interior cell centre in pmlib_remesh order (k-j-i, x fastest;
 source/remesh/pmlib_remesh.f:151-226), jittered by U(-0.1 h, 0.1 h) per axis.  The
@@ -121,3 +127,64 @@ def model_bytes(n: int, nghost: int = 4, w: int = 4, npart: int | None = None) -
     passes["solve"] = sum(passes[k] for k in ("x_fwd", "y_fwd", "z_pass", "y_inv", "x_inv"))
     passes["step"] = passes["solve"] + passes["deposit"] + passes["m2p"]
     return passes
+
+
+BC_TYPES = {"fff": (0, 0, 0), "ppf": (1, 1, 0), "pff": (1, 0, 0)}
+
+
+def batch_specs(count: int = 96, nmin: int = 32, nmax: int = 192, seed_id: int = 3, h: float = 1.0 / 64):
+    """Patch descriptions of the batched workload: dicts with xmin, xmax, dx,
+    bound_cond, bc (name) and axis (vorticity direction), before pmlib_patch_adjust."""
+    rng = np.random.Generator(np.random.Philox(SEED + seed_id))
+    out = []
+    for _ in range(count):
+        n = np.exp(rng.uniform(np.log(nmin), np.log(nmax), 3))
+        bcn = ("fff", "ppf", "pff")[int(rng.integers(0, 3))]
+        bc = BC_TYPES[bcn]
+        cells = []
+        for d in range(3):
+            c = int(round(n[d]))
+            if bc[d]:
+                c += c % 2  # periodic transform lengths must be even
+            cells.append(c)
+        L = np.array(cells, dtype=np.float64) * h
+        out.append({"xmin": tuple(-0.5 * L), "xmax": tuple(0.5 * L), "dx": (h, h, h), "bound_cond": bc,
+                    "bc": bcn, "ncell": tuple(cells), "axis": int(rng.integers(0, 3))})
+    return out
+
+
+def blob_field(topo, axis: int, xp=np):
+    """Vorticity exp(-r^2 / (0.2 L)^2) e_axis on the cuboid of `topo` (ghosts included),
+    as an array of shape (nz', ny', nx', 3) (``xp`` = numpy or torch)."""
+    axes = []
+    for d in range(3):
+        lo, hi = 1 - topo.nghost[2 * d], topo.ncell[d] + topo.nghost[2 * d + 1]
+        i = np.arange(lo, hi + 1, dtype=np.float64)
+        axes.append(topo.xmin[d] + (i - 0.5) * topo.dx[d])
+    c = [0.5 * (topo.xmin[d] + topo.xmax[d]) for d in range(3)]
+    L = max(topo.xmax[d] - topo.xmin[d] for d in range(3))
+    if xp is np:
+        z, y, x = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
+        g = np.exp(-((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2) / (0.2 * L) ** 2)
+        out = np.zeros(g.shape + (3,))
+        out[..., axis] = g
+        return out
+    import torch
+    dev = "cuda"
+    ax = [torch.as_tensor(a, device=dev) for a in axes]
+    z, y, x = torch.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+    g = torch.exp(-((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2) / (0.2 * L) ** 2)
+    out = torch.zeros(g.shape + (3,), dtype=torch.float64, device=dev)
+    out[..., axis] = g
+    return out
+
+
+def solve_bytes(M, P, w: int = 4) -> int:
+    """Algorithmic bytes of one velocity solve (5-pass model) on a grid with FFT
+    lengths M and pencil extents P (free axis: M = 2P)."""
+    H = M[0] // 2 + 1
+    c = 2 * w
+    V = P[0] * P[1] * P[2]
+    X = H * P[1] * P[2]
+    Y = H * M[1] * P[2]
+    return 3 * w * V + 3 * c * X * 4 + 3 * c * Y * 4 + w * H * M[1] * M[2] + 3 * w * V
