@@ -29,7 +29,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "256^3 vortex steps/s (FP32 form; FP64 plain path and rel-L2 alongside)"
+METRIC = "256^3 vortex steps/s (FP32 form; FP64 plain path and rel-L2 alongside; batched and served solves/s, p50/p99)"
 L2_NOTE = "inputs and intermediates larger than the 126 MB L2 (no flush)"
 
 
@@ -155,6 +155,72 @@ def run_reference(args):
     return 0
 
 
+# ------------------------------------------------------------------ batched and served solves
+def run_batched(P, Wl, torch, steps, warmup, count=96):
+    """96 patches of uneven sizes and boundary types (FP32 form), one batch solve per
+    step replayed from a CUDA graph; solves/s and the 5-pass model bytes per second."""
+    specs = Wl.batch_specs(count)
+    par = P.make_params(order=6, kernel=1, radius=2.0, interp=3)
+    patches, topos, vort, nbytes = [], [], [], 0
+    for s in specs:
+        pa = P.make_patch(s["xmin"], s["xmax"], s["dx"], bound_cond=s["bound_cond"], nghost=4)
+        assert P.pmlib_patch_adjust(pa) == 0
+        ierr, t = P.pmlib_topology_cuboid(pa, 3)
+        patches.append(pa)
+        topos.append(t)
+        vort.append(Wl.blob_field(t, s["axis"], xp=torch).float().contiguous())
+        per = [t.bound_cond[2 * d] != 0 for d in range(3)]
+        Pp = [t.ncell[d] if per[d] else t.ncell[d] + t.nghost[2 * d] + t.nghost[2 * d + 1] for d in range(3)]
+        M = [Pp[d] if per[d] else 2 * Pp[d] for d in range(3)]
+        nbytes += Wl.solve_bytes(M, Pp, 4)
+    t0 = time.perf_counter()
+    b = P.Batch(patches, topos, par, P.FP32)
+    setup_s = time.perf_counter() - t0
+    vel = [torch.empty_like(w) for w in vort]
+    wp, up = [w.data_ptr() for w in vort], [u.data_ptr() for u in vel]
+    st = torch.cuda.Stream()
+    with torch.cuda.stream(st):
+        for _ in range(max(2, warmup)):
+            assert b.solve(wp, up, st.cuda_stream) == 0, P.last_error()
+        st.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            b.solve(wp, up, st.cuda_stream)
+        e1.record(st)
+        st.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    cells = sum(int(np.prod(s["ncell"])) for s in specs)
+    b.close()
+    return {"workload": f"batched{count}: {count} patches, cells per axis log-uniform in [32,192] before "
+                        f"pmlib_patch_adjust, bc from {{fff, ppf, pff}}, Gaussian blob along a random axis, "
+                        f"h = 1/64, FP32 form, FP64 Green's set-up",
+            "solves_per_s": count / (ms / 1e3), "ms_per_batch": ms, "cells": cells,
+            "model_bytes_per_batch": nbytes, "achieved_gbs": nbytes / (ms / 1e3) / 1e9,
+            "setup_s": setup_s, "graph": "captured CUDA graph, 8 internal streams"}
+
+
+def run_served(P, torch, rates=(100.0, 300.0, 1000.0), count=60, budget_gb=24.0):
+    """Served stream at swept Poisson arrival rates (FP32 form): solves/s, p50/p99."""
+    from pmlib3d_b200 import serve as S
+    par = P.make_params(order=6, kernel=1, radius=2.0, interp=3)
+    out = []
+    for k, rate in enumerate(rates):
+        reqs = S.request_stream(count, rate=rate, seed=10 + k)
+        torch.cuda.synchronize()
+        srv = S.Server(par, precision=P.FP32, slots=8, budget=int(budget_gb * 1e9))
+        rep = srv.run(reqs)
+        srv.close()
+        rep["rate_per_s"] = rate
+        out.append(rep)
+        del reqs
+        torch.cuda.empty_cache()
+    return {"workload": f"served: Poisson arrivals, cells per axis log-uniform 32-256, bc from {{fff, ppf, pff}}, "
+                        f"Gaussian blob or ring along a random axis, FP32 form, {count} requests per rate, "
+                        f"HBM budget {budget_gb:g} GB, 8 slots, Green's spectra cached per grid",
+            "sweep": out}
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -169,6 +235,7 @@ def main():
                     help="profile: only the FP32 warm-up and timed steps (for ncu captures)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"],
                     help="precision of --mode profile")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched and served measurements")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -325,6 +392,16 @@ def main():
         e2e = {"value": world * ke / dt, "unit": "steps/s", "h2d_bytes_per_step": 24 * n,
                "d2h_bytes_per_step": 12 * n, "api": "pmgpu_step (host pointers, pinned)"}
 
+    # ---- batched uneven patches (every rank: replicas) and the served stream (rank 0)
+    batched = served = None
+    if not args.no_batched:
+        batched = run_batched(P, Wl, torch, max(3, args.steps // 2), args.warmup)
+        bt = max_over_ranks(batched["ms_per_batch"])
+        batched["solves_per_s"] = world * 96 / (bt / 1e3)
+        if rank == 0:
+            served = run_served(P, torch)
+        barrier()
+
     # ---- CPU baseline: the oracle on this box's host cores (rank 0, one GPU only)
     cpu = None
     if not args.no_cpu_baseline and world == 1 and rank == 0:
@@ -350,7 +427,7 @@ def main():
             "fp32_speedup_vs_fp64": value / value64,
             "accuracy": {"rel_l2_fp32_vs_fp64": rel_l2, "max_rel_err": max_err},
             "roofline": roofline, "kernels": kernels, "gpu_launches": launches32,
-            "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
+            "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "batched": batched, "served": served,
         }
         print(json.dumps(line), flush=True)
     for p in (plan32, plan64):

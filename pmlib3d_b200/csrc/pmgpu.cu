@@ -116,22 +116,30 @@ struct DevBuf {
   void *p = nullptr;
   size_t cap = 0;
   bool fixed = false;  // a view of preallocated memory: never allocates or frees
+  bool stream_ordered = false;  // allocate / free ordered on the legacy stream (no device-wide sync)
   int ensure(size_t bytes, const char *caller) {
     if (bytes <= cap && p) return 0;
     if (fixed) {
       set_error(caller, "scratch size exceeds the fixed device scratch area.");
       return -1;
     }
-    if (p) cudaFree(p);
+    if (p) {
+      if (stream_ordered) cudaFreeAsync(p, 0);
+      else cudaFree(p);
+    }
     p = nullptr;
     cap = 0;
     size_t b = std::max<size_t>(bytes, 256);
-    CK(cudaMalloc(&p, b), caller);
+    if (stream_ordered) CK(cudaMallocAsync(&p, b, 0), caller);
+    else CK(cudaMalloc(&p, b), caller);
     cap = b;
     return 0;
   }
   void release() {
-    if (p && !fixed) cudaFree(p);
+    if (p && !fixed) {
+      if (stream_ordered) cudaFreeAsync(p, 0);
+      else cudaFree(p);
+    }
     p = nullptr;
     cap = 0;
   }
@@ -733,7 +741,10 @@ template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller)
   gg.Hp = G.Hp;
   gg.N2 = G.N2;
   std::vector<cld> tw;
+  // temporaries are stream-ordered on the legacy stream, so a set-up does not wait
+  // for (or stall) solves running on other streams
   DevBuf tx, ty, tz, gr, gX, gY;
+  for (DevBuf *t : {&tx, &ty, &tz, &gr, &gX, &gY}) t->stream_ordered = true;
   int rc = -1;
   do {
     if (!make_fft(G.N2, G.M[0], gg.fx, tw) || upload_tw<double>(tw, tx, caller)) break;
@@ -761,11 +772,12 @@ template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller)
         gY.as<double2>(), G.M[1], G.H, G.Hp, pl->gM1, pl->gM2, f, pl->green.as<R>());
     PM_LAUNCHED();
     if (!cuda_ok(cudaGetLastError(), caller)) break;
-    if (!cuda_ok(cudaDeviceSynchronize(), caller)) break;
+    if (!cuda_ok(cudaStreamSynchronize(0), caller)) break;
     g_green_cache[key] = own;
     rc = 0;
   } while (0);
   tx.release(); ty.release(); tz.release(); gr.release(); gX.release(); gY.release();
+  cudaStreamSynchronize(0);
   return rc;
 }
 
