@@ -133,7 +133,10 @@ int pmgpu_regularise(pmgpu_plan *plan, double *mesh, int nvar, int reg_order, do
 int pmgpu_regularise_f32(pmgpu_plan *plan, float *mesh, int nvar, int reg_order,
                          double filter_width);
 
-/* replaces the deallocation of mesh%pkernel_fft (source/pmlib_finalise.f:63) */
+/* Replaces the deallocation of mesh%pkernel_fft (source/pmlib_finalise.f:63).  The
+ * plan's device memory returns to the device's stream-ordered pool without
+ * synchronising the device, so call it only when no work that uses the plan is still
+ * in flight on any stream. */
 void pmgpu_plan_destroy(pmgpu_plan *plan);
 
 /* ---- the whole step: P2M -> unbounded solve + curl -> M2P ----

@@ -107,16 +107,30 @@ static int ensure_device(const char *caller) {
     set_error(caller, "could not upload the DFT constant tables.");
     return -1;
   }
+  {
+    // the Green's-function set-up takes its temporaries from the device's stream-
+    // ordered pool; keep freed blocks in the pool instead of returning them to the
+    // driver at every synchronisation (remapping gigabytes per plan)
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      unsigned long long thr = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+  }
   if (dev >= 0 && dev < 128) g_dev_ready[dev] = true;
   return 0;
 }
 
 // ------------------------------------------------------------------ device buffers
+// Device buffers come from the device's stream-ordered pool (freed blocks stay in
+// the pool): allocating or freeing never synchronises the whole device, so plans can
+// be created and destroyed while other streams run.  A buffer is freed in order on
+// the legacy stream; its owner frees it only when no work using it is in flight.
 struct DevBuf {
   void *p = nullptr;
   size_t cap = 0;
   bool fixed = false;  // a view of preallocated memory: never allocates or frees
-  bool stream_ordered = false;  // allocate / free ordered on the legacy stream (no device-wide sync)
+  bool stream_ordered = true;
   int ensure(size_t bytes, const char *caller) {
     if (bytes <= cap && p) return 0;
     if (fixed) {
@@ -130,8 +144,12 @@ struct DevBuf {
     p = nullptr;
     cap = 0;
     size_t b = std::max<size_t>(bytes, 256);
-    if (stream_ordered) CK(cudaMallocAsync(&p, b, 0), caller);
-    else CK(cudaMalloc(&p, b), caller);
+    if (stream_ordered) {
+      CK(cudaMallocAsync(&p, b, 0), caller);
+      CK(cudaStreamSynchronize(0), caller);  // usable from every stream from here on
+    } else {
+      CK(cudaMalloc(&p, b), caller);
+    }
     cap = b;
     return 0;
   }
@@ -744,7 +762,6 @@ template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller)
   // temporaries are stream-ordered on the legacy stream, so a set-up does not wait
   // for (or stall) solves running on other streams
   DevBuf tx, ty, tz, gr, gX, gY;
-  for (DevBuf *t : {&tx, &ty, &tz, &gr, &gX, &gY}) t->stream_ordered = true;
   int rc = -1;
   do {
     if (!make_fft(G.N2, G.M[0], gg.fx, tw) || upload_tw<double>(tw, tx, caller)) break;
