@@ -138,16 +138,17 @@ __global__ void k_green_real(GreenParams gp, double *__restrict__ gr) {
   }
 }
 
-// octant of the real spectrum, scaled by dx dy dz / (Mx My Mz), in the plan precision
+// octant of the real spectrum, scaled by dx dy dz / (Mx My Mz), in the plan precision;
+// yrow / zrow: frequency -> row of the transformed spectrum along y / z
 template <typename R>
 __global__ void k_green_octant(const double2 *__restrict__ spec, int M1, int H, int Hp, int gM1, int gM2, double f,
-                               R *__restrict__ out) {
+                               const int *__restrict__ yrow, const int *__restrict__ zrow, R *__restrict__ out) {
   const size_t total = (size_t)gM2 * gM1 * H;
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
     const int kx = (int)(t % H);
     const int iy = (int)((t / H) % gM1);
     const int iz = (int)(t / ((size_t)H * gM1));
-    out[t] = (R)(spec[((size_t)iz * M1 + iy) * Hp + kx].x * f);
+    out[t] = (R)(spec[((size_t)zrow[iz] * M1 + yrow[iy]) * Hp + kx].x * f);
   }
 }
 

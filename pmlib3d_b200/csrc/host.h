@@ -52,41 +52,42 @@ static inline int pick_tk(int n, int nc, size_t csize, int ntw) {
 static inline size_t lines_smem(int n, int nc, int tk, size_t csize, int ntw) {
   return tw_bytes(ntw, csize) + 3 * (size_t)nc * tk * n * csize;
 }
-// register engine: twiddles w_n^q + position table + wavenumbers + one tile buffer
-static inline size_t reg_smem(int n, int nc, int tk, size_t csize) {
-  return (((size_t)n * csize + 15) & ~(size_t)15) + (((size_t)n * 4 + 15) & ~(size_t)15) +
-         (((size_t)n * csize / 2 + 15) & ~(size_t)15) + (size_t)nc * tk * n * csize;
+// register engine: twiddles w_m^q + position table + wavenumbers (+ Bluestein chirp
+// and spectrum) + one tile buffer; n = line length, m = transform length (m = n
+// unless Bluestein)
+static inline size_t reg_smem(int n, int m, int nc, int tk, size_t csize) {
+  const size_t blue = m != n ? (((size_t)(n + m) * csize + 15) & ~(size_t)15) : 0;
+  return (((size_t)m * csize + 15) & ~(size_t)15) + (((size_t)n * 4 + 15) & ~(size_t)15) +
+         (((size_t)n * csize / 2 + 15) & ~(size_t)15) + blue + (size_t)nc * tk * m * csize;
 }
 // shared memory per CTA that lets the register-engine kernels run as many CTAs per
 // SM as their register budget allows (FP32: 3, FP64: 2; 228 KB per SM)
 static inline size_t reg_budget(size_t rsize) { return rsize == 4 ? (size_t)74 * 1024 : (size_t)112 * 1024; }
 // kx tile of the register engine: within the budget if possible, else one CTA per SM
-static inline int pick_tk_reg(int n, int nc, size_t csize, int Hp, size_t budget1) {
+static inline int pick_tk_reg(int n, int m, int nc, size_t csize, int Hp, size_t budget1) {
   for (size_t budget : {budget1, PASS_SMEM_BUDGET})
     for (int tk = 8; tk >= 1; tk /= 2) {
       if (Hp % tk) continue;
-      if (reg_smem(n, nc, tk, csize) <= budget) return tk;
+      if (reg_smem(n, m, nc, tk, csize) <= budget) return tk;
     }
   return 0;
 }
 // rows per tile of the register-engine x passes (table bytes + staging + buffer),
 // two CTAs per SM if possible
-static inline int pick_rb_reg(int N, int H, int P0, int Hp, int nc, size_t csize, size_t rsize, bool inverse,
-                              size_t budget1) {
-  const size_t tabs = (((size_t)N * csize + 15) & ~(size_t)15) + (((size_t)H * csize + 15) & ~(size_t)15) +
-                      (((size_t)N * 4 + 15) & ~(size_t)15);
-  for (size_t budget : {budget1, PASS_SMEM_BUDGET})
-    for (int rb = 16; rb >= 1; rb--) {
-      const size_t stage = inverse ? (size_t)rb * Hp * nc * csize : (((size_t)rb * P0 * nc * rsize + 15) / 16) * 16;
-      if (tabs + stage + (size_t)nc * rb * N * csize <= budget) return rb;
-    }
-  return 0;
-}
-static inline size_t rx_smem(int N, int H, int P0, int Hp, int nc, int rb, size_t csize, size_t rsize, bool inverse) {
-  const size_t tabs = (((size_t)N * csize + 15) & ~(size_t)15) + (((size_t)H * csize + 15) & ~(size_t)15) +
-                      (((size_t)N * 4 + 15) & ~(size_t)15);
+static inline size_t rx_smem(int N, int m, int H, int P0, int Hp, int nc, int rb, size_t csize, size_t rsize,
+                             bool inverse) {
+  const size_t blue = m != N ? (((size_t)(N + m) * csize + 15) & ~(size_t)15) : 0;
+  const size_t tabs = (((size_t)m * csize + 15) & ~(size_t)15) + (((size_t)H * csize + 15) & ~(size_t)15) +
+                      (((size_t)N * 4 + 15) & ~(size_t)15) + blue;
   const size_t stage = inverse ? (size_t)rb * Hp * nc * csize : (((size_t)rb * P0 * nc * rsize + 15) / 16) * 16;
-  return tabs + stage + (size_t)nc * rb * N * csize;
+  return tabs + stage + (size_t)nc * rb * m * csize;
+}
+static inline int pick_rb_reg(int N, int m, int H, int P0, int Hp, int nc, size_t csize, size_t rsize, bool inverse,
+                              size_t budget1) {
+  for (size_t budget : {budget1, PASS_SMEM_BUDGET})
+    for (int rb = 16; rb >= 1; rb--)
+      if (rx_smem(N, m, H, P0, Hp, nc, rb, csize, rsize, inverse) <= budget) return rb;
+  return 0;
 }
 
 // rows per tile of the x passes

@@ -25,8 +25,9 @@ static int launch_lines(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typ
                         const char *caller) {
   typedef typename cplx_t<R>::type C;
   const int n = g.M[axis];
-  if ((axis == 1 ? g.ry_ok : g.rz_ok) && !(lmode == L_FWD && axis == 2)) {
-    const int TK = pick_tk_reg(n, NC, sizeof(C), g.Hp, reg_budget(sizeof(R)));
+  if (axis == 1 ? g.ry_ok : g.rz_ok) {
+    const int mt = (axis == 1 ? g.ry : g.rz).n;  // transform length (Bluestein: > n)
+    const int TK = pick_tk_reg(n, mt, NC, sizeof(C), g.Hp, reg_budget(sizeof(R)));
     if (TK > 0) {
       LineTiles lt;
       lt.n = n;
@@ -40,7 +41,7 @@ static int launch_lines(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typ
       lt.nkt = g.Hp / TK;
       lt.TK = TK;
       lt.dLG = make_fastdiv((unsigned)(NC * TK / RVec<R>::G));
-      const size_t sm = reg_smem(n, NC, TK, sizeof(C));
+      const size_t sm = reg_smem(n, mt, NC, TK, sizeof(C));
       CK(cudaFuncSetAttribute(k_rlines<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
       int per = 1;
       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rlines<R, NC>, RL_THREADS, sm) != cudaSuccess ||
@@ -86,9 +87,9 @@ int fwd_xy(SolveGeom<R> &g, const R *in, typename cplx_t<R>::type *X, typename c
   const bool vec16r = cs == NC && ((size_t)g.ext[0] * NC * sizeof(R)) % 16 == 0 &&
                       ((size_t)g.off[0] * NC * sizeof(R)) % 16 == 0 && ((size_t)g.P[0] * NC * sizeof(R)) % 16 == 0;
   if (g.rx_ok) {
-    const int RB = pick_rb_reg(g.N2, g.H, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), false, reg_budget(sizeof(R)));
+    const int RB = pick_rb_reg(g.N2, g.rx.n, g.H, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), false, reg_budget(sizeof(R)));
     if (RB > 0) {
-      const size_t sm = rx_smem(g.N2, g.H, g.P[0], g.Hp, NC, RB, sizeof(C), sizeof(R), false);
+      const size_t sm = rx_smem(g.N2, g.rx.n, g.H, g.P[0], g.Hp, NC, RB, sizeof(C), sizeof(R), false);
       CK(cudaFuncSetAttribute(k_rxfwd<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
       const int rows = g.P[1] * g.P[2];
       const int ntiles = (rows + RB - 1) / RB;
@@ -152,9 +153,9 @@ int inv_yx(SolveGeom<R> &g, const pmgpu_topo *topo, typename cplx_t<R>::type *Y,
       return -1;
   }
   const int rows = g.P[1] * g.P[2];
-  const int RBr = g.rx_ok ? pick_rb_reg(g.N2, g.H, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), true, reg_budget(sizeof(R))) : 0;
+  const int RBr = g.rx_ok ? pick_rb_reg(g.N2, g.rx.n, g.H, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), true, reg_budget(sizeof(R))) : 0;
   if (RBr > 0) {
-    const size_t sm = rx_smem(g.N2, g.H, g.P[0], g.Hp, NC, RBr, sizeof(C), sizeof(R), true);
+    const size_t sm = rx_smem(g.N2, g.rx.n, g.H, g.P[0], g.Hp, NC, RBr, sizeof(C), sizeof(R), true);
     CK(cudaFuncSetAttribute(k_rxinv<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
     const int ntiles = (rows + RBr - 1) / RBr;
     int per = 1;

@@ -338,6 +338,65 @@ static std::vector<int> regplan_positions(const RegPlan &pl) {
   return k;
 }
 
+// forward DFT in long double, any length whose prime factors are small (mixed radix,
+// decimation in time, recursive); used for the Bluestein spectra
+static void host_dft(std::vector<cld> &a) {
+  const size_t n = a.size();
+  if (n <= 1) return;
+  size_t p = 2;
+  while (p * p <= n && n % p) p++;
+  if (n % p) p = n;
+  const size_t m = n / p;
+  std::vector<std::vector<cld>> sub(p, std::vector<cld>(m));
+  for (size_t j = 0; j < m; j++)
+    for (size_t r = 0; r < p; r++) sub[r][j] = a[j * p + r];
+  if (m > 1)
+    for (size_t r = 0; r < p; r++) host_dft(sub[r]);
+  const long double twopi = 2.0L * acosl(-1.0L);
+  for (size_t k = 0; k < n; k++) {
+    cld acc(0.0L, 0.0L);
+    for (size_t r = 0; r < p; r++) {
+      const long double ang = -twopi * (long double)((r * k) % n) / (long double)n;
+      acc += sub[r][k % m] * cld(cosl(ang), sinl(ang));
+    }
+    a[k] = acc;
+  }
+}
+
+// Bluestein plan for a line of length n: the convolution length m is the smallest
+// m >= 2n - 1 with a register plan
+static bool make_bluestein(int n, RegPlan &pl) {
+  for (int m = 2 * n - 1; m <= 4 * n; m++)
+    if (make_regplan(m, pl)) {
+      pl.bl = 1;
+      pl.bn = n;
+      return true;
+    }
+  return false;
+}
+
+// chirp c[j] = exp(-i pi j^2 / n) and B = DFT_m of conj(c) wrapped (B[q] at the
+// plan's position q)
+template <typename C, typename R>
+static void bluestein_tables(const RegPlan &pl, std::vector<C> &chirp, std::vector<C> &bpos) {
+  const int n = pl.bn, m = pl.n;
+  const long double pi = acosl(-1.0L);
+  std::vector<cld> c(n), b(m, cld(0.0L, 0.0L));
+  for (int j = 0; j < n; j++) {
+    const long long q = ((long long)j * j) % (2LL * n);
+    const long double a = -pi * (long double)q / (long double)n;
+    c[j] = cld(cosl(a), sinl(a));
+  }
+  b[0] = std::conj(c[0]);
+  for (int j = 1; j < n; j++) b[j] = b[m - j] = std::conj(c[j]);
+  host_dft(b);
+  const std::vector<int> kp = regplan_positions(pl);
+  chirp.resize(n);
+  bpos.resize(m);
+  for (int j = 0; j < n; j++) chirp[j] = mk((R)c[j].real(), (R)c[j].imag());
+  for (int q = 0; q < m; q++) bpos[q] = mk((R)b[kp[q]].real(), (R)b[kp[q]].imag());
+}
+
 static int g_nsm = 0;
 int num_sms() {
   if (g_nsm == 0) {
@@ -377,6 +436,7 @@ struct pmgpu_plan {
   int rx_ok, ry_ok, rz_ok;
   RegPlan rx, ry, rz;
   DevBuf rtwx, rtwy, rtwz, yk, zk, rextx, xpos;
+  DevBuf rchx, rchy, rchz, rbx, rby, rbz;  // Bluestein chirps and spectra
   DevBuf mesh_w, mesh_u, mesh_a, mesh_b;
   DevBuf h_pos, h_val, h_out;  // device mirrors used by host-pointer calls
   // particle scratch
@@ -386,7 +446,8 @@ struct pmgpu_plan {
   ~pmgpu_plan() {
     DevBuf *bs[] = {&twx, &twy, &twz, &kxt, &kyt, &kzt, &X, &Y, &Y2, &Y3, &mesh_w, &mesh_u,
                     &mesh_a, &mesh_b, &h_pos, &h_val, &h_out, &key, &val, &key2, &val2, &counts,
-                    &start, &spart, &hist, &rtwx, &rtwy, &rtwz, &yk, &zk, &rextx, &xpos};
+                    &start, &spart, &hist, &rtwx, &rtwy, &rtwz, &yk, &zk, &rextx, &xpos,
+                    &rchx, &rchy, &rchz, &rbx, &rby, &rbz};
     for (DevBuf *b : bs) b->release();
   }
 };
@@ -608,6 +669,12 @@ template <typename R> static SolveGeom<R> solve_geom(const pmgpu_plan *pl) {
   g.eps2pi = (R)(2.0 * 3.14159265358979323846 * pl->eps);
   g.order = pl->par.poisson_order;
   g.allper = pl->g.allper;
+  g.rchx = pl->rchx.as<C>();
+  g.rchy = pl->rchy.as<C>();
+  g.rchz = pl->rchz.as<C>();
+  g.rbx = pl->rbx.as<C>();
+  g.rby = pl->rby.as<C>();
+  g.rbz = pl->rbz.as<C>();
   g.rx_ok = pl->rx_ok;
   g.rx = pl->rx;
   g.rtwx = pl->rtwx.as<C>();
@@ -710,6 +777,8 @@ static void attach_green(pmgpu_plan *pl, const std::shared_ptr<DevBuf> &sp) {
   pl->green.fixed = true;
 }
 
+template <typename R> static int reg_tables(pmgpu_plan *pl, const char *caller);
+
 template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller) {
   const Geometry &G = pl->g;
   pl->gM1 = G.M[1] / 2 + 1;
@@ -746,30 +815,51 @@ template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller)
   gp.eps = pl->par.regularisation_radius * mdx;
   gp.order = pl->par.poisson_order;
   gp.kernel = pl->par.poisson_kernel;
-  // FP64 transform of the sampled kernel, with FP64 tables of the same lengths
-  SolveGeom<double> gg;
-  memset(&gg, 0, sizeof(gg));
+  // FP64 transform of the sampled kernel on the full grid (ext = P = M): a temporary
+  // FP64 plan provides the transform tables of the same lengths
+  pmgpu_plan tmp;
+  tmp.prec = PMGPU_FP64;
+  tmp.g = G;
   for (int e = 0; e < 3; e++) {
-    gg.ext[e] = G.M[e];
-    gg.off[e] = 0;
-    gg.P[e] = G.M[e];
-    gg.M[e] = G.M[e];
+    tmp.g.ext[e] = tmp.g.P[e] = G.M[e];
+    tmp.g.off[e] = 0;
   }
-  gg.H = G.H;
-  gg.Hp = G.Hp;
-  gg.N2 = G.N2;
+  tmp.par = pl->par;
+  tmp.eps = 0.0;
+  tmp.perm = nullptr;
+  tmp.perm_n = 0;
+  tmp.gM1 = tmp.gM2 = 0;
   std::vector<cld> tw;
   // temporaries are stream-ordered on the legacy stream, so a set-up does not wait
   // for (or stall) solves running on other streams
-  DevBuf tx, ty, tz, gr, gX, gY;
+  DevBuf gr, gX, gY, yinv, zinv;
   int rc = -1;
   do {
-    if (!make_fft(G.N2, G.M[0], gg.fx, tw) || upload_tw<double>(tw, tx, caller)) break;
-    if (!make_fft(G.M[1], 0, gg.fy, tw) || upload_tw<double>(tw, ty, caller)) break;
-    if (!make_fft(G.M[2], 0, gg.fz, tw) || upload_tw<double>(tw, tz, caller)) break;
-    gg.twx = tx.as<double2>();
-    gg.twy = ty.as<double2>();
-    gg.twz = tz.as<double2>();
+    if (!make_fft(G.N2, G.M[0], tmp.fx, tw) || upload_tw<double>(tw, tmp.twx, caller)) break;
+    if (!make_fft(G.M[1], 0, tmp.fy, tw) || upload_tw<double>(tw, tmp.twy, caller)) break;
+    if (!make_fft(G.M[2], 0, tmp.fz, tw) || upload_tw<double>(tw, tmp.twz, caller)) break;
+    if (reg_tables<double>(&tmp, caller)) break;
+    SolveGeom<double> gg = solve_geom<double>(&tmp);
+    // spectrum rows after the y and z transforms: frequency -> row
+    std::vector<int> yi(G.M[1]), zi(G.M[2]);
+    bool rows_ok = true;
+    for (int a = 0; a < 2 && rows_ok; a++) {
+      const int n = G.M[1 + a];
+      std::vector<int> &inv = a == 0 ? yi : zi;
+      const int ok = a == 0 ? tmp.ry_ok : tmp.rz_ok;
+      for (int q = 0; q < n; q++) inv[q] = q;
+      if (ok) {
+        std::vector<int> kp(n);
+        rows_ok = cuda_ok(cudaMemcpy(kp.data(), (a == 0 ? tmp.yk : tmp.zk).p, sizeof(int) * n,
+                                     cudaMemcpyDeviceToHost), caller);
+        if (rows_ok)
+          for (int q = 0; q < n; q++) inv[kp[q]] = q;
+      }
+    }
+    if (!rows_ok) break;
+    if (yinv.ensure(sizeof(int) * G.M[1], caller) || zinv.ensure(sizeof(int) * G.M[2], caller)) break;
+    if (!cuda_ok(cudaMemcpy(yinv.p, yi.data(), sizeof(int) * G.M[1], cudaMemcpyHostToDevice), caller)) break;
+    if (!cuda_ok(cudaMemcpy(zinv.p, zi.data(), sizeof(int) * G.M[2], cudaMemcpyHostToDevice), caller)) break;
     const size_t npts = (size_t)G.M[0] * G.M[1] * G.M[2];
     const size_t nspec = (size_t)G.M[2] * G.M[1] * G.Hp;
     if (gr.ensure(sizeof(double) * npts, caller) || gX.ensure(sizeof(double2) * nspec, caller) ||
@@ -780,20 +870,22 @@ template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller)
     if (!cuda_ok(cudaGetLastError(), caller)) break;
     if (fwd_xy<double, 1>(gg, gr.as<double>(), gX.as<double2>(), gY.as<double2>(), 0, caller)) break;
     if (zpass<double, 1>(gg, gY.as<double2>(), gY.as<double2>(), Z_FORWARD, 0, 0, G.M[1], 0, caller)) break;
+    if (!cuda_ok(cudaStreamSynchronize(0), caller)) break;
     const size_t noct = (size_t)pl->gM2 * pl->gM1 * G.H;
     if (own->ensure(sizeof(R) * noct, caller)) break;
     attach_green(pl, own);
     const double f = pl->patch.dx[0] * pl->patch.dx[1] * pl->patch.dx[2] /
                      ((double)G.M[0] * (double)G.M[1] * (double)G.M[2]);
     k_green_octant<R><<<(unsigned)std::min<size_t>((noct + 255) / 256, 148 * 64), 256>>>(
-        gY.as<double2>(), G.M[1], G.H, G.Hp, pl->gM1, pl->gM2, f, pl->green.as<R>());
+        gY.as<double2>(), G.M[1], G.H, G.Hp, pl->gM1, pl->gM2, f, yinv.as<int>(), zinv.as<int>(),
+        pl->green.as<R>());
     PM_LAUNCHED();
     if (!cuda_ok(cudaGetLastError(), caller)) break;
     if (!cuda_ok(cudaStreamSynchronize(0), caller)) break;
     g_green_cache[key] = own;
     rc = 0;
   } while (0);
-  tx.release(); ty.release(); tz.release(); gr.release(); gX.release(); gY.release();
+  gr.release(); gX.release(); gY.release(); yinv.release(); zinv.release();
   cudaStreamSynchronize(0);
   return rc;
 }
@@ -823,29 +915,50 @@ template <typename R> static int reg_tables(pmgpu_plan *pl, const char *caller) 
   pl->rx_ok = pl->ry_ok = pl->rz_ok = 0;
   if (g_force_stockham) return 0;
   const long double twopi = 2.0L * acosl(-1.0L);
+  // twiddles w_m^q of a plan's transform length m
+  auto twiddles = [&](int mm) {
+    std::vector<C> tw(mm);
+    for (int q = 0; q < mm; q++) {
+      const long double a = twopi * (long double)q / (long double)mm;
+      tw[q] = mk((R)cosl(a), (R)-sinl(a));
+    }
+    return tw;
+  };
+  // Bluestein chirp and spectrum of a plan (nothing for a direct plan)
+  auto upload_blue = [&](const RegPlan &rp, DevBuf &ch, DevBuf &bp) -> int {
+    if (!rp.bl) return 0;
+    std::vector<C> c, b;
+    bluestein_tables<C, R>(rp, c, b);
+    if (ch.ensure(sizeof(C) * c.size(), caller) || bp.ensure(sizeof(C) * b.size(), caller)) return -1;
+    CK(cudaMemcpy(ch.p, c.data(), sizeof(C) * c.size(), cudaMemcpyHostToDevice), caller);
+    CK(cudaMemcpy(bp.p, b.data(), sizeof(C) * b.size(), cudaMemcpyHostToDevice), caller);
+    return 0;
+  };
   {
     // x passes: half-length complex transform N = Mx / 2
     RegPlan rp;
     const int N = pl->g.N2, H = pl->g.H, Mx = pl->g.M[0];
-    if (make_regplan(N, rp)) {
-      std::vector<C> tw(N), ext(H);
-      for (int q = 0; q < N; q++) {
-        const long double a = twopi * (long double)q / (long double)N;
-        tw[q] = mk((R)cosl(a), (R)-sinl(a));
-      }
+    if (make_regplan(N, rp) || make_bluestein(N, rp)) {
+      const std::vector<C> tw = twiddles(rp.n);
+      std::vector<C> ext(H);
       for (int k = 0; k < H; k++) {
         const long double a = twopi * (long double)k / (long double)Mx;
         ext[k] = mk((R)cosl(a), (R)-sinl(a));
       }
-      const std::vector<int> kp = regplan_positions(rp);
       std::vector<int> xp(N);
-      for (int q = 0; q < N; q++) xp[kp[q]] = q;
-      if (pl->rtwx.ensure(sizeof(C) * N, caller) || pl->rextx.ensure(sizeof(C) * H, caller) ||
+      if (rp.bl) {
+        for (int q = 0; q < N; q++) xp[q] = q;  // natural order
+      } else {
+        const std::vector<int> kp = regplan_positions(rp);
+        for (int q = 0; q < N; q++) xp[kp[q]] = q;
+      }
+      if (pl->rtwx.ensure(sizeof(C) * tw.size(), caller) || pl->rextx.ensure(sizeof(C) * H, caller) ||
           pl->xpos.ensure(sizeof(int) * N, caller))
         return -1;
-      CK(cudaMemcpy(pl->rtwx.p, tw.data(), sizeof(C) * N, cudaMemcpyHostToDevice), caller);
+      CK(cudaMemcpy(pl->rtwx.p, tw.data(), sizeof(C) * tw.size(), cudaMemcpyHostToDevice), caller);
       CK(cudaMemcpy(pl->rextx.p, ext.data(), sizeof(C) * H, cudaMemcpyHostToDevice), caller);
       CK(cudaMemcpy(pl->xpos.p, xp.data(), sizeof(int) * N, cudaMemcpyHostToDevice), caller);
+      if (upload_blue(rp, pl->rchx, pl->rbx)) return -1;
       pl->rx = rp;
       pl->rx_ok = 1;
     }
@@ -853,18 +966,20 @@ template <typename R> static int reg_tables(pmgpu_plan *pl, const char *caller) 
   for (int axis = 1; axis <= 2; axis++) {
     RegPlan rp;
     const int n = pl->g.M[axis];
-    if (!make_regplan(n, rp)) continue;
-    std::vector<C> tw(n);
-    for (int q = 0; q < n; q++) {
-      const long double a = twopi * (long double)q / (long double)n;
-      tw[q] = mk((R)cosl(a), (R)-sinl(a));
+    if (!make_regplan(n, rp) && !make_bluestein(n, rp)) continue;
+    const std::vector<C> tw = twiddles(rp.n);
+    std::vector<int> kp(n);
+    if (rp.bl) {
+      for (int q = 0; q < n; q++) kp[q] = q;  // natural order
+    } else {
+      kp = regplan_positions(rp);
     }
-    const std::vector<int> kp = regplan_positions(rp);
     DevBuf &tb = axis == 1 ? pl->rtwy : pl->rtwz;
     DevBuf &kb = axis == 1 ? pl->yk : pl->zk;
-    if (tb.ensure(sizeof(C) * n, caller) || kb.ensure(sizeof(int) * n, caller)) return -1;
-    CK(cudaMemcpy(tb.p, tw.data(), sizeof(C) * n, cudaMemcpyHostToDevice), caller);
+    if (tb.ensure(sizeof(C) * tw.size(), caller) || kb.ensure(sizeof(int) * n, caller)) return -1;
+    CK(cudaMemcpy(tb.p, tw.data(), sizeof(C) * tw.size(), cudaMemcpyHostToDevice), caller);
     CK(cudaMemcpy(kb.p, kp.data(), sizeof(int) * n, cudaMemcpyHostToDevice), caller);
+    if (upload_blue(rp, axis == 1 ? pl->rchy : pl->rchz, axis == 1 ? pl->rby : pl->rbz)) return -1;
     if (axis == 1) {
       pl->ry = rp;
       pl->ry_ok = 1;

@@ -58,6 +58,9 @@ struct RegPlan {
   int str[RP_MAX];  // stride s_p = B_p / R_p
   int twm[RP_MAX];  // n / B_p: w_{B_p}^q = w_n^{twm q}
   FastDiv dstr[RP_MAX];
+  // Bluestein: a line of length bn (with a prime factor above 17) is transformed as
+  // a convolution of length n >= 2 bn - 1 (the phases above describe that length)
+  int bl, bn;
 };
 
 // radices with a register DFT
@@ -243,6 +246,76 @@ __device__ __forceinline__ void rfft_inv(const RegPlan &pl, typename RVec<R>::V 
     rphase_any<true, R>(pl, p, buf, LG, dLG, tw, gs, glast && p == 0, p < pl.np - 1, gl, gs ? gl.rows_in : pl.n);
     __syncthreads();
   }
+}
+
+// ---------------------------------------------------------------------------
+// Bluestein (chirp-z) transform of lines of length n with a plan of length m >= 2n-1:
+//   X[k] = c[k] sum_j (x[j] c[j]) conj(c[k - j]),   c[j] = exp(-i pi j^2 / n),
+// a circular convolution of length m: forward transform of the chirped input (zero
+// beyond n), product with B = FFT_m(conj c wrapped), inverse transform, chirp.  The
+// inverse DFT is conj(forward(conj x)).  `bpos` holds B at the plan's digit-reversed
+// positions, so the product needs no reordering; the scale 1/m is folded into the
+// output chirp.  Input and output are in natural order (first nin / nout points),
+// read from global rows or buf, written to global rows or buf.
+template <typename R>
+__device__ __forceinline__ void bl_chirp_in(typename RVec<R>::V *buf, int L, const FastDiv &dL,
+                                            const typename cplx_t<R>::type *__restrict__ chirp, int nin, bool conj_in,
+                                            bool gsrc, const PhaseGlobal &gl) {
+  typedef typename cplx_t<R>::type C;
+  const C *gin = reinterpret_cast<const C *>(gl.in);
+  const unsigned total = (unsigned)nin * (unsigned)L;
+  for (unsigned t = threadIdx.x; t < total; t += blockDim.x) {
+    const unsigned j = fdiv(t, dL);
+    const int l = (int)(t - j * (unsigned)L);
+    C v = gsrc ? ldg_vec<R>(gin + (long long)j * gl.rs_in + l) : buf[j * L + l];
+    if (conj_in) v.y = -v.y;
+    buf[j * L + l] = cmul(v, chirp[j]);
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void bl_mul(typename RVec<R>::V *buf, int L, const FastDiv &dL,
+                                       const typename cplx_t<R>::type *__restrict__ bpos, int m) {
+  const unsigned total = (unsigned)m * (unsigned)L;
+  for (unsigned t = threadIdx.x; t < total; t += blockDim.x) {
+    const unsigned q = fdiv(t, dL);
+    buf[t] = cmul(buf[t], bpos[q]);
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void bl_chirp_out(typename RVec<R>::V *buf, int L, const FastDiv &dL,
+                                             const typename cplx_t<R>::type *__restrict__ chirp, R scale, int nout,
+                                             bool conj_out, bool gdst, const PhaseGlobal &gl) {
+  typedef typename cplx_t<R>::type C;
+  C *gout = reinterpret_cast<C *>(gl.out);
+  const unsigned total = (unsigned)nout * (unsigned)L;
+  for (unsigned t = threadIdx.x; t < total; t += blockDim.x) {
+    const unsigned k = fdiv(t, dL);
+    const int l = (int)(t - k * (unsigned)L);
+    C v = cscale(cmul(buf[k * L + l], chirp[k]), scale);
+    if (conj_out) v.y = -v.y;
+    if (gdst) gout[(long long)k * gl.rs_out + l] = v;
+    else buf[k * L + l] = v;
+  }
+}
+
+// ends with a barrier
+template <typename R, bool INV>
+__device__ __forceinline__ void bfft(const RegPlan &pl, typename RVec<R>::V *buf, int L, const FastDiv &dL,
+                                     const typename cplx_t<R>::type *tw, const typename cplx_t<R>::type *chirp,
+                                     const typename cplx_t<R>::type *bpos, bool gsrc, bool gdst,
+                                     const PhaseGlobal &gl, int nin, int nout) {
+  bl_chirp_in<R>(buf, L, dL, chirp, nin, INV, gsrc, gl);
+  __syncthreads();
+  PhaseGlobal none = gl;
+  none.rows_in = none.rows_out = pl.n;
+  rfft_fwd<R>(pl, buf, L, dL, tw, false, false, none, nin);
+  bl_mul<R>(buf, L, dL, bpos, pl.n);
+  __syncthreads();
+  rfft_inv<R>(pl, buf, L, dL, tw, false, false, none);
+  bl_chirp_out<R>(buf, L, dL, chirp, R(1) / R(pl.n), nout, INV, gdst, gl);
+  __syncthreads();
 }
 
 }  // namespace pmgpu

@@ -50,6 +50,8 @@ template <typename R> struct SolveGeom {
   const C *rtwx, *rtwy, *rtwz;  // w_n^q, q < n
   const C *rextx;            // exp(-2 pi i k / Mx), k < H
   const int *xpos;           // frequency -> position of the x transform
+  const C *rchx, *rchy, *rchz;  // Bluestein plans: chirp exp(-i pi j^2 / n), j < n
+  const C *rbx, *rby, *rbz;     // Bluestein plans: FFT of the wrapped chirp, by position
   const int *yk;             // row of the y spectrum -> ky index (nullptr: natural order)
   const int *zk;             // position of the z transform -> kz index
 };
@@ -324,19 +326,32 @@ __global__ void __launch_bounds__(RL_THREADS, RMinBlocks<R>::v) k_rlines(SolveGe
   constexpr int G = RVec<R>::G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const RegPlan &pl = (axis == 1) ? g.ry : g.rz;
-  const int n = pl.n, TK = lt.TK, L = NC * TK, LG = L / G;
-  C *tw = reinterpret_cast<C *>(smem_raw);
-  int *zpos = reinterpret_cast<int *>(smem_raw + (((size_t)n * sizeof(C) + 15) & ~(size_t)15));
-  R *kzs = reinterpret_cast<R *>(reinterpret_cast<unsigned char *>(zpos) + (((size_t)n * sizeof(int) + 15) & ~(size_t)15));
-  V *buf = reinterpret_cast<V *>(reinterpret_cast<unsigned char *>(kzs) + (((size_t)n * sizeof(R) + 15) & ~(size_t)15));
+  const int m = pl.n, nl = lt.n, TK = lt.TK, L = NC * TK, LG = L / G;  // m: transform length
+  const bool blue = pl.bl != 0;
+  unsigned char *sp = smem_raw;
+  C *tw = reinterpret_cast<C *>(sp);
+  sp += ((size_t)m * sizeof(C) + 15) & ~(size_t)15;
+  int *zpos = reinterpret_cast<int *>(sp);
+  sp += ((size_t)nl * sizeof(int) + 15) & ~(size_t)15;
+  R *kzs = reinterpret_cast<R *>(sp);
+  sp += ((size_t)nl * sizeof(R) + 15) & ~(size_t)15;
+  C *chirp = reinterpret_cast<C *>(sp);
+  C *bpos = chirp + nl;
+  if (blue) sp += ((size_t)(nl + m) * sizeof(C) + 15) & ~(size_t)15;
+  V *buf = reinterpret_cast<V *>(sp);
   {
     const C *twg = (axis == 1) ? g.rtwy : g.rtwz;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = twg[i];
+    for (int i = threadIdx.x; i < m; i += blockDim.x) tw[i] = twg[i];
     if (lmode == L_Z)
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      for (int i = threadIdx.x; i < nl; i += blockDim.x) {
         zpos[i] = g.zk[i];
         kzs[i] = g.kzt[i];
       }
+    if (blue) {
+      const C *cg = (axis == 1) ? g.rchy : g.rchz, *bg = (axis == 1) ? g.rby : g.rbz;
+      for (int i = threadIdx.x; i < nl; i += blockDim.x) chirp[i] = cg[i];
+      for (int i = threadIdx.x; i < m; i += blockDim.x) bpos[i] = bg[i];
+    }
   }
   __syncthreads();
   const int ntiles = lt.nouter * lt.nkt;
@@ -350,15 +365,19 @@ __global__ void __launch_bounds__(RL_THREADS, RMinBlocks<R>::v) k_rlines(SolveGe
     gl.rows_in = lt.rows_in;
     gl.rows_out = lt.rows_out;
     if (lmode == L_FWD) {
-      rfft_fwd<R>(pl, buf, LG, lt.dLG, tw, true, true, gl);
+      if (blue) bfft<R, false>(pl, buf, LG, lt.dLG, tw, chirp, bpos, true, true, gl, lt.rows_in, nl);
+      else rfft_fwd<R>(pl, buf, LG, lt.dLG, tw, true, true, gl);
     } else if (lmode == L_INV) {
-      rfft_inv<R>(pl, buf, LG, lt.dLG, tw, true, true, gl);
+      if (blue) bfft<R, true>(pl, buf, LG, lt.dLG, tw, chirp, bpos, true, true, gl, nl, lt.rows_out);
+      else rfft_inv<R>(pl, buf, LG, lt.dLG, tw, true, true, gl);
     } else {
-      rfft_fwd<R>(pl, buf, LG, lt.dLG, tw, true, false, gl);
+      if (blue) bfft<R, false>(pl, buf, LG, lt.dLG, tw, chirp, bpos, true, false, gl, lt.rows_in, nl);
+      else rfft_fwd<R>(pl, buf, LG, lt.dLG, tw, true, false, gl);
       z_multiply<R, NC>(g, reinterpret_cast<C *>(buf), L, TK, kt * TK, g.yk ? g.yk[o] : o, zmode, reproj, use_zeta,
-                        zpos, kzs);
+                        blue ? nullptr : zpos, kzs);
       __syncthreads();
-      rfft_inv<R>(pl, buf, LG, lt.dLG, tw, false, true, gl);
+      if (blue) bfft<R, true>(pl, buf, LG, lt.dLG, tw, chirp, bpos, false, true, gl, nl, lt.rows_out);
+      else rfft_inv<R>(pl, buf, LG, lt.dLG, tw, false, true, gl);
     }
   }
 }
@@ -377,24 +396,30 @@ __global__ void __launch_bounds__(RL_THREADS, RMinBlocks<R>::v) k_rxfwd(SolveGeo
   constexpr int G = RVec<R>::G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const RegPlan &pl = g.rx;
-  const int N = pl.n, L = NC * RB, LG = L / G, H = g.H;
+  const bool blue = pl.bl != 0;
+  const int N = blue ? pl.bn : pl.n, m = pl.n, L = NC * RB, LG = L / G, H = g.H;
   const int P0 = g.P[0];
   unsigned char *sp = smem_raw;
   C *tw = reinterpret_cast<C *>(sp);
-  sp += ((size_t)N * sizeof(C) + 15) & ~(size_t)15;
+  sp += ((size_t)m * sizeof(C) + 15) & ~(size_t)15;
   C *ext = reinterpret_cast<C *>(sp);
   sp += ((size_t)H * sizeof(C) + 15) & ~(size_t)15;
   int *xpos = reinterpret_cast<int *>(sp);
   sp += ((size_t)N * sizeof(int) + 15) & ~(size_t)15;
+  C *chirp = reinterpret_cast<C *>(sp);
+  C *bpos = chirp + N;
+  if (blue) sp += ((size_t)(N + m) * sizeof(C) + 15) & ~(size_t)15;
   R *Sr = reinterpret_cast<R *>(sp);
   sp += ((size_t)RB * P0 * NC * sizeof(R) + 15) & ~(size_t)15;
   V *buf = reinterpret_cast<V *>(sp);
   C *Bc = reinterpret_cast<C *>(buf);
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
-    tw[i] = g.rtwx[i];
-    xpos[i] = g.xpos[i];
-  }
+  for (int i = threadIdx.x; i < m; i += blockDim.x) tw[i] = g.rtwx[i];
+  for (int i = threadIdx.x; i < N; i += blockDim.x) xpos[i] = g.xpos[i];
   for (int i = threadIdx.x; i < H; i += blockDim.x) ext[i] = g.rextx[i];
+  if (blue) {
+    for (int i = threadIdx.x; i < N; i += blockDim.x) chirp[i] = g.rchx[i];
+    for (int i = threadIdx.x; i < m; i += blockDim.x) bpos[i] = g.rbx[i];
+  }
   const int nrows = g.P[1] * g.P[2];
   const int ntiles = (nrows + RB - 1) / RB;
   const int npk = (P0 + 1) / 2;  // packed points that hold data
@@ -446,7 +471,8 @@ __global__ void __launch_bounds__(RL_THREADS, RMinBlocks<R>::v) k_rxfwd(SolveGeo
     gl.out = nullptr;
     gl.rs_in = gl.rs_out = 0;
     gl.rows_in = gl.rows_out = N;
-    rfft_fwd<R>(pl, buf, LG, dLG, tw, false, false, gl, npk);
+    if (blue) bfft<R, false>(pl, buf, LG, dLG, tw, chirp, bpos, false, false, gl, npk, N);
+    else rfft_fwd<R>(pl, buf, LG, dLG, tw, false, false, gl, npk);
     for (int t = threadIdx.x; t < RB * g.Hp; t += blockDim.x) {
       const int rr = t / g.Hp, k = t - rr * g.Hp;
       const int row = row0 + rr;
@@ -486,24 +512,30 @@ __global__ void __launch_bounds__(RL_THREADS, RMinBlocks<R>::v) k_rxinv(SolveGeo
   constexpr int G = RVec<R>::G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const RegPlan &pl = g.rx;
-  const int N = pl.n, L = NC * RB, LG = L / G, H = g.H;
+  const bool blue = pl.bl != 0;
+  const int N = blue ? pl.bn : pl.n, m = pl.n, L = NC * RB, LG = L / G, H = g.H;
   const size_t rowc = (size_t)g.Hp * NC;  // complex per X row
   unsigned char *sp = smem_raw;
   C *tw = reinterpret_cast<C *>(sp);
-  sp += ((size_t)N * sizeof(C) + 15) & ~(size_t)15;
+  sp += ((size_t)m * sizeof(C) + 15) & ~(size_t)15;
   C *ext = reinterpret_cast<C *>(sp);
   sp += ((size_t)H * sizeof(C) + 15) & ~(size_t)15;
   int *xpos = reinterpret_cast<int *>(sp);
   sp += ((size_t)N * sizeof(int) + 15) & ~(size_t)15;
+  C *chirp = reinterpret_cast<C *>(sp);
+  C *bpos = chirp + N;
+  if (blue) sp += ((size_t)(N + m) * sizeof(C) + 15) & ~(size_t)15;
   C *Sc = reinterpret_cast<C *>(sp);
   sp += (size_t)RB * rowc * sizeof(C);
   V *buf = reinterpret_cast<V *>(sp);
   C *Bc = reinterpret_cast<C *>(buf);
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
-    tw[i] = g.rtwx[i];
-    xpos[i] = g.xpos[i];
-  }
+  for (int i = threadIdx.x; i < m; i += blockDim.x) tw[i] = g.rtwx[i];
+  for (int i = threadIdx.x; i < N; i += blockDim.x) xpos[i] = g.xpos[i];
   for (int i = threadIdx.x; i < H; i += blockDim.x) ext[i] = g.rextx[i];
+  if (blue) {
+    for (int i = threadIdx.x; i < N; i += blockDim.x) chirp[i] = g.rchx[i];
+    for (int i = threadIdx.x; i < m; i += blockDim.x) bpos[i] = g.rbx[i];
+  }
   const int nrows = g.P[1] * g.P[2];
   const int ntiles = (nrows + RB - 1) / RB;
   auto load = [&](int tile) {
@@ -552,9 +584,10 @@ __global__ void __launch_bounds__(RL_THREADS, RMinBlocks<R>::v) k_rxinv(SolveGeo
     gl.out = nullptr;
     gl.rs_in = gl.rs_out = 0;
     gl.rows_in = gl.rows_out = N;
-    rfft_inv<R>(pl, buf, LG, dLG, tw, false, false, gl);
     const int P0 = g.P[0];
     const int nout = (P0 + 1) / 2;
+    if (blue) bfft<R, true>(pl, buf, LG, dLG, tw, chirp, bpos, false, false, gl, N, nout);
+    else rfft_inv<R>(pl, buf, LG, dLG, tw, false, false, gl);
     for (int t = threadIdx.x; t < RB * nout; t += blockDim.x) {
       const int rr = t / nout, m = t - rr * nout;
       const int row = row0 + rr;

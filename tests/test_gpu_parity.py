@@ -97,6 +97,10 @@ def test_solve_fp32(name, xmin, xmax, dx, bc, ng):
 # grids whose y or z FFT length needs three register phases (M = 528 = 16*11*3,
 # 264 = 12*11*2, periodic 240 = 12*10*2) or two with radix 17 / 13 (272, 208)
 LONG_CASES = [
+    # Bluestein lengths: P = 53, 38, 46 -> M = 106 (2 x 53), 76 (4 x 19), 92 (4 x 23); x half-length 53
+    ("fff-bluestein", (-2.8125, -1.875, -2.375), (2.8125, 1.875, 2.375), (0.125,) * 3, (0, 0, 0), 4),
+    # periodic 58 (2 x 29) and 62 (2 x 31) with a free z of 2 x 47
+    ("ppf-bluestein", (0, 0, -2.4375), (3.625, 3.875, 2.4375), (0.0625, 0.0625, 0.125), (1, 1, 0), 4),
     ("fff-y528", (-1, -16, -1), (1, 16, 1), (0.125,) * 3, (0, 0, 0), 4),
     ("fff-z264", (-1, -1, -7.75), (1, 1, 7.75), (0.125,) * 3, (0, 0, 0), 4),
     ("pff-y240", (0, 0, -1), (2, 30, 1), (0.125,) * 3, (1, 1, 0), 4),
@@ -123,7 +127,8 @@ def test_solve_register_phases(name, xmin, xmax, dx, bc, ng, prec):
     assert rel_l2(vp, vp_o) < tol
 
 
-@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", [CASES[0], CASES[1], CASES[2], CASES[5], LONG_CASES[0]])
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", [CASES[0], CASES[1], CASES[2], CASES[5], LONG_CASES[0],
+                                                      LONG_CASES[1], LONG_CASES[2]])
 @pytest.mark.parametrize("prec", [P.FP64, P.FP32])
 def test_fft_engines_agree(name, xmin, xmax, dx, bc, ng, prec):
     """The register passes and the Stockham passes give the same solve to round-off."""
