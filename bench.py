@@ -270,12 +270,14 @@ def main():
 
     w = Wl.make(args.config)
     n = w.npart
+    P.fft_tune(True)  # schedules (radix sequence, kx tile) measured when the plans are made
     patch = P.make_patch(w.xmin, w.xmax, w.dx, bound_cond=w.bound_cond, nghost=w.nghost)
     ierr, topo = P.pmlib_topology_cuboid(patch, w.interp)
     params = P.make_params(order=w.order, kernel=1, radius=w.radius, interp=w.interp)
     ierr32, plan32 = P.pmlib_poisson_setup(patch, topo, params, P.FP32)
     ierr64, plan64 = P.pmlib_poisson_setup(patch, topo, params, P.FP64)
     assert ierr32 == 0 and ierr64 == 0, P.last_error()
+    P.fft_tune(False)  # batched and served plans: many short-lived lengths, no tuning
 
     dev = torch.device("cuda", local)
     pos64 = torch.from_numpy(w.pos).to(dev)
@@ -426,6 +428,7 @@ def main():
                                    f"{n} particles, order 6 Green's function, eps = 2h, M4'",
                        "grid": f"N={w.n}, nghost={w.nghost}, FFT M={2 * (w.n + 2 * w.nghost)}",
                        "parallelism": f"replicas x{world}", "l2": L2_NOTE},
+            "fft_schedules": [e for e in P.fft_tuned() if e["length"] in (2 * (w.n + 2 * w.nghost),)],
             "fp64_plain": {"value": value64, "unit": "steps/s", "ms_per_step": ms64 / k64},
             "fp32_speedup_vs_fp64": value / value64,
             "accuracy": {"rel_l2_fp32_vs_fp64": rel_l2, "max_rel_err": max_err},

@@ -183,6 +183,17 @@ void pmgpu_batch_destroy(pmgpu_batch *batch);
  * the same results to round-off; returns the previous setting. */
 int pmgpu_fft_engine(int engine);
 
+/* Schedule autotuner (no counterpart in the reference).  While on, creating a plan
+ * times, for every y / z transform length and precision not measured before, the y
+ * forward pass and the fused z pass with the best few radix sequences (by the
+ * engine's cost model) and kx tiles of 8, 4 and 2, and keeps the fastest for this and
+ * later plans of that length (process-wide; plans made with tuning off also use the
+ * table).  Tuning adds tens of milliseconds per new length to plan creation.  pmgpu_fft_tune returns the previous setting; pmgpu_fft_tuned reads
+ * entry `index` of the table (radices[3], 0-padded), -1 past the end. */
+int pmgpu_fft_tune(int on);
+int pmgpu_fft_tuned(int index, int *length, int *precision, int *axis, int *radices, int *tile,
+                    double *ms);
+
 /* ---- allocation-free deposition (no counterpart in the reference) ----
  * For callers that cannot allocate device memory while they run, e.g. a host
  * program that reserved the GPU's memory up front for its own pool, or a loop that

@@ -114,6 +114,11 @@ template <typename R, int NC>
 int inv_yx(SolveGeom<R> &g, const pmgpu_topo *topo, typename cplx_t<R>::type *Y, typename cplx_t<R>::type *X, R *out,
            cudaStream_t st, const char *caller, int cs = NC, bool ghosts = true);
 
+// one pass along y (forward X -> Y, or inverse Y -> X)
+template <typename R, int NC>
+int ypass(SolveGeom<R> &g, const typename cplx_t<R>::type *X, typename cplx_t<R>::type *Y, int inverse,
+          cudaStream_t st, const char *caller);
+
 // each pass unit holds its own copy of the DFT constant tables
 int upload_cs_f32_1(const void *t32, const void *t64);
 int upload_cs_f32_3(const void *t32, const void *t64);

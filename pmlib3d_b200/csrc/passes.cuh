@@ -27,7 +27,9 @@ static int launch_lines(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typ
   const int n = g.M[axis];
   if (axis == 1 ? g.ry_ok : g.rz_ok) {
     const int mt = (axis == 1 ? g.ry : g.rz).n;  // transform length (Bluestein: > n)
-    const int TK = pick_tk_reg(n, mt, NC, sizeof(C), g.Hp, reg_budget(sizeof(R)));
+    int TK = axis == 1 ? g.tky : g.tkz;  // a tuned tile, if it fits
+    if (TK <= 0 || g.Hp % TK || reg_smem(n, mt, NC, TK, sizeof(C)) > PASS_SMEM_BUDGET)
+      TK = pick_tk_reg(n, mt, NC, sizeof(C), g.Hp, reg_budget(sizeof(R)));
     if (TK > 0) {
       LineTiles lt;
       lt.n = n;
@@ -131,14 +133,27 @@ int fwd_xy(SolveGeom<R> &g, const R *in, typename cplx_t<R>::type *X, typename c
                              (long long)g.M[1] * Hp, Hp, g.P[2], st, caller);
 }
 
+// one forward (or inverse) pass along y over the X layout -> Y layout, as in fwd_xy
+template <typename R, int NC>
+int ypass(SolveGeom<R> &g, const typename cplx_t<R>::type *X, typename cplx_t<R>::type *Y, int inverse,
+          cudaStream_t st, const char *caller) {
+  const long long Hp = g.Hp;
+  if (inverse)
+    return launch_lines<R, NC>(g, Y, (typename cplx_t<R>::type *)X, 1, L_INV, 0, 0, 0, g.M[1], g.P[1],
+                               (long long)g.M[1] * Hp, Hp, (long long)g.P[1] * Hp, Hp, g.P[2], st, caller);
+  return launch_lines<R, NC>(g, X, Y, 1, L_FWD, 0, 0, 0, g.P[1], g.M[1], (long long)g.P[1] * Hp, Hp,
+                             (long long)g.M[1] * Hp, Hp, g.P[2], st, caller);
+}
+
 template <typename R, int NC>
 int zpass(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typename cplx_t<R>::type *out, int mode,
                  int reproj, int use_zeta, int rows_y, cudaStream_t st, const char *caller) {
   const long long Hp = g.Hp;
-  const int rows = (mode == Z_FORWARD) ? g.M[2] : g.P[2];
+  // Z_FORWARD: forward transform only, P rows in (the rest zero), M rows out
+  const int rows_in = g.P[2], rows_out = (mode == Z_FORWARD) ? g.M[2] : g.P[2];
   KTimer kt_(KC_ZPASS, st);
-  return launch_lines<R, NC>(g, in, out, 2, mode == Z_FORWARD ? L_FWD : L_Z, mode, reproj, use_zeta, rows, rows, Hp,
-                             (long long)g.M[1] * Hp, Hp, (long long)g.M[1] * Hp, rows_y, st, caller);
+  return launch_lines<R, NC>(g, in, out, 2, mode == Z_FORWARD ? L_FWD : L_Z, mode, reproj, use_zeta, rows_in,
+                             rows_out, Hp, (long long)g.M[1] * Hp, Hp, (long long)g.M[1] * Hp, rows_y, st, caller);
 }
 
 template <typename R, int NC>
@@ -214,5 +229,7 @@ static int upload_cs_local(const void *t32, const void *t64) {
                             cudaStream_t, const char *);                                                       \
   template int inv_yx<R, NC>(SolveGeom<R> &, const pmgpu_topo *, cplx_t<R>::type *, cplx_t<R>::type *, R *,    \
                              cudaStream_t, const char *, int, bool);                                           \
+  template int ypass<R, NC>(SolveGeom<R> &, const cplx_t<R>::type *, cplx_t<R>::type *, int, cudaStream_t,      \
+                            const char *);                                                                     \
   int upload_cs_##NAME(const void *t32, const void *t64) { return upload_cs_local(t32, t64); }                 \
   }

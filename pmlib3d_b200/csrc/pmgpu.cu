@@ -18,6 +18,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <tuple>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -269,57 +270,79 @@ static double radix_cost(int r) {
   }
 }
 
-static bool make_regplan(int n, RegPlan &pl) {
+// a plan from an explicit radix sequence (outermost first)
+static void regplan_from(int n, const int *r, int np, RegPlan &pl) {
+  memset(&pl, 0, sizeof(pl));
+  pl.n = n;
+  pl.np = np;
+  int B = n;
+  for (int p = 0; p < np; p++) {
+    pl.rad[p] = r[p];
+    pl.blk[p] = B;
+    pl.str[p] = B / r[p];
+    pl.twm[p] = n / B;
+    pl.dstr[p] = make_fastdiv((unsigned)pl.str[p]);
+    B /= r[p];
+  }
+}
+
+// radix sequences of at most three register radices whose product is n, best model
+// score first
+struct RadixSeq {
+  int np;
+  int r[3];
+  double cost;
+};
+static std::vector<RadixSeq> regplan_candidates(int n) {
   static const int S[] = {16, 17, 13, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2};
-  double best = 1e18;
-  int br[3] = {0, 0, 0}, bnp = 0;
-  auto consider = [&](int np, const int *r) {
-    double c = 0.0;
-    for (int i = 0; i < np; i++) c += 1.5 + radix_cost(r[i]);
-    if (r[0] % 2) c += 0.5;  // the zero half of a padded line is skipped only with an even first radix
-    if (c < best - 1e-9) {
-      best = c;
-      bnp = np;
-      for (int i = 0; i < 3; i++) br[i] = i < np ? r[i] : 0;
-    }
+  std::vector<RadixSeq> out;
+  auto add = [&](int np, int a, int b, int c) {
+    RadixSeq q;
+    q.np = np;
+    q.r[0] = a;
+    q.r[1] = b;
+    q.r[2] = c;
+    q.cost = 0.0;
+    for (int i = 0; i < np; i++) q.cost += 1.5 + radix_cost(q.r[i]);
+    if (a % 2) q.cost += 0.5;  // the zero half of a padded line is skipped only with an even first radix
+    out.push_back(q);
   };
   for (int a : S) {
     if (n % a) continue;
     const int n1 = n / a;
     if (n1 == 1) {
-      int r[3] = {a, 0, 0};
-      consider(1, r);
+      add(1, a, 0, 0);
       continue;
     }
     for (int b : S) {
       if (n1 % b) continue;
       const int n2 = n1 / b;
-      if (n2 == 1) {
-        int r[3] = {a, b, 0};
-        consider(2, r);
-        continue;
-      }
-      if (reg_radix(n2)) {
-        int r[3] = {a, b, n2};
-        consider(3, r);
-      }
+      if (n2 == 1) add(2, a, b, 0);
+      else if (reg_radix(n2)) add(3, a, b, n2);
     }
   }
-  if (bnp == 0) return false;
-  memset(&pl, 0, sizeof(pl));
-  pl.n = n;
-  pl.np = bnp;
-  int B = n;
-  for (int p = 0; p < bnp; p++) {
-    pl.rad[p] = br[p];
-    pl.blk[p] = B;
-    pl.str[p] = B / br[p];
-    pl.twm[p] = n / B;
-    pl.dstr[p] = make_fastdiv((unsigned)pl.str[p]);
-    B /= br[p];
-  }
+  std::stable_sort(out.begin(), out.end(), [](const RadixSeq &x, const RadixSeq &y) { return x.cost < y.cost; });
+  return out;
+}
+
+static bool make_regplan(int n, RegPlan &pl) {
+  const std::vector<RadixSeq> c = regplan_candidates(n);
+  if (c.empty()) return false;
+  regplan_from(n, c[0].r, c[0].np, pl);
   return true;
 }
+
+// Autotuned schedules: (length, precision, axis) -> radix sequence and kx tile, the
+// fastest measured forward pass among the candidates (process-wide, filled when
+// plans are created while tuning is on).
+struct TunedSchedule {
+  int np;
+  int r[3];
+  int tk;
+  double ms;
+};
+static std::map<std::tuple<int, int, int>, TunedSchedule> g_tuned;
+static int g_tune = 0;
 
 // position -> frequency index of the digit-reversed output of a plan
 static std::vector<int> regplan_positions(const RegPlan &pl) {
@@ -435,6 +458,7 @@ struct pmgpu_plan {
   // register-engine plans along y and z (in-place, digit-reversed spectra)
   int rx_ok, ry_ok, rz_ok;
   RegPlan rx, ry, rz;
+  int tky = 0, tkz = 0;  // tuned kx tiles (0: chosen by shared memory)
   DevBuf rtwx, rtwy, rtwz, yk, zk, rextx, xpos;
   DevBuf rchx, rchy, rchz, rbx, rby, rbz;  // Bluestein chirps and spectra
   DevBuf mesh_w, mesh_u, mesh_a, mesh_b;
@@ -675,6 +699,8 @@ template <typename R> static SolveGeom<R> solve_geom(const pmgpu_plan *pl) {
   g.rbx = pl->rbx.as<C>();
   g.rby = pl->rby.as<C>();
   g.rbz = pl->rbz.as<C>();
+  g.tky = pl->tky;
+  g.tkz = pl->tkz;
   g.rx_ok = pl->rx_ok;
   g.rx = pl->rx;
   g.rtwx = pl->rtwx.as<C>();
@@ -777,7 +803,7 @@ static void attach_green(pmgpu_plan *pl, const std::shared_ptr<DevBuf> &sp) {
   pl->green.fixed = true;
 }
 
-template <typename R> static int reg_tables(pmgpu_plan *pl, const char *caller);
+template <typename R> static int reg_tables(pmgpu_plan *pl, const char *caller, bool tune_ok);
 
 template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller) {
   const Geometry &G = pl->g;
@@ -838,7 +864,7 @@ template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller)
     if (!make_fft(G.N2, G.M[0], tmp.fx, tw) || upload_tw<double>(tw, tmp.twx, caller)) break;
     if (!make_fft(G.M[1], 0, tmp.fy, tw) || upload_tw<double>(tw, tmp.twy, caller)) break;
     if (!make_fft(G.M[2], 0, tmp.fz, tw) || upload_tw<double>(tw, tmp.twz, caller)) break;
-    if (reg_tables<double>(&tmp, caller)) break;
+    if (reg_tables<double>(&tmp, caller, false)) break;
     SolveGeom<double> gg = solve_geom<double>(&tmp);
     // spectrum rows after the y and z transforms: frequency -> row
     std::vector<int> yi(G.M[1]), zi(G.M[2]);
@@ -910,7 +936,84 @@ template <typename R> static int upload_wavenumbers(pmgpu_plan *pl, const char *
   return 0;
 }
 
-template <typename R> static int reg_tables(pmgpu_plan *pl, const char *caller) {
+// Times the pass along `axis` of this plan's geometry (y: the forward pass; z: the
+// fused transform / multiply / inverse pass of the velocity solve) for the candidate
+// radix sequences (the five best by the model) and kx tiles, on scratch arrays; the
+// fastest goes to the tuning table.  The plan's Green's function must exist.
+template <typename R> static int tune_axis(pmgpu_plan *pl, int axis, TunedSchedule &best, const char *caller) {
+  typedef typename cplx_t<R>::type C;
+  const Geometry &G = pl->g;
+  const int n = G.M[axis];
+  std::vector<RadixSeq> cands = regplan_candidates(n);
+  if (cands.size() > 5) cands.resize(5);
+  DevBuf A, B, tw, kp;
+  const size_t nx = (size_t)G.P[1] * G.P[2] * G.Hp * 3;
+  const size_t ny = (size_t)G.M[1] * G.P[2] * G.Hp * 3;
+  if ((axis == 1 && A.ensure(sizeof(C) * nx, caller)) || B.ensure(sizeof(C) * ny, caller)) return -1;
+  if (axis == 1) CK(cudaMemsetAsync(A.p, 0, sizeof(C) * nx, 0), caller);
+  CK(cudaMemsetAsync(B.p, 0, sizeof(C) * ny, 0), caller);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0), caller);
+  CK(cudaEventCreate(&e1), caller);
+  best.ms = 1e30;
+  best.np = 0;
+  const long double twopi = 2.0L * acosl(-1.0L);
+  for (const RadixSeq &c : cands) {
+    RegPlan rp;
+    regplan_from(n, c.r, c.np, rp);
+    std::vector<C> t(n);
+    for (int q = 0; q < n; q++) {
+      const long double a = twopi * (long double)q / (long double)n;
+      t[q] = mk((R)cosl(a), (R)-sinl(a));
+    }
+    const std::vector<int> pos = regplan_positions(rp);
+    if (tw.ensure(sizeof(C) * n, caller) || kp.ensure(sizeof(int) * n, caller)) break;
+    if (!cuda_ok(cudaMemcpy(tw.p, t.data(), sizeof(C) * n, cudaMemcpyHostToDevice), caller) ||
+        !cuda_ok(cudaMemcpy(kp.p, pos.data(), sizeof(int) * n, cudaMemcpyHostToDevice), caller))
+      break;
+    for (int tk : {8, 4, 2}) {
+      if (G.Hp % tk || reg_smem(n, n, 3, tk, sizeof(C)) > PASS_SMEM_BUDGET) continue;
+      SolveGeom<R> g = solve_geom<R>(pl);
+      if (axis == 1) {
+        g.ry = rp;
+        g.ry_ok = 1;
+        g.rtwy = tw.as<C>();
+        g.yk = kp.as<int>();
+        g.tky = tk;
+      } else {
+        g.rz = rp;
+        g.rz_ok = 1;
+        g.rtwz = tw.as<C>();
+        g.zk = kp.as<int>();
+        g.tkz = tk;
+      }
+      auto run = [&]() {
+        return axis == 1 ? ypass<R, 3>(g, A.as<C>(), B.as<C>(), 0, 0, caller)
+                         : zpass<R, 3>(g, B.as<C>(), B.as<C>(), Z_VEL, 0, 0, G.M[1], 0, caller);
+      };
+      if (run()) continue;
+      cudaEventRecord(e0, 0);
+      bool ok = true;
+      for (int r = 0; r < 3 && ok; r++) ok = run() == 0;
+      cudaEventRecord(e1, 0);
+      if (!ok || cudaEventSynchronize(e1) != cudaSuccess) continue;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms / 3 < best.ms) {
+        best.ms = ms / 3;
+        best.np = c.np;
+        for (int i = 0; i < 3; i++) best.r[i] = c.r[i];
+        best.tk = tk;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGetLastError();
+  return best.np > 0 ? 0 : -1;
+}
+
+template <typename R> static int reg_tables(pmgpu_plan *pl, const char *caller, bool tune_ok) {
   typedef typename cplx_t<R>::type C;
   pl->rx_ok = pl->ry_ok = pl->rz_ok = 0;
   if (g_force_stockham) return 0;
@@ -967,6 +1070,14 @@ template <typename R> static int reg_tables(pmgpu_plan *pl, const char *caller) 
     RegPlan rp;
     const int n = pl->g.M[axis];
     if (!make_regplan(n, rp) && !make_bluestein(n, rp)) continue;
+    if (!rp.bl && tune_ok) {
+      // a schedule measured earlier for this length
+      auto it = g_tuned.find(std::make_tuple(n, (int)sizeof(R), axis));
+      if (it != g_tuned.end()) {
+        regplan_from(n, it->second.r, it->second.np, rp);
+        (axis == 1 ? pl->tky : pl->tkz) = it->second.tk;
+      }
+    }
     const std::vector<C> tw = twiddles(rp.n);
     std::vector<int> kp(n);
     if (rp.bl) {
@@ -991,14 +1102,34 @@ template <typename R> static int reg_tables(pmgpu_plan *pl, const char *caller) 
   return 0;
 }
 
+// while tuning is on: measure the schedules of lengths not yet in the table, then
+// rebuild the register plans from the table
+template <typename R> static int apply_tuning(pmgpu_plan *pl, const char *caller) {
+  if (!g_tune || g_force_stockham) return 0;
+  bool fresh = false;
+  for (int axis = 1; axis <= 2; axis++) {
+    const RegPlan &rp = axis == 1 ? pl->ry : pl->rz;
+    if (!(axis == 1 ? pl->ry_ok : pl->rz_ok) || rp.bl) continue;
+    const auto key = std::make_tuple(pl->g.M[axis], (int)sizeof(R), axis);
+    if (g_tuned.count(key)) continue;
+    TunedSchedule ts;
+    if (tune_axis<R>(pl, axis, ts, caller) == 0) {
+      g_tuned.emplace(key, ts);
+      fresh = true;
+    }
+  }
+  return fresh ? reg_tables<R>(pl, caller, true) : 0;
+}
+
 template <typename R> static int plan_tables(pmgpu_plan *pl, const char *caller) {
   std::vector<cld> tw;
   if (!make_fft(pl->g.N2, pl->g.M[0], pl->fx, tw) || upload_tw<R>(tw, pl->twx, caller)) return -1;
   if (!make_fft(pl->g.M[1], 0, pl->fy, tw) || upload_tw<R>(tw, pl->twy, caller)) return -1;
   if (!make_fft(pl->g.M[2], 0, pl->fz, tw) || upload_tw<R>(tw, pl->twz, caller)) return -1;
   if (upload_wavenumbers<R>(pl, caller)) return -1;
-  if (reg_tables<R>(pl, caller)) return -1;
-  return setup_green<R>(pl, caller);
+  if (reg_tables<R>(pl, caller, true)) return -1;
+  if (setup_green<R>(pl, caller)) return -1;
+  return apply_tuning<R>(pl, caller);
 }
 
 static int check_params(const pmgpu_params *par) {
@@ -1787,4 +1918,26 @@ pmgpu_plan *pmgpu_batch_plan(pmgpu_batch *b, int i) {
 void pmgpu_batch_destroy(pmgpu_batch *b) {
   std::lock_guard<std::mutex> lk(g_mu);
   delete b;
+}
+
+int pmgpu_fft_tune(int on) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int old = g_tune;
+  g_tune = on ? 1 : 0;
+  return old;
+}
+
+int pmgpu_fft_tuned(int index, int *length, int *precision, int *axis, int *radices, int *tile, double *ms) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (index < 0 || index >= (int)g_tuned.size()) return -1;
+  auto it = g_tuned.begin();
+  std::advance(it, index);
+  if (length) *length = std::get<0>(it->first);
+  if (precision) *precision = std::get<1>(it->first) == 8 ? PMGPU_FP64 : PMGPU_FP32;
+  if (axis) *axis = std::get<2>(it->first);
+  if (radices)
+    for (int i = 0; i < 3; i++) radices[i] = i < it->second.np ? it->second.r[i] : 0;
+  if (tile) *tile = it->second.tk;
+  if (ms) *ms = it->second.ms;
+  return 0;
 }

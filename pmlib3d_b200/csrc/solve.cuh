@@ -50,6 +50,7 @@ template <typename R> struct SolveGeom {
   const C *rtwx, *rtwy, *rtwz;  // w_n^q, q < n
   const C *rextx;            // exp(-2 pi i k / Mx), k < H
   const int *xpos;           // frequency -> position of the x transform
+  int tky, tkz;              // kx tile of the y / z register passes (0: chosen by shared memory)
   const C *rchx, *rchy, *rchz;  // Bluestein plans: chirp exp(-i pi j^2 / n), j < n
   const C *rbx, *rby, *rbz;     // Bluestein plans: FFT of the wrapped chirp, by position
   const int *yk;             // row of the y spectrum -> ky index (nullptr: natural order)

@@ -253,6 +253,27 @@ class Batch:
             pass
 
 
+def fft_tune(on: bool) -> int:
+    """Turns the schedule autotuner on or off for plans created afterwards; returns
+    the previous setting."""
+    return lib().pmgpu_fft_tune(int(bool(on)))
+
+
+def fft_tuned() -> list:
+    """The tuning table: dicts with length, precision, axis, radices, tile, ms."""
+    out = []
+    i = 0
+    while True:
+        n, pr, ax, tk = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        rad = (C.c_int * 3)()
+        ms = C.c_double()
+        if lib().pmgpu_fft_tuned(i, C.byref(n), C.byref(pr), C.byref(ax), rad, C.byref(tk), C.byref(ms)) != 0:
+            return out
+        out.append({"length": n.value, "precision": "fp64" if pr.value == FP64 else "fp32", "axis": ax.value,
+                    "radices": [r for r in rad if r], "tile": tk.value, "ms": ms.value})
+        i += 1
+
+
 def fft_engine(engine: int) -> int:
     """Line-FFT engine of plans created afterwards: 0 = register passes where the
     lengths allow (default), 1 = Stockham passes.  Returns the previous setting."""

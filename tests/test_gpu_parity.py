@@ -149,6 +149,38 @@ def test_fft_engines_agree(name, xmin, xmax, dx, bc, ng, prec):
     assert rel_l2(outs[1], outs[0]) < (1e-14 if prec == P.FP64 else 1e-6), rel_l2(outs[1], outs[0])
 
 
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", [CASES[0], LONG_CASES[2]])
+def test_autotuned_schedules(name, xmin, xmax, dx, bc, ng):
+    """Plans made while the autotuner is on record a schedule per length and still
+    match the oracle; the untuned plan agrees to round-off."""
+    po, to, qo, pg, tg, qg = setup_pair(xmin, xmax, dx, bc, ng, interp=3, order=6)
+    w = gaussian_field(to, seed=21, noise=0.01)
+    vel_o, _, _ = oracle_solve(po, to, qo, w)
+    ierr, plain = P.pmlib_poisson_setup(pg, tg, qg, P.FP64)
+    old = P.fft_tune(True)
+    try:
+        ierr, tuned = P.pmlib_poisson_setup(pg, tg, qg, P.FP64)
+    finally:
+        P.fft_tune(old)
+    assert ierr == 0, P.last_error()
+    table = P.fft_tuned()
+    lengths = {(e["length"], e["axis"]) for e in table if e["precision"] == "fp64"}
+    M = O.kernel_dims(po, qo)[0]
+    assert (M[1], 1) in lengths and (M[2], 2) in lengths, table
+    for e in table:
+        prod = 1
+        for r in e["radices"]:
+            prod *= r
+        assert prod == e["length"] and e["tile"] in (2, 4, 8) and e["ms"] > 0
+    out = []
+    for plan in (tuned, plain):
+        vel = np.zeros_like(w)
+        assert P.pmlib_poisson_solve(plan, w.copy(), vel) == 0
+        out.append(vel)
+    assert rel_l2(out[0], vel_o) < TOL64
+    assert rel_l2(out[0], out[1]) < 1e-14
+
+
 def test_mixedbc_convergence_pin_on_gpu():
     """The GPU FP64 solve reproduces validation/mixedbc__/convergence.dat (h = 1/16, 1/32)."""
     def gpu_solver(patch, t, par, vort, reg_vort=True, calc_vecpot=False):
