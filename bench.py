@@ -430,7 +430,7 @@ def main():
                        "parallelism": f"replicas x{world}", "l2": L2_NOTE},
             "fft_schedules": [e for e in P.fft_tuned() if e["length"] in (2 * (w.n + 2 * w.nghost),)],
             "fp64_plain": {"value": value64, "unit": "steps/s", "ms_per_step": ms64 / k64},
-            "fp32_speedup_vs_fp64": value / value64,
+            "particles_per_s": value * n, "fp32_speedup_vs_fp64": value / value64,
             "accuracy": {"rel_l2_fp32_vs_fp64": rel_l2, "max_rel_err": max_err},
             "roofline": roofline, "kernels": kernels, "gpu_launches": launches32,
             "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "batched": batched, "served": served,

@@ -183,6 +183,17 @@ void pmgpu_batch_destroy(pmgpu_batch *batch);
  * the same results to round-off; returns the previous setting. */
 int pmgpu_fft_engine(int engine);
 
+/* Global particle diagnostics accumulated in FP64 for FP32 or FP64 particle arrays
+ * (device pointers, (3, npart) component fastest), the quantities of
+ * vortex_codes/vortex_structures/source/diagnostics/diagnostics_knot.f:75-175:
+ *   out[0..2] impulse, out[3..5] angular impulse, out[6] kinetic energy,
+ *   out[7] enstrophy, out[8] helicity, out[9..11] enstrophy centroid,
+ *   out[12] ring radius (both normalised by the enstrophy), out[13] max |vorticity|.
+ * Deterministic (fixed reduction order); synchronises `stream`. */
+int pmgpu_particle_diagnostics(const double dx[3], const void *d_pos, const void *d_vel,
+                               const void *d_vort, int npart, int precision, double out[14],
+                               void *stream);
+
 /* Schedule autotuner (no counterpart in the reference).  While on, creating a plan
  * times, for every y / z transform length and precision not measured before, the y
  * forward pass and the fused z pass with the best few radix sequences (by the

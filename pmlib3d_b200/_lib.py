@@ -20,7 +20,7 @@ EXPORTS = (
     "pmgpu_timing_enable", "pmgpu_timing_reset", "pmgpu_timing_get",
     "pmgpu_interp_particle_mesh_noalloc", "pmgpu_fft_engine", "pmgpu_poisson_solve_dev",
     "pmgpu_batch_create", "pmgpu_batch_solve", "pmgpu_batch_size", "pmgpu_batch_plan", "pmgpu_batch_destroy",
-    "pmgpu_fft_tune", "pmgpu_fft_tuned",
+    "pmgpu_fft_tune", "pmgpu_fft_tuned", "pmgpu_particle_diagnostics",
 )
 
 
@@ -93,6 +93,7 @@ def lib():
         "pmgpu_batch_destroy": [vp],
         "pmgpu_fft_tune": [C.c_int],
         "pmgpu_fft_tuned": [C.c_int, ip, ip, ip, ip, ip, dp],
+        "pmgpu_particle_diagnostics": [dp, vp, vp, vp, C.c_int, C.c_int, dp, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

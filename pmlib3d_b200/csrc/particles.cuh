@@ -736,6 +736,68 @@ __global__ void __launch_bounds__(M2P_THREADS) k_m2p_tile(PartGeom<R> g, const R
   }
 }
 
+// ------------------------------------------------------------------ diagnostics
+// Global particle diagnostics in FP64 whatever the field precision
+// (vortex_codes/vortex_structures/source/diagnostics/diagnostics_knot.f:75-158):
+//   0-2 impulse 1/2 sum x*w, 3-5 angular impulse 1/3 sum x*(x*w), 6 kinetic energy
+//   sum u.(x*w), 7 enstrophy sum |w|^2, 8 helicity sum u.w (all times dx dy dz),
+//   9-11 sum |w|^2 x and 12 sum |w|^2 sqrt(y^2 + z^2) (normalised by the enstrophy
+//   on the host), 13 max |w|.  Each block sums a fixed slice in a fixed order, so
+//   the totals are the same on every run.
+constexpr int DIAG_N = 14;
+constexpr int DIAG_THREADS = 256;
+template <typename R>
+__global__ void __launch_bounds__(DIAG_THREADS) k_diag_partial(const R *__restrict__ pos, const R *__restrict__ vel,
+                                                               const R *__restrict__ vort, int n, double dv,
+                                                               double *__restrict__ part) {
+  double acc[DIAG_N];
+#pragma unroll
+  for (int i = 0; i < DIAG_N; i++) acc[i] = 0.0;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const double x = pos[3 * (size_t)p], y = pos[3 * (size_t)p + 1], z = pos[3 * (size_t)p + 2];
+    const double u = vel[3 * (size_t)p], v = vel[3 * (size_t)p + 1], w = vel[3 * (size_t)p + 2];
+    const double a = vort[3 * (size_t)p], b = vort[3 * (size_t)p + 1], c = vort[3 * (size_t)p + 2];
+    const double m1x = y * c - z * b, m1y = z * a - x * c, m1z = x * b - y * a;  // x * w
+    const double m2x = y * m1z - z * m1y, m2y = z * m1x - x * m1z, m2z = x * m1y - y * m1x;
+    const double e = a * a + b * b + c * c;
+    acc[0] += 0.5 * m1x * dv;
+    acc[1] += 0.5 * m1y * dv;
+    acc[2] += 0.5 * m1z * dv;
+    acc[3] += (1.0 / 3.0) * m2x * dv;
+    acc[4] += (1.0 / 3.0) * m2y * dv;
+    acc[5] += (1.0 / 3.0) * m2z * dv;
+    acc[6] += (u * m1x + v * m1y + w * m1z) * dv;
+    acc[7] += e * dv;
+    acc[8] += (u * a + v * b + w * c) * dv;
+    acc[9] += e * x * dv;
+    acc[10] += e * y * dv;
+    acc[11] += e * z * dv;
+    acc[12] += e * sqrt(y * y + z * z) * dv;
+    acc[13] = fmax(acc[13], sqrt(e));
+  }
+  __shared__ double sh[DIAG_THREADS];
+  for (int i = 0; i < DIAG_N; i++) {
+    sh[threadIdx.x] = acc[i];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if ((int)threadIdx.x < s) sh[threadIdx.x] = i == 13 ? fmax(sh[threadIdx.x], sh[threadIdx.x + s])
+                                                          : sh[threadIdx.x] + sh[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) part[(size_t)blockIdx.x * DIAG_N + i] = sh[0];
+    __syncthreads();
+  }
+}
+
+// one thread per quantity sums the block partials in block order
+__global__ void k_diag_final(const double *__restrict__ part, int nblk, double *__restrict__ out) {
+  const int i = threadIdx.x;
+  if (i >= DIAG_N) return;
+  double s = 0.0;
+  for (int b = 0; b < nblk; b++) s = i == 13 ? fmax(s, part[(size_t)b * DIAG_N + i]) : s + part[(size_t)b * DIAG_N + i];
+  out[i] = s;
+}
+
 // ------------------------------------------------------------------ remesh
 // source/remesh/pmlib_remesh.f:84-226: a particle per kept cell, cells in k-j-i order
 __global__ void k_remesh_flag(PartGeom<double> g, const double *__restrict__ vort,

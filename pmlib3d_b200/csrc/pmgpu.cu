@@ -482,6 +482,7 @@ namespace pmgpu {
 struct Scratch {
   DevBuf key, val, key2, val2, counts, start, spart, hist;
   DevBuf a, b, c, d, e, f, g, h;
+  DevBuf diag;  // diagnostics partial sums
 };
 static Scratch &scratch() {
   static Scratch s;
@@ -1939,5 +1940,41 @@ int pmgpu_fft_tuned(int index, int *length, int *precision, int *axis, int *radi
     for (int i = 0; i < 3; i++) radices[i] = i < it->second.np ? it->second.r[i] : 0;
   if (tile) *tile = it->second.tk;
   if (ms) *ms = it->second.ms;
+  return 0;
+}
+
+// ------------------------------------------------------------------ diagnostics
+int pmgpu_particle_diagnostics(const double dx[3], const void *d_pos, const void *d_vel, const void *d_vort,
+                               int npart, int precision, double out[14], void *stream) {
+  const char *caller = "pmgpu_particle_diagnostics";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!dx || !out || npart < 0 || (npart > 0 && (!d_pos || !d_vel || !d_vort))) {
+    set_error(caller, "missing argument.");
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  Scratch &s = scratch();
+  const int nblk = 2 * num_sms();
+  if (s.diag.ensure(sizeof(double) * ((size_t)nblk * DIAG_N + DIAG_N), caller)) return -1;
+  double *part = s.diag.as<double>(), *dout = part + (size_t)nblk * DIAG_N;
+  cudaStream_t st = (cudaStream_t)stream;
+  const double dv = dx[0] * dx[1] * dx[2];
+  if (precision == PMGPU_FP64)
+    k_diag_partial<double><<<nblk, DIAG_THREADS, 0, st>>>((const double *)d_pos, (const double *)d_vel,
+                                                          (const double *)d_vort, npart, dv, part);
+  else
+    k_diag_partial<float><<<nblk, DIAG_THREADS, 0, st>>>((const float *)d_pos, (const float *)d_vel,
+                                                         (const float *)d_vort, npart, dv, part);
+  PM_LAUNCHED();
+  k_diag_final<<<1, 32, 0, st>>>(part, nblk, dout);
+  PM_LAUNCHED();
+  CKL(caller);
+  double h[DIAG_N];
+  CK(cudaMemcpyAsync(h, dout, sizeof(h), cudaMemcpyDeviceToHost, st), caller);
+  CK(cudaStreamSynchronize(st), caller);
+  for (int i = 0; i < DIAG_N; i++) out[i] = h[i];
+  if (h[7] > 0.0) {
+    for (int i = 9; i < 13; i++) out[i] = h[i] / h[7];  // centroid and ring radius (diagnostics_knot.f:171-175)
+  }
   return 0;
 }

@@ -253,6 +253,22 @@ class Batch:
             pass
 
 
+DIAGNOSTICS = ("impulse_x", "impulse_y", "impulse_z", "angular_impulse_x", "angular_impulse_y",
+               "angular_impulse_z", "kinetic_energy", "enstrophy", "helicity", "centroid_x", "centroid_y",
+               "centroid_z", "ring_radius", "max_vorticity")
+
+
+def particle_diagnostics(dx, d_pos: int, d_vel: int, d_vort: int, npart: int, precision: int,
+                         stream: int = 0) -> dict:
+    """Global diagnostics of the particle field in FP64 (diagnostics_knot.f:75-175)."""
+    out = (C.c_double * 14)()
+    d = (C.c_double * 3)(*dx)
+    if lib().pmgpu_particle_diagnostics(d, C.c_void_p(d_pos), C.c_void_p(d_vel), C.c_void_p(d_vort), int(npart),
+                                        int(precision), out, C.c_void_p(stream or None)) != 0:
+        raise RuntimeError(last_error())
+    return dict(zip(DIAGNOSTICS, list(out)))
+
+
 def fft_tune(on: bool) -> int:
     """Turns the schedule autotuner on or off for plans created afterwards; returns
     the previous setting."""

@@ -386,3 +386,32 @@ def test_odd_periodic_length_rejected():
     ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP64)
     assert ierr == -1
     assert "nfft is an odd number." in P.last_error()
+
+
+@pytest.mark.parametrize("prec", [P.FP64, P.FP32])
+def test_particle_diagnostics(prec):
+    """FP64 global diagnostics (diagnostics_knot.f:75-175) of FP32 / FP64 particle
+    arrays against the same sums in NumPy; identical on a rerun."""
+    import torch
+    rng = np.random.default_rng(30)
+    n = 100003
+    pos = rng.uniform(-1, 1, (n, 3))
+    vel = rng.standard_normal((n, 3))
+    vort = rng.standard_normal((n, 3))
+    dt = torch.float64 if prec == P.FP64 else torch.float32
+    tp, tu, tw = (torch.from_numpy(a).to("cuda", dt) for a in (pos, vel, vort))
+    x, u, w = (t.double().cpu().numpy() for t in (tp, tu, tw))
+    dx = (0.01, 0.02, 0.015)
+    d = P.particle_diagnostics(dx, tp.data_ptr(), tu.data_ptr(), tw.data_ptr(), n, prec)
+    dv = dx[0] * dx[1] * dx[2]
+    m1 = np.cross(x, w)
+    m2 = np.cross(x, m1)
+    e = np.sum(w * w, axis=1)
+    ens = e.sum() * dv
+    ref = np.concatenate([0.5 * m1.sum(0) * dv, m2.sum(0) * dv / 3.0, [np.sum(u * m1) * dv, ens, np.sum(u * w) * dv],
+                          (e[:, None] * x).sum(0) * dv / ens, [np.sum(e * np.hypot(x[:, 1], x[:, 2])) * dv / ens,
+                                                               np.sqrt(e.max())]])
+    got = np.array([d[k] for k in P.DIAGNOSTICS])
+    assert np.allclose(got, ref, rtol=1e-10, atol=1e-12 * np.abs(ref).max())
+    d2 = P.particle_diagnostics(dx, tp.data_ptr(), tu.data_ptr(), tw.data_ptr(), n, prec)
+    assert d2 == d
