@@ -39,6 +39,26 @@ template <int DIR, typename C> __host__ __device__ __forceinline__ C cmul_mi(C a
 }
 template <typename C> __host__ __device__ __forceinline__ C cconj(C a) { return mk(a.x, -a.y); }
 
+// a + s * c for a complex s and a real c
+template <typename C, typename R> __host__ __device__ __forceinline__ C cfma_r(C s, R c, C a) {
+  return mk(a.x + s.x * c, a.y + s.y * c);
+}
+
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+// FP32 complex values as one packed register pair: additions and real scalings are
+// single FP32x2 instructions (same rounding as the two scalar operations)
+template <> __device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b) { return __fadd2_rn(a, b); }
+template <> __device__ __forceinline__ float2 csub<float2>(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+}
+template <> __device__ __forceinline__ float2 cscale<float2, float>(float2 a, float s) {
+  return __fmul2_rn(a, make_float2(s, s));
+}
+template <> __device__ __forceinline__ float2 cfma_r<float2, float>(float2 s, float c, float2 a) {
+  return __ffma2_rn(s, make_float2(c, c), a);
+}
+#endif
+
 // kernel launch accounting (read by pmgpu_launch_count)
 extern long long g_launches;
 

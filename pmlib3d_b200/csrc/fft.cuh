@@ -91,8 +91,8 @@ template <int R, bool INV, typename C> __device__ __forceinline__ void dft_prime
     for (int n = 1; n <= h; n++) {
       const int m = (n * k) % R;
       const T c = cs_c<T>(R, m), sn = cs_s<T>(R, m);
-      a = mk(a.x + s[n].x * c, a.y + s[n].y * c);
-      b = mk(b.x + d[n].x * sn, b.y + d[n].y * sn);
+      a = cfma_r(s[n], c, a);
+      b = cfma_r(d[n], sn, b);
     }
     if (!INV) {
       v[k] = mk(a.x + b.y, a.y - b.x);
