@@ -339,9 +339,17 @@ template <int W> struct WStride { static constexpr int v = W == 4 ? 4 : 8; };
 
 // shared-memory bytes of k_deposit for `cap` staged particles
 template <typename R, int W> __host__ __device__ constexpr size_t deposit_smem(int cap) {
-  return (size_t)cap * (3 * WStride<W>::v + 4) * sizeof(R) + (size_t)cap * sizeof(int) +
+  return (size_t)cap * (3 * WStride<W>::v + 4) * sizeof(R) +
          sizeof(int) * (DEP_LB * (DEP_TY + W - 1) * (DEP_TX + W) + DEP_LB * (DEP_TY + W - 1) + 2);
 }
+
+// an int carried in a value slot (bit pattern)
+template <typename R> __device__ __forceinline__ R int_bits(int v);
+template <> __device__ __forceinline__ float int_bits<float>(int v) { return __int_as_float(v); }
+template <> __device__ __forceinline__ double int_bits<double>(int v) { return __longlong_as_double((long long)v); }
+template <typename R> __device__ __forceinline__ int bits_int(R v);
+template <> __device__ __forceinline__ int bits_int<float>(float v) { return __float_as_int(v); }
+template <> __device__ __forceinline__ int bits_int<double>(double v) { return (int)__double_as_longlong(v); }
 
 template <typename R> __device__ __forceinline__ void lds4(const R *p, R *o);
 template <> __device__ __forceinline__ void lds4<float>(const float *p, float *o) {
@@ -371,12 +379,14 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit(PartGeom<R> g, const R 
   constexpr int NA = W + DEP_LB - 1;   // accumulator layers
   constexpr int NROW = DEP_LB * BY;    // bin rows of one batch
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R *wxs = reinterpret_cast<R *>(smem_raw);  // [cap][WS]
-  R *wys = wxs + (size_t)WS * cap;           // [cap][WS]
+  // x and y weights weight-major (threads reading consecutive particles hit
+  // consecutive banks), z weights and values particle-major for 16-byte loads; the
+  // value vector's last slot carries the particle's bin x within the tile
+  R *wxs = reinterpret_cast<R *>(smem_raw);  // [WS][cap]
+  R *wys = wxs + (size_t)WS * cap;           // [WS][cap]
   R *wzs = wys + (size_t)WS * cap;           // [cap][WS]
   R *vs = wzs + (size_t)WS * cap;            // [cap][4]
-  int *sbx = reinterpret_cast<int *>(vs + (size_t)4 * cap);  // [cap] bin x within the tile
-  int *sraw = sbx + cap;                                     // [NROW][BX+1] start of bin (row clamp)
+  int *sraw = reinterpret_cast<int *>(vs + (size_t)4 * cap);  // [NROW][BX+1] start of bin (row clamp)
   int *rowo = sraw + NROW * (BX + 1);                        // [NROW+1] staged offset of each row
 
   const int tx = threadIdx.x % DEP_TX, ty = threadIdx.x / DEP_TX;
@@ -453,16 +463,17 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit(PartGeom<R> g, const R 
           for (int t = W; t < WS; t++) wv[e][t] = R(0);
         }
 #pragma unroll
-        for (int t = 0; t < WS; t += 4) {
-          sts4<R>(wxs + i * WS + t, wv[0][t], wv[0][t + 1], wv[0][t + 2], wv[0][t + 3]);
-          sts4<R>(wys + i * WS + t, wv[1][t], wv[1][t + 1], wv[1][t + 2], wv[1][t + 3]);
-          sts4<R>(wzs + i * WS + t, wv[2][t], wv[2][t + 1], wv[2][t + 2], wv[2][t + 3]);
+        for (int t = 0; t < W; t++) {
+          wxs[t * cap + i] = wv[0][t];
+          wys[t * cap + i] = wv[1][t];
         }
+#pragma unroll
+        for (int t = 0; t < WS; t += 4) sts4<R>(wzs + i * WS + t, wv[2][t], wv[2][t + 1], wv[2][t + 2], wv[2][t + 3]);
         R vv[4] = {R(0), R(0), R(0), R(0)};
 #pragma unroll
         for (int c = 0; c < NV; c++) vv[c] = val[(size_t)vstride * p + c];
+        vv[3] = int_bits<R>((int)(bxi - g.blo[0]) - x0);
         sts4<R>(vs + i * 4, vv[0], vv[1], vv[2], vv[3]);
-        sbx[i] = (int)(bxi - g.blo[0]) - x0;
       }
       __syncthreads();
       if (active) {
@@ -477,15 +488,17 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit(PartGeom<R> g, const R 
               const int b0 = sr[0];
               const int lo = max(rowo[row] + sr[tx] - b0, c0);
               const int hi = min(rowo[row] + sr[tx + W] - b0, c1);
+              const R *wyrow = wys + sy * cap - c0;
+              const R *wxtx = wxs + (W - 1 + tx) * cap - c0;  // wx[W - 1 - (bx - tx)] = wxtx[q - bx cap]
 #pragma unroll 1
               for (int q = lo; q < hi; q++) {
                 const int i = q - c0;
-                const int sx = W - 1 - (sbx[i] - tx);
-                const R wxy = wxs[i * WS + sx] * wys[i * WS + sy];
                 R wz[WS], v[4];
+                lds4<R>(vs + i * 4, v);
                 lds4<R>(wzs + i * WS, wz);
                 if constexpr (WS == 8) lds4<R>(wzs + i * WS + 4, wz + 4);
-                lds4<R>(vs + i * 4, v);
+                const int bx = bits_int<R>(v[3]);
+                const R wxy = wxtx[q - bx * cap] * wyrow[q];
 #pragma unroll
                 for (int sz = 0; sz < W; sz++) {
                   const R w = wxy * wz[sz];
