@@ -5,7 +5,10 @@
 // kernel topology, pmlib_topology_kernel.f:109-110) and stored already shifted so
 // that r = 0 sits at index 0 (the fft_shift of pmlib_fft).  Periodic axes add the
 // images at +-1 patch length (:229-256).  The transform of this real, even sequence
-// is real and even in every axis, so the solve keeps one octant of it.
+// is real and even in every axis, so the solve keeps one octant of it.  Kernel 2
+// (three components p_c k2(r)) is odd along its own axis apart from the plane at
+// -M_c/2 dx_c, which has no mirror; its spectrum is kept as an odd imaginary
+// octant plus the plane's real spectrum.
 #pragma once
 
 #include "common.cuh"
@@ -135,6 +138,92 @@ __global__ void k_green_real(GreenParams gp, double *__restrict__ gr) {
           acc += green_k1(gp, sqrt(px * px + py * py + pz * pz));
         }
     gr[t] = acc;
+  }
+}
+
+// Kernel 2 (the derivative kernel, :1466-1500 and the Gaussian orders before it):
+// component c is p_c k2(r); k2 = 0 at r = 0.
+__device__ __forceinline__ double green_k2(const GreenParams &gp, double r) {
+  const double PI = 3.14159265358979323846;
+  if (r == 0.0) return 0.0;
+  const int o = gp.order;
+  const double r3 = r * r * r;
+  if (o == 100) {
+    const double rh = PI * r / gp.mdx;
+    return (sin(rh) - dev_si(rh)) / (2.0 * PI * PI * r3);
+  }
+  double f = 1.0;
+  if (o != 0) {
+    const double c_1_sqrt2 = 0.70710678118654752440;
+    const double c_1_sqrt2pi = 1.0 / sqrt(2.0 * PI);
+    const double rho = r / gp.eps;
+    const double q2 = rho * rho, q3 = q2 * rho, q5 = q3 * q2, q7 = q5 * q2, q9 = q7 * q2;
+    const double ex = exp(-0.5 * q2) * c_1_sqrt2pi;
+    const double er = erf(c_1_sqrt2 * rho);
+    double poly;
+    switch (o) {
+      case 2: poly = -2.0 * rho; break;
+      case 4: poly = -2.0 * rho + q3; break;
+      case 6: poly = -2.0 * rho + 2.25 * q3 - 0.25 * q5; break;
+      case 8: poly = -2.0 * rho + (89.0 / 24.0) * q3 + (-20.0 / 24.0) * q5 + (1.0 / 24.0) * q7; break;
+      default:
+        poly = -2.0 * rho + (1027.0 / 192.0) * q3 + (-349.0 / 192.0) * q5 + (35.0 / 192.0) * q7 +
+               (-1.0 / 192.0) * q9;
+        break;
+    }
+    f = poly * ex + er;
+  }
+  return -0.25 / PI * f / r3;
+}
+
+// component c of the real kernel 2 on the shifted grid (images as for kernel 1)
+__global__ void k_green_real2(GreenParams gp, int c, double *__restrict__ gr) {
+  const size_t total = (size_t)gp.M[0] * gp.M[1] * gp.M[2];
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    int s[3];
+    s[0] = (int)(t % gp.M[0]);
+    s[1] = (int)((t / gp.M[0]) % gp.M[1]);
+    s[2] = (int)(t / ((size_t)gp.M[0] * gp.M[1]));
+    double p0[3];
+    for (int e = 0; e < 3; e++) {
+      const int h = gp.M[e] / 2;
+      const int iu = s[e] < h ? s[e] + h + 1 : s[e] - h + 1;
+      p0[e] = gp.xmin[e] + ((double)(iu - 1) + 0.5) * gp.dx[e];
+    }
+    double acc = 0.0;
+    for (int kk = -gp.bc[2]; kk <= gp.bc[2]; kk++)
+      for (int jj = -gp.bc[1]; jj <= gp.bc[1]; jj++)
+        for (int ii = -gp.bc[0]; ii <= gp.bc[0]; ii++) {
+          const double p[3] = {p0[0] + gp.plen[0] * (double)ii, p0[1] + gp.plen[1] * (double)jj,
+                               p0[2] + gp.plen[2] * (double)kk};
+          acc += p[c] * green_k2(gp, sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]));
+        }
+    gr[t] = acc;
+  }
+}
+
+// Splits the spectrum of kernel-2 component c (kx < H, rows through yrow / zrow)
+// into S_c = Im, one octant (kx, |ky|, |kz|) with the Nyquist index of axis c
+// zeroed (S_c is odd along c), and E_c = Re at k_c = 0 (the plane's spectrum, even
+// in the other two axes; zero when M_c is odd): E_x (|kz|, |ky|), E_y (|kz|, kx),
+// E_z (|ky|, kx).  Both scaled by f = dx dy dz / (Mx My Mz).
+template <typename R>
+__global__ void k_green2_split(const double2 *__restrict__ spec, int c, int M0, int M1, int M2, int H, int Hp,
+                               int gM1, int gM2, double f, const int *__restrict__ yrow,
+                               const int *__restrict__ zrow, R *__restrict__ S, R *__restrict__ E) {
+  const size_t total = (size_t)gM2 * gM1 * H;
+  const int Mc = c == 0 ? M0 : (c == 1 ? M1 : M2);
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int kx = (int)(t % H);
+    const int iy = (int)((t / H) % gM1);
+    const int iz = (int)(t / ((size_t)H * gM1));
+    const int kc = c == 0 ? kx : (c == 1 ? iy : iz);
+    const double2 v = spec[((size_t)zrow[iz] * M1 + yrow[iy]) * Hp + kx];
+    S[t] = (2 * kc == Mc) ? R(0) : (R)(v.y * f);
+    if (kc == 0) {
+      const size_t e = c == 0 ? (size_t)iz * gM1 + iy : (c == 1 ? (size_t)iz * H + kx : (size_t)iy * H + kx);
+      E[e] = (Mc & 1) ? R(0) : (R)(v.x * f);
+    }
   }
 }
 

@@ -690,6 +690,7 @@ template <typename R> static SolveGeom<R> solve_geom(const pmgpu_plan *pl) {
   g.green = pl->green.as<R>();
   g.gM1 = pl->gM1;
   g.gM2 = pl->gM2;
+  g.kernel2 = pl->par.poisson_kernel == 2;
   g.scale = (R)(1.0 / ((double)g.M[0] * (double)g.M[1] * (double)g.M[2]));
   g.eps2pi = (R)(2.0 * 3.14159265358979323846 * pl->eps);
   g.order = pl->par.poisson_order;
@@ -892,22 +893,46 @@ template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller)
     if (gr.ensure(sizeof(double) * npts, caller) || gX.ensure(sizeof(double2) * nspec, caller) ||
         gY.ensure(sizeof(double2) * nspec, caller))
       break;
-    k_green_real<<<(unsigned)std::min<size_t>((npts + 255) / 256, 148 * 64), 256>>>(gp, gr.as<double>());
-    PM_LAUNCHED();
-    if (!cuda_ok(cudaGetLastError(), caller)) break;
-    if (fwd_xy<double, 1>(gg, gr.as<double>(), gX.as<double2>(), gY.as<double2>(), 0, caller)) break;
-    if (zpass<double, 1>(gg, gY.as<double2>(), gY.as<double2>(), Z_FORWARD, 0, 0, G.M[1], 0, caller)) break;
-    if (!cuda_ok(cudaStreamSynchronize(0), caller)) break;
     const size_t noct = (size_t)pl->gM2 * pl->gM1 * G.H;
-    if (own->ensure(sizeof(R) * noct, caller)) break;
-    attach_green(pl, own);
     const double f = pl->patch.dx[0] * pl->patch.dx[1] * pl->patch.dx[2] /
                      ((double)G.M[0] * (double)G.M[1] * (double)G.M[2]);
-    k_green_octant<R><<<(unsigned)std::min<size_t>((noct + 255) / 256, 148 * 64), 256>>>(
-        gY.as<double2>(), G.M[1], G.H, G.Hp, pl->gM1, pl->gM2, f, yinv.as<int>(), zinv.as<int>(),
-        pl->green.as<R>());
-    PM_LAUNCHED();
-    if (!cuda_ok(cudaGetLastError(), caller)) break;
+    const unsigned nb_real = (unsigned)std::min<size_t>((npts + 255) / 256, 148 * 64);
+    const unsigned nb_oct = (unsigned)std::min<size_t>((noct + 255) / 256, 148 * 64);
+    if (gp.kernel == 1) {
+      k_green_real<<<nb_real, 256>>>(gp, gr.as<double>());
+      PM_LAUNCHED();
+      if (!cuda_ok(cudaGetLastError(), caller)) break;
+      if (fwd_xy<double, 1>(gg, gr.as<double>(), gX.as<double2>(), gY.as<double2>(), 0, caller)) break;
+      if (zpass<double, 1>(gg, gY.as<double2>(), gY.as<double2>(), Z_FORWARD, 0, 0, G.M[1], 0, caller)) break;
+      if (!cuda_ok(cudaStreamSynchronize(0), caller)) break;
+      if (own->ensure(sizeof(R) * noct, caller)) break;
+      attach_green(pl, own);
+      k_green_octant<R><<<nb_oct, 256>>>(gY.as<double2>(), G.M[1], G.H, G.Hp, pl->gM1, pl->gM2, f, yinv.as<int>(),
+                                         zinv.as<int>(), pl->green.as<R>());
+      PM_LAUNCHED();
+      if (!cuda_ok(cudaGetLastError(), caller)) break;
+    } else {
+      // three octants S_x, S_y, S_z, then the planes E_x, E_y, E_z
+      const size_t nE = (size_t)pl->gM2 * pl->gM1 + (size_t)pl->gM2 * G.H + (size_t)pl->gM1 * G.H;
+      if (own->ensure(sizeof(R) * (3 * noct + nE), caller)) break;
+      attach_green(pl, own);
+      R *S = pl->green.as<R>(), *E = S + 3 * noct;
+      R *Ec[3] = {E, E + (size_t)pl->gM2 * pl->gM1, E + (size_t)pl->gM2 * (pl->gM1 + G.H)};
+      bool ok = true;
+      for (int c = 0; c < 3 && ok; c++) {
+        k_green_real2<<<nb_real, 256>>>(gp, c, gr.as<double>());
+        PM_LAUNCHED();
+        ok = cuda_ok(cudaGetLastError(), caller) &&
+             !fwd_xy<double, 1>(gg, gr.as<double>(), gX.as<double2>(), gY.as<double2>(), 0, caller) &&
+             !zpass<double, 1>(gg, gY.as<double2>(), gY.as<double2>(), Z_FORWARD, 0, 0, G.M[1], 0, caller);
+        if (!ok) break;
+        k_green2_split<R><<<nb_oct, 256>>>(gY.as<double2>(), c, G.M[0], G.M[1], G.M[2], G.H, G.Hp, pl->gM1, pl->gM2,
+                                           f, yinv.as<int>(), zinv.as<int>(), S + c * noct, Ec[c]);
+        PM_LAUNCHED();
+        ok = cuda_ok(cudaGetLastError(), caller);
+      }
+      if (!ok) break;
+    }
     if (!cuda_ok(cudaStreamSynchronize(0), caller)) break;
     g_green_cache[key] = own;
     rc = 0;
@@ -1370,10 +1395,6 @@ static int create_plan(const pmgpu_patch *patch, const pmgpu_topo *cuboid, const
   if (check_params(par)) return -1;
   if (precision != PMGPU_FP64 && precision != PMGPU_FP32) {
     set_error(caller, "precision unknown.");
-    return -1;
-  }
-  if (par->poisson_kernel != 1) {
-    set_error(caller, "Poisson kernel 2 is not available on the GPU path.");
     return -1;
   }
   int seen = 0;

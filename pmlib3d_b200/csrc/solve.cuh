@@ -40,6 +40,7 @@ template <typename R> struct SolveGeom {
   const R *kxt, *kyt, *kzt;  // wavenumbers (cycles / length), Nyquist index included
   const R *green;            // real octant G(kx, |ky|, |kz|) * dx dy dz / (Mx My Mz)
   int gM1, gM2;              // My / 2 + 1, Mz / 2 + 1
+  int kernel2;               // derivative kernel (3 components); green holds its spectrum
   R scale;                   // 1 / (Mx My Mz)
   R eps2pi;                  // 2 pi epsilon (filter argument scale)
   int order;                 // filter order (poisson order or reg_order)
@@ -207,6 +208,45 @@ __device__ __forceinline__ void z_multiply(const SolveGeom<R> &g, typename cplx_
     if constexpr (NC == 3) {
       R zt = R(1);
       if (use_zeta) zt = zeta_filter<R>(g.order, g.eps2pi * sqrt(kmag));
+      if (g.kernel2 && !g.allper) {
+        // derivative kernel K (pmlib_poisson_solve.f, kernel 2): component c is
+        // i S_c + (-1)^(k_c) E_c, S_c odd along axis c and even along the others
+        // (stored for |ky|, |kz| with the sign of the odd axis applied here), E_c the
+        // spectrum of the kernel's plane at -M_c/2 dx_c
+        const size_t noct = (size_t)g.gM2 * g.gM1 * g.H;
+        const int iz = min(z, g.M[2] - z);
+        const size_t oc = ((size_t)iz * g.gM1 + iy) * g.H + kx_i;
+        const R *E = g.green + 3 * noct;
+        R sx = g.green[oc], sy = g.green[noct + oc], sz = g.green[2 * noct + oc];
+        if (2 * y > g.M[1]) sy = -sy;
+        if (2 * z > g.M[2]) sz = -sz;
+        R ex = E[(size_t)iz * g.gM1 + iy];
+        R ey = E[(size_t)g.gM2 * g.gM1 + (size_t)iz * g.H + kx_i];
+        R ez = E[(size_t)g.gM2 * (g.gM1 + g.H) + (size_t)iy * g.H + kx_i];
+        if (kx_i & 1) ex = -ex;
+        if (y & 1) ey = -ey;
+        if (z & 1) ez = -ez;
+        const C Kx = mk(ex, sx), Ky = mk(ey, sy), Kz = mk(ez, sz);
+        const C w1 = v[0], w2 = v[1], w3 = v[2];
+        if (zmode == Z_VEL) {
+          v[0] = csub(cmul(Ky, w3), cmul(Kz, w2));
+          v[1] = csub(cmul(Kz, w1), cmul(Kx, w3));
+          v[2] = csub(cmul(Kx, w2), cmul(Ky, w1));
+        } else {  // Z_VORT: zeta w (+ K 2 pi i (k . w), Nyquist components dropped)
+          C o1 = cscale(w1, zt * g.scale), o2 = cscale(w2, zt * g.scale), o3 = cscale(w3, zt * g.scale);
+          if (reproj) {
+            const C da = cadd(cadd(cscale(w1, kxc), cscale(w2, kyc)), cscale(w3, kzc));
+            const C dv = mk(-twopi * da.y, twopi * da.x);
+            o1 = cadd(o1, cmul(Kx, dv));
+            o2 = cadd(o2, cmul(Ky, dv));
+            o3 = cadd(o3, cmul(Kz, dv));
+          }
+          v[0] = o1;
+          v[1] = o2;
+          v[2] = o3;
+        }
+        continue;
+      }
       R G;
       if (g.allper) {
         G = (kmag > R(0)) ? zt / (twopi * twopi * kmag) * g.scale : R(0);

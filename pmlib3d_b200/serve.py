@@ -45,10 +45,11 @@ def grid_key(r: Request):
             tuple(int(b) for b in r.bound_cond))
 
 
-def plan_bytes(topo, precision: int) -> int:
+def plan_bytes(topo, precision: int, kernel: int = 1) -> int:
     """Device bytes a plan holds for one velocity solve: the work spectra X and Y
     (3 components, half spectrum along x padded to a multiple of 8) and the Green
-    octant (shared, counted once per plan as an upper bound)."""
+    octant (three octants and three planes for kernel 2; shared, counted once per
+    plan as an upper bound)."""
     w = 4 if precision == P.FP32 else 8
     P_ = [topo.ncell[d] + topo.nghost[2 * d] + topo.nghost[2 * d + 1] for d in range(3)]
     per = [topo.bound_cond[2 * d] != 0 for d in range(3)]
@@ -58,7 +59,10 @@ def plan_bytes(topo, precision: int) -> int:
     Hp = (H + 7) // 8 * 8
     X = 3 * Hp * Pp[1] * Pp[2] * 2 * w
     Y = 3 * Hp * M[1] * Pp[2] * 2 * w
-    G = (M[2] // 2 + 1) * (M[1] // 2 + 1) * H * w
+    gM1, gM2 = M[1] // 2 + 1, M[2] // 2 + 1
+    G = gM2 * gM1 * H * w
+    if kernel == 2:
+        G = 3 * G + (gM2 * gM1 + gM2 * H + gM1 * H) * w
     return X + Y + G
 
 
@@ -124,7 +128,7 @@ class Server:
         if plans:
             self.idle.move_to_end(r.key)
             return plans.pop()
-        need = plan_bytes(r.topo, self.precision)
+        need = plan_bytes(r.topo, self.precision, self.params.poisson_kernel)
         while self.held + self.inflight_io + r.nbytes + need > self.budget:
             if not self._evict_one():
                 return None

@@ -94,6 +94,6 @@ def test_green_spectra_shared_between_plans():
 
 def test_batch_errors():
     specs, patches, topos, fields = _batch_inputs(2, seed=42)
-    par = P.make_params(order=6, kernel=2, radius=2.0, interp=3)
+    par = P.make_params(order=6, kernel=3, radius=2.0, interp=3)  # unknown kernel
     with pytest.raises(RuntimeError):
         P.Batch(patches, topos, par, P.FP32)
