@@ -222,6 +222,50 @@ int pmgpu_interp_particle_mesh_noalloc(const pmgpu_topo *topo, const pmgpu_param
                                        int npart, double *d_mesh, int nvar_mesh, int clear,
                                        int clear_ghost, void *stream);
 
+/* ---- the particle step around the solve ---- */
+
+/* The vorticity right-hand side of the vortex client's step
+ * (vortex_codes/vortex_structures/source/particle_derivatives/part_deriv_vorticity.f:5-213,
+ * which pmlib3d's clients call between the solve and the interpolation to particles):
+ *   dvort_l = visc (d2/dx2 + d2/dy2 + d2/dz2) vort_l + vort . grad vel_l
+ * on the interior cells, fd_order 2 or 4 (pmlib_fd_order, checked as
+ * source/parameters/pmlib_parameters_check.f:74-79 does), then the ghost map of
+ * dvort: periodic ghosts copy the far interior, free-axis ghosts keep the values
+ * the array held.  Meshes (3, nx', ny', nz') component fastest. */
+int pmgpu_deriv_vorticity(const pmgpu_topo *topo, int fd_order, double visc,
+                          const double *mesh_vort, const double *mesh_vel, double *mesh_dvort);
+int pmgpu_deriv_vorticity_f32(const pmgpu_topo *topo, int fd_order, double visc,
+                              const float *mesh_vort, const float *mesh_vel, float *mesh_dvort);
+/* the same on device meshes of `precision`, queued on `stream` */
+int pmgpu_deriv_vorticity_dev(const pmgpu_topo *topo, int fd_order, double visc, int precision,
+                              const void *d_vort, const void *d_vel, void *d_dvort, void *stream);
+
+/* pmlib_particles_advance (source/particles/pmlib_particles_advance.f:5-213, one rank):
+ * stage `itimestage` of the low-storage Runge-Kutta scheme of order `time_order`
+ * (pmlib_time_integration_order, 1-3; euler_vort as the optional argument), then the
+ * particle map of source/particles/pmlib_particles_map.f per axis: particles that
+ * leave across a free face are dropped, across a periodic face wrapped by the patch
+ * length, and the arrays are reordered as the reference's communication lists do.
+ * pos, vort, vel_rk, dvort_rk (3, npart) are updated and compacted in place; vel and
+ * dvort are read only (the reference reallocates them afterwards).  For time_order 1
+ * vel_rk and dvort_rk come back zero.  *npart_out and topo->npart get the new count.
+ * A particle that would need more than two wraps along one axis is an error. */
+int pmgpu_particles_advance(const pmgpu_patch *patch, pmgpu_topo *topo, int time_order,
+                            int itimestage, double dtime, int euler_vort, double *pos,
+                            double *vort, const double *vel, const double *dvort,
+                            double *vel_rk, double *dvort_rk, int npart, int *npart_out);
+int pmgpu_particles_advance_f32(const pmgpu_patch *patch, pmgpu_topo *topo, int time_order,
+                                int itimestage, double dtime, int euler_vort, float *pos,
+                                float *vort, const float *vel, const float *dvort,
+                                float *vel_rk, float *dvort_rk, int npart, int *npart_out);
+/* the same on device arrays of `precision`; synchronises `stream` (the count is
+ * returned to the host) */
+int pmgpu_particles_advance_dev(const pmgpu_patch *patch, pmgpu_topo *topo, int time_order,
+                                int itimestage, double dtime, int euler_vort, int precision,
+                                void *d_pos, void *d_vort, const void *d_vel, const void *d_dvort,
+                                void *d_vel_rk, void *d_dvort_rk, int npart, int *npart_out,
+                                void *stream);
+
 /* ---- diagnostics (no counterpart in the reference, which has no timers) ---- */
 const char *pmgpu_last_error(void);
 /* number of this library's kernels launched since the last reset */

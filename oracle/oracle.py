@@ -95,6 +95,9 @@ def lib():
                                         dp, dp, dp, C.c_int, C.c_int, C.c_int]
         L.pmo_regularise.argtypes = [C.POINTER(Patch), C.POINTER(Topo), dp, C.c_int, C.c_int,
                                      C.c_double]
+        L.pmo_deriv_vorticity.argtypes = [C.POINTER(Topo), C.c_int, C.c_double, dp, dp, dp]
+        L.pmo_particles_advance.argtypes = [C.POINTER(Patch), C.POINTER(Topo), C.c_int, C.c_int, C.c_double,
+                                            C.c_int, dp, dp, dp, dp, dp, dp, C.c_int, ip]
         L.pmo_si.argtypes = [C.c_double]
         L.pmo_si.restype = C.c_double
         _lib = L
@@ -241,3 +244,20 @@ def regularise(patch, t, mesh, reg_order, filter_width):
 
 def si(x: float) -> float:
     return lib().pmo_si(float(x))
+
+
+def deriv_vorticity(t, fd_order, visc, vort, vel, dvort):
+    """dvort (updated in place on the interior and periodic ghosts) = visc lap(vort) +
+    (vort . grad) vel; returns ierr."""
+    return lib().pmo_deriv_vorticity(C.byref(t), int(fd_order), float(visc), _p(vort), _p(vel), _p(dvort))
+
+
+def particles_advance(patch, t, time_order, stage, dtime, pos, vort, vel, dvort, vel_rk, dvort_rk,
+                      euler_vort=False):
+    """RK stage + particle map; the (np, 3) arrays pos, vort, vel_rk, dvort_rk are
+    compacted in place.  Returns (ierr, npart)."""
+    n = C.c_int(0)
+    ierr = lib().pmo_particles_advance(C.byref(patch), C.byref(t), int(time_order), int(stage), float(dtime),
+                                       int(bool(euler_vort)), _p(pos), _p(vort), _p(vel), _p(dvort), _p(vel_rk),
+                                       _p(dvort_rk), pos.shape[0], C.byref(n))
+    return ierr, n.value

@@ -1166,3 +1166,216 @@ int pmo_regularise(const pmo_patch *pa, const pmo_topo *cub, double *mesh, int n
   }
   return inverse_two_axes(pa, cub, &w, mesh);
 }
+
+/* ------------------------------------------------------------------------- */
+/* The vorticity right-hand side of the particle step, computed on the mesh by the
+ * client around the solve (vortex_codes/vortex_structures/source/particle_derivatives/
+ * part_deriv_vorticity.f:57-193): on every interior cell and component l
+ *   dvort_l = visc (d2/dx2 + d2/dy2 + d2/dz2) vort_l + w1 du_l/dx + w2 du_l/dy + w3 du_l/dz
+ * with second-order (:57-112) or fourth-order (:117-193) central differences, then
+ * the ghost map of dvort (:199-206; pmlib_mesh_map_ghost.f incl_edges = .FALSE., op 0
+ * for one rank): periodic ghosts copy the far interior, free-axis ghosts keep what
+ * the array held. */
+int pmo_deriv_vorticity(const pmo_topo *t, int fd_order, double visc, const double *vort,
+                        const double *vel, double *dvort) {
+  if (fd_order != 2 && fd_order != 4) {
+    pm_write("pmlib_parameters_check", "pmlib_fd_order is incorrectly set.");
+    return -1;
+  }
+  const int *nc = t->ncell;
+  const double c_1_dx2 = 1.0 / (t->dx[0] * t->dx[0]), c_1_dy2 = 1.0 / (t->dx[1] * t->dx[1]),
+               c_1_dz2 = 1.0 / (t->dx[2] * t->dx[2]);
+  const double c_1_2dx = 1.0 / (2.0 * t->dx[0]), c_1_2dy = 1.0 / (2.0 * t->dx[1]),
+               c_1_2dz = 1.0 / (2.0 * t->dx[2]);
+  const double c1 = -1.0 / 12.0, c2 = 4.0 / 3.0, c3 = 1.0 / 6.0, c4 = 4.0 / 3.0;
+  int nth = g_threads;
+#pragma omp parallel for schedule(static) num_threads(nth)
+  for (int k = 1; k <= nc[2]; k++)
+    for (int j = 1; j <= nc[1]; j++)
+      for (int i = 1; i <= nc[0]; i++) {
+        const double w1 = vort[midx(t, 3, 0, i, j, k)], w2 = vort[midx(t, 3, 1, i, j, k)],
+                     w3 = vort[midx(t, 3, 2, i, j, k)];
+        for (int l = 0; l < 3; l++) {
+#define V(ii, jj, kk) vort[midx(t, 3, l, ii, jj, kk)]
+#define U(ii, jj, kk) vel[midx(t, 3, l, ii, jj, kk)]
+          double ddx, ddy, ddz, d1, d2, d3;
+          if (fd_order == 2) {
+            ddx = (1.0 * V(i - 1, j, k) - 2.0 * V(i, j, k) + 1.0 * V(i + 1, j, k)) * c_1_dx2;
+            d1 = (-1.0 * U(i - 1, j, k) + 1.0 * U(i + 1, j, k)) * c_1_2dx;
+            ddy = (1.0 * V(i, j - 1, k) - 2.0 * V(i, j, k) + 1.0 * V(i, j + 1, k)) * c_1_dy2;
+            d2 = (-1.0 * U(i, j - 1, k) + 1.0 * U(i, j + 1, k)) * c_1_2dy;
+            ddz = (1.0 * V(i, j, k - 1) - 2.0 * V(i, j, k) + 1.0 * V(i, j, k + 1)) * c_1_dz2;
+            d3 = (-1.0 * U(i, j, k - 1) + 1.0 * U(i, j, k + 1)) * c_1_2dz;
+          } else {
+            ddx = (c1 * V(i - 2, j, k) + c2 * V(i - 1, j, k) - 2.5 * V(i, j, k) + c2 * V(i + 1, j, k) +
+                   c1 * V(i + 2, j, k)) * c_1_dx2;
+            d1 = (c3 * U(i - 2, j, k) - c4 * U(i - 1, j, k) + c4 * U(i + 1, j, k) - c3 * U(i + 2, j, k)) * c_1_2dx;
+            ddy = (c1 * V(i, j - 2, k) + c2 * V(i, j - 1, k) - 2.5 * V(i, j, k) + c2 * V(i, j + 1, k) +
+                   c1 * V(i, j + 2, k)) * c_1_dy2;
+            d2 = (c3 * U(i, j - 2, k) - c4 * U(i, j - 1, k) + c4 * U(i, j + 1, k) - c3 * U(i, j + 2, k)) * c_1_2dy;
+            ddz = (c1 * V(i, j, k - 2) + c2 * V(i, j, k - 1) - 2.5 * V(i, j, k) + c2 * V(i, j, k + 1) +
+                   c1 * V(i, j, k + 2)) * c_1_dz2;
+            d3 = (c3 * U(i, j, k - 2) - c4 * U(i, j, k - 1) + c4 * U(i, j, k + 1) - c3 * U(i, j, k + 2)) * c_1_2dz;
+          }
+#undef V
+#undef U
+          dvort[midx(t, 3, l, i, j, k)] = visc * (ddx + ddy + ddz) + w1 * d1 + w2 * d2 + w3 * d3;
+        }
+      }
+  /* ghost map, one axis after the other over the full extent of the other axes */
+  int ext[3];
+  pmo_topo_extent(t, ext);
+  for (int d = 0; d < 3; d++) {
+    if (t->bound_cond[2 * d] == 0 || t->bound_cond[2 * d + 1] == 0) continue;
+    const int N = nc[d], ngl = t->nghost[2 * d], ngh = t->nghost[2 * d + 1];
+    const int o1 = (d == 0) ? 1 : 0, o2 = (d == 2) ? 1 : 2;
+    for (int q = 0; q < ext[o2]; q++)
+      for (int p = 0; p < ext[o1]; p++) {
+        int ijk[3];
+        ijk[o1] = p + 1 - t->nghost[2 * o1];
+        ijk[o2] = q + 1 - t->nghost[2 * o2];
+        for (int s = 0; s < ngh + ngl; s++) {
+          const int to = s < ngh ? N + 1 + s : 1 - ngl + (s - ngh);
+          const int from = s < ngh ? 1 + s : N - ngl + 1 + (s - ngh);
+          for (int c = 0; c < 3; c++) {
+            ijk[d] = from;
+            const double v = dvort[midx(t, 3, c, ijk[0], ijk[1], ijk[2])];
+            ijk[d] = to;
+            dvort[midx(t, 3, c, ijk[0], ijk[1], ijk[2])] = v;
+          }
+        }
+      }
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Low-storage Runge-Kutta coefficients a, b, c of each stage for position (1) and
+ * vorticity (2) (source/particles/pmlib_particles_advance.f:49-88) */
+static int rk_coefficients(int order, int euler_vort, double a1[3], double b1[3], double c1[3], double a2[3],
+                           double b2[3], double c2[3]) {
+  for (int s = 0; s < 3; s++) a1[s] = b1[s] = c1[s] = a2[s] = b2[s] = c2[s] = 0.0;
+  if (order == 1) {
+    b1[0] = c1[0] = b2[0] = c2[0] = 1.0;
+  } else if (order == 2) {
+    a1[1] = -0.5; b1[0] = 1.0; b1[1] = 1.0; c1[0] = 0.5; c1[1] = 1.0;
+    if (euler_vort) {
+      a2[1] = 1.0; b2[0] = 1.0; c2[0] = 0.5; c2[1] = 0.5;
+    } else {
+      a2[1] = -0.5; b2[0] = 1.0; b2[1] = 1.0; c2[0] = 0.5; c2[1] = 1.0;
+    }
+  } else if (order == 3) {
+    a1[1] = -5.0 / 9.0; a1[2] = -153.0 / 128.0;
+    b1[0] = b1[1] = b1[2] = 1.0;
+    c1[0] = 1.0 / 3.0; c1[1] = 15.0 / 16.0; c1[2] = 8.0 / 15.0;
+    if (euler_vort) {
+      a2[1] = 1.0; a2[2] = 1.0; b2[0] = 1.0;
+      c2[0] = c2[1] = c2[2] = 1.0 / 3.0;
+    } else {
+      a2[1] = -5.0 / 9.0; a2[2] = -153.0 / 128.0;
+      b2[0] = b2[1] = b2[2] = 1.0;
+      c2[0] = 1.0 / 3.0; c2[1] = 15.0 / 16.0; c2[2] = 8.0 / 15.0;
+    }
+  } else {
+    return -1;
+  }
+  return 0;
+}
+
+/* source/particles/pmlib_particles_advance.f:5-213 with pmlib_particles_map.f:5-260
+ * and the particle pack / unpack of source/communication (one rank):
+ *   vel_rk = a1 vel_rk + b1 dt vel,  dvort_rk = a2 dvort_rk + b2 dt dvort,
+ *   pos += c1 vel_rk,  vort += c2 dvort_rk                                (:95-113)
+ * then per axis x, y, z (:121-175) the map, repeated while a particle is still
+ * outside a periodic side: particles with pos < topo xmin (> = xmax) leave on that
+ * side; on a free side they are dropped, on a periodic side they are wrapped by
+ * the patch length when outside the patch (particles_map.f:107-127).  The new order
+ * is the low-side leavers, the high-side leavers, then the rest, each in the old
+ * order (the order of the communication list, :131-190, and of unpack_part).
+ * For order 1 vel_rk and dvort_rk are zeroed at the end (:198-208).  Arrays
+ * (3, npart) are compacted in place; *npart_out and topo->npart get the new count. */
+int pmo_particles_advance(const pmo_patch *pa, pmo_topo *t, int time_order, int stage, double dtime,
+                          int euler_vort, double *pos, double *vort, const double *vel, const double *dvort,
+                          double *vel_rk, double *dvort_rk, int npart, int *npart_out) {
+  const char *caller = "pmlib_particles_advance";
+  double a1[3], b1[3], c1[3], a2[3], b2[3], c2[3];
+  if (rk_coefficients(time_order, euler_vort, a1, b1, c1, a2, b2, c2)) {
+    /* the message of source/parameters/pmlib_parameters_check.f:90-96 */
+    pm_write("pmlib_parameters_check", "pmlib_interpolation_order is incorrectly set.");
+    return -1;
+  }
+  if (stage < 1 || stage > time_order) {
+    pm_write(caller, "Time stage out of range.");
+    return -1;
+  }
+  const int s = stage - 1;
+  for (int i = 0; i < npart; i++)
+    for (int e = 0; e < 3; e++) {
+      const size_t q = (size_t)3 * i + e;
+      vel_rk[q] = a1[s] * vel_rk[q] + b1[s] * dtime * vel[q];
+      dvort_rk[q] = a2[s] * dvort_rk[q] + b2[s] * dtime * dvort[q];
+      pos[q] = pos[q] + c1[s] * vel_rk[q];
+      vort[q] = vort[q] + c2[s] * dvort_rk[q];
+    }
+  /* map: work on an order of particle indices, gather at the end */
+  int n = npart;
+  int *ord = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  int *nxt = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  unsigned char *side = (unsigned char *)malloc((size_t)(n > 0 ? n : 1));
+  if (!ord || !nxt || !side) { free(ord); free(nxt); free(side); pm_write(caller, "out of memory."); return -1; }
+  for (int i = 0; i < n; i++) ord[i] = i;
+  for (int d = 0; d < 3; d++) {
+    const double xmin = t->xmin[d], xmax = t->xmax[d];
+    const double len = pa->xmax[d] - pa->xmin[d];
+    const int per_lo = t->bound_cond[2 * d] != 0, per_hi = t->bound_cond[2 * d + 1] != 0;
+    int done = 0;
+    for (int iter = 0; !done; iter++) {
+      if (iter >= 1000) {
+        free(ord); free(nxt); free(side);
+        pm_write(caller, "Particle map does not converge.");
+        return -1;
+      }
+      for (int q = 0; q < n; q++) {  /* sides before any wrap (particles_map.f:63-83) */
+        const double x = pos[(size_t)3 * ord[q] + d];
+        side[q] = x < xmin ? 1 : (x >= xmax ? 2 : 0);
+      }
+      int m = 0;
+      for (int pass = 0; pass < 3; pass++)  /* low-side leavers, high-side leavers, the rest */
+        for (int q = 0; q < n; q++) {
+          if (side[q] != (pass == 2 ? 0 : pass + 1)) continue;
+          if (side[q] == 1 && !per_lo) continue;  /* dropped */
+          if (side[q] == 2 && !per_hi) continue;
+          const int i = ord[q];
+          double *x = &pos[(size_t)3 * i + d];
+          if (side[q] == 1 && *x < pa->xmin[d]) *x = *x + len;
+          if (side[q] == 2 && *x >= pa->xmax[d]) *x = *x - len;
+          nxt[m++] = i;
+        }
+      int *tmp = ord; ord = nxt; nxt = tmp;
+      n = m;
+      done = 1;
+      for (int q = 0; q < n; q++) {
+        const double x = pos[(size_t)3 * ord[q] + d];
+        if ((x < xmin && per_lo) || (x >= xmax && per_hi)) done = 0;
+      }
+    }
+  }
+  /* gather in the new order */
+  free(side);
+  double *buf = (double *)malloc(sizeof(double) * 3 * (size_t)(n > 0 ? n : 1));
+  if (!buf) { free(ord); free(nxt); pm_write(caller, "out of memory."); return -1; }
+  double *arr[4] = {pos, vort, vel_rk, dvort_rk};
+  for (int a = 0; a < 4; a++) {
+    for (int q = 0; q < n; q++)
+      for (int e = 0; e < 3; e++) buf[(size_t)3 * q + e] = arr[a][(size_t)3 * ord[q] + e];
+    memcpy(arr[a], buf, sizeof(double) * 3 * (size_t)n);
+  }
+  if (time_order == 1) {
+    memset(vel_rk, 0, sizeof(double) * 3 * (size_t)n);
+    memset(dvort_rk, 0, sizeof(double) * 3 * (size_t)n);
+  }
+  free(buf); free(ord); free(nxt);
+  t->npart = n;
+  *npart_out = n;
+  return 0;
+}

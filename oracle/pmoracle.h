@@ -90,6 +90,18 @@ int pmo_poisson_solve(const pmo_patch *patch, const pmo_topo *cuboid, const pmo_
 int pmo_regularise(const pmo_patch *patch, const pmo_topo *cuboid, double *mesh, int nvar,
                    int reg_order, double filter_width);
 
+/* dvort = visc lap(vort) + (vort . grad) vel on the interior, fd_order 2 or 4, then
+ * the periodic ghost map of dvort (the client's part_deriv_vorticity) */
+int pmo_deriv_vorticity(const pmo_topo *topo, int fd_order, double visc, const double *vort,
+                        const double *vel, double *dvort);
+
+/* pmlib_particles_advance (one rank): RK stage update, then the particle map per
+ * axis (drop across free sides, wrap across periodic ones, reorder); arrays (3, npart)
+ * compacted in place, new count in *npart_out and topo->npart */
+int pmo_particles_advance(const pmo_patch *patch, pmo_topo *topo, int time_order, int stage, double dtime,
+                          int euler_vort, double *pos, double *vort, const double *vel, const double *dvort,
+                          double *vel_rk, double *dvort_rk, int npart, int *npart_out);
+
 /* helper: sine integral used by the order-100 kernel */
 double pmo_si(double x);
 

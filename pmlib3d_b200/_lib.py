@@ -21,6 +21,8 @@ EXPORTS = (
     "pmgpu_interp_particle_mesh_noalloc", "pmgpu_fft_engine", "pmgpu_poisson_solve_dev",
     "pmgpu_batch_create", "pmgpu_batch_solve", "pmgpu_batch_size", "pmgpu_batch_plan", "pmgpu_batch_destroy",
     "pmgpu_fft_tune", "pmgpu_fft_tuned", "pmgpu_particle_diagnostics",
+    "pmgpu_deriv_vorticity", "pmgpu_deriv_vorticity_f32", "pmgpu_deriv_vorticity_dev",
+    "pmgpu_particles_advance", "pmgpu_particles_advance_f32", "pmgpu_particles_advance_dev",
 )
 
 
@@ -94,6 +96,15 @@ def lib():
         "pmgpu_fft_tune": [C.c_int],
         "pmgpu_fft_tuned": [C.c_int, ip, ip, ip, ip, ip, dp],
         "pmgpu_particle_diagnostics": [dp, vp, vp, vp, C.c_int, C.c_int, dp, vp],
+        "pmgpu_deriv_vorticity": [TP, C.c_int, C.c_double, dp, dp, dp],
+        "pmgpu_deriv_vorticity_f32": [TP, C.c_int, C.c_double, fp, fp, fp],
+        "pmgpu_deriv_vorticity_dev": [TP, C.c_int, C.c_double, C.c_int, vp, vp, vp, vp],
+        "pmgpu_particles_advance": [PP, TP, C.c_int, C.c_int, C.c_double, C.c_int, dp, dp, dp, dp, dp, dp,
+                                    C.c_int, ip],
+        "pmgpu_particles_advance_f32": [PP, TP, C.c_int, C.c_int, C.c_double, C.c_int, fp, fp, fp, fp, fp, fp,
+                                        C.c_int, ip],
+        "pmgpu_particles_advance_dev": [PP, TP, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, vp, vp, vp, vp,
+                                        vp, vp, C.c_int, ip, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

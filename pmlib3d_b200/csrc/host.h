@@ -14,7 +14,7 @@
 namespace pmgpu {
 
 enum KClass { KC_BIN, KC_SCAN, KC_PLACE, KC_FIXUP, KC_DEPOSIT, KC_GADD, KC_XFWD, KC_YFWD, KC_ZPASS, KC_YINV,
-              KC_XINV, KC_GFILL, KC_M2P, KC_OTHER, KC_N };
+              KC_XINV, KC_GFILL, KC_M2P, KC_DERIV, KC_ADVANCE, KC_MAP, KC_OTHER, KC_N };
 
 // brackets one launch with CUDA events on its stream while timing is enabled
 struct KTimer {

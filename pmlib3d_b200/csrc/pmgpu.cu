@@ -9,6 +9,7 @@
 #include "green.cuh"
 #include "host.h"
 #include "particles.cuh"
+#include "advance.cuh"
 #include "solve.cuh"
 
 #include <algorithm>
@@ -31,7 +32,8 @@ long long g_launches = 0;
 // When enabled, every launch of the library is bracketed by CUDA events on its
 // stream; pmgpu_timing_get sums the elapsed times per kernel class.
 static const char *kc_names[KC_N] = {"bin", "scan", "place", "fixup", "deposit", "ghost_add",
-                                     "x_fwd", "y_fwd", "z_pass", "y_inv", "x_inv", "ghost_fill", "m2p", "other"};
+                                     "x_fwd", "y_fwd", "z_pass", "y_inv", "x_inv", "ghost_fill", "m2p",
+                                     "deriv_vorticity", "advance", "map", "other"};
 static bool g_timing = false;
 struct PendingEv {
   int cls;
@@ -483,6 +485,7 @@ struct Scratch {
   DevBuf key, val, key2, val2, counts, start, spart, hist;
   DevBuf a, b, c, d, e, f, g, h;
   DevBuf diag;  // diagnostics partial sums
+  DevBuf adv_code, adv_stats, adv_cnt, adv_start, adv_ord, adv_tmp;  // particle advance and map
 };
 static Scratch &scratch() {
   static Scratch s;
@@ -1998,4 +2001,301 @@ int pmgpu_particle_diagnostics(const double dx[3], const void *d_pos, const void
     for (int i = 9; i < 13; i++) out[i] = h[i] / h[7];  // centroid and ring radius (diagnostics_knot.f:171-175)
   }
   return 0;
+}
+
+// ------------------------------------------------------------------ particle step around the solve
+// dvort = visc lap(vort) + (vort . grad) vel on the interior, then the periodic ghost
+// map (the client's part_deriv_vorticity, vortex_structures/source/particle_derivatives/
+// part_deriv_vorticity.f:57-206) on device meshes (3, nx', ny', nz')
+template <typename R>
+static int run_deriv_vorticity(const pmgpu_topo *t, int fd_order, double visc, const R *vort, const R *vel, R *dvort,
+                               cudaStream_t st, const char *caller) {
+  if (fd_order != 2 && fd_order != 4) {
+    set_error("pmlib_parameters_check", "pmlib_fd_order is incorrectly set.");
+    return -1;
+  }
+  DerivGeom<R> g;
+  for (int e = 0; e < 3; e++) {
+    g.ext[e] = t->ncell[e] + t->nghost[2 * e] + t->nghost[2 * e + 1];
+    g.ngl[e] = t->nghost[2 * e];
+    g.nc[e] = t->ncell[e];
+    if (t->nghost[2 * e] < fd_order / 2 || t->nghost[2 * e + 1] < fd_order / 2) {
+      set_error(caller, "Too few ghost cells for the finite differences.");
+      return -1;
+    }
+    g.c_1_dx2[e] = R(1) / ((R)t->dx[e] * (R)t->dx[e]);
+    g.c_1_2dx[e] = R(1) / (R(2) * (R)t->dx[e]);
+  }
+  g.visc = (R)visc;
+  if (g.nc[0] > 0 && g.nc[1] > 0 && g.nc[2] > 0) {
+    const dim3 blk(32, 8), grid((g.nc[0] + 31) / 32, (g.nc[1] + 7) / 8, g.nc[2]);
+    KTimer kt_(KC_DERIV, st);
+    if (fd_order == 2) k_deriv_vorticity<R, 2><<<grid, blk, 0, st>>>(g, vort, vel, dvort);
+    else k_deriv_vorticity<R, 4><<<grid, blk, 0, st>>>(g, vort, vel, dvort);
+    PM_LAUNCHED();
+    CKL(caller);
+  }
+  for (int d = 0; d < 3; d++) {
+    if (t->bound_cond[2 * d] == 0 || t->bound_cond[2 * d + 1] == 0) continue;
+    const int S = t->nghost[2 * d] + t->nghost[2 * d + 1];
+    const long long total = (long long)S * g.ext[(d + 1) % 3] * g.ext[(d + 2) % 3];
+    const int nblk = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+    { KTimer kt_(KC_GFILL, st); k_ghost_fill<R><<<std::max(nblk, 1), 256, 0, st>>>(dvort, g.ext[0], g.ext[1], g.ext[2], 3, d,
+                                                                                    t->ncell[d], t->nghost[2 * d],
+                                                                                    t->nghost[2 * d + 1]); }
+    PM_LAUNCHED();
+    CKL(caller);
+  }
+  return 0;
+}
+
+// Runge-Kutta coefficients of source/particles/pmlib_particles_advance.f:49-88 in the
+// working precision (the reference forms them as REAL(MK) constants)
+template <typename R> static int rk_coef(int order, int stage, int euler, R &a1, R &b1, R &c1, R &a2, R &b2, R &c2) {
+  const R z = R(0), o = R(1), h = R(0.5);
+  R A1[3] = {z, z, z}, B1[3] = {z, z, z}, C1[3] = {z, z, z}, A2[3] = {z, z, z}, B2[3] = {z, z, z}, C2[3] = {z, z, z};
+  if (order == 1) {
+    B1[0] = C1[0] = B2[0] = C2[0] = o;
+  } else if (order == 2) {
+    A1[1] = -h; B1[0] = B1[1] = o; C1[0] = h; C1[1] = o;
+    if (euler) { A2[1] = o; B2[0] = o; C2[0] = h; C2[1] = h; }
+    else { A2[1] = -h; B2[0] = B2[1] = o; C2[0] = h; C2[1] = o; }
+  } else if (order == 3) {
+    A1[1] = R(-5) / R(9); A1[2] = R(-153) / R(128);
+    B1[0] = B1[1] = B1[2] = o;
+    C1[0] = R(1) / R(3); C1[1] = R(15) / R(16); C1[2] = R(8) / R(15);
+    if (euler) { A2[1] = A2[2] = o; B2[0] = o; C2[0] = C2[1] = C2[2] = R(1) / R(3); }
+    else {
+      A2[1] = R(-5) / R(9); A2[2] = R(-153) / R(128);
+      B2[0] = B2[1] = B2[2] = o;
+      C2[0] = R(1) / R(3); C2[1] = R(15) / R(16); C2[2] = R(8) / R(15);
+    }
+  } else {
+    return -1;
+  }
+  if (stage < 1 || stage > order) return -2;
+  a1 = A1[stage - 1]; b1 = B1[stage - 1]; c1 = C1[stage - 1];
+  a2 = A2[stage - 1]; b2 = B2[stage - 1]; c2 = C2[stage - 1];
+  return 0;
+}
+
+// pmlib_particles_advance (source/particles/pmlib_particles_advance.f:5-213, one rank)
+// on device arrays (3, npart): stage update in place, then the map as one stable
+// bucket sort of the survivors (arrays compacted in place).  Waits for the stream:
+// the new count is needed on the host.
+template <typename R>
+static int run_advance(const pmgpu_patch *pa, pmgpu_topo *t, int order, int stage, double dtime, int euler, R *pos,
+                       R *vort, const R *vel, const R *dvort, R *vel_rk, R *dvort_rk, int n, int *nout,
+                       cudaStream_t st, const char *caller) {
+  AdvanceCoef<R> c;
+  memset(&c, 0, sizeof(c));
+  R b1, b2;
+  const int rc = rk_coef<R>(order, stage, euler, c.a1, b1, c.c1, c.a2, b2, c.c2);
+  if (rc == -1) {
+    // the message of source/parameters/pmlib_parameters_check.f:90-96
+    set_error("pmlib_parameters_check", "pmlib_interpolation_order is incorrectly set.");
+    return -1;
+  }
+  if (rc == -2) {
+    set_error(caller, "Time stage out of range.");
+    return -1;
+  }
+  if (n < 0 || (n > 0 && (!pos || !vort || !vel || !dvort || !vel_rk || !dvort_rk))) {
+    set_error(caller, "missing argument.");
+    return -1;
+  }
+  c.b1dt = b1 * (R)dtime;
+  c.b2dt = b2 * (R)dtime;
+  c.zero_rk = order == 1;
+  for (int e = 0; e < 3; e++) {
+    c.xmin[e] = (R)t->xmin[e];
+    c.xmax[e] = (R)t->xmax[e];
+    c.pmin[e] = (R)pa->xmin[e];
+    c.pmax[e] = (R)pa->xmax[e];
+    c.plen[e] = (R)pa->xmax[e] - (R)pa->xmin[e];
+    c.per_lo[e] = t->bound_cond[2 * e] != 0;
+    c.per_hi[e] = t->bound_cond[2 * e + 1] != 0;
+  }
+  *nout = n;
+  if (n == 0) {
+    t->npart = 0;
+    return 0;
+  }
+  Scratch &s = scratch();
+  if (s.adv_code.ensure(sizeof(unsigned) * (size_t)n, caller) || s.adv_stats.ensure(sizeof(unsigned) * 8, caller))
+    return -1;
+  unsigned *stats = s.adv_stats.as<unsigned>();
+  CK(cudaMemsetAsync(stats, 0, sizeof(unsigned) * 8, st), caller);
+  const int nblk = std::min((n + 255) / 256, 148 * 16);
+  { KTimer kt_(KC_ADVANCE, st); k_advance<R><<<nblk, 256, 0, st>>>(c, n, pos, vort, vel, dvort, vel_rk, dvort_rk,
+                                                                   s.adv_code.as<unsigned>(), stats); }
+  PM_LAUNCHED();
+  CKL(caller);
+  unsigned h[8];
+  CK(cudaMemcpyAsync(h, stats, sizeof(h), cudaMemcpyDeviceToHost, st), caller);
+  CK(cudaStreamSynchronize(st), caller);
+  if (h[4]) {
+    set_error(caller, "A particle moved more than one patch length in one step.");
+    return -1;
+  }
+  if (!h[0]) {  // nobody left or was dropped: the order stays
+    t->npart = n;
+    return 0;
+  }
+  const int K0 = (int)h[1], K1 = (int)h[2], K2 = (int)h[3];
+  unsigned nbk = 1;
+  for (int k : {K0, K1, K2})
+    for (int i = 0; i < k; i++) nbk *= 3u;
+  const int nb = (n + MAP_CHUNK - 1) / MAP_CHUNK;
+  const size_t ncnt = (size_t)(nbk + 1) * nb;
+  if (s.adv_cnt.ensure(sizeof(unsigned) * (ncnt + 1), caller) ||
+      s.adv_start.ensure(sizeof(unsigned) * (ncnt + 1), caller) || s.adv_ord.ensure(sizeof(int) * (size_t)n, caller) ||
+      s.adv_tmp.ensure(sizeof(R) * 3 * (size_t)n, caller))
+    return -1;
+  { KTimer kt_(KC_MAP, st); k_map_count<<<nb, MAP_THREADS, 0, st>>>(s.adv_code.as<unsigned>(), n, K0, K1, K2, nbk,
+                                                                    s.adv_cnt.as<unsigned>()); }
+  PM_LAUNCHED();
+  CKL(caller);
+  if (exclusive_scan(s.adv_cnt.as<unsigned>(), s.adv_start.as<unsigned>(), ncnt, s.spart, st, caller)) return -1;
+  { KTimer kt_(KC_MAP, st); k_map_scatter<<<nb, MAP_THREADS, 0, st>>>(s.adv_code.as<unsigned>(), n, K0, K1, K2, nbk,
+                                                                      s.adv_start.as<unsigned>(),
+                                                                      s.adv_ord.as<int>()); }
+  PM_LAUNCHED();
+  CKL(caller);
+  unsigned live = 0;  // first slot of the dropped bucket = survivors
+  CK(cudaMemcpyAsync(&live, s.adv_start.as<unsigned>() + (size_t)nbk * nb, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                     st), caller);
+  CK(cudaStreamSynchronize(st), caller);
+  const int m = (int)live;
+  R *arrs[4] = {pos, vort, vel_rk, dvort_rk};
+  for (R *a : arrs) {
+    if (m > 0) {
+      { KTimer kt_(KC_MAP, st); k_gather3<R><<<std::min((m + 255) / 256, 148 * 16), 256, 0, st>>>(
+          s.adv_ord.as<int>(), m, a, s.adv_tmp.as<R>()); }
+      PM_LAUNCHED();
+      CK(cudaMemcpyAsync(a, s.adv_tmp.p, sizeof(R) * 3 * (size_t)m, cudaMemcpyDeviceToDevice, st), caller);
+    }
+  }
+  CKL(caller);
+  CK(cudaStreamSynchronize(st), caller);
+  *nout = m;
+  t->npart = m;
+  return 0;
+}
+
+template <typename R>
+static int deriv_host(const pmgpu_topo *t, int fd_order, double visc, const R *vort, const R *vel, R *dvort) {
+  const char *caller = "part_deriv_vorticity";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!t || !vort || !vel || !dvort) {
+    set_error(caller, "missing argument.");
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  Scratch &s = scratch();
+  const size_t nm = mesh_points(t) * 3;
+  if (s.c.ensure(sizeof(R) * nm, caller) || s.d.ensure(sizeof(R) * nm, caller) || s.e.ensure(sizeof(R) * nm, caller))
+    return -1;
+  CK(cudaMemcpy(s.c.p, vort, sizeof(R) * nm, cudaMemcpyHostToDevice), caller);
+  CK(cudaMemcpy(s.d.p, vel, sizeof(R) * nm, cudaMemcpyHostToDevice), caller);
+  CK(cudaMemcpy(s.e.p, dvort, sizeof(R) * nm, cudaMemcpyHostToDevice), caller);  // free-axis ghosts are kept
+  if (run_deriv_vorticity<R>(t, fd_order, visc, s.c.as<R>(), s.d.as<R>(), s.e.as<R>(), 0, caller)) return -1;
+  CK(cudaMemcpy(dvort, s.e.p, sizeof(R) * nm, cudaMemcpyDeviceToHost), caller);
+  return 0;
+}
+
+int pmgpu_deriv_vorticity(const pmgpu_topo *topo, int fd_order, double visc, const double *mesh_vort,
+                          const double *mesh_vel, double *mesh_dvort) {
+  return deriv_host<double>(topo, fd_order, visc, mesh_vort, mesh_vel, mesh_dvort);
+}
+int pmgpu_deriv_vorticity_f32(const pmgpu_topo *topo, int fd_order, double visc, const float *mesh_vort,
+                              const float *mesh_vel, float *mesh_dvort) {
+  return deriv_host<float>(topo, fd_order, visc, mesh_vort, mesh_vel, mesh_dvort);
+}
+int pmgpu_deriv_vorticity_dev(const pmgpu_topo *topo, int fd_order, double visc, int precision, const void *d_vort,
+                              const void *d_vel, void *d_dvort, void *stream) {
+  const char *caller = "part_deriv_vorticity";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!topo || !d_vort || !d_vel || !d_dvort) {
+    set_error(caller, "missing argument.");
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (precision == PMGPU_FP64)
+    return run_deriv_vorticity<double>(topo, fd_order, visc, (const double *)d_vort, (const double *)d_vel,
+                                       (double *)d_dvort, st, caller);
+  if (precision == PMGPU_FP32)
+    return run_deriv_vorticity<float>(topo, fd_order, visc, (const float *)d_vort, (const float *)d_vel,
+                                      (float *)d_dvort, st, caller);
+  set_error(caller, "precision unknown.");
+  return -1;
+}
+
+template <typename R>
+static int advance_host(const pmgpu_patch *pa, pmgpu_topo *t, int order, int stage, double dtime, int euler, R *pos,
+                        R *vort, const R *vel, const R *dvort, R *vel_rk, R *dvort_rk, int npart, int *nout) {
+  const char *caller = "pmlib_particles_advance";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!pa || !t || !nout || npart < 0) {
+    set_error(caller, "missing argument.");
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  Scratch &s = scratch();
+  const size_t b = sizeof(R) * 3 * (size_t)std::max(npart, 1);
+  DevBuf *bufs[6] = {&s.c, &s.d, &s.e, &s.f, &s.g, &s.h};
+  for (DevBuf *d : bufs)
+    if (d->ensure(b, caller)) return -1;
+  const R *src[6] = {pos, vort, vel, dvort, vel_rk, dvort_rk};
+  for (int i = 0; i < 6; i++)
+    if (npart > 0 && src[i]) CK(cudaMemcpy(bufs[i]->p, src[i], sizeof(R) * 3 * (size_t)npart, cudaMemcpyHostToDevice), caller);
+  if (npart > 0 && (!pos || !vort || !vel || !dvort || !vel_rk || !dvort_rk)) {
+    set_error(caller, "missing argument.");
+    return -1;
+  }
+  if (run_advance<R>(pa, t, order, stage, dtime, euler, s.c.as<R>(), s.d.as<R>(), s.e.as<R>(), s.f.as<R>(),
+                     s.g.as<R>(), s.h.as<R>(), npart, nout, 0, caller))
+    return -1;
+  R *dst[4] = {pos, vort, vel_rk, dvort_rk};
+  DevBuf *from[4] = {&s.c, &s.d, &s.g, &s.h};
+  for (int i = 0; i < 4; i++)
+    if (*nout > 0) CK(cudaMemcpy(dst[i], from[i]->p, sizeof(R) * 3 * (size_t)*nout, cudaMemcpyDeviceToHost), caller);
+  return 0;
+}
+
+int pmgpu_particles_advance(const pmgpu_patch *patch, pmgpu_topo *topo, int time_order, int itimestage,
+                            double dtime, int euler_vort, double *pos, double *vort, const double *vel,
+                            const double *dvort, double *vel_rk, double *dvort_rk, int npart, int *npart_out) {
+  return advance_host<double>(patch, topo, time_order, itimestage, dtime, euler_vort, pos, vort, vel, dvort, vel_rk,
+                              dvort_rk, npart, npart_out);
+}
+int pmgpu_particles_advance_f32(const pmgpu_patch *patch, pmgpu_topo *topo, int time_order, int itimestage,
+                                double dtime, int euler_vort, float *pos, float *vort, const float *vel,
+                                const float *dvort, float *vel_rk, float *dvort_rk, int npart, int *npart_out) {
+  return advance_host<float>(patch, topo, time_order, itimestage, dtime, euler_vort, pos, vort, vel, dvort, vel_rk,
+                             dvort_rk, npart, npart_out);
+}
+int pmgpu_particles_advance_dev(const pmgpu_patch *patch, pmgpu_topo *topo, int time_order, int itimestage,
+                                double dtime, int euler_vort, int precision, void *d_pos, void *d_vort,
+                                const void *d_vel, const void *d_dvort, void *d_vel_rk, void *d_dvort_rk, int npart,
+                                int *npart_out, void *stream) {
+  const char *caller = "pmlib_particles_advance";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!patch || !topo || !npart_out) {
+    set_error(caller, "missing argument.");
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (precision == PMGPU_FP64)
+    return run_advance<double>(patch, topo, time_order, itimestage, dtime, euler_vort, (double *)d_pos,
+                               (double *)d_vort, (const double *)d_vel, (const double *)d_dvort, (double *)d_vel_rk,
+                               (double *)d_dvort_rk, npart, npart_out, st, caller);
+  if (precision == PMGPU_FP32)
+    return run_advance<float>(patch, topo, time_order, itimestage, dtime, euler_vort, (float *)d_pos,
+                              (float *)d_vort, (const float *)d_vel, (const float *)d_dvort, (float *)d_vel_rk,
+                              (float *)d_dvort_rk, npart, npart_out, st, caller);
+  set_error(caller, "precision unknown.");
+  return -1;
 }

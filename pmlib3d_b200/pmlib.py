@@ -310,3 +310,49 @@ def step_dev(plan: Plan, d_pos: int, d_part_vort: int, npart: int, d_part_vel: i
     """The same step on device pointers (e.g. ``tensor.data_ptr()``) on a CUDA stream."""
     return lib().pmgpu_step_dev(plan.handle, C.c_void_p(d_pos), C.c_void_p(d_part_vort), int(npart),
                                 C.c_void_p(d_part_vel), C.c_void_p(stream))
+
+
+def part_deriv_vorticity(topo: Topo, fd_order: int, visc: float, vort, vel, dvort) -> int:
+    """The vorticity right-hand side dvort = visc lap(vort) + (vort . grad) vel
+    (vortex_structures/source/particle_derivatives/part_deriv_vorticity.f:5-213):
+    dvort (a mesh like vort, FP64 or FP32) is written on the interior and the periodic
+    ghosts."""
+    dt = vort.dtype.type
+    f = lib().pmgpu_deriv_vorticity if dt == np.float64 else lib().pmgpu_deriv_vorticity_f32
+    return f(C.byref(topo), int(fd_order), float(visc), _ptr(vort, dt), _ptr(vel, dt), _ptr(dvort, dt))
+
+
+def part_deriv_vorticity_dev(topo: Topo, fd_order: int, visc: float, precision: int, d_vort: int, d_vel: int,
+                             d_dvort: int, stream: int = 0) -> int:
+    """part_deriv_vorticity on device meshes, queued on ``stream``."""
+    return lib().pmgpu_deriv_vorticity_dev(C.byref(topo), int(fd_order), float(visc), int(precision),
+                                           C.c_void_p(d_vort), C.c_void_p(d_vel), C.c_void_p(d_dvort),
+                                           C.c_void_p(stream or None))
+
+
+def pmlib_particles_advance(patch: Patch, topo: Topo, time_order: int, itimestage: int, dtime: float, pos, vort,
+                            vel, dvort, vel_rk, dvort_rk, euler_vort: bool = False):
+    """source/particles/pmlib_particles_advance.f:5-213 (one rank): RK stage update and
+    particle map.  pos, vort, vel_rk, dvort_rk ((np, 3), FP64 or FP32) are updated and
+    compacted in place; returns (ierr, npart) with the survivors in the first npart
+    rows.  topo.npart is updated."""
+    dt = pos.dtype.type
+    f = lib().pmgpu_particles_advance if dt == np.float64 else lib().pmgpu_particles_advance_f32
+    n = C.c_int(0)
+    ierr = f(C.byref(patch), C.byref(topo), int(time_order), int(itimestage), float(dtime), int(bool(euler_vort)),
+             _ptr(pos, dt), _ptr(vort, dt), _ptr(vel, dt), _ptr(dvort, dt), _ptr(vel_rk, dt), _ptr(dvort_rk, dt),
+             int(pos.shape[0]), C.byref(n))
+    return ierr, n.value
+
+
+def pmlib_particles_advance_dev(patch: Patch, topo: Topo, time_order: int, itimestage: int, dtime: float,
+                                precision: int, d_pos: int, d_vort: int, d_vel: int, d_dvort: int, d_vel_rk: int,
+                                d_dvort_rk: int, npart: int, euler_vort: bool = False, stream: int = 0):
+    """pmlib_particles_advance on device arrays; returns (ierr, npart)."""
+    n = C.c_int(0)
+    ierr = lib().pmgpu_particles_advance_dev(C.byref(patch), C.byref(topo), int(time_order), int(itimestage),
+                                             float(dtime), int(bool(euler_vort)), int(precision), C.c_void_p(d_pos),
+                                             C.c_void_p(d_vort), C.c_void_p(d_vel), C.c_void_p(d_dvort),
+                                             C.c_void_p(d_vel_rk), C.c_void_p(d_dvort_rk), int(npart), C.byref(n),
+                                             C.c_void_p(stream or None))
+    return ierr, n.value

@@ -1,0 +1,164 @@
+"""GPU parity of the particle step around the solve: the vorticity right-hand side
+on the mesh and the Runge-Kutta stage update with the particle map, against the
+oracle on the same seeded inputs.  FP64: the stage update and map are
+bit-identical (unfused arithmetic in the reference's order, same particle order and
+count); the right-hand side to rel-L2 1e-12.  FP32: rel-L2 1e-5 (right-hand side)
+and 1e-6 (positions), with the same order and count."""
+import copy
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from pmlib3d_b200 import pmlib as P
+from tests.helpers import rel_l2, setup_pair
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    ("fff", (-1, -1, -1), (1, 1, 1), (0.125,) * 3, (0, 0, 0), 4),
+    ("ppf", (-1, -1, -0.5), (1, 1, 0.5), (0.125, 0.125, 0.0625), (1, 1, 0), 4),
+    ("pff", (0, -1, -1), (2, 1, 1), (0.125, 0.1, 0.125), (1, 0, 0), 3),
+    ("ppp", (0, 0, 0), (1, 1, 2), (1 / 16, 1 / 16, 1 / 16), (1, 1, 1), 4),
+]
+
+
+def _fields(t, seed):
+    rng = np.random.default_rng(seed)
+    shape = O.topo_shape(t, 3)
+    ext = [t.ncell[d] + t.nghost[2 * d] + t.nghost[2 * d + 1] for d in range(3)]
+    ax = [t.xmin[d] + (np.arange(ext[d]) - t.nghost[2 * d] + 0.5) * t.dx[d] for d in range(3)]
+    z, y, x = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+    g = np.exp(-(x ** 2 + y ** 2 + z ** 2))
+    vort = np.stack([g * np.sin(3 * y), g * np.cos(2 * z), g * x], -1) + 0.01 * rng.standard_normal(shape)
+    vel = np.stack([g * y, -g * x, g * np.sin(z)], -1) + 0.01 * rng.standard_normal(shape)
+    dvort = rng.standard_normal(shape)  # ghosts on free axes must come back unchanged
+    return [np.ascontiguousarray(a) for a in (vort, vel, dvort)]
+
+
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", CASES)
+@pytest.mark.parametrize("fd", [2, 4])
+def test_deriv_vorticity_fp64(name, xmin, xmax, dx, bc, ng, fd):
+    _, to, _, _, tg, _ = setup_pair(xmin, xmax, dx, bc, ng)
+    vort, vel, dvort = _fields(to, 1)
+    d_o = dvort.copy()
+    assert O.deriv_vorticity(to, fd, 0.003, vort, vel, d_o) == 0
+    d_g = dvort.copy()
+    assert P.part_deriv_vorticity(tg, fd, 0.003, vort, vel, d_g) == 0, P.last_error()
+    assert rel_l2(d_g, d_o) < 1e-12, rel_l2(d_g, d_o)
+
+
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", [CASES[0], CASES[1]])
+def test_deriv_vorticity_fp32(name, xmin, xmax, dx, bc, ng):
+    _, to, _, _, tg, _ = setup_pair(xmin, xmax, dx, bc, ng)
+    vort, vel, dvort = _fields(to, 2)
+    d_o = dvort.copy()
+    assert O.deriv_vorticity(to, 4, 0.003, vort, vel, d_o) == 0
+    d_g = dvort.astype(np.float32)
+    assert P.part_deriv_vorticity(tg, 4, 0.003, vort.astype(np.float32), vel.astype(np.float32), d_g) == 0
+    assert rel_l2(d_g, d_o) < 1e-5, rel_l2(d_g, d_o)
+
+
+def test_deriv_vorticity_errors(capfd):
+    _, to, _, _, tg, _ = setup_pair(*CASES[0][1:])
+    vort, vel, dvort = _fields(to, 3)
+    assert P.part_deriv_vorticity(tg, 3, 0.0, vort, vel, dvort) == -1
+    assert "pmlib_fd_order is incorrectly set." in capfd.readouterr().out
+
+
+def _particles(t, n, seed, spill=0.15, speed=0.05, far=0, dtype=np.float64):
+    """Particles over the cuboid and a margin of `spill` patch lengths around it, so
+    that some leave across every face; `far` of them two patch lengths out."""
+    rng = np.random.default_rng(seed)
+    lo = np.array(t.xmin)
+    L = np.array(t.xmax) - lo
+    pos = lo + L * rng.uniform(-spill, 1 + spill, (n, 3))
+    if far:
+        pos[:far] = lo + L * rng.uniform(-1.6, -1.1, (far, 3))
+    vort = rng.standard_normal((n, 3))
+    vel = speed * rng.standard_normal((n, 3))
+    dv = rng.standard_normal((n, 3))
+    vr = 0.1 * rng.standard_normal((n, 3))
+    dr = 0.1 * rng.standard_normal((n, 3))
+    return [np.ascontiguousarray(a.astype(dtype)) for a in (pos, vort, vel, dv, vr, dr)]
+
+
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", CASES)
+@pytest.mark.parametrize("order,stage,euler", [(1, 1, False), (2, 2, False), (2, 2, True), (3, 1, False),
+                                               (3, 3, False), (3, 2, True)])
+def test_particles_advance_fp64(name, xmin, xmax, dx, bc, ng, order, stage, euler):
+    po, to, _, pg, tg, _ = setup_pair(xmin, xmax, dx, bc, ng)
+    arrs = _particles(to, 20000, seed=order * 10 + stage, far=40 if bc[0] else 0)
+    ao = [a.copy() for a in arrs]
+    ag = [a.copy() for a in arrs]
+    ierr, mo = O.particles_advance(po, to, order, stage, 0.05, ao[0], ao[1], ao[2], ao[3], ao[4], ao[5],
+                                   euler_vort=euler)
+    assert ierr == 0
+    ierr, mg = P.pmlib_particles_advance(pg, tg, order, stage, 0.05, ag[0], ag[1], ag[2], ag[3], ag[4], ag[5],
+                                         euler_vort=euler)
+    assert ierr == 0, P.last_error()
+    assert mg == mo and tg.npart == mo
+    for i in (0, 1, 4, 5):  # pos, vort, vel_rk, dvort_rk: same values in the same order
+        assert np.array_equal(ag[i][:mg], ao[i][:mo]), i
+
+
+def test_particles_advance_nothing_leaves():
+    """All particles stay inside: the order is kept (no map work on the GPU)."""
+    po, to, _, pg, tg, _ = setup_pair(*CASES[0][1:])
+    arrs = _particles(to, 5000, seed=7, spill=-0.2, speed=0.001)
+    ao = [a.copy() for a in arrs]
+    ag = [a.copy() for a in arrs]
+    _, mo = O.particles_advance(po, to, 3, 2, 0.01, *ao)
+    ierr, mg = P.pmlib_particles_advance(pg, tg, 3, 2, 0.01, *ag)
+    assert ierr == 0 and mg == mo == 5000
+    for i in (0, 1, 4, 5):
+        assert np.array_equal(ag[i], ao[i])
+
+
+def test_particles_advance_fp32():
+    po, to, _, pg, tg, _ = setup_pair(*CASES[1][1:])
+    arrs = _particles(to, 20000, seed=11)
+    # keep FP32 rounding away from the faces: drop particles whose advanced FP64
+    # position lies within 1e-5 of a face
+    probe = [a.copy() for a in arrs]
+    vr = probe[4] * 0.0 + probe[2] * 0.05  # stage 1 of order 1: vel_rk = dt vel
+    x = probe[0] + vr
+    near = np.zeros(len(x), bool)
+    for d in range(3):
+        for f in (to.xmin[d], to.xmax[d]):
+            near |= np.abs(x[:, d] - f) < 1e-5
+    arrs = [np.ascontiguousarray(a[~near]) for a in arrs]
+    ao = [a.copy() for a in arrs]
+    ag = [a.astype(np.float32) for a in arrs]
+    _, mo = O.particles_advance(po, to, 1, 1, 0.05, *ao)
+    ierr, mg = P.pmlib_particles_advance(pg, tg, 1, 1, 0.05, *ag)
+    assert ierr == 0 and mg == mo
+    assert rel_l2(ag[0][:mg], ao[0][:mo]) < 1e-6
+    assert rel_l2(ag[1][:mg], ao[1][:mo]) < 1e-6
+    assert np.all(ag[4][:mg] == 0) and np.all(ag[5][:mg] == 0)  # first order clears the stage storage
+
+
+def test_particles_advance_dev_matches_host():
+    import torch
+    po, to, _, pg, tg, _ = setup_pair(*CASES[3][1:])
+    arrs = _particles(to, 30000, seed=5)
+    ah = [a.copy() for a in arrs]
+    th = copy.deepcopy(tg)
+    ierr, mh = P.pmlib_particles_advance(pg, th, 2, 1, 0.05, *ah)
+    assert ierr == 0
+    d = [torch.from_numpy(a).cuda() for a in arrs]
+    ierr, md = P.pmlib_particles_advance_dev(pg, tg, 2, 1, 0.05, P.FP64, *(t.data_ptr() for t in d), len(arrs[0]))
+    assert ierr == 0 and md == mh
+    for i in (0, 1, 4, 5):
+        assert np.array_equal(d[i][:md].cpu().numpy(), ah[i][:mh])
+
+
+def test_particles_advance_errors(capfd):
+    po, to, _, pg, tg, _ = setup_pair(*CASES[3][1:])
+    arrs = _particles(to, 100, seed=3)
+    assert P.pmlib_particles_advance(pg, tg, 4, 1, 0.1, *[a.copy() for a in arrs])[0] == -1
+    assert "pmlib_interpolation_order is incorrectly set." in capfd.readouterr().out
+    assert P.pmlib_particles_advance(pg, tg, 2, 3, 0.1, *[a.copy() for a in arrs])[0] == -1
+    far = [a.copy() for a in arrs]
+    far[0][0] = np.array(to.xmin) - 3.5 * (np.array(to.xmax) - np.array(to.xmin))  # three wraps needed
+    assert P.pmlib_particles_advance(pg, tg, 1, 1, 0.0, *far)[0] == -1
