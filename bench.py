@@ -241,6 +241,7 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"],
                     help="precision of --mode profile")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched and served measurements")
+    ap.add_argument("--no-stage", action="store_true", help="skip the full vortex-stage measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -401,6 +402,42 @@ def main():
         e2e = {"value": world * ke / dt, "unit": "steps/s", "h2d_bytes_per_step": 24 * n,
                "d2h_bytes_per_step": 12 * n, "api": "pmgpu_step (host pointers, pinned)"}
 
+    # ---- one full stage of the vortex client's RK3 step (P2M, solve, right-hand side,
+    # M2P of velocity and right-hand side, stage update with the particle map)
+    stage = None
+    if not args.no_stage:
+        sp, sv = pos32.clone(), vort32.clone()
+        srk, sdrk = torch.zeros_like(sp), torch.zeros_like(sp)
+        su, sdw = torch.empty_like(sp), torch.empty_like(sp)
+        h = float(w.dx[0])
+        dt_stage = 0.05 * h / max(float(vel32.abs().max().item()), 1e-30)  # CFL 0.05 on the last velocity
+        live = [n]
+
+        def one_stage(i):
+            rc, m = P.vortex_stage_dev(plan32, 3, 1 + i % 3, dt_stage, 4, 1e-4, sp.data_ptr(), sv.data_ptr(),
+                                       srk.data_ptr(), sdrk.data_ptr(), live[0], su.data_ptr(), sdw.data_ptr(),
+                                       stream=sptr)
+            if rc != 0:
+                raise RuntimeError(P.last_error())
+            live[0] = m
+
+        for i in range(args.warmup):
+            one_stage(i)
+        torch.cuda.synchronize()
+        barrier()
+        ks = 3 * max(1, args.steps // 6)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(ks):
+            one_stage(i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sms = max_over_ranks(e0.elapsed_time(e1)) / ks
+        stage = {"value": world * 1000.0 / sms, "unit": "stages/s", "ms_per_stage": sms, "stages": ks,
+                 "particles_after": live[0],
+                 "scheme": "low-storage RK3 (stages 1-3 in turn), fd_order 4, visc 1e-4, CFL 0.05",
+                 "api": "pmgpu_vortex_stage_dev (device arrays; the map's particle count comes back to the host)"}
+
     # ---- batched uneven patches (every rank: replicas) and the served stream (rank 0)
     batched = served = None
     if not args.no_batched:
@@ -436,6 +473,7 @@ def main():
             "accuracy": {"rel_l2_fp32_vs_fp64": rel_l2, "max_rel_err": max_err},
             "roofline": roofline, "kernels": kernels, "gpu_launches": launches32,
             "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "batched": batched, "served": served,
+            "vortex_stage": stage,
         }
         print(json.dumps(line), flush=True)
     for p in (plan32, plan64):

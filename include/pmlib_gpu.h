@@ -266,6 +266,18 @@ int pmgpu_particles_advance_dev(const pmgpu_patch *patch, pmgpu_topo *topo, int 
                                 void *d_vel_rk, void *d_dvort_rk, int npart, int *npart_out,
                                 void *stream);
 
+/* One stage of the vortex client's time step (vortex_codes/vortex_structures/source/
+ * main.f:396-510 without remeshing and diagnostics), from the pieces above on the
+ * plan's grid: P2M of the particle vorticity, the solve, the vorticity right-hand
+ * side (fd_order, visc), M2P of velocity and right-hand side, and
+ * pmlib_particles_advance.  Device arrays (3, npart) of the plan's precision;
+ * d_part_vel / d_part_dvort receive the interpolated fields (before the map);
+ * synchronises `stream`. */
+int pmgpu_vortex_stage_dev(pmgpu_plan *plan, int time_order, int itimestage, double dtime,
+                           int euler_vort, int fd_order, double visc, void *d_pos, void *d_vort,
+                           void *d_vel_rk, void *d_dvort_rk, int npart, void *d_part_vel,
+                           void *d_part_dvort, int *npart_out, void *stream);
+
 /* ---- diagnostics (no counterpart in the reference, which has no timers) ---- */
 const char *pmgpu_last_error(void);
 /* number of this library's kernels launched since the last reset */

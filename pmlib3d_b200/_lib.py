@@ -23,6 +23,7 @@ EXPORTS = (
     "pmgpu_fft_tune", "pmgpu_fft_tuned", "pmgpu_particle_diagnostics",
     "pmgpu_deriv_vorticity", "pmgpu_deriv_vorticity_f32", "pmgpu_deriv_vorticity_dev",
     "pmgpu_particles_advance", "pmgpu_particles_advance_f32", "pmgpu_particles_advance_dev",
+    "pmgpu_vortex_stage_dev",
 )
 
 
@@ -105,6 +106,8 @@ def lib():
                                         C.c_int, ip],
         "pmgpu_particles_advance_dev": [PP, TP, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, vp, vp, vp, vp,
                                         vp, vp, C.c_int, ip, vp],
+        "pmgpu_vortex_stage_dev": [vp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_double, vp, vp, vp, vp,
+                                   C.c_int, vp, vp, ip, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

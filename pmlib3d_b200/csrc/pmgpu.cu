@@ -2299,3 +2299,59 @@ int pmgpu_particles_advance_dev(const pmgpu_patch *patch, pmgpu_topo *topo, int 
   set_error(caller, "precision unknown.");
   return -1;
 }
+
+// ------------------------------------------------------------------ one stage of the vortex client
+// The stage of vortex_codes/vortex_structures/source/main.f:396-510 without remeshing
+// and diagnostics, from this library's pieces: P2M of the particle vorticity (mesh
+// cleared first), the solve for the mesh velocity, the vorticity right-hand side on
+// the mesh (its free-face ghosts start at zero), M2P of velocity and right-hand side
+// in the bin order of the deposition, and the stage update with the particle map.
+template <typename R>
+static int vortex_stage(pmgpu_plan *pl, int order, int stage, double dtime, int euler, int fd_order, double visc,
+                        R *pos, R *vort, R *vel_rk, R *dvort_rk, int n, R *pvel, R *pdvort, int *nout,
+                        cudaStream_t st) {
+  const char *caller = "pmgpu_vortex_stage";
+  const size_t nm = mesh_points(&pl->topo) * 3;
+  if (pl->mesh_w.ensure(sizeof(R) * nm, caller) || pl->mesh_u.ensure(sizeof(R) * nm, caller) ||
+      pl->mesh_a.ensure(sizeof(R) * nm, caller))
+    return -1;
+  pmgpu_topo t = pl->topo;
+  t.npart = n;
+  PartScratchRefs r{&pl->key, &pl->val, &pl->key2, &pl->val2, &pl->counts, &pl->start, &pl->spart, &pl->hist};
+  const int *perm = nullptr;
+  if (run_p2m<R>(&t, pl->par.interpolation_order, pos, vort, 3, n, pl->mesh_w.as<R>(), 3, 1, r, st, &perm, caller))
+    return -1;
+  if (run_solve<R>(pl, pl->mesh_w.as<R>(), pl->mesh_u.as<R>(), nullptr, nullptr, 0, 0, 0, st, caller)) return -1;
+  CK(cudaMemsetAsync(pl->mesh_a.p, 0, sizeof(R) * nm, st), caller);
+  if (run_deriv_vorticity<R>(&t, fd_order, visc, pl->mesh_w.as<R>(), pl->mesh_u.as<R>(), pl->mesh_a.as<R>(), st,
+                             caller))
+    return -1;
+  if (run_m2p_sorted<R>(&t, pl->par.interpolation_order, pos, pl->start.as<unsigned>(), perm, n, pl->mesh_u.as<R>(),
+                        pvel, st, caller) ||
+      run_m2p_sorted<R>(&t, pl->par.interpolation_order, pos, pl->start.as<unsigned>(), perm, n, pl->mesh_a.as<R>(),
+                        pdvort, st, caller))
+    return -1;
+  return run_advance<R>(&pl->patch, &t, order, stage, dtime, euler, pos, vort, pvel, pdvort, vel_rk, dvort_rk, n,
+                        nout, st, caller);
+}
+
+int pmgpu_vortex_stage_dev(pmgpu_plan *plan, int time_order, int itimestage, double dtime, int euler_vort,
+                           int fd_order, double visc, void *d_pos, void *d_vort, void *d_vel_rk, void *d_dvort_rk,
+                           int npart, void *d_part_vel, void *d_part_dvort, int *npart_out, void *stream) {
+  const char *caller = "pmgpu_vortex_stage";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!plan || !npart_out || npart < 0 ||
+      (npart > 0 && (!d_pos || !d_vort || !d_vel_rk || !d_dvort_rk || !d_part_vel || !d_part_dvort))) {
+    set_error(caller, "missing argument.");
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->prec == PMGPU_FP64)
+    return vortex_stage<double>(plan, time_order, itimestage, dtime, euler_vort, fd_order, visc, (double *)d_pos,
+                                (double *)d_vort, (double *)d_vel_rk, (double *)d_dvort_rk, npart,
+                                (double *)d_part_vel, (double *)d_part_dvort, npart_out, st);
+  return vortex_stage<float>(plan, time_order, itimestage, dtime, euler_vort, fd_order, visc, (float *)d_pos,
+                             (float *)d_vort, (float *)d_vel_rk, (float *)d_dvort_rk, npart, (float *)d_part_vel,
+                             (float *)d_part_dvort, npart_out, st);
+}

@@ -356,3 +356,18 @@ def pmlib_particles_advance_dev(patch: Patch, topo: Topo, time_order: int, itime
                                              C.c_void_p(d_vel_rk), C.c_void_p(d_dvort_rk), int(npart), C.byref(n),
                                              C.c_void_p(stream or None))
     return ierr, n.value
+
+
+def vortex_stage_dev(plan: Plan, time_order: int, itimestage: int, dtime: float, fd_order: int, visc: float,
+                     d_pos: int, d_vort: int, d_vel_rk: int, d_dvort_rk: int, npart: int, d_part_vel: int,
+                     d_part_dvort: int, euler_vort: bool = False, stream: int = 0):
+    """One stage of the vortex client's step on device particle arrays of the plan's
+    precision (P2M, solve, right-hand side, M2P, advance with the map); returns
+    (ierr, npart)."""
+    n = C.c_int(0)
+    ierr = lib().pmgpu_vortex_stage_dev(plan.handle, int(time_order), int(itimestage), float(dtime),
+                                        int(bool(euler_vort)), int(fd_order), float(visc), C.c_void_p(d_pos),
+                                        C.c_void_p(d_vort), C.c_void_p(d_vel_rk), C.c_void_p(d_dvort_rk), int(npart),
+                                        C.c_void_p(d_part_vel), C.c_void_p(d_part_dvort), C.byref(n),
+                                        C.c_void_p(stream or None))
+    return ierr, n.value

@@ -162,3 +162,46 @@ def test_particles_advance_errors(capfd):
     far = [a.copy() for a in arrs]
     far[0][0] = np.array(to.xmin) - 3.5 * (np.array(to.xmax) - np.array(to.xmin))  # three wraps needed
     assert P.pmlib_particles_advance(pg, tg, 1, 1, 0.0, *far)[0] == -1
+
+
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", [CASES[0], CASES[2]])
+def test_vortex_stage_matches_oracle_pieces(name, xmin, xmax, dx, bc, ng):
+    """P2M -> solve -> right-hand side -> M2P (velocity, right-hand side) -> advance
+    in one call against the same chain of oracle functions."""
+    import torch
+    from tests.helpers import jittered_particles
+    po, to, qo, pg, tg, qg = setup_pair(xmin, xmax, dx, bc, ng, interp=3, order=6)
+    pos, val = jittered_particles(to, seed=4, jitter=0.1)
+    n = len(pos)
+    to.npart = n
+    tg.npart = n
+    rng = np.random.default_rng(9)
+    vr = 0.01 * rng.standard_normal((n, 3))
+    dr = 0.01 * rng.standard_normal((n, 3))
+    dt, visc = 0.02, 0.001
+    # oracle chain
+    mesh = np.zeros(O.topo_shape(to, 3))
+    assert O.interp_particle_mesh(to, 3, pos, val, mesh, clear=True, clear_ghost=False) == 0
+    ierr, pk = O.poisson_setup(po, qo)
+    ierr, vel, _ = O.poisson_solve(po, to, qo, pk, mesh.copy())
+    dvort = np.zeros_like(mesh)
+    assert O.deriv_vorticity(to, 4, visc, mesh, vel, dvort) == 0
+    _, pvel = O.interp_mesh_particle(to, 3, vel, pos)
+    _, pdv = O.interp_mesh_particle(to, 3, dvort, pos)
+    ao = [pos.copy(), val.copy(), pvel.copy(), pdv.copy(), vr.copy(), dr.copy()]
+    ierr, mo = O.particles_advance(po, to, 2, 1, dt, *ao)
+    assert ierr == 0
+    # GPU
+    ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP64)
+    assert ierr == 0
+    d = [torch.from_numpy(a.copy()).cuda() for a in (pos, val, vr, dr)]
+    uo = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    wo = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    ierr, mg = P.vortex_stage_dev(plan, 2, 1, dt, 4, visc, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(),
+                                  d[3].data_ptr(), n, uo.data_ptr(), wo.data_ptr())
+    assert ierr == 0, P.last_error()
+    assert rel_l2(uo.cpu().numpy(), pvel) < 1e-12
+    assert rel_l2(wo.cpu().numpy(), pdv) < 1e-11
+    assert mg == mo
+    for i, j in ((0, 0), (1, 1), (2, 4), (3, 5)):
+        assert np.allclose(d[i][:mg].cpu().numpy(), ao[j][:mo], rtol=0, atol=1e-12), i
