@@ -12,6 +12,7 @@
 !   pmlib_poisson_setup(patch,topo_all,mesh,ierr)
 !   pmlib_poisson_solve(patch,topo_all,mesh,ierr,reg_vort,reproj,calc_vecpot)
 !   pmlib_regularise(patch,topo_all,mesh,reg_order,filter_width,ierr)
+!   pmlib_particles_advance(patch,topo,part,itimestage,dtime,ierr,euler_vort)
 !   pmlib_gpu_finalise()                 (frees the plan; call from pmlib_finalise)
 !
 ! They read the same module globals as the originals (pmlib_poisson_order,
@@ -127,6 +128,28 @@ MODULE pmlib_gpu_c
       INTEGER(C_INT), VALUE :: incl_ghost, max_part
       INTEGER(C_INT) :: npart
     END FUNCTION
+    INTEGER(C_INT) FUNCTION pmgpu_particles_advance(patch, topo, time_order, itimestage, dtime, &
+        euler_vort, pos, vort, vel, dvort, vel_rk, dvort_rk, npart, npart_out) &
+        BIND(C, NAME='pmgpu_particles_advance')
+      IMPORT
+      TYPE(pmgpu_patch) :: patch
+      TYPE(pmgpu_topo) :: topo
+      INTEGER(C_INT), VALUE :: time_order, itimestage, euler_vort, npart
+      REAL(C_DOUBLE), VALUE :: dtime
+      TYPE(C_PTR), VALUE :: pos, vort, vel, dvort, vel_rk, dvort_rk
+      INTEGER(C_INT) :: npart_out
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION pmgpu_particles_advance_f32(patch, topo, time_order, itimestage, dtime, &
+        euler_vort, pos, vort, vel, dvort, vel_rk, dvort_rk, npart, npart_out) &
+        BIND(C, NAME='pmgpu_particles_advance_f32')
+      IMPORT
+      TYPE(pmgpu_patch) :: patch
+      TYPE(pmgpu_topo) :: topo
+      INTEGER(C_INT), VALUE :: time_order, itimestage, euler_vort, npart
+      REAL(C_DOUBLE), VALUE :: dtime
+      TYPE(C_PTR), VALUE :: pos, vort, vel, dvort, vel_rk, dvort_rk
+      INTEGER(C_INT) :: npart_out
+    END FUNCTION
   END INTERFACE
 END MODULE pmlib_gpu_c
 
@@ -142,7 +165,7 @@ MODULE pmlib_gpu_drop_in
   IMPLICIT NONE
   PRIVATE
   PUBLIC :: pmlib_interp_particle_mesh, pmlib_interp_mesh_particle, pmlib_poisson_setup, &
-          & pmlib_poisson_solve, pmlib_regularise, pmlib_gpu_finalise
+          & pmlib_poisson_solve, pmlib_regularise, pmlib_particles_advance, pmlib_gpu_finalise
 
   TYPE(C_PTR), SAVE :: gpu_plan = C_NULL_PTR
   LOGICAL, PARAMETER :: single = MK .NE. KIND(1D0)
@@ -313,6 +336,58 @@ CONTAINS
       ierr = pmgpu_regularise(gpu_plan, first4(mesh), SIZE(mesh,1), reg_order, REAL(filter_width, C_DOUBLE))
     END IF
   END SUBROUTINE pmlib_regularise
+
+  ! keeps the first n columns of a (3, :) particle array
+  SUBROUTINE shrink(a, n)
+    REAL(MK), DIMENSION(:,:), POINTER :: a
+    INTEGER, INTENT(IN) :: n
+    REAL(MK), DIMENSION(:,:), POINTER :: b
+    IF (SIZE(a,2) .EQ. n) RETURN
+    ALLOCATE(b(SIZE(a,1), n))
+    b = a(:, 1:n)
+    DEALLOCATE(a)
+    a => b
+  END SUBROUTINE shrink
+
+  ! source/particles/pmlib_particles_advance.f:5-213: stage update and particle map
+  ! on the GPU, then the arrays resized to the new count as the reference's unpack
+  ! and reallocation leave them (vel and dvort reallocated without values)
+  SUBROUTINE pmlib_particles_advance(patch, topo, part, itimestage, dtime, ierr, euler_vort)
+    TYPE(class_patch), INTENT(IN) :: patch
+    TYPE(class_topology), DIMENSION(:), POINTER, INTENT(INOUT) :: topo
+    TYPE(class_particles), INTENT(INOUT) :: part
+    INTEGER, INTENT(IN) :: itimestage
+    REAL(MK), INTENT(IN) :: dtime
+    INTEGER, INTENT(OUT) :: ierr
+    LOGICAL, INTENT(IN), OPTIONAL :: euler_vort
+    TYPE(pmgpu_patch) :: p
+    TYPE(pmgpu_topo) :: t
+    INTEGER(C_INT) :: fe, n, nout
+    p = c_patch(patch)
+    t = c_topo(topo(mpi_rank))
+    fe = 0
+    IF (PRESENT(euler_vort)) fe = flag(.TRUE., euler_vort)
+    n = topo(mpi_rank)%npart
+    IF (single) THEN
+      ierr = pmgpu_particles_advance_f32(p, t, pmlib_time_integration_order, itimestage, &
+           & REAL(dtime, C_DOUBLE), fe, first2(part%pos), first2(part%vort), first2(part%vel), &
+           & first2(part%dvort), first2(part%vel_rk), first2(part%dvort_rk), n, nout)
+    ELSE
+      ierr = pmgpu_particles_advance(p, t, pmlib_time_integration_order, itimestage, &
+           & REAL(dtime, C_DOUBLE), fe, first2(part%pos), first2(part%vort), first2(part%vel), &
+           & first2(part%dvort), first2(part%vel_rk), first2(part%dvort_rk), n, nout)
+    END IF
+    IF (ierr .NE. 0) RETURN
+    topo(mpi_rank)%npart = nout
+    CALL shrink(part%pos, nout)
+    CALL shrink(part%vort, nout)
+    CALL shrink(part%vel_rk, nout)
+    CALL shrink(part%dvort_rk, nout)
+    DEALLOCATE(part%vel)
+    ALLOCATE(part%vel(pmlib_ndim, nout))
+    DEALLOCATE(part%dvort)
+    ALLOCATE(part%dvort(pmlib_ndim, nout))
+  END SUBROUTINE pmlib_particles_advance
 
   SUBROUTINE pmlib_gpu_finalise()
     IF (C_ASSOCIATED(gpu_plan)) CALL pmgpu_plan_destroy(gpu_plan)
