@@ -204,6 +204,12 @@ int pmgpu_particle_diagnostics(const double dx[3], const void *d_pos, const void
 int pmgpu_fft_tune(int on);
 int pmgpu_fft_tuned(int index, int *length, int *precision, int *axis, int *radices, int *tile,
                     double *ms);
+/* Puts a schedule into the table for plans created afterwards (a saved tuning, or a
+ * schedule to test): radices[3] outermost first, 0-padded, multiplying to `length`;
+ * FP32 may also use the wide composite radices 18, 20, 22, 24 (two-phase schedules
+ * such as 528 = 22 x 24); tile 0 lets the plan choose.  radices = NULL removes the
+ * entry. */
+int pmgpu_fft_set_schedule(int length, int precision, int axis, const int *radices, int tile);
 
 /* ---- allocation-free deposition (no counterpart in the reference) ----
  * For callers that cannot allocate device memory while they run, e.g. a host

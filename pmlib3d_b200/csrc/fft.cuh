@@ -32,10 +32,12 @@ struct FftDesc {
   int next;                  // entries of the extra table
 };
 
-// (cos, sin)(2 pi m / R) for R <= 17, m < R; every translation unit that runs the
-// transforms holds its own copy, filled once per device by the host
-static __constant__ float c_cs32[18][17][2];
-static __constant__ double c_cs64[18][17][2];
+// (cos, sin)(2 pi m / R) for R <= 32 (prime radices and the composite radices'
+// internal twiddles), m < R; every translation unit that runs the transforms holds
+// its own copy, filled once per device by the host
+constexpr int CS_R = 33, CS_M = 32;
+static __constant__ float c_cs32[CS_R][CS_M][2];
+static __constant__ double c_cs64[CS_R][CS_M][2];
 
 template <typename T> __device__ __forceinline__ T cs_c(int R, int m);
 template <typename T> __device__ __forceinline__ T cs_s(int R, int m);
@@ -157,6 +159,18 @@ template <int R, bool INV, typename C> __device__ __forceinline__ void dft(C *v)
     dft_comp<4, 3, INV>(v);
   } else if constexpr (R == 16) {
     dft_comp<4, 4, INV>(v);
+  } else if constexpr (R == 18) {
+    dft_comp<6, 3, INV>(v);
+  } else if constexpr (R == 20) {
+    dft_comp<5, 4, INV>(v);
+  } else if constexpr (R == 22) {
+    dft_comp<11, 2, INV>(v);
+  } else if constexpr (R == 24) {
+    dft_comp<8, 3, INV>(v);
+  } else if constexpr (R == 26) {
+    dft_comp<13, 2, INV>(v);
+  } else if constexpr (R == 32) {
+    dft_comp<8, 4, INV>(v);
   } else {
     dft_prime<R, INV>(v);
   }

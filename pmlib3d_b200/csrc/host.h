@@ -63,6 +63,8 @@ static inline size_t reg_smem(int n, int m, int nc, int tk, size_t csize) {
 // shared memory per CTA that lets the register-engine kernels run as many CTAs per
 // SM as their register budget allows (FP32: 3, FP64: 2; 228 KB per SM)
 static inline size_t reg_budget(size_t rsize) { return rsize == 4 ? (size_t)74 * 1024 : (size_t)112 * 1024; }
+// the wide-radix FP32 kernels run two CTAs per SM
+static inline size_t reg_budget_wide() { return (size_t)112 * 1024; }
 // kx tile of the register engine: within the budget if possible, else one CTA per SM
 static inline int pick_tk_reg(int n, int m, int nc, size_t csize, int Hp, size_t budget1) {
   for (size_t budget : {budget1, PASS_SMEM_BUDGET})

@@ -26,10 +26,17 @@ static int launch_lines(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typ
   typedef typename cplx_t<R>::type C;
   const int n = g.M[axis];
   if (axis == 1 ? g.ry_ok : g.rz_ok) {
-    const int mt = (axis == 1 ? g.ry : g.rz).n;  // transform length (Bluestein: > n)
+    const RegPlan &rp = axis == 1 ? g.ry : g.rz;
+    const int mt = rp.n;  // transform length (Bluestein: > n)
+    bool wide = false;
+    for (int p = 0; p < rp.np; p++) wide = wide || reg_radix_wide(rp.rad[p]);
+    if (wide && sizeof(R) != 4) {
+      set_error(caller, "wide radices are FP32 only.");
+      return -1;
+    }
     int TK = axis == 1 ? g.tky : g.tkz;  // a tuned tile, if it fits
     if (TK <= 0 || g.Hp % TK || reg_smem(n, mt, NC, TK, sizeof(C)) > PASS_SMEM_BUDGET)
-      TK = pick_tk_reg(n, mt, NC, sizeof(C), g.Hp, reg_budget(sizeof(R)));
+      TK = pick_tk_reg(n, mt, NC, sizeof(C), g.Hp, wide ? reg_budget_wide() : reg_budget(sizeof(R)));
     if (TK > 0) {
       LineTiles lt;
       lt.n = n;
@@ -44,16 +51,21 @@ static int launch_lines(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typ
       lt.TK = TK;
       lt.dLG = make_fastdiv((unsigned)(NC * TK / RVec<R>::G));
       const size_t sm = reg_smem(n, mt, NC, TK, sizeof(C));
-      CK(cudaFuncSetAttribute(k_rlines<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
-      int per = 1;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rlines<R, NC>, RL_THREADS, sm) != cudaSuccess ||
-          per < 1)
-        per = 1;
-      const int grid = std::max(1, std::min(lt.nouter * lt.nkt, per * num_sms()));
-      k_rlines<R, NC><<<grid, RL_THREADS, sm, st>>>(g, lt, in, out, axis, lmode, zmode, reproj, use_zeta);
-      PM_LAUNCHED();
-      CKL(caller);
-      return 0;
+      auto launch = [&](auto kern) -> int {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+        int per = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, RL_THREADS, sm) != cudaSuccess || per < 1)
+          per = 1;
+        const int grid = std::max(1, std::min(lt.nouter * lt.nkt, per * num_sms()));
+        kern<<<grid, RL_THREADS, sm, st>>>(g, lt, in, out, axis, lmode, zmode, reproj, use_zeta);
+        PM_LAUNCHED();
+        CKL(caller);
+        return 0;
+      };
+      if constexpr (sizeof(R) == 4) {
+        if (wide) return launch(k_rlines<R, NC, true>);
+      }
+      return launch(k_rlines<R, NC, false>);
     }
   }
   const int ntw = (axis == 1) ? g.fy.ntw : g.fz.ntw;

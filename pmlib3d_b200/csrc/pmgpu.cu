@@ -94,11 +94,11 @@ static int ensure_device(const char *caller) {
   int dev = 0;
   CK(cudaGetDevice(&dev), caller);
   if (dev >= 0 && dev < 128 && g_dev_ready[dev]) return 0;
-  static float t32[18][17][2];
-  static double t64[18][17][2];
+  static float t32[CS_R][CS_M][2];
+  static double t64[CS_R][CS_M][2];
   const long double twopi = 2.0L * acosl(-1.0L);
-  for (int R = 1; R < 18; R++)
-    for (int m = 0; m < 17; m++) {
+  for (int R = 1; R < CS_R; R++)
+    for (int m = 0; m < CS_M; m++) {
       long double a = (m < R) ? twopi * (long double)m / (long double)R : 0.0L;
       t64[R][m][0] = (double)cosl(a);
       t64[R][m][1] = (double)sinl(a);
@@ -322,6 +322,27 @@ static std::vector<RadixSeq> regplan_candidates(int n) {
       if (n2 == 1) add(2, a, b, 0);
       else if (reg_radix(n2)) add(3, a, b, n2);
     }
+  }
+  std::stable_sort(out.begin(), out.end(), [](const RadixSeq &x, const RadixSeq &y) { return x.cost < y.cost; });
+  return out;
+}
+
+// two-phase sequences with at least one wide composite radix (the wide FP32 kernel
+// variant), fewest points per thread first; only the autotuner tries them
+static std::vector<RadixSeq> regplan_candidates_wide(int n) {
+  static const int S[] = {24, 22, 20, 18, 17, 16, 13, 12, 11, 10, 9, 8};
+  std::vector<RadixSeq> out;
+  for (int a : S) {
+    if (n % a) continue;
+    const int b = n / a;
+    if (!(reg_radix(b) || reg_radix_wide(b)) || !(reg_radix_wide(a) || reg_radix_wide(b))) continue;
+    RadixSeq q;
+    q.np = 2;
+    q.r[0] = a;
+    q.r[1] = b;
+    q.r[2] = 0;
+    q.cost = (double)std::max(a, b) + (a % 2 ? 0.5 : 0.0);
+    out.push_back(q);
   }
   std::stable_sort(out.begin(), out.end(), [](const RadixSeq &x, const RadixSeq &y) { return x.cost < y.cost; });
   return out;
@@ -975,6 +996,11 @@ template <typename R> static int tune_axis(pmgpu_plan *pl, int axis, TunedSchedu
   const int n = G.M[axis];
   std::vector<RadixSeq> cands = regplan_candidates(n);
   if (cands.size() > 5) cands.resize(5);
+  if (sizeof(R) == 4) {
+    std::vector<RadixSeq> w = regplan_candidates_wide(n);
+    if (w.size() > 3) w.resize(3);
+    cands.insert(cands.end(), w.begin(), w.end());
+  }
   DevBuf A, B, tw, kp;
   const size_t nx = (size_t)G.P[1] * G.P[2] * G.Hp * 3;
   const size_t ny = (size_t)G.M[1] * G.P[2] * G.Hp * 3;
@@ -1964,6 +1990,41 @@ int pmgpu_fft_tuned(int index, int *length, int *precision, int *axis, int *radi
     for (int i = 0; i < 3; i++) radices[i] = i < it->second.np ? it->second.r[i] : 0;
   if (tile) *tile = it->second.tk;
   if (ms) *ms = it->second.ms;
+  return 0;
+}
+
+int pmgpu_fft_set_schedule(int length, int precision, int axis, const int *radices, int tile) {
+  const char *caller = "pmgpu_fft_set_schedule";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if ((precision != PMGPU_FP32 && precision != PMGPU_FP64) || (axis != 1 && axis != 2) || length < 2) {
+    set_error(caller, "length, precision or axis out of range.");
+    return -1;
+  }
+  const auto key = std::make_tuple(length, precision == PMGPU_FP64 ? 8 : 4, axis);
+  if (!radices) {
+    g_tuned.erase(key);
+    return 0;
+  }
+  TunedSchedule ts;
+  ts.np = 0;
+  long long prod = 1;
+  for (int i = 0; i < 3 && radices[i] > 0; i++) {
+    const int r = radices[i];
+    if (!(reg_radix(r) || (precision == PMGPU_FP32 && reg_radix_wide(r)))) {
+      set_error(caller, "radix not available.");
+      return -1;
+    }
+    ts.r[ts.np++] = r;
+    prod *= r;
+  }
+  for (int i = ts.np; i < 3; i++) ts.r[i] = 0;
+  if (ts.np == 0 || prod != length || (tile != 0 && tile != 1 && tile != 2 && tile != 4 && tile != 8)) {
+    set_error(caller, "radices do not multiply to the length, or tile not in {0, 1, 2, 4, 8}.");
+    return -1;
+  }
+  ts.tk = tile;
+  ts.ms = 0.0;
+  g_tuned[key] = ts;
   return 0;
 }
 

@@ -68,6 +68,10 @@ __host__ __device__ constexpr bool reg_radix(int r) {
   return r == 2 || r == 3 || r == 4 || r == 5 || r == 6 || r == 7 || r == 8 || r == 9 || r == 10 || r == 11 ||
          r == 12 || r == 13 || r == 16 || r == 17;
 }
+// composite radices of the wide variant of the y / z passes (FP32 only): a thread
+// holds up to 24 points, so lengths such as 528 = 22 x 24 take two phases instead
+// of three; the kernels that may run them are compiled for two CTAs per SM
+__host__ __device__ constexpr bool reg_radix_wide(int r) { return r == 18 || r == 20 || r == 22 || r == 24; }
 
 // where a phase reads from / writes to
 struct PhaseGlobal {
@@ -196,10 +200,19 @@ __device__ __forceinline__ void rphase(const RegPlan &pl, int p, typename RVec<R
   }
 }
 
-template <bool INV, typename R>
+template <bool INV, typename R, bool WIDE = false>
 __device__ __forceinline__ void rphase_any(const RegPlan &pl, int p, typename RVec<R>::V *buf, int LG,
                                            const FastDiv &dLG, const typename cplx_t<R>::type *tw, bool gsrc,
                                            bool gdst, bool twid, const PhaseGlobal &gl, int nz) {
+  if constexpr (WIDE) {
+    switch (pl.rad[p]) {
+      case 18: rphase<18, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); return;
+      case 20: rphase<20, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); return;
+      case 22: rphase<22, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); return;
+      case 24: rphase<24, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); return;
+      default: break;
+    }
+  }
   switch (pl.rad[p]) {
     case 2: rphase<2, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); break;
     case 3: rphase<3, INV, R>(pl, p, buf, LG, dLG, tw, gsrc, gdst, twid, gl, nz); break;
@@ -223,27 +236,28 @@ __device__ __forceinline__ void rphase_any(const RegPlan &pl, int p, typename RV
 // digit-reversed output in buf, or in global memory when glast.  The caller
 // synchronises before; every phase but a final global one ends with a barrier.
 // nz0: nonzero leading points of an input in buf (the rest is zero padding)
-template <typename R>
+template <typename R, bool WIDE = false>
 __device__ __forceinline__ void rfft_fwd(const RegPlan &pl, typename RVec<R>::V *buf, int LG, const FastDiv &dLG,
                                          const typename cplx_t<R>::type *tw, bool gfirst, bool glast,
                                          const PhaseGlobal &gl, int nz0 = -1) {
   for (int p = 0; p < pl.np; p++) {
     const bool last = p == pl.np - 1;
     const int nz = p > 0 ? pl.n : gfirst ? gl.rows_in : nz0 >= 0 ? nz0 : pl.n;
-    rphase_any<false, R>(pl, p, buf, LG, dLG, tw, gfirst && p == 0, glast && last, !last, gl, nz);
+    rphase_any<false, R, WIDE>(pl, p, buf, LG, dLG, tw, gfirst && p == 0, glast && last, !last, gl, nz);
     __syncthreads();
   }
 }
 
 // inverse transform: digit-reversed input (global when gfirst, else buf), natural
 // output in buf, or in global memory (rows < rows_out) when glast
-template <typename R>
+template <typename R, bool WIDE = false>
 __device__ __forceinline__ void rfft_inv(const RegPlan &pl, typename RVec<R>::V *buf, int LG, const FastDiv &dLG,
                                          const typename cplx_t<R>::type *tw, bool gfirst, bool glast,
                                          const PhaseGlobal &gl) {
   for (int p = pl.np - 1; p >= 0; p--) {
     const bool gs = gfirst && p == pl.np - 1;
-    rphase_any<true, R>(pl, p, buf, LG, dLG, tw, gs, glast && p == 0, p < pl.np - 1, gl, gs ? gl.rows_in : pl.n);
+    rphase_any<true, R, WIDE>(pl, p, buf, LG, dLG, tw, gs, glast && p == 0, p < pl.np - 1, gl,
+                              gs ? gl.rows_in : pl.n);
     __syncthreads();
   }
 }

@@ -357,8 +357,8 @@ __global__ void __launch_bounds__(PASS_THREADS, 1) k_lines(SolveGeom<R> g, LineT
 // one CTA's loads overlap another's transforms.
 constexpr int RL_THREADS = 256;
 
-template <typename R, int NC>
-__global__ void __launch_bounds__(RL_THREADS, RMinBlocks<R>::v) k_rlines(SolveGeom<R> g, LineTiles lt,
+template <typename R, int NC, bool WIDE = false>
+__global__ void __launch_bounds__(RL_THREADS, WIDE ? 2 : RMinBlocks<R>::v) k_rlines(SolveGeom<R> g, LineTiles lt,
                                                           const typename cplx_t<R>::type *in,
                                                           typename cplx_t<R>::type *out, int axis, int lmode,
                                                           int zmode, int reproj, int use_zeta) {
@@ -407,18 +407,18 @@ __global__ void __launch_bounds__(RL_THREADS, RMinBlocks<R>::v) k_rlines(SolveGe
     gl.rows_out = lt.rows_out;
     if (lmode == L_FWD) {
       if (blue) bfft<R, false>(pl, buf, LG, lt.dLG, tw, chirp, bpos, true, true, gl, lt.rows_in, nl);
-      else rfft_fwd<R>(pl, buf, LG, lt.dLG, tw, true, true, gl);
+      else rfft_fwd<R, WIDE>(pl, buf, LG, lt.dLG, tw, true, true, gl);
     } else if (lmode == L_INV) {
       if (blue) bfft<R, true>(pl, buf, LG, lt.dLG, tw, chirp, bpos, true, true, gl, nl, lt.rows_out);
-      else rfft_inv<R>(pl, buf, LG, lt.dLG, tw, true, true, gl);
+      else rfft_inv<R, WIDE>(pl, buf, LG, lt.dLG, tw, true, true, gl);
     } else {
       if (blue) bfft<R, false>(pl, buf, LG, lt.dLG, tw, chirp, bpos, true, false, gl, lt.rows_in, nl);
-      else rfft_fwd<R>(pl, buf, LG, lt.dLG, tw, true, false, gl);
+      else rfft_fwd<R, WIDE>(pl, buf, LG, lt.dLG, tw, true, false, gl);
       z_multiply<R, NC>(g, reinterpret_cast<C *>(buf), L, TK, kt * TK, g.yk ? g.yk[o] : o, zmode, reproj, use_zeta,
                         blue ? nullptr : zpos, kzs);
       __syncthreads();
       if (blue) bfft<R, true>(pl, buf, LG, lt.dLG, tw, chirp, bpos, false, true, gl, nl, lt.rows_out);
-      else rfft_inv<R>(pl, buf, LG, lt.dLG, tw, false, true, gl);
+      else rfft_inv<R, WIDE>(pl, buf, LG, lt.dLG, tw, false, true, gl);
     }
   }
 }

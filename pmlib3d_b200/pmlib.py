@@ -275,6 +275,13 @@ def fft_tune(on: bool) -> int:
     return lib().pmgpu_fft_tune(int(bool(on)))
 
 
+def fft_set_schedule(length: int, precision: int, axis: int, radices=None, tile: int = 0) -> int:
+    """Puts a radix schedule (or, with radices None, removes one) into the table that
+    plans created afterwards use."""
+    r = None if radices is None else (C.c_int * 3)(*(list(radices) + [0, 0, 0])[:3])
+    return lib().pmgpu_fft_set_schedule(int(length), int(precision), int(axis), r, int(tile))
+
+
 def fft_tuned() -> list:
     """The tuning table: dicts with length, precision, axis, radices, tile, ms."""
     out = []

@@ -494,3 +494,53 @@ def test_particle_diagnostics(prec):
     assert np.allclose(got, ref, rtol=1e-10, atol=1e-12 * np.abs(ref).max())
     d2 = P.particle_diagnostics(dx, tp.data_ptr(), tu.data_ptr(), tw.data_ptr(), n, prec)
     assert d2 == d
+
+
+WIDE_CASES = [
+    # y 528 = 22 x 24, z 48 = 24 x 2
+    ("fff-y528", (-1, -16, -1), (1, 16, 1), (0.125,) * 3, (0, 0, 0), 4, {1: (22, 24), 2: (24, 2)}),
+    # z 264 = 24 x 11, y 48 = 2 x 24
+    ("fff-z264", (-1, -1, -7.75), (1, 1, 7.75), (0.125,) * 3, (0, 0, 0), 4, {1: (2, 24), 2: (24, 11)}),
+    # z 40 = 20 x 2, y 36 = 18 x 2
+    ("fff-20-18", (-1, -0.625, -0.75), (1, 0.625, 0.75), (0.125,) * 3, (0, 0, 0), 4, {1: (18, 2), 2: (20, 2)}),
+    # periodic y of 20 cells: one phase of radix 20
+    ("ppf-20", (0, 0, -1), (2, 2.5, 1), (0.125, 0.125, 0.125), (1, 1, 0), 4, {1: (20,), 2: None}),
+]
+
+
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng,sched", WIDE_CASES)
+def test_wide_radix_schedules(name, xmin, xmax, dx, bc, ng, sched):
+    """The two-phase wide-radix schedules of the FP32 passes (set explicitly) against
+    the oracle: velocity and reprojected vorticity."""
+    po, to, qo, pg, tg, qg = setup_pair(xmin, xmax, dx, bc, ng, interp=3, order=6)
+    M = O.kernel_dims(po, qo)[0]
+    w = gaussian_field(to, seed=21, noise=0.01)
+    vel_o, vort_o, _ = oracle_solve(po, to, qo, w, reproj=True)
+    applied = []
+    try:
+        for axis, rad in sched.items():
+            if rad is None:
+                continue
+            assert int(np.prod(rad)) == M[axis], (M, axis, rad)
+            assert P.fft_set_schedule(M[axis], P.FP32, axis, rad, 0) == 0, P.last_error()
+            applied.append((M[axis], axis))
+        ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP32)
+        assert ierr == 0, P.last_error()
+        vel = np.zeros(w.shape, np.float32)
+        wg = w.astype(np.float32)
+        assert P.pmlib_poisson_solve(plan, wg, vel, reproj=True) == 0
+        assert rel_l2(vel, vel_o) < TOL32, rel_l2(vel, vel_o)
+        assert rel_l2(wg, vort_o) < TOL32, rel_l2(wg, vort_o)
+        table = {(e["length"], e["axis"]): e["radices"] for e in P.fft_tuned() if e["precision"] == "fp32"}
+        for n, axis in applied:
+            assert tuple(table[(n, axis)]) == tuple(sched[axis])
+    finally:
+        for n, axis in applied:
+            P.fft_set_schedule(n, P.FP32, axis, None)
+
+
+def test_schedule_errors():
+    assert P.fft_set_schedule(528, P.FP32, 1, (22, 23), 0) == -1   # 23 is not a radix
+    assert P.fft_set_schedule(528, P.FP64, 1, (22, 24), 0) == -1   # wide radices are FP32 only
+    assert P.fft_set_schedule(528, P.FP32, 1, (16, 11, 2), 0) == -1  # product 352
+    assert P.fft_set_schedule(528, P.FP32, 3, (22, 24), 0) == -1   # axis
