@@ -150,6 +150,14 @@ int pmgpu_step(pmgpu_plan *plan, const void *pos, const void *part_vort, int npa
 int pmgpu_step_dev(pmgpu_plan *plan, const void *d_pos, const void *d_part_vort, int npart,
                    void *d_part_vel, void *stream);
 
+/* Steps of independent particle sets through one plan, from host arrays (pinned
+ * for the copies to overlap): step i+1's inputs go to the GPU and step i-1's
+ * velocities come back while step i runs (two copy streams, double-buffered device
+ * arrays).  pos[i], part_vort[i] and part_vel[i] hold npart[i] particles (3, np) of
+ * the plan's precision.  Returns when every velocity is in host memory. */
+int pmgpu_step_many(pmgpu_plan *plan, int nsteps, const void *const *pos,
+                    const void *const *part_vort, const int *npart, void *const *part_vel);
+
 /* ---- remesh (source/remesh/pmlib_remesh.f:5-28) ----
  * Two calls, as the Fortran wrapper needs to ALLOCATE between them: the first with
  * pos == NULL returns the count in *npart; the second fills pos/vort/dvort/vel

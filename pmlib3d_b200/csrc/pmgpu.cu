@@ -464,8 +464,29 @@ struct Geometry {
   int allper;
 };
 
+// streams, events and double-buffered particle arrays of pmgpu_step_many
+struct StepPipe {
+  cudaStream_t s[3] = {nullptr, nullptr, nullptr};  // host->device, compute, device->host
+  cudaEvent_t h2d[2] = {nullptr, nullptr}, comp[2] = {nullptr, nullptr}, d2h[2] = {nullptr, nullptr};
+  DevBuf pos[2], val[2], out[2];
+  ~StepPipe() {
+    for (int i = 0; i < 3; i++)
+      if (s[i]) cudaStreamSynchronize(s[i]);
+    for (int i = 0; i < 2; i++) {
+      pos[i].release();
+      val[i].release();
+      out[i].release();
+      for (cudaEvent_t e : {h2d[i], comp[i], d2h[i]})
+        if (e) cudaEventDestroy(e);
+    }
+    for (int i = 0; i < 3; i++)
+      if (s[i]) cudaStreamDestroy(s[i]);
+  }
+};
+
 struct pmgpu_plan {
   int prec;
+  StepPipe pipe;
   pmgpu_patch patch;
   pmgpu_topo topo;
   pmgpu_params par;
@@ -1611,6 +1632,94 @@ int pmgpu_step_dev(pmgpu_plan *plan, const void *d_pos, const void *d_part_vort,
   if (plan->prec == PMGPU_FP64)
     return step_dev<double>(plan, (const double *)d_pos, (const double *)d_part_vort, npart, (double *)d_part_vel, st);
   return step_dev<float>(plan, (const float *)d_pos, (const float *)d_part_vort, npart, (float *)d_part_vel, st);
+}
+
+// Grows every buffer a step of up to n particles uses, so that steps queued on other
+// streams never reallocate (a reallocation frees on the legacy stream).
+template <typename R> static int ensure_step_scratch(pmgpu_plan *pl, int n, const char *caller) {
+  const size_t nm = mesh_points(&pl->topo) * 3;
+  const int W = pl->par.interpolation_order == 3 ? 4 : 6;
+  PartGeom<R> g = part_geom<R>(&pl->topo, W);
+  const size_t nn = (size_t)std::max(n, 1);
+  typedef typename cplx_t<R>::type C;
+  const Geometry &G = pl->g;
+  const size_t nX = (size_t)G.P[1] * G.P[2] * G.Hp * 3, nY = (size_t)G.M[1] * G.P[2] * G.Hp * 3;
+  if (pl->mesh_w.ensure(sizeof(R) * nm, caller) || pl->mesh_u.ensure(sizeof(R) * nm, caller) ||
+      pl->X.ensure(sizeof(C) * nX, caller) || pl->Y.ensure(sizeof(C) * nY, caller) ||
+      pl->key.ensure(sizeof(unsigned) * nn, caller) || pl->val.ensure(sizeof(unsigned) * nn, caller) ||
+      pl->key2.ensure(sizeof(int) * nn, caller) || pl->val2.ensure(sizeof(int) * nn, caller) ||
+      pl->hist.ensure(sizeof(unsigned) * (nn / (FIX_SMALL + 1) + 2), caller) ||
+      pl->counts.ensure(sizeof(unsigned) * (g.nbins + 1), caller) ||
+      pl->start.ensure(sizeof(unsigned) * (g.nbins + 1), caller))
+    return -1;
+  const size_t nb = (g.nbins + 1 + SCAN_TILE - 1) / SCAN_TILE;
+  return pl->spart.ensure(sizeof(unsigned) * (nb + 1), caller);
+}
+
+int pmgpu_step_many(pmgpu_plan *plan, int nsteps, const void *const *pos, const void *const *part_vort,
+                    const int *npart, void *const *part_vel) {
+  const char *caller = "pmgpu_step";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!plan || nsteps < 0 || (nsteps > 0 && (!pos || !part_vort || !npart || !part_vel))) {
+    set_error(caller, "missing argument.");
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  int nmax = 0;
+  for (int i = 0; i < nsteps; i++) {
+    if (npart[i] < 0 || (npart[i] > 0 && (!pos[i] || !part_vort[i] || !part_vel[i]))) {
+      set_error(caller, "missing argument.");
+      return -1;
+    }
+    nmax = std::max(nmax, npart[i]);
+  }
+  const bool f64 = plan->prec == PMGPU_FP64;
+  const size_t es = f64 ? 8 : 4;
+  if ((f64 ? ensure_step_scratch<double>(plan, nmax, caller) : ensure_step_scratch<float>(plan, nmax, caller)))
+    return -1;
+  StepPipe &P = plan->pipe;
+  if (!P.s[0]) {
+    for (int i = 0; i < 3; i++) CK(cudaStreamCreateWithFlags(&P.s[i], cudaStreamNonBlocking), caller);
+    for (int i = 0; i < 2; i++) {
+      CK(cudaEventCreateWithFlags(&P.h2d[i], cudaEventDisableTiming), caller);
+      CK(cudaEventCreateWithFlags(&P.comp[i], cudaEventDisableTiming), caller);
+      CK(cudaEventCreateWithFlags(&P.d2h[i], cudaEventDisableTiming), caller);
+    }
+  }
+  const size_t nb = es * 3 * (size_t)std::max(nmax, 1);
+  for (int i = 0; i < 2; i++)
+    if (P.pos[i].ensure(nb, caller) || P.val[i].ensure(nb, caller) || P.out[i].ensure(nb, caller)) return -1;
+  cudaStream_t sh = P.s[0], sc = P.s[1], sd = P.s[2];
+  for (int i = 0; i < nsteps; i++) {
+    const int b = i & 1, n = npart[i];
+    const size_t bytes = es * 3 * (size_t)n;
+    // the slot's inputs are free once step i-2 has computed, its output once copied out
+    if (i >= 2) CK(cudaStreamWaitEvent(sh, P.comp[b], 0), caller);
+    if (n > 0) {
+      CK(cudaMemcpyAsync(P.pos[b].p, pos[i], bytes, cudaMemcpyHostToDevice, sh), caller);
+      CK(cudaMemcpyAsync(P.val[b].p, part_vort[i], bytes, cudaMemcpyHostToDevice, sh), caller);
+    }
+    CK(cudaEventRecord(P.h2d[b], sh), caller);
+    CK(cudaStreamWaitEvent(sc, P.h2d[b], 0), caller);
+    if (i >= 2) CK(cudaStreamWaitEvent(sc, P.d2h[b], 0), caller);
+    const int rc = f64 ? step_dev<double>(plan, P.pos[b].as<double>(), P.val[b].as<double>(), n,
+                                          P.out[b].as<double>(), sc)
+                       : step_dev<float>(plan, P.pos[b].as<float>(), P.val[b].as<float>(), n, P.out[b].as<float>(), sc);
+    if (rc) {
+      cudaStreamSynchronize(sh);
+      cudaStreamSynchronize(sc);
+      cudaStreamSynchronize(sd);
+      return -1;
+    }
+    CK(cudaEventRecord(P.comp[b], sc), caller);
+    CK(cudaStreamWaitEvent(sd, P.comp[b], 0), caller);
+    if (n > 0) CK(cudaMemcpyAsync(part_vel[i], P.out[b].p, bytes, cudaMemcpyDeviceToHost, sd), caller);
+    CK(cudaEventRecord(P.d2h[b], sd), caller);
+  }
+  CK(cudaStreamSynchronize(sd), caller);
+  CK(cudaStreamSynchronize(sc), caller);
+  CK(cudaStreamSynchronize(sh), caller);
+  return 0;
 }
 
 int pmgpu_step(pmgpu_plan *plan, const void *pos, const void *part_vort, int npart, void *part_vel) {

@@ -313,6 +313,23 @@ def step(plan: Plan, pos, part_vort, part_vel) -> int:
                             part_vel.ctypes.data)
 
 
+def step_many(plan: Plan, pos_list, vort_list, vel_list) -> int:
+    """Independent steps through host arrays with the copies of the neighbouring steps
+    overlapped with each step's GPU work (pinned arrays let the copies overlap)."""
+    dt = np.float64 if plan.precision == FP64 else np.float32
+    k = len(pos_list)
+    if not (len(vort_list) == k and len(vel_list) == k):
+        raise ValueError("pos_list, vort_list and vel_list differ in length")
+    for group in (pos_list, vort_list, vel_list):
+        for a in group:
+            _ptr(a, dt)
+    P_ = (C.c_void_p * k)(*[a.ctypes.data for a in pos_list])
+    V_ = (C.c_void_p * k)(*[a.ctypes.data for a in vort_list])
+    U_ = (C.c_void_p * k)(*[a.ctypes.data for a in vel_list])
+    N_ = (C.c_int * k)(*[a.shape[0] for a in pos_list])
+    return lib().pmgpu_step_many(plan.handle, k, P_, V_, N_, U_)
+
+
 def step_dev(plan: Plan, d_pos: int, d_part_vort: int, npart: int, d_part_vel: int, stream: int = 0) -> int:
     """The same step on device pointers (e.g. ``tensor.data_ptr()``) on a CUDA stream."""
     return lib().pmgpu_step_dev(plan.handle, C.c_void_p(d_pos), C.c_void_p(d_part_vort), int(npart),

@@ -544,3 +544,31 @@ def test_schedule_errors():
     assert P.fft_set_schedule(528, P.FP64, 1, (22, 24), 0) == -1   # wide radices are FP32 only
     assert P.fft_set_schedule(528, P.FP32, 1, (16, 11, 2), 0) == -1  # product 352
     assert P.fft_set_schedule(528, P.FP32, 3, (22, 24), 0) == -1   # axis
+
+
+def test_step_many_matches_single_steps():
+    """Pipelined independent steps from host arrays (pinned and pageable) give the
+    same velocities, bit for bit, as one pmgpu_step per input; steps of different
+    particle counts included."""
+    import torch
+    po, to, qo, pg, tg, qg = setup_pair(*CASES[0][1:], interp=3, order=6)
+    ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP32)
+    assert ierr == 0
+    inputs = []
+    for seed, cut in ((30, None), (31, 5000), (32, None), (33, 7000), (34, None)):
+        pos, val = jittered_particles(to, seed=seed)
+        if cut:
+            pos, val = pos[:cut], val[:cut]
+        inputs.append((pos.astype(np.float32), val.astype(np.float32)))
+    ref = []
+    for pos, val in inputs:
+        up = np.zeros_like(pos)
+        assert P.step(plan, pos, val, up) == 0
+        ref.append(up)
+    pinned = [(torch.from_numpy(p).pin_memory().numpy(), torch.from_numpy(v).pin_memory().numpy())
+              for p, v in inputs]
+    for src in (inputs, pinned):
+        outs = [np.full_like(p, np.nan) for p, _ in src]
+        assert P.step_many(plan, [p for p, _ in src], [v for _, v in src], outs) == 0, P.last_error()
+        for o, r in zip(outs, ref):
+            assert np.array_equal(o, r)
