@@ -625,15 +625,17 @@ __global__ void k_m2p(PartGeom<R> g, const R *__restrict__ pos, const int *__res
 
 // M2P over particles sorted by bin (the order of the preceding deposition): a CTA
 // owns TX x TY x TZ bins, stages the cells their stencils reach in shared memory
-// (one 16- or 32-byte vector per cell, zero outside the cuboid, where the weight is
-// zero as well) and interpolates the particles of those bins from there.  The
-// particles of one bin row are one contiguous range of the sorted order.  Same
-// index and weight rules as k_m2p; particles with the sentinel key (outside every
-// bin) are left to k_m2p.
-constexpr int M2P_TX = 32, M2P_TY = 8, M2P_TZ = 4, M2P_THREADS = 256;
+// (one plane per component, zero outside the cuboid, where the weight is zero as
+// well) and interpolates the particles of those bins from there.  A warp's lanes
+// take consecutive particles of a bin row, so each per-component load of a stencil
+// point reads words of neighbouring cells: one shared-memory wavefront, bank
+// conflicts only where the warp spans two bin rows.  The particles of one bin row
+// are one contiguous range of the sorted order.  Same index and weight rules as
+// k_m2p; particles with the sentinel key (outside every bin) are left to k_m2p.
+constexpr int M2P_TX = 32, M2P_TY = 8, M2P_TZ = 8, M2P_THREADS = 256;
 
 template <typename R, int W> __host__ __device__ constexpr size_t m2p_tile_smem() {
-  return (size_t)(M2P_TX + W - 1) * (M2P_TY + W - 1) * (M2P_TZ + W - 1) * 4 * sizeof(R);
+  return (size_t)(M2P_TX + W - 1) * (M2P_TY + W - 1) * (M2P_TZ + W - 1) * 3 * sizeof(R);
 }
 
 template <typename R, int W>
@@ -643,8 +645,9 @@ __global__ void __launch_bounds__(M2P_THREADS) k_m2p_tile(PartGeom<R> g, const R
                                                           R *__restrict__ o) {
   constexpr int off = Stencil<W>::off;
   constexpr int CX = M2P_TX + W - 1, CY = M2P_TY + W - 1, CZ = M2P_TZ + W - 1, NR = M2P_TY * M2P_TZ;
+  constexpr int PLANE = CZ * CY * CX;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R *cells = reinterpret_cast<R *>(smem_raw);  // [CZ][CY][CX][4]
+  R *cells = reinterpret_cast<R *>(smem_raw);  // [3][CZ][CY][CX]
   __shared__ int rs[NR + 1], rg[NR];
   const int x0 = blockIdx.x * M2P_TX, y0 = blockIdx.y * M2P_TY, z0 = blockIdx.z * M2P_TZ;
   const int cx0 = x0 - (W - 1), cy0 = y0 - (W - 1), cz0 = z0 - (W - 1);
@@ -661,12 +664,12 @@ __global__ void __launch_bounds__(M2P_THREADS) k_m2p_tile(PartGeom<R> g, const R
       const int cx = cx0 + xx;
       ok[k] = e < CX * 3 && cx >= 0 && cx < g.ext[0];
       so[k] = cx * 3 + c;
-      dof[k] = e < CX * 3 ? xx * 4 + c : -1;
+      dof[k] = e < CX * 3 ? c * PLANE + xx : -1;
     }
     for (int row = wid; row < CZ * CY; row += nw) {
       const int yy = row % CY, zz = row / CY;
       const int cy = cy0 + yy, cz = cz0 + zz;
-      R *dst = cells + (size_t)row * CX * 4;
+      R *dst = cells + (size_t)row * CX;
       const bool rowin = cy >= 0 && cy < g.ext[1] && cz >= 0 && cz < g.ext[2];
       const R *src = f + (((size_t)(rowin ? cz : 0) * g.ext[1] + (rowin ? cy : 0)) * g.ext[0]) * 3;
       R v[NE];
@@ -677,26 +680,34 @@ __global__ void __launch_bounds__(M2P_THREADS) k_m2p_tile(PartGeom<R> g, const R
         if (dof[k] >= 0) dst[dof[k]] = v[k];
     }
   }
-  // ---- particle ranges of the bin rows
+  // ---- particle ranges of the bin rows (two rows a lane, NR <= 64)
+  static_assert(NR <= 64, "one warp scans the bin rows of a tile");
   if (threadIdx.x < 32) {
-    int len = 0, gs = 0;
-    if (lane < NR) {
-      const int by = y0 + lane % M2P_TY, bz = z0 + lane / M2P_TY;
-      if (by < g.nb[1] && bz < g.nb[2]) {
-        const unsigned rb = (unsigned)g.nb[0] * ((unsigned)by + (unsigned)g.nb[1] * (unsigned)bz);
-        gs = (int)start[rb + x0];
-        len = (int)start[rb + (unsigned)min(x0 + M2P_TX, g.nb[0])] - gs;
+    int len[2] = {0, 0};
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int r = 2 * lane + h;
+      int gs = 0;
+      if (r < NR) {
+        const int by = y0 + r % M2P_TY, bz = z0 + r / M2P_TY;
+        if (by < g.nb[1] && bz < g.nb[2]) {
+          const unsigned rb = (unsigned)g.nb[0] * ((unsigned)by + (unsigned)g.nb[1] * (unsigned)bz);
+          gs = (int)start[rb + x0];
+          len[h] = (int)start[rb + (unsigned)min(x0 + M2P_TX, g.nb[0])] - gs;
+        }
+        rg[r] = gs;
       }
-      rg[lane] = gs;
     }
-    int x = len;
+    int x = len[0] + len[1];
 #pragma unroll
     for (int o2 = 1; o2 < 32; o2 <<= 1) {
       const int y = __shfl_up_sync(0xffffffffu, x, o2);
       if (lane >= o2) x += y;
     }
-    if (lane < NR) rs[lane] = x - len;
-    if (lane == NR - 1) rs[NR] = x;
+    const int ex = x - len[0] - len[1];
+    if (2 * lane < NR) rs[2 * lane] = ex;
+    if (2 * lane + 1 < NR) rs[2 * lane + 1] = ex + len[0];
+    if (lane == 31) rs[NR] = x;
   }
   __syncthreads();
   const int total = rs[NR];
@@ -725,22 +736,20 @@ __global__ void __launch_bounds__(M2P_THREADS) k_m2p_tile(PartGeom<R> g, const R
       // first stencil cell relative to the tile: bin - tile origin
       tb[e] = b - g.blo[e] - (e == 0 ? x0 : e == 1 ? y0 : z0);
     }
-    const R *base = cells + ((tb[2] * CY + tb[1]) * CX + tb[0]) * 4;
+    const R *base = cells + (tb[2] * CY + tb[1]) * CX + tb[0];
     R a0 = R(0), a1 = R(0), a2 = R(0);
 #pragma unroll
     for (int sk = 0; sk < W; sk++)
 #pragma unroll
       for (int sj = 0; sj < W; sj++) {
         const R wjk = w[1][sj] * w[2][sk];
-        const R *row = base + (sk * CY + sj) * CX * 4;
+        const R *row = base + (sk * CY + sj) * CX;
 #pragma unroll
         for (int si = 0; si < W; si++) {
           const R wt = w[0][si] * wjk;
-          R v[4];
-          lds4<R>(row + si * 4, v);
-          a0 += wt * v[0];
-          a1 += wt * v[1];
-          a2 += wt * v[2];
+          a0 += wt * row[si];
+          a1 += wt * row[PLANE + si];
+          a2 += wt * row[2 * PLANE + si];
         }
       }
     o[(size_t)3 * p + 0] = a0;
