@@ -292,6 +292,28 @@ int pmgpu_vortex_stage_dev(pmgpu_plan *plan, int time_order, int itimestage, dou
                            void *d_vel_rk, void *d_dvort_rk, int npart, void *d_part_vel,
                            void *d_part_dvort, int *npart_out, void *stream);
 
+/* Iterative Brinkman penalisation of a solid body, the vortex client's
+ * penalisation_solve (vortex_codes/vortex_penalisation/source/penalisation/
+ * penalisation_solve.f:5-430, one rank), with this library's solves in place of the
+ * client's Poisson solver.  `plan` is the main grid, `penal_plan` a plan of the
+ * penalisation box (a free patch aligned with the main cells, as
+ * flowcases/flowcases_sphere.f:38-89 builds it).  d_solid (1, box cuboid) is the
+ * mask, d_solid_vel (3, box cuboid) the body velocity.  The main velocity is mapped
+ * onto the box; passes of vort_box += relaxation curl(solid (vel_pen - vel_box))
+ * (fd_order 2 or 4) and box solves run until the force increment falls to
+ * `tolerance` of the force (at least one pass, at most max_iter); the box vorticity
+ * is then added to d_vort, the main solve rewrites d_vel (and reprojects d_vort when
+ * `reproject`), and vel_inf is added as the client adds it (its third statement
+ * adds vel_inf[2] to the second component).  Returns the accumulated force
+ * -sum(x x dvort) dx dy dz / dtime, the number of passes and the final residuals
+ * (velocity, force, enstrophy).  Arrays of the plans' precision; synchronises
+ * `stream` once a pass (the loop test is on the host). */
+int pmgpu_penalisation_solve_dev(pmgpu_plan *plan, pmgpu_plan *penal_plan, const void *d_solid,
+                                 const void *d_solid_vel, double relaxation, double tolerance,
+                                 int max_iter, double dtime, int fd_order, int reproject,
+                                 const double vel_inf[3], void *d_vort, void *d_vel, double force[3],
+                                 int *niter, double residuals[3], void *stream);
+
 /* ---- diagnostics (no counterpart in the reference, which has no timers) ---- */
 const char *pmgpu_last_error(void);
 /* number of this library's kernels launched since the last reset */

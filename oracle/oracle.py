@@ -98,6 +98,10 @@ def lib():
         L.pmo_deriv_vorticity.argtypes = [C.POINTER(Topo), C.c_int, C.c_double, dp, dp, dp]
         L.pmo_particles_advance.argtypes = [C.POINTER(Patch), C.POINTER(Topo), C.c_int, C.c_int, C.c_double,
                                             C.c_int, dp, dp, dp, dp, dp, dp, C.c_int, ip]
+        L.pmo_mesh_map.argtypes = [C.POINTER(Topo), C.POINTER(Topo), C.c_int, dp, dp, C.c_int, C.c_int]
+        L.pmo_penalisation_solve.argtypes = [C.POINTER(Patch), C.POINTER(Topo), C.POINTER(Params),
+                                             C.POINTER(Patch), C.POINTER(Topo), dp, dp, C.c_double, C.c_double,
+                                             C.c_int, C.c_double, C.c_int, C.c_int, dp, dp, dp, dp, ip, dp]
         L.pmo_si.argtypes = [C.c_double]
         L.pmo_si.restype = C.c_double
         _lib = L
@@ -261,3 +265,23 @@ def particles_advance(patch, t, time_order, stage, dtime, pos, vort, vel, dvort,
                                        int(bool(euler_vort)), _p(pos), _p(vort), _p(vel), _p(dvort), _p(vel_rk),
                                        _p(dvort_rk), pos.shape[0], C.byref(n))
     return ierr, n.value
+
+
+def mesh_map(ts, tr, src, dst, op=0, map_ghost=True):
+    """pmlib_mesh_map of one rank: dst (= or += ) src on the intersection of the cuboids."""
+    return lib().pmo_mesh_map(C.byref(ts), C.byref(tr), src.shape[-1], _p(src), _p(dst), int(op), int(map_ghost))
+
+
+def penalisation_solve(pa, t, par, pp, tp, solid, solid_vel, vort, vel, relax=1.0, tol=1e-3, max_iter=20,
+                       dtime=0.01, fd_order=4, reproject=False, vel_inf=(0.0, 0.0, 0.0)):
+    """The vortex client's Brinkman penalisation; vort and vel (main mesh) updated in
+    place.  Returns (ierr, force, passes, (residual_vel, residual_force, residual_enst))."""
+    force = np.zeros(3)
+    res = np.zeros(3)
+    n = C.c_int(0)
+    vi = np.ascontiguousarray(vel_inf, dtype=np.float64)
+    ierr = lib().pmo_penalisation_solve(C.byref(pa), C.byref(t), C.byref(par), C.byref(pp), C.byref(tp), _p(solid),
+                                        _p(solid_vel), float(relax), float(tol), int(max_iter), float(dtime),
+                                        int(fd_order), int(bool(reproject)), _p(vi), _p(vort), _p(vel), _p(force),
+                                        C.byref(n), _p(res))
+    return ierr, force, n.value, tuple(res)

@@ -1379,3 +1379,219 @@ int pmo_particles_advance(const pmo_patch *pa, pmo_topo *t, int time_order, int 
   *npart_out = n;
   return 0;
 }
+
+/* ------------------------------------------------------------------------- */
+/* Index ranges of source/mesh/pmlib_mesh_map.f:85-176 for one axis (one rank on
+ * each side): first sent / received index (1-based, ghosts negative) and count.
+ * Returns -1 when the boxes do not intersect or the case is not recognised. */
+int pmo_mesh_map_range(const pmo_topo *s, const pmo_topo *r, int i, int map_ghost, int *imin_s,
+                       int *imin_r, int *count) {
+  const double dx = r->dx[i];
+  const int ds = nint((r->xmin[i] - s->xmin[i]) / dx); /* receiver start relative to sender */
+  const int bcs_lo = s->bound_cond[2 * i], bcs_hi = s->bound_cond[2 * i + 1];
+  const int bcr_lo = r->bound_cond[2 * i], bcr_hi = r->bound_cond[2 * i + 1];
+  const int ngs_lo = s->nghost[2 * i], ngs_hi = s->nghost[2 * i + 1];
+  const int ngr_lo = r->nghost[2 * i], ngr_hi = r->nghost[2 * i + 1];
+  int ng, smin, rmin, smax, rmax;
+  if (nint((r->xmax[i] - s->xmin[i]) / dx) <= 0 || nint((s->xmax[i] - r->xmin[i]) / dx) <= 0) return -1;
+  if (ds == 0) {
+    ng = (map_ghost && bcr_lo == 0) ? (ngr_lo < ngs_lo ? ngr_lo : ngs_lo) : 0;
+    smin = 1 - ng; rmin = 1 - ng;
+  } else if (ds < 0) { /* sender starts inside the receiver */
+    ng = 0;
+    if (map_ghost && bcs_lo == 0) { ng = -ds + ngr_lo; if (ngs_lo < ng) ng = ngs_lo; }
+    smin = 1 - ng; rmin = 1 - ds - ng;
+  } else {
+    ng = 0;
+    if (map_ghost && bcr_lo == 0) { ng = ds + ngs_lo; if (ngr_lo < ng) ng = ngr_lo; }
+    smin = 1 + ds - ng; rmin = 1 - ng;
+  }
+  const int de = nint((r->xmax[i] - s->xmax[i]) / dx);
+  if (de == 0) {
+    ng = (map_ghost && bcr_hi == 0) ? (ngr_hi < ngs_hi ? ngr_hi : ngs_hi) : 0;
+    smax = s->ncell[i] + ng; rmax = r->ncell[i] + ng;
+  } else if (de > 0) { /* receiver reaches beyond the sender */
+    ng = 0;
+    if (map_ghost && bcs_hi == 0) { ng = de + ngr_hi; if (ngs_hi < ng) ng = ngs_hi; }
+    smax = s->ncell[i] + ng; rmax = nint((s->xmax[i] - r->xmin[i]) / dx) + ng;
+  } else {
+    ng = 0;
+    if (map_ghost && bcr_hi == 0) { ng = -de + ngs_hi; if (ngr_hi < ng) ng = ngr_hi; }
+    smax = nint((r->xmax[i] - s->xmin[i]) / dx) + ng; rmax = r->ncell[i] + ng;
+  }
+  if (smax - smin != rmax - rmin || smax < smin) return -1;
+  *imin_s = smin; *imin_r = rmin; *count = smax - smin + 1;
+  return 0;
+}
+
+/* pmlib_mesh_map + pack / unpack of one rank: dst (op 0: =, op 1: +=) the sender's
+ * values on the intersection of the two cuboids (with ghosts when map_ghost) */
+int pmo_mesh_map(const pmo_topo *s, const pmo_topo *r, int nv, const double *src, double *dst, int op,
+                 int map_ghost) {
+  int ms[3], mr[3], n[3];
+  for (int i = 0; i < 3; i++)
+    if (pmo_mesh_map_range(s, r, i, map_ghost, &ms[i], &mr[i], &n[i])) {
+      pm_write("pmlib_mesh_map", "Failed to identify intersection indexes");
+      return -1;
+    }
+  for (int k = 0; k < n[2]; k++)
+    for (int j = 0; j < n[1]; j++)
+      for (int i = 0; i < n[0]; i++)
+        for (int c = 0; c < nv; c++) {
+          const double v = src[midx(s, nv, c, ms[0] + i, ms[1] + j, ms[2] + k)];
+          double *d = &dst[midx(r, nv, c, mr[0] + i, mr[1] + j, mr[2] + k)];
+          *d = op ? *d + v : v;
+        }
+  return 0;
+}
+
+/* Iterative Brinkman penalisation of the vortex client
+ * (vortex_codes/vortex_penalisation/source/penalisation/penalisation_solve.f:5-430,
+ * one rank, the client's Poisson solver replaced by this restatement's solve):
+ *   vel_pen = solid_vel - vel (the main velocity mapped onto the penalisation box),
+ *   vel = solid vel_pen; then until |dforce| / |force| <= tolerance (at least one
+ *   pass, at most max_iter): vort += relax curl(vel) (FD 2 / 4, interior),
+ *   vel = solve(vort) on the box, vel = solid (vel_pen - vel), with the force
+ *   increment dforce = -sum(x x dvort) dx dy dz / dt; then the box vorticity is
+ *   added to the main vorticity, the main ghosts mapped, the main solve run (with
+ *   reprojection when asked) and vel_inf added as the client adds it (:415-419:
+ *   its third statement adds vel_inf(3) to the second component).  force, the
+ *   number of passes and the final residuals (velocity, force, enstrophy) are
+ *   returned for the caller's drag history. */
+int pmo_penalisation_solve(const pmo_patch *pa, const pmo_topo *t, const pmo_params *par, const pmo_patch *pp,
+                           const pmo_topo *tp, const double *solid, const double *solid_vel, double relax,
+                           double tol, int max_iter, double dtime, int fd_order, int reproject,
+                           const double vel_inf[3], double *vort, double *vel, double force[3], int *niter,
+                           double resid[3]) {
+  const char *caller = "penalisation";
+  if (fd_order != 2 && fd_order != 4) {
+    pm_write("pmlib_parameters_check", "pmlib_fd_order is incorrectly set.");
+    return -1;
+  }
+  int ep[3], em[3];
+  pmo_topo_extent(tp, ep);
+  pmo_topo_extent(t, em);
+  const size_t np = (size_t)ep[0] * ep[1] * ep[2], nm = (size_t)em[0] * em[1] * em[2];
+  double *vel_pen = (double *)calloc(3 * np, sizeof(double));
+  double *pvel = (double *)calloc(3 * np, sizeof(double));
+  double *pvort = (double *)calloc(3 * np, sizeof(double));
+  int Mp[3], nkp, Mm[3], nkm;
+  pmo_kernel_dims(pp, par, Mp, &nkp);
+  pmo_kernel_dims(pa, par, Mm, &nkm);
+  double *pkp = (double *)malloc(sizeof(double) * 2 * (size_t)nkp * Mp[0] * Mp[1] * Mp[2]);
+  double *pkm = (double *)malloc(sizeof(double) * 2 * (size_t)nkm * Mm[0] * Mm[1] * Mm[2]);
+  int rc = -1;
+  if (!vel_pen || !pvel || !pvort || !pkp || !pkm) { pm_write(caller, "out of memory."); goto done; }
+  if (pmo_poisson_setup(pp, par, pkp) || pmo_poisson_setup(pa, par, pkm)) goto done;
+  /* :61-77 main velocity onto the box (cleared), ghost map of a free box: nothing */
+  if (pmo_mesh_map(t, tp, 3, vel, vel_pen, 0, 1)) goto done;
+  double sum_vel_pen = 0.0;
+  for (size_t q = 0; q < np; q++) {  /* :84-107 over the box with its ghosts */
+    for (int c = 0; c < 3; c++) {
+      vel_pen[3 * q + c] = solid_vel[3 * q + c] - vel_pen[3 * q + c];
+      pvel[3 * q + c] = solid[q] * vel_pen[3 * q + c];
+    }
+    sum_vel_pen += sqrt(pvel[3 * q] * pvel[3 * q] + pvel[3 * q + 1] * pvel[3 * q + 1] + pvel[3 * q + 2] * pvel[3 * q + 2]);
+  }
+  const double dx = tp->dx[0], dy = tp->dx[1], dz = tp->dx[2];
+  const double c_1_2dx2 = 1.0 / (2.0 * dx), c_1_2dy2 = 1.0 / (2.0 * dy), c_1_2dz2 = 1.0 / (2.0 * dz);
+  const double c_1_dt = 1.0 / dtime, c1 = 1.0 / 6.0, c2 = 4.0 / 3.0;
+  double residual_force = 0.0, residual_vel = 0.0, residual_enst = 0.0;
+  int npen = 0;
+  for (int c = 0; c < 3; c++) force[c] = 0.0;
+  while ((residual_force > tol && npen < max_iter) || npen == 0) {
+    npen++;
+    double sdf[3] = {0.0, 0.0, 0.0}, res_enst = 0.0, sum_enst_pen = 0.0;
+    for (int k = 1; k <= tp->ncell[2]; k++) {
+      const double pz = tp->xmin[2] + ((double)(k - 1) + 0.5) * dz;
+      for (int j = 1; j <= tp->ncell[1]; j++) {
+        const double py = tp->xmin[1] + ((double)(j - 1) + 0.5) * dy;
+        for (int i = 1; i <= tp->ncell[0]; i++) {
+          const double px = tp->xmin[0] + ((double)(i - 1) + 0.5) * dx;
+#define U(c, ii, jj, kk) pvel[midx(tp, 3, c, ii, jj, kk)]
+          double dvdx, dwdx, dudy, dwdy, dudz, dvdz;
+          if (fd_order == 2) {
+            dvdx = (-1.0 * U(1, i - 1, j, k) + 1.0 * U(1, i + 1, j, k)) * c_1_2dx2;
+            dwdx = (-1.0 * U(2, i - 1, j, k) + 1.0 * U(2, i + 1, j, k)) * c_1_2dx2;
+            dudy = (-1.0 * U(0, i, j - 1, k) + 1.0 * U(0, i, j + 1, k)) * c_1_2dy2;
+            dwdy = (-1.0 * U(2, i, j - 1, k) + 1.0 * U(2, i, j + 1, k)) * c_1_2dy2;
+            dudz = (-1.0 * U(0, i, j, k - 1) + 1.0 * U(0, i, j, k + 1)) * c_1_2dz2;
+            dvdz = (-1.0 * U(1, i, j, k - 1) + 1.0 * U(1, i, j, k + 1)) * c_1_2dz2;
+          } else {
+            dvdx = (c1 * U(1, i - 2, j, k) - c2 * U(1, i - 1, j, k) + c2 * U(1, i + 1, j, k) - c1 * U(1, i + 2, j, k)) * c_1_2dx2;
+            dwdx = (c1 * U(2, i - 2, j, k) - c2 * U(2, i - 1, j, k) + c2 * U(2, i + 1, j, k) - c1 * U(2, i + 2, j, k)) * c_1_2dx2;
+            dudy = (c1 * U(0, i, j - 2, k) - c2 * U(0, i, j - 1, k) + c2 * U(0, i, j + 1, k) - c1 * U(0, i, j + 2, k)) * c_1_2dy2;
+            dwdy = (c1 * U(2, i, j - 2, k) - c2 * U(2, i, j - 1, k) + c2 * U(2, i, j + 1, k) - c1 * U(2, i, j + 2, k)) * c_1_2dy2;
+            dudz = (c1 * U(0, i, j, k - 2) - c2 * U(0, i, j, k - 1) + c2 * U(0, i, j, k + 1) - c1 * U(0, i, j, k + 2)) * c_1_2dz2;
+            dvdz = (c1 * U(1, i, j, k - 2) - c2 * U(1, i, j, k - 1) + c2 * U(1, i, j, k + 1) - c1 * U(1, i, j, k + 2)) * c_1_2dz2;
+          }
+#undef U
+          const double d0 = relax * (dwdy - dvdz), d1 = relax * (dudz - dwdx), d2 = relax * (dvdx - dudy);
+          double *w = &pvort[midx(tp, 3, 0, i, j, k)];
+          w[0] += d0; w[1] += d1; w[2] += d2;
+          sdf[0] += py * d2 - pz * d1;
+          sdf[1] += pz * d0 - px * d2;
+          sdf[2] += px * d1 - py * d0;
+          res_enst += d0 * d0 + d1 * d1 + d2 * d2;
+          sum_enst_pen += w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+        }
+      }
+    }
+    double *vv = (double *)malloc(sizeof(double) * 3 * np);
+    double *wc = (double *)malloc(sizeof(double) * 3 * np);
+    double *dum = NULL;
+    if (!vv || !wc) { free(vv); free(wc); pm_write(caller, "out of memory."); goto done; }
+    memcpy(wc, pvort, sizeof(double) * 3 * np);
+    int e = pmo_poisson_solve(pp, tp, par, pkp, wc, vv, dum, 0, 0, 0);
+    free(wc);
+    if (e) { free(vv); goto done; }
+    double res_vel = 0.0;
+    for (size_t q = 0; q < np; q++) {
+      for (int c = 0; c < 3; c++) pvel[3 * q + c] = solid[q] * (vel_pen[3 * q + c] - vv[3 * q + c]);
+      res_vel += sqrt(pvel[3 * q] * pvel[3 * q] + pvel[3 * q + 1] * pvel[3 * q + 1] + pvel[3 * q + 2] * pvel[3 * q + 2]);
+    }
+    free(vv);
+    double df[3];
+    for (int c = 0; c < 3; c++) {
+      df[c] = -sdf[c] * dx * dy * dz * c_1_dt;
+      force[c] = force[c] + df[c];
+    }
+    residual_enst = res_enst / sum_enst_pen;
+    residual_vel = res_vel / sum_vel_pen;
+    residual_force = sqrt(df[0] * df[0] + df[1] * df[1] + df[2] * df[2]) /
+                     sqrt(force[0] * force[0] + force[1] * force[1] + force[2] * force[2]);
+  }
+  /* :345-360 box vorticity added to the main vorticity, main ghost map */
+  if (pmo_mesh_map(tp, t, 3, pvort, vort, 1, 1)) goto done;
+  {
+    cbox b;
+    int lo[3], n[3];
+    cuboid_region(t, lo, n);
+    b = cb_alloc(lo, n, 3);
+    for (size_t q = 0; q < 3 * nm; q++) { b.d[2 * q] = vort[q]; b.d[2 * q + 1] = 0.0; }
+    cb_ghost_fill(&b, t);
+    for (size_t q = 0; q < 3 * nm; q++) vort[q] = b.d[2 * q];
+    cb_free(&b);
+  }
+  /* :364-406 main solve (the vorticity comes back reprojected when asked) */
+  {
+    double *vv = (double *)malloc(sizeof(double) * 3 * nm);
+    if (!vv) { pm_write(caller, "out of memory."); goto done; }
+    if (pmo_poisson_solve(pa, t, par, pkm, vort, vv, NULL, 0, reproject ? 1 : 0, 0)) { free(vv); goto done; }
+    for (size_t q = 0; q < nm; q++) {  /* :411-419 */
+      vel[3 * q] = vv[3 * q] + vel_inf[0];
+      vel[3 * q + 1] = vv[3 * q + 1] + vel_inf[1];
+      vel[3 * q + 1] = vel[3 * q + 1] + vel_inf[2];
+      vel[3 * q + 2] = vv[3 * q + 2];
+    }
+    free(vv);
+  }
+  *niter = npen;
+  resid[0] = residual_vel;
+  resid[1] = residual_force;
+  resid[2] = residual_enst;
+  rc = 0;
+done:
+  free(vel_pen); free(pvel); free(pvort); free(pkp); free(pkm);
+  return rc;
+}

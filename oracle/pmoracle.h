@@ -102,6 +102,20 @@ int pmo_particles_advance(const pmo_patch *patch, pmo_topo *topo, int time_order
                           int euler_vort, double *pos, double *vort, const double *vel, const double *dvort,
                           double *vel_rk, double *dvort_rk, int npart, int *npart_out);
 
+/* pmlib_mesh_map of one rank: index ranges per axis, and the mapped copy / add */
+int pmo_mesh_map_range(const pmo_topo *s, const pmo_topo *r, int axis, int map_ghost, int *imin_s,
+                       int *imin_r, int *count);
+int pmo_mesh_map(const pmo_topo *s, const pmo_topo *r, int nv, const double *src, double *dst, int op,
+                 int map_ghost);
+
+/* the vortex client's iterative Brinkman penalisation on a box (pp, tp) inside the
+ * main grid (pa, t): main vort and vel updated in place; force, passes, residuals */
+int pmo_penalisation_solve(const pmo_patch *pa, const pmo_topo *t, const pmo_params *par, const pmo_patch *pp,
+                           const pmo_topo *tp, const double *solid, const double *solid_vel, double relax,
+                           double tol, int max_iter, double dtime, int fd_order, int reproject,
+                           const double vel_inf[3], double *vort, double *vel, double force[3], int *niter,
+                           double resid[3]);
+
 /* helper: sine integral used by the order-100 kernel */
 double pmo_si(double x);
 

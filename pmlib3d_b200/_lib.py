@@ -23,7 +23,7 @@ EXPORTS = (
     "pmgpu_fft_tune", "pmgpu_fft_tuned", "pmgpu_particle_diagnostics",
     "pmgpu_deriv_vorticity", "pmgpu_deriv_vorticity_f32", "pmgpu_deriv_vorticity_dev",
     "pmgpu_particles_advance", "pmgpu_particles_advance_f32", "pmgpu_particles_advance_dev",
-    "pmgpu_vortex_stage_dev", "pmgpu_fft_set_schedule", "pmgpu_step_many",
+    "pmgpu_vortex_stage_dev", "pmgpu_fft_set_schedule", "pmgpu_step_many", "pmgpu_penalisation_solve_dev",
 )
 
 
@@ -98,6 +98,8 @@ def lib():
         "pmgpu_fft_tuned": [C.c_int, ip, ip, ip, ip, ip, dp],
         "pmgpu_fft_set_schedule": [C.c_int, C.c_int, C.c_int, ip, C.c_int],
         "pmgpu_step_many": [vp, C.c_int, C.POINTER(vp), C.POINTER(vp), ip, C.POINTER(vp)],
+        "pmgpu_penalisation_solve_dev": [vp, vp, vp, vp, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
+                                         C.c_int, dp, vp, vp, dp, ip, dp, vp],
         "pmgpu_particle_diagnostics": [dp, vp, vp, vp, C.c_int, C.c_int, dp, vp],
         "pmgpu_deriv_vorticity": [TP, C.c_int, C.c_double, dp, dp, dp],
         "pmgpu_deriv_vorticity_f32": [TP, C.c_int, C.c_double, fp, fp, fp],

@@ -10,6 +10,7 @@
 #include "host.h"
 #include "particles.cuh"
 #include "advance.cuh"
+#include "penal.cuh"
 #include "solve.cuh"
 
 #include <algorithm>
@@ -528,6 +529,7 @@ struct Scratch {
   DevBuf a, b, c, d, e, f, g, h;
   DevBuf diag;  // diagnostics partial sums
   DevBuf adv_code, adv_stats, adv_cnt, adv_start, adv_ord, adv_tmp;  // particle advance and map
+  DevBuf pen_part, pen_out;                                           // penalisation sums
 };
 static Scratch &scratch() {
   static Scratch s;
@@ -2524,4 +2526,222 @@ int pmgpu_vortex_stage_dev(pmgpu_plan *plan, int time_order, int itimestage, dou
   return vortex_stage<float>(plan, time_order, itimestage, dtime, euler_vort, fd_order, visc, (float *)d_pos,
                              (float *)d_vort, (float *)d_vel_rk, (float *)d_dvort_rk, npart, (float *)d_part_vel,
                              (float *)d_part_dvort, npart_out, st);
+}
+
+// ------------------------------------------------------------------ Brinkman penalisation
+static int nint_d(double x) { return (int)lround(x); }
+
+// index ranges of source/mesh/pmlib_mesh_map.f:85-176 (one rank), as array offsets
+static int mesh_map_box(const pmgpu_topo *s, const pmgpu_topo *r, int map_ghost, MapBox &m, const char *caller) {
+  for (int i = 0; i < 3; i++) {
+    const double dx = r->dx[i];
+    if (dx != s->dx[i]) {
+      set_error("pmlib_mesh_map", "Mesh cell size does not coinside.");
+      return -1;
+    }
+    if (nint_d((r->xmax[i] - s->xmin[i]) / dx) <= 0 || nint_d((s->xmax[i] - r->xmin[i]) / dx) <= 0) {
+      set_error(caller, "The penalisation box does not intersect the grid.");
+      return -1;
+    }
+    const int ds = nint_d((r->xmin[i] - s->xmin[i]) / dx);
+    const int ngs_lo = s->nghost[2 * i], ngs_hi = s->nghost[2 * i + 1];
+    const int ngr_lo = r->nghost[2 * i], ngr_hi = r->nghost[2 * i + 1];
+    int ng, smin, rmin, smax, rmax;
+    if (ds == 0) {
+      ng = (map_ghost && r->bound_cond[2 * i] == 0) ? std::min(ngr_lo, ngs_lo) : 0;
+      smin = 1 - ng;
+      rmin = 1 - ng;
+    } else if (ds < 0) {  // the sender starts inside the receiver
+      ng = (map_ghost && s->bound_cond[2 * i] == 0) ? std::min(ngs_lo, -ds + ngr_lo) : 0;
+      smin = 1 - ng;
+      rmin = 1 - ds - ng;
+    } else {
+      ng = (map_ghost && r->bound_cond[2 * i] == 0) ? std::min(ngr_lo, ds + ngs_lo) : 0;
+      smin = 1 + ds - ng;
+      rmin = 1 - ng;
+    }
+    const int de = nint_d((r->xmax[i] - s->xmax[i]) / dx);
+    if (de == 0) {
+      ng = (map_ghost && r->bound_cond[2 * i + 1] == 0) ? std::min(ngr_hi, ngs_hi) : 0;
+      smax = s->ncell[i] + ng;
+      rmax = r->ncell[i] + ng;
+    } else if (de > 0) {  // the receiver reaches beyond the sender
+      ng = (map_ghost && s->bound_cond[2 * i + 1] == 0) ? std::min(ngs_hi, de + ngr_hi) : 0;
+      smax = s->ncell[i] + ng;
+      rmax = nint_d((s->xmax[i] - r->xmin[i]) / dx) + ng;
+    } else {
+      ng = (map_ghost && r->bound_cond[2 * i + 1] == 0) ? std::min(ngr_hi, -de + ngs_hi) : 0;
+      smax = nint_d((r->xmax[i] - s->xmin[i]) / dx) + ng;
+      rmax = r->ncell[i] + ng;
+    }
+    if (smax - smin != rmax - rmin || smax < smin) {
+      set_error("pmlib_mesh_map", "Number of sended and recieved cells does not correspond");
+      return -1;
+    }
+    m.s0[i] = smin - 1 + s->nghost[2 * i];
+    m.r0[i] = rmin - 1 + r->nghost[2 * i];
+    m.n[i] = smax - smin + 1;
+    m.es[i] = s->ncell[i] + s->nghost[2 * i] + s->nghost[2 * i + 1];
+    m.er[i] = r->ncell[i] + r->nghost[2 * i] + r->nghost[2 * i + 1];
+    if (m.s0[i] < 0 || m.r0[i] < 0 || m.s0[i] + m.n[i] > m.es[i] || m.r0[i] + m.n[i] > m.er[i]) {
+      set_error("pmlib_mesh_map", "Sending or receiving index out of range");
+      return -1;
+    }
+  }
+  return 0;
+}
+
+template <typename R>
+static int launch_mesh_map(const MapBox &m, const R *src, R *dst, int op, cudaStream_t st, const char *caller) {
+  const long long total = (long long)m.n[0] * m.n[1] * m.n[2];
+  if (total <= 0) return 0;
+  { KTimer kt_(KC_OTHER, st);
+    k_mesh_map<R><<<(unsigned)std::min<long long>((total + 255) / 256, 148 * 16), 256, 0, st>>>(m, 3, src, dst, op); }
+  PM_LAUNCHED();
+  CKL(caller);
+  return 0;
+}
+
+// The vortex client's iterative Brinkman penalisation (vortex_codes/vortex_penalisation/
+// source/penalisation/penalisation_solve.f:5-430, one rank) on device arrays: the box
+// is the penalisation plan's cuboid, the box fields live in that plan's mesh buffers
+// (vel_pen, vel, vort), and its Poisson solves are that plan's solves.
+template <typename R>
+static int run_penal(pmgpu_plan *pm, pmgpu_plan *pp, const R *solid, const R *svel, double relax, double tol,
+                     int max_iter, double dtime, int fd_order, int reproject, const double vel_inf[3], R *vort,
+                     R *vel, double force[3], int *niter, double resid[3], cudaStream_t st) {
+  const char *caller = "penalisation";
+  if (fd_order != 2 && fd_order != 4) {
+    set_error("pmlib_parameters_check", "pmlib_fd_order is incorrectly set.");
+    return -1;
+  }
+  for (int e = 0; e < 3; e++)
+    if (pp->topo.nghost[2 * e] < fd_order / 2 || pp->topo.nghost[2 * e + 1] < fd_order / 2) {
+      set_error(caller, "Too few ghost cells in the penalisation box for the finite differences.");
+      return -1;
+    }
+  MapBox to_box, to_main;
+  if (mesh_map_box(&pm->topo, &pp->topo, 1, to_box, caller) || mesh_map_box(&pp->topo, &pm->topo, 1, to_main, caller))
+    return -1;
+  const size_t npp = mesh_points(&pp->topo), npm = mesh_points(&pm->topo);
+  if (pp->mesh_a.ensure(sizeof(R) * 3 * npp, caller) || pp->mesh_u.ensure(sizeof(R) * 3 * npp, caller) ||
+      pp->mesh_w.ensure(sizeof(R) * 3 * npp, caller))
+    return -1;
+  Scratch &sc = scratch();
+  if (sc.pen_part.ensure(sizeof(double) * PEN_BLOCKS * PEN_NV, caller) || sc.pen_out.ensure(sizeof(double) * 8, caller))
+    return -1;
+  R *vel_pen = pp->mesh_a.as<R>(), *pvel = pp->mesh_u.as<R>(), *pvort = pp->mesh_w.as<R>();
+  double *part = sc.pen_part.as<double>(), *dout = sc.pen_out.as<double>();
+  auto sums = [&](int nv, double *h) -> int {
+    k_pen_final<<<1, 32 * nv, 0, st>>>(part, PEN_BLOCKS, nv, dout);
+    PM_LAUNCHED();
+    CK(cudaMemcpyAsync(h, dout, sizeof(double) * nv, cudaMemcpyDeviceToHost, st), caller);
+    CK(cudaStreamSynchronize(st), caller);
+    return 0;
+  };
+  // :61-107 main velocity onto the cleared box; vel_pen = solid_vel - vel; vel = solid vel_pen
+  CK(cudaMemsetAsync(vel_pen, 0, sizeof(R) * 3 * npp, st), caller);
+  CK(cudaMemsetAsync(pvort, 0, sizeof(R) * 3 * npp, st), caller);
+  if (launch_mesh_map<R>(to_box, vel, vel_pen, 0, st, caller)) return -1;
+  { KTimer kt_(KC_OTHER, st);
+    k_pen_init<R><<<PEN_BLOCKS, PEN_THREADS, 0, st>>>((long long)npp, solid, svel, vel_pen, pvel, part); }
+  PM_LAUNCHED();
+  CKL(caller);
+  double sum_vel_pen = 0.0;
+  if (sums(1, &sum_vel_pen)) return -1;
+  PenGeom<R> g;
+  for (int e = 0; e < 3; e++) {
+    g.ext[e] = pp->topo.ncell[e] + pp->topo.nghost[2 * e] + pp->topo.nghost[2 * e + 1];
+    g.ngl[e] = pp->topo.nghost[2 * e];
+    g.nc[e] = pp->topo.ncell[e];
+    g.c_1_2dx[e] = R(1) / (R(2) * (R)pp->topo.dx[e]);
+    g.xmin[e] = (R)pp->topo.xmin[e];
+    g.dx[e] = (R)pp->topo.dx[e];
+  }
+  g.relax = (R)relax;
+  const double dvol = pp->topo.dx[0] * pp->topo.dx[1] * pp->topo.dx[2], c_1_dt = 1.0 / dtime;
+  double residual_force = 0.0, residual_vel = 0.0, residual_enst = 0.0;
+  int npen = 0;
+  for (int c = 0; c < 3; c++) force[c] = 0.0;
+  while ((residual_force > tol && npen < max_iter) || npen == 0) {
+    npen++;
+    { KTimer kt_(KC_OTHER, st);
+      if (fd_order == 2) k_pen_curl<R, 2><<<PEN_BLOCKS, PEN_THREADS, 0, st>>>(g, pvel, pvort, part);
+      else k_pen_curl<R, 4><<<PEN_BLOCKS, PEN_THREADS, 0, st>>>(g, pvel, pvort, part); }
+    PM_LAUNCHED();
+    CKL(caller);
+    double h[PEN_NV];
+    if (sums(PEN_NV, h)) return -1;
+    if (run_solve<R>(pp, pvort, pvel, nullptr, nullptr, 0, 0, 0, st, caller)) return -1;
+    { KTimer kt_(KC_OTHER, st);
+      k_pen_vel<R><<<PEN_BLOCKS, PEN_THREADS, 0, st>>>((long long)npp, solid, vel_pen, pvel, part); }
+    PM_LAUNCHED();
+    CKL(caller);
+    double res_vel = 0.0;
+    if (sums(1, &res_vel)) return -1;
+    double df[3];
+    for (int c = 0; c < 3; c++) {
+      df[c] = -h[c] * dvol * c_1_dt;
+      force[c] = force[c] + df[c];
+    }
+    residual_enst = h[3] / h[4];
+    residual_vel = res_vel / sum_vel_pen;
+    residual_force = sqrt(df[0] * df[0] + df[1] * df[1] + df[2] * df[2]) /
+                     sqrt(force[0] * force[0] + force[1] * force[1] + force[2] * force[2]);
+  }
+  // :345-360 box vorticity added to the main vorticity, then the main ghost map
+  if (launch_mesh_map<R>(to_main, pvort, vort, 1, st, caller)) return -1;
+  const pmgpu_topo *t = &pm->topo;
+  for (int d = 0; d < 3; d++) {
+    if (t->bound_cond[2 * d] == 0 || t->bound_cond[2 * d + 1] == 0) continue;
+    const int ext[3] = {to_main.er[0], to_main.er[1], to_main.er[2]};
+    const int S = t->nghost[2 * d] + t->nghost[2 * d + 1];
+    const long long total = (long long)S * ext[(d + 1) % 3] * ext[(d + 2) % 3];
+    const int nblk = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+    { KTimer kt_(KC_GFILL, st);
+      k_ghost_fill<R><<<std::max(nblk, 1), 256, 0, st>>>(vort, ext[0], ext[1], ext[2], 3, d, t->ncell[d],
+                                                         t->nghost[2 * d], t->nghost[2 * d + 1]); }
+    PM_LAUNCHED();
+    CKL(caller);
+  }
+  // :364-419 main solve (vorticity reprojected when asked), free-stream velocity
+  if (run_solve<R>(pm, vort, vel, reproject ? vort : nullptr, nullptr, 0, reproject ? 1 : 0, 0, st, caller))
+    return -1;
+  { KTimer kt_(KC_OTHER, st);
+    k_add_vel_inf<R><<<(unsigned)std::min<size_t>((npm + 255) / 256, 148 * 16), 256, 0, st>>>(
+        (long long)npm, vel, (R)vel_inf[0], (R)vel_inf[1], (R)vel_inf[2]); }
+  PM_LAUNCHED();
+  CKL(caller);
+  CK(cudaStreamSynchronize(st), caller);
+  *niter = npen;
+  resid[0] = residual_vel;
+  resid[1] = residual_force;
+  resid[2] = residual_enst;
+  return 0;
+}
+
+int pmgpu_penalisation_solve_dev(pmgpu_plan *plan, pmgpu_plan *penal_plan, const void *d_solid,
+                                 const void *d_solid_vel, double relaxation, double tolerance, int max_iter,
+                                 double dtime, int fd_order, int reproject, const double vel_inf[3], void *d_vort,
+                                 void *d_vel, double force[3], int *niter, double residuals[3], void *stream) {
+  const char *caller = "penalisation";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!plan || !penal_plan || !d_solid || !d_solid_vel || !vel_inf || !d_vort || !d_vel || !force || !niter ||
+      !residuals || max_iter < 1 || !(dtime != 0.0)) {
+    set_error(caller, "missing or invalid argument.");
+    return -1;
+  }
+  if (plan->prec != penal_plan->prec) {
+    set_error(caller, "the grid and the penalisation box plans differ in precision.");
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->prec == PMGPU_FP64)
+    return run_penal<double>(plan, penal_plan, (const double *)d_solid, (const double *)d_solid_vel, relaxation,
+                             tolerance, max_iter, dtime, fd_order, reproject, vel_inf, (double *)d_vort,
+                             (double *)d_vel, force, niter, residuals, st);
+  return run_penal<float>(plan, penal_plan, (const float *)d_solid, (const float *)d_solid_vel, relaxation, tolerance,
+                          max_iter, dtime, fd_order, reproject, vel_inf, (float *)d_vort, (float *)d_vel, force,
+                          niter, residuals, st);
 }

@@ -395,3 +395,23 @@ def vortex_stage_dev(plan: Plan, time_order: int, itimestage: int, dtime: float,
                                         C.c_void_p(d_part_vel), C.c_void_p(d_part_dvort), C.byref(n),
                                         C.c_void_p(stream or None))
     return ierr, n.value
+
+
+def penalisation_solve_dev(plan: Plan, penal_plan: Plan, d_solid: int, d_solid_vel: int, d_vort: int, d_vel: int,
+                           relaxation: float = 1.0, tolerance: float = 1e-3, max_iter: int = 20, dtime: float = 0.01,
+                           fd_order: int = 4, reproject: bool = False, vel_inf=(0.0, 0.0, 0.0), stream: int = 0):
+    """The vortex client's iterative Brinkman penalisation on device arrays (main
+    vorticity and velocity updated in place).  Returns (force, passes, (residual_vel,
+    residual_force, residual_enst)); raises on error."""
+    force = (C.c_double * 3)()
+    res = (C.c_double * 3)()
+    n = C.c_int(0)
+    vi = (C.c_double * 3)(*vel_inf)
+    rc = lib().pmgpu_penalisation_solve_dev(plan.handle, penal_plan.handle, C.c_void_p(d_solid),
+                                            C.c_void_p(d_solid_vel), float(relaxation), float(tolerance),
+                                            int(max_iter), float(dtime), int(fd_order), int(bool(reproject)), vi,
+                                            C.c_void_p(d_vort), C.c_void_p(d_vel), force, C.byref(n), res,
+                                            C.c_void_p(stream or None))
+    if rc != 0:
+        raise RuntimeError(last_error())
+    return list(force), n.value, tuple(res)

@@ -205,3 +205,92 @@ def test_vortex_stage_matches_oracle_pieces(name, xmin, xmax, dx, bc, ng):
     assert mg == mo
     for i, j in ((0, 0), (1, 1), (2, 4), (3, 5)):
         assert np.allclose(d[i][:mg].cpu().numpy(), ao[j][:mo], rtol=0, atol=1e-12), i
+
+
+PENAL_CASES = [
+    # main grid, penalisation box (free, aligned with the main cells)
+    ("fff", ((-1, -1, -1), (1, 1, 1), (0.125,) * 3, (0, 0, 0)), ((-0.5, -0.5, -0.5), (0.5, 0.5, 0.5))),
+    ("ppf", ((-1, -1, -0.75), (1, 1, 0.75), (0.125,) * 3, (1, 1, 0)), ((-0.625, -0.5, -0.5), (0.5, 0.625, 0.5))),
+]
+
+
+def _penal_setup(main, box):
+    (xmin, xmax, dx, bc) = main
+    po, to, qo, pg, tg, qg = setup_pair(xmin, xmax, dx, bc, 4, interp=3, order=6)
+    ppo = O.make_patch(box[0], box[1], dx, bound_cond=(0, 0, 0), nghost=4)
+    ppg = P.make_patch(box[0], box[1], dx, bound_cond=(0, 0, 0), nghost=4)
+    ierr, tpo = O.topology_cuboid(ppo, 3)
+    assert ierr == 0
+    ierr, tpg = P.pmlib_topology_cuboid(ppg, 3)
+    assert ierr == 0
+    ext = [tpo.ncell[d] + tpo.nghost[2 * d] + tpo.nghost[2 * d + 1] for d in range(3)]
+    ax = [tpo.xmin[d] + (np.arange(ext[d]) - tpo.nghost[2 * d] + 0.5) * tpo.dx[d] for d in range(3)]
+    z, y, x = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+    c = [0.5 * (box[0][d] + box[1][d]) for d in range(3)]
+    solid = ((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2 <= 0.3 ** 2).astype(np.float64)[..., None]
+    svel = np.zeros(O.topo_shape(tpo, 3))
+    svel[..., 2] = 0.1 * solid[..., 0]  # a body moving along z
+    from tests.helpers import gaussian_field
+    w = gaussian_field(to, seed=17)
+    ierr, pk = O.poisson_setup(po, qo)
+    ierr, vel, _ = O.poisson_solve(po, to, qo, pk, w.copy())
+    vel[..., 0] += 1.0
+    return po, to, qo, pg, tg, qg, ppo, tpo, ppg, tpg, np.ascontiguousarray(solid), svel, w, np.ascontiguousarray(vel)
+
+
+@pytest.mark.parametrize("name,main,box", PENAL_CASES)
+@pytest.mark.parametrize("fd,reproject", [(4, False), (2, True)])
+def test_penalisation_fp64(name, main, box, fd, reproject):
+    """Brinkman penalisation (penalisation_solve.f) against the oracle: a fixed number
+    of passes (tolerance 0), then a converging run whose pass count must agree."""
+    import torch
+    po, to, qo, pg, tg, qg, ppo, tpo, ppg, tpg, solid, svel, w, vel = _penal_setup(main, box)
+    ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP64)
+    assert ierr == 0
+    ierr, pplan = P.pmlib_poisson_setup(ppg, tpg, qg, P.FP64)
+    assert ierr == 0, P.last_error()
+    for tol, mx in ((0.0, 4), (0.05, 30)):
+        wo, vo = w.copy(), vel.copy()
+        ierr, fo, no, ro = O.penalisation_solve(po, to, qo, ppo, tpo, solid, svel, wo, vo, relax=1.0, tol=tol,
+                                                max_iter=mx, dtime=0.01, fd_order=fd, reproject=reproject,
+                                                vel_inf=(1.0, 0.0, 0.2))
+        assert ierr == 0
+        d = [torch.from_numpy(a.copy()).cuda() for a in (solid, svel, w, vel)]
+        fg, ng, rg = P.penalisation_solve_dev(plan, pplan, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(),
+                                              d[3].data_ptr(), relaxation=1.0, tolerance=tol, max_iter=mx,
+                                              dtime=0.01, fd_order=fd, reproject=reproject, vel_inf=(1.0, 0.0, 0.2))
+        assert ng == no, (ng, no)
+        assert np.allclose(fg, fo, rtol=1e-10, atol=1e-12 * np.abs(fo).max()), (fg, fo)
+        assert np.allclose(rg, ro, rtol=1e-8)
+        assert rel_l2(d[2].cpu().numpy(), wo) < 1e-12
+        assert rel_l2(d[3].cpu().numpy(), vo) < 1e-12
+
+
+def test_penalisation_fp32():
+    import torch
+    po, to, qo, pg, tg, qg, ppo, tpo, ppg, tpg, solid, svel, w, vel = _penal_setup(*PENAL_CASES[0][1:])
+    ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP32)
+    ierr, pplan = P.pmlib_poisson_setup(ppg, tpg, qg, P.FP32)
+    wo, vo = w.copy(), vel.copy()
+    ierr, fo, no, ro = O.penalisation_solve(po, to, qo, ppo, tpo, solid, svel, wo, vo, tol=0.0, max_iter=3,
+                                            vel_inf=(1.0, 0.0, 0.0))
+    d = [torch.from_numpy(a.astype(np.float32)).cuda() for a in (solid, svel, w, vel)]
+    fg, ng, rg = P.penalisation_solve_dev(plan, pplan, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(),
+                                          d[3].data_ptr(), tolerance=0.0, max_iter=3, vel_inf=(1.0, 0.0, 0.0))
+    assert ng == no == 3
+    assert np.allclose(fg, fo, rtol=1e-4, atol=1e-5 * np.abs(fo).max())
+    assert rel_l2(d[2].cpu().numpy(), wo) < 1e-5
+    assert rel_l2(d[3].cpu().numpy(), vo) < 1e-5
+
+
+def test_penalisation_errors():
+    po, to, qo, pg, tg, qg, ppo, tpo, ppg, tpg, solid, svel, w, vel = _penal_setup(*PENAL_CASES[0][1:])
+    import torch
+    ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP64)
+    ierr, pplan32 = P.pmlib_poisson_setup(ppg, tpg, qg, P.FP32)
+    ierr, pplan = P.pmlib_poisson_setup(ppg, tpg, qg, P.FP64)
+    d = [torch.from_numpy(a.copy()).cuda() for a in (solid, svel, w, vel)]
+    with pytest.raises(RuntimeError):  # precisions differ
+        P.penalisation_solve_dev(plan, pplan32, *(t.data_ptr() for t in d))
+    with pytest.raises(RuntimeError, match="pmlib_fd_order"):
+        P.penalisation_solve_dev(plan, pplan, *(t.data_ptr() for t in d), fd_order=3)
