@@ -242,6 +242,7 @@ def main():
                     help="precision of --mode profile")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched and served measurements")
     ap.add_argument("--no-stage", action="store_true", help="skip the full vortex-stage measurement")
+    ap.add_argument("--no-penal", action="store_true", help="skip the penalisation measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -455,6 +456,57 @@ def main():
                  "scheme": "low-storage RK3 (stages 1-3 in turn), fd_order 4, visc 1e-4, CFL 0.05",
                  "api": "pmgpu_vortex_stage_dev (device arrays; the map's particle count comes back to the host)"}
 
+    # ---- Brinkman penalisation of a sphere (radius 1/8 at the centre) on a box of the
+    # grid with a 5-cell buffer: 10 passes (tolerance 0), then the main solve
+    penal = None
+    if not args.no_penal:
+        h = float(w.dx[0])
+        r0, nbuff = 0.125, 5
+        lo = [round((-r0 - w.xmin[d]) / h - nbuff) * h + w.xmin[d] for d in range(3)]
+        hi = [round((r0 - w.xmin[d]) / h + nbuff) * h + w.xmin[d] for d in range(3)]
+        bpatch = P.make_patch(lo, hi, w.dx, bound_cond=(0, 0, 0), nghost=4)
+        ierr, btopo = P.pmlib_topology_cuboid(bpatch, w.interp)
+        ierr, bplan = P.pmlib_poisson_setup(bpatch, btopo, params, P.FP32)
+        assert ierr == 0, P.last_error()
+        bx = []
+        for d in range(3):
+            i = torch.arange(1 - btopo.nghost[2 * d], btopo.ncell[d] + btopo.nghost[2 * d + 1] + 1, dtype=torch.float64,
+                             device=dev)
+            bx.append(btopo.xmin[d] + (i - 0.5) * btopo.dx[d])
+        bz, by, bxx = torch.meshgrid(bx[2], bx[1], bx[0], indexing="ij")
+        solid = ((bxx ** 2 + by ** 2 + bz ** 2) <= r0 * r0).float().unsqueeze(-1).contiguous()
+        svel = torch.zeros(solid.shape[:3] + (3,), dtype=torch.float32, device=dev)
+        pw = Wl.blob_field(topo, 0, xp=torch).float().contiguous()
+        pu = torch.empty_like(pw)
+        if P.pmlib_poisson_solve_dev(plan32, pw.data_ptr(), pu.data_ptr(), stream=sptr) != 0:
+            raise RuntimeError(P.last_error())
+        pu[..., 0] += 1.0
+        w0, u0 = pw.clone(), pu.clone()
+
+        def penal_once():
+            pw.copy_(w0)
+            pu.copy_(u0)
+            return P.penalisation_solve_dev(plan32, bplan, solid.data_ptr(), svel.data_ptr(), pw.data_ptr(),
+                                            pu.data_ptr(), relaxation=1.0, tolerance=0.0, max_iter=10, dtime=0.01,
+                                            fd_order=4, vel_inf=(1.0, 0.0, 0.0), stream=sptr)
+
+        penal_once()
+        torch.cuda.synchronize()
+        kp = 3
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(kp):
+            force, npass, res = penal_once()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pms = max_over_ranks(e0.elapsed_time(e1)) / kp
+        penal = {"ms_per_solve": pms, "passes": npass, "force": force, "residuals": list(res),
+                 "box_cells": list(btopo.ncell),
+                 "workload": f"sphere r = {r0} at the centre, box with a {nbuff}-cell buffer, relaxation 1, "
+                             f"FD 4, 10 passes (tolerance 0) + the main {w.n}^3 solve, FP32",
+                 "api": "pmgpu_penalisation_solve_dev (the host tests the residual after every pass)"}
+        bplan.close()
+
     # ---- batched uneven patches (every rank: replicas) and the served stream (rank 0)
     batched = served = None
     if not args.no_batched:
@@ -490,7 +542,7 @@ def main():
             "accuracy": {"rel_l2_fp32_vs_fp64": rel_l2, "max_rel_err": max_err},
             "roofline": roofline, "kernels": kernels, "gpu_launches": launches32,
             "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "batched": batched, "served": served,
-            "vortex_stage": stage,
+            "vortex_stage": stage, "penalisation": penal,
         }
         print(json.dumps(line), flush=True)
     for p in (plan32, plan64):
