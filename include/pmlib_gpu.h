@@ -314,6 +314,34 @@ int pmgpu_penalisation_solve_dev(pmgpu_plan *plan, pmgpu_plan *penal_plan, const
                                  const double vel_inf[3], void *d_vort, void *d_vel, double force[3],
                                  int *niter, double residuals[3], void *stream);
 
+/* ---- files around the step (host code; `device` = 1 when the arrays live on the GPU) ---- */
+
+/* pmlib_output_mesh (source/output/pmlib_output_mesh.f:5-189), one rank: writes
+ * <outdir><tag>.pvti and <outdir><tag>_P00000.vti, the interior cells' vorticity
+ * and velocity as Float32 cell data appended raw, the bytes the reference writes. */
+int pmgpu_output_mesh(const char *outdir, const char *tag, const pmgpu_patch *patch,
+                      const pmgpu_topo *topo, int precision, const void *mesh_vort,
+                      const void *mesh_vel, int device);
+/* the .pvti of pmlib_output_mesh (:43-80) for npieces cuboids (icell / ncell: three
+ * ints a piece, icell 1-based as topo%icell) */
+int pmgpu_output_pvti(const char *path, const char *tag, const pmgpu_patch *patch, int npieces,
+                      const int *icell, const int *ncell);
+/* pmlib_output_topology (source/output/pmlib_output_topology.f:5-72), one rank:
+ * <tag>.dat; ptype is patch%ptype */
+int pmgpu_output_topology(const char *tag, const pmgpu_patch *patch, int ptype, const pmgpu_topo *topo);
+/* The vortex client's particle restart file
+ * (vortex_codes/vortex_structures/source/output/output_particles.f:5-95): <tag>.dat,
+ * unformatted sequential records itime_next (the client writes itime + 1),
+ * time_next (time + dtime, REAL of the precision), npart, then one record
+ * (pos(3), vort(3)) a particle. */
+int pmgpu_output_particles(const char *tag, int itime_next, double time_next, int precision, int npart,
+                           const void *pos, const void *vort, int device);
+/* Reads such a file back as input/input_particles.f:62-100 does: the particles whose
+ * |vort| >= trunc, at most max_part of them into host arrays pos / vort (NULL to
+ * count only); *npart gets their number.  No particle above trunc is an error. */
+int pmgpu_input_particles(const char *file, double trunc, int precision, int max_part, void *pos,
+                          void *vort, int *npart, int *itime, double *time);
+
 /* ---- diagnostics (no counterpart in the reference, which has no timers) ---- */
 const char *pmgpu_last_error(void);
 /* number of this library's kernels launched since the last reset */

@@ -24,6 +24,8 @@ EXPORTS = (
     "pmgpu_deriv_vorticity", "pmgpu_deriv_vorticity_f32", "pmgpu_deriv_vorticity_dev",
     "pmgpu_particles_advance", "pmgpu_particles_advance_f32", "pmgpu_particles_advance_dev",
     "pmgpu_vortex_stage_dev", "pmgpu_fft_set_schedule", "pmgpu_step_many", "pmgpu_penalisation_solve_dev",
+    "pmgpu_output_mesh", "pmgpu_output_pvti", "pmgpu_output_topology", "pmgpu_output_particles",
+    "pmgpu_input_particles",
 )
 
 
@@ -100,6 +102,11 @@ def lib():
         "pmgpu_step_many": [vp, C.c_int, C.POINTER(vp), C.POINTER(vp), ip, C.POINTER(vp)],
         "pmgpu_penalisation_solve_dev": [vp, vp, vp, vp, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
                                          C.c_int, dp, vp, vp, dp, ip, dp, vp],
+        "pmgpu_output_mesh": [C.c_char_p, C.c_char_p, PP, TP, C.c_int, vp, vp, C.c_int],
+        "pmgpu_output_pvti": [C.c_char_p, C.c_char_p, PP, C.c_int, ip, ip],
+        "pmgpu_output_topology": [C.c_char_p, PP, C.c_int, TP],
+        "pmgpu_output_particles": [C.c_char_p, C.c_int, C.c_double, C.c_int, C.c_int, vp, vp, C.c_int],
+        "pmgpu_input_particles": [C.c_char_p, C.c_double, C.c_int, C.c_int, vp, vp, ip, ip, dp],
         "pmgpu_particle_diagnostics": [dp, vp, vp, vp, C.c_int, C.c_int, dp, vp],
         "pmgpu_deriv_vorticity": [TP, C.c_int, C.c_double, dp, dp, dp],
         "pmgpu_deriv_vorticity_f32": [TP, C.c_int, C.c_double, fp, fp, fp],

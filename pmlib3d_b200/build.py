@@ -21,7 +21,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libpmgpu.so")
 BUILD = os.path.join(HERE, "_build")
-UNITS = [os.path.join(CSRC, "pmgpu.cu")] + sorted(glob.glob(os.path.join(CSRC, "passes_*.cu")))
+UNITS = ([os.path.join(CSRC, "pmgpu.cu")] + sorted(glob.glob(os.path.join(CSRC, "passes_*.cu"))) +
+         [os.path.join(CSRC, "output.cu")])
 HEADERS = sorted(glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))) + [
     os.path.join(os.path.dirname(HERE), "include", "pmlib_gpu.h")]
 

@@ -415,3 +415,50 @@ def penalisation_solve_dev(plan: Plan, penal_plan: Plan, d_solid: int, d_solid_v
     if rc != 0:
         raise RuntimeError(last_error())
     return list(force), n.value, tuple(res)
+
+
+def _prec_of(a) -> int:
+    return FP64 if a.dtype == np.float64 else FP32
+
+
+def pmlib_output_mesh(outdir: str, tag: str, patch: Patch, topo: Topo, vort, vel) -> int:
+    """source/output/pmlib_output_mesh.f:5-189 (one rank) for host meshes (FP64 or FP32)."""
+    dt = vort.dtype.type
+    return lib().pmgpu_output_mesh(outdir.encode(), tag.encode(), C.byref(patch), C.byref(topo), _prec_of(vort),
+                                   _ptr(vort, dt), _ptr(vel, dt), 0)
+
+
+def output_pvti(path: str, tag: str, patch: Patch, icell, ncell) -> int:
+    """The .pvti of pmlib_output_mesh for several pieces (icell, ncell: (npieces, 3))."""
+    ic = np.ascontiguousarray(icell, dtype=np.int32).reshape(-1)
+    nc = np.ascontiguousarray(ncell, dtype=np.int32).reshape(-1)
+    return lib().pmgpu_output_pvti(path.encode(), tag.encode(), C.byref(patch), len(ic) // 3,
+                                   ic.ctypes.data_as(C.POINTER(C.c_int)), nc.ctypes.data_as(C.POINTER(C.c_int)))
+
+
+def pmlib_output_topology(tag: str, patch: Patch, topo: Topo, ptype: int = 1) -> int:
+    """source/output/pmlib_output_topology.f:5-72 (one rank): <tag>.dat."""
+    return lib().pmgpu_output_topology(tag.encode(), C.byref(patch), int(ptype), C.byref(topo))
+
+
+def output_particles(tag: str, itime_next: int, time_next: float, pos, vort) -> int:
+    """The vortex client's particle restart file <tag>.dat (host arrays (np, 3))."""
+    dt = pos.dtype.type
+    return lib().pmgpu_output_particles(tag.encode(), int(itime_next), float(time_next), _prec_of(pos), pos.shape[0],
+                                        _ptr(pos, dt), _ptr(vort, dt), 0)
+
+
+def input_particles(path: str, trunc: float = 0.0, precision: int = FP64):
+    """Reads a particle restart file: (ierr, pos, vort, itime, time) with the particles
+    whose |vort| >= trunc."""
+    n, it, tm = C.c_int(0), C.c_int(0), C.c_double(0.0)
+    L = lib()
+    ierr = L.pmgpu_input_particles(path.encode(), float(trunc), int(precision), 0, None, None, C.byref(n), None, None)
+    if ierr:
+        return ierr, None, None, None, None
+    dt = np.float64 if precision == FP64 else np.float32
+    pos = np.zeros((n.value, 3), dt)
+    vort = np.zeros((n.value, 3), dt)
+    ierr = L.pmgpu_input_particles(path.encode(), float(trunc), int(precision), n.value, pos.ctypes.data,
+                                   vort.ctypes.data, C.byref(n), C.byref(it), C.byref(tm))
+    return ierr, pos, vort, it.value, tm.value
