@@ -133,6 +133,17 @@ int pmgpu_regularise(pmgpu_plan *plan, double *mesh, int nvar, int reg_order, do
 int pmgpu_regularise_f32(pmgpu_plan *plan, float *mesh, int nvar, int reg_order,
                          double filter_width);
 
+/* pmlib_poisson_setup with the spectral Green's function of the
+ * periodic-periodic-free validation program
+ * (validation/poisson_ppf/sources/poisson/poisson_setup_ppf.f:5-503): for patches
+ * periodic in x and y and free in z, kernel 1, orders 0-10.  The kernel is the
+ * regularised 1-D Green's function of |k_perp| in z, exact in the periodic
+ * directions (no image truncation); like the validation program it leaves out the
+ * k_perp = 0 mode, and its orders 2-10 carry the program's 1/dx normalisation (order 0
+ * divides by dx dy).  Solves, regularisation and steps then use the plan as any. */
+int pmgpu_poisson_setup_ppf(const pmgpu_patch *patch, const pmgpu_topo *cuboid,
+                            const pmgpu_params *par, int precision, pmgpu_plan **plan);
+
 /* Replaces the deallocation of mesh%pkernel_fft (source/pmlib_finalise.f:63).  The
  * plan's device memory returns to the device's stream-ordered pool without
  * synchronising the device, so call it only when no work that uses the plan is still

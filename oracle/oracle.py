@@ -102,6 +102,7 @@ def lib():
         L.pmo_penalisation_solve.argtypes = [C.POINTER(Patch), C.POINTER(Topo), C.POINTER(Params),
                                              C.POINTER(Patch), C.POINTER(Topo), dp, dp, C.c_double, C.c_double,
                                              C.c_int, C.c_double, C.c_int, C.c_int, dp, dp, dp, dp, ip, dp]
+        L.pmo_poisson_setup_ppf.argtypes = [C.POINTER(Patch), C.POINTER(Params), dp]
         L.pmo_si.argtypes = [C.c_double]
         L.pmo_si.restype = C.c_double
         _lib = L
@@ -285,3 +286,12 @@ def penalisation_solve(pa, t, par, pp, tp, solid, solid_vel, vort, vel, relax=1.
                                         int(fd_order), int(bool(reproject)), _p(vi), _p(vort), _p(vel), _p(force),
                                         C.byref(n), _p(res))
     return ierr, force, n.value, tuple(res)
+
+
+def poisson_setup_ppf(patch, par):
+    """The periodic-periodic-free validation program's spectral kernel, in the layout
+    of poisson_setup: (ierr, pkernel_fft (Mz, My, Mx, 1))."""
+    M, nk = kernel_dims(patch, par)
+    buf = np.zeros(2 * M[0] * M[1] * M[2])
+    ierr = lib().pmo_poisson_setup_ppf(C.byref(patch), C.byref(par), _p(buf))
+    return ierr, buf.view(np.complex128).reshape(M[2], M[1], M[0], 1)

@@ -1595,3 +1595,86 @@ done:
   free(vel_pen); free(pvel); free(pvort); free(pkp); free(pkm);
   return rc;
 }
+
+/* ------------------------------------------------------------------------- */
+/* The spectral Green's function of the periodic-periodic-free validation program
+ * (validation/poisson_ppf/sources/poisson/poisson_setup_ppf.f:160-486, one rank):
+ * on the kernel grid the two periodic axes hold wavenumbers (natural order, the
+ * formula of :184-209) and the free axis positions centred on zero; the kernel is
+ * the regularised 1-D Green's function of |k_perp| along z, then transformed along
+ * the free axis only (fft_shift, :482-484).  pkf gets the same layout as
+ * pmo_poisson_setup: (Mz, My, Mx) complex, x fastest.  Kernel 1, orders 0-10. */
+int pmo_poisson_setup_ppf(const pmo_patch *pa, const pmo_params *par, double *pkf) {
+  const char *caller = "pmlib_poisson_setup";
+  if (!(pa->bound_cond[0] == 1 && pa->bound_cond[1] == 1 && pa->bound_cond[2] == 0)) {
+    pm_write(caller, "The spectral kernel needs periodic x and y and a free z.");
+    return -1;
+  }
+  if (par->poisson_kernel != 1) {
+    pm_write(caller, "Velocity kernel is not implemented.");
+    return -1;
+  }
+  const int o = par->poisson_order;
+  if (o != 0 && o != 2 && o != 4 && o != 6 && o != 8 && o != 10) {
+    pm_write(caller, "Integration kernel unknown - change POISSON ORDER.");
+    return -1;
+  }
+  int M[3], nk;
+  pmo_kernel_dims(pa, par, M, &nk);
+  const double PI = acos(-1.0);
+  double dx[3], mdx = 0.0;
+  for (int e = 0; e < 3; e++) { dx[e] = pa->dx[e]; if (dx[e] > mdx) mdx = dx[e]; }
+  const double eps = par->regularisation_radius * mdx;
+  const double c_1_2pi = 0.5 / PI, c_sqrt_2_pi = sqrt(2.0 / PI), c_1_sqrt2 = 1.0 / sqrt(2.0);
+  const double zmin = -(0.5 * (double)M[2] + 0.5) * dx[2]; /* the kernel topology (:66-71) */
+  int lo[3] = {1, 1, 1};
+  cbox w = cb_alloc(lo, M, 1);
+  for (int k = 1; k <= M[2]; k++) {
+    const double pz = zmin + ((double)(k - 1) + 0.5) * dx[2];
+    for (int j = 1; j <= M[1]; j++) {
+      const double kj = wavenumber(j, 0, M[1], -0.5 / dx[1], 1.0 / (M[1] * dx[1]), 0.5 / dx[1]);
+      for (int i = 1; i <= M[0]; i++) {
+        const double ki = wavenumber(i, 0, M[0], -0.5 / dx[0], 1.0 / (M[0] * dx[0]), 0.5 / dx[0]);
+        const double kp = sqrt(ki * ki + kj * kj);
+        const double r = sqrt(pz * pz);
+        double g = 0.0;
+        if (o == 0) {
+          if (kp != 0.0) g = 0.5 * c_1_2pi * exp(-2.0 * PI * kp * r) / kp / (dx[0] * dx[1]);
+        } else {
+          const double rho = r / eps, s = eps * 2.0 * PI * kp;
+          if (s != 0.0 && rho * s < 700.0) {
+            const double a = 0.25 / (2.0 * PI * kp) *
+                             ((1.0 - erf(c_1_sqrt2 * (s - rho))) * exp(-s * rho) +
+                              (1.0 - erf(c_1_sqrt2 * (s + rho))) * exp(s * rho));
+            const double s2 = s * s, r2 = rho * rho, ex = exp(-0.5 * (s2 + r2));
+            double b = 0.0;
+            switch (o) {
+              case 4: b = eps * c_sqrt_2_pi * 0.25 * ex; break;
+              case 6: b = eps * c_sqrt_2_pi * (5.0 / 16.0 + 1.0 / 16.0 * (s2 - r2)) * ex; break;
+              case 8:
+                b = eps * c_sqrt_2_pi *
+                    (11.0 / 32.0 + 1.0 / 12.0 * s2 - 1.0 / 8.0 * r2 - 1.0 / 48.0 * s2 * r2 +
+                     1.0 / 96.0 * (s2 * s2 + r2 * r2)) * ex;
+                break;
+              case 10:
+                b = eps * c_sqrt_2_pi *
+                    (93.0 / 256.0 + 73.0 / 768.0 * s2 - 47.0 / 256.0 * r2 - 17.0 / 384.0 * s2 * r2 +
+                     11.0 / 768.0 * s2 * s2 + 23.0 / 768.0 * r2 * r2 + 1.0 / 256.0 * s2 * r2 * r2 -
+                     1.0 / 256.0 * s2 * s2 * r2 + 1.0 / 768.0 * (s2 * s2 * s2 - r2 * r2 * r2)) * ex;
+                break;
+              default: break;
+            }
+            g = (a + b) / dx[0];
+          }
+        }
+        const size_t q = cb_idx(&w, 0, i - 1, j - 1, k - 1);
+        w.d[q] = g;
+        w.d[q + 1] = 0.0;
+      }
+    }
+  }
+  if (cb_fft_axis(&w, 2, 0, 1, "pmlib_fft")) { cb_free(&w); return -1; }
+  memcpy(pkf, w.d, sizeof(double) * 2 * (size_t)M[0] * M[1] * M[2]);
+  cb_free(&w);
+  return 0;
+}

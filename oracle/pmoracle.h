@@ -116,6 +116,10 @@ int pmo_penalisation_solve(const pmo_patch *pa, const pmo_topo *t, const pmo_par
                            const double vel_inf[3], double *vort, double *vel, double force[3], int *niter,
                            double resid[3]);
 
+/* the spectral Green's function of the periodic-periodic-free validation program,
+ * same output layout as pmo_poisson_setup */
+int pmo_poisson_setup_ppf(const pmo_patch *patch, const pmo_params *par, double *pkernel_fft);
+
 /* helper: sine integral used by the order-100 kernel */
 double pmo_si(double x);
 

@@ -25,7 +25,7 @@ EXPORTS = (
     "pmgpu_particles_advance", "pmgpu_particles_advance_f32", "pmgpu_particles_advance_dev",
     "pmgpu_vortex_stage_dev", "pmgpu_fft_set_schedule", "pmgpu_step_many", "pmgpu_penalisation_solve_dev",
     "pmgpu_output_mesh", "pmgpu_output_pvti", "pmgpu_output_topology", "pmgpu_output_particles",
-    "pmgpu_input_particles",
+    "pmgpu_input_particles", "pmgpu_poisson_setup_ppf",
 )
 
 
@@ -75,6 +75,7 @@ def lib():
         "pmgpu_interp_mesh_particle": [TP, QP, dp, dp, dp, dp, C.c_int, dp, dp, dp],
         "pmgpu_interp_mesh_particle_f32": [TP, QP, fp, fp, fp, fp, C.c_int, fp, fp, fp],
         "pmgpu_poisson_setup": [PP, TP, QP, C.c_int, C.POINTER(vp)],
+        "pmgpu_poisson_setup_ppf": [PP, TP, QP, C.c_int, C.POINTER(vp)],
         "pmgpu_poisson_solve": [vp, dp, dp, dp, C.c_int, C.c_int, C.c_int],
         "pmgpu_poisson_solve_f32": [vp, fp, fp, fp, C.c_int, C.c_int, C.c_int],
         "pmgpu_regularise": [vp, dp, C.c_int, C.c_int, C.c_double],

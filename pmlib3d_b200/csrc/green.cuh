@@ -227,6 +227,67 @@ __global__ void k_green2_split(const double2 *__restrict__ spec, int c, int M0, 
   }
 }
 
+// The spectral kernel of the periodic-periodic-free validation program
+// (validation/poisson_ppf/sources/poisson/poisson_setup_ppf.f:160-486): written into
+// the y-transformed spectrum layout spec[z][row][kx] (kx < Hp, zero from H on; row ->
+// ky through yk, natural order when null) at the shifted z positions, so that a
+// transform along z alone completes it.  Its x and y axes hold the wavenumbers
+// (natural order) of the periodic axes; the value is the regularised 1-D Green's
+// function of |k_perp| at |z|.  Orders 2-10 divide by dx only and order 0 by dx dy,
+// as the validation program does.
+__global__ void k_green_ppf(GreenParams gp, int H, int Hp, const int *__restrict__ yk, double2 *__restrict__ spec) {
+  const double PI = 3.14159265358979323846;
+  const size_t total = (size_t)gp.M[2] * gp.M[1] * Hp;
+  const double c_1_2pi = 0.5 / PI, c_sqrt_2_pi = sqrt(2.0 / PI), c_1_sqrt2 = 0.70710678118654752440;
+  const double eps = gp.eps;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int kx = (int)(t % Hp);
+    const int row = (int)((t / Hp) % gp.M[1]);
+    const int z = (int)(t / ((size_t)Hp * gp.M[1]));
+    double g = 0.0;
+    if (kx < H) {
+      const int ky = yk ? yk[row] : row;
+      const double ki = (double)(2 * kx < gp.M[0] ? kx : kx - gp.M[0]) / ((double)gp.M[0] * gp.dx[0]);
+      const double kj = (double)(2 * ky < gp.M[1] ? ky : ky - gp.M[1]) / ((double)gp.M[1] * gp.dx[1]);
+      const int h = gp.M[2] / 2;
+      const int iu = z < h ? z + h + 1 : z - h + 1;  // unshifted 1-based index
+      const double pz = gp.xmin[2] + ((double)(iu - 1) + 0.5) * gp.dx[2];
+      const double kp = sqrt(ki * ki + kj * kj), r = fabs(pz);
+      if (gp.order == 0) {
+        if (kp != 0.0) g = 0.5 * c_1_2pi * exp(-2.0 * PI * kp * r) / kp / (gp.dx[0] * gp.dx[1]);
+      } else {
+        const double rho = r / eps, s = eps * 2.0 * PI * kp;
+        if (s != 0.0 && rho * s < 700.0) {
+          const double a = 0.25 / (2.0 * PI * kp) *
+                           ((1.0 - erf(c_1_sqrt2 * (s - rho))) * exp(-s * rho) +
+                            (1.0 - erf(c_1_sqrt2 * (s + rho))) * exp(s * rho));
+          const double s2 = s * s, r2 = rho * rho, ex = exp(-0.5 * (s2 + r2));
+          double b = 0.0;
+          switch (gp.order) {
+            case 4: b = eps * c_sqrt_2_pi * 0.25 * ex; break;
+            case 6: b = eps * c_sqrt_2_pi * (5.0 / 16.0 + 1.0 / 16.0 * (s2 - r2)) * ex; break;
+            case 8:
+              b = eps * c_sqrt_2_pi *
+                  (11.0 / 32.0 + 1.0 / 12.0 * s2 - 1.0 / 8.0 * r2 - 1.0 / 48.0 * s2 * r2 + 1.0 / 96.0 * (s2 * s2 + r2 * r2)) *
+                  ex;
+              break;
+            case 10:
+              b = eps * c_sqrt_2_pi *
+                  (93.0 / 256.0 + 73.0 / 768.0 * s2 - 47.0 / 256.0 * r2 - 17.0 / 384.0 * s2 * r2 +
+                   11.0 / 768.0 * s2 * s2 + 23.0 / 768.0 * r2 * r2 + 1.0 / 256.0 * s2 * r2 * r2 -
+                   1.0 / 256.0 * s2 * s2 * r2 + 1.0 / 768.0 * (s2 * s2 * s2 - r2 * r2 * r2)) *
+                  ex;
+              break;
+            default: break;
+          }
+          g = (a + b) / gp.dx[0];
+        }
+      }
+    }
+    spec[t] = make_double2(g, 0.0);
+  }
+}
+
 // octant of the real spectrum, scaled by dx dy dz / (Mx My Mz), in the plan precision;
 // yrow / zrow: frequency -> row of the transformed spectrum along y / z
 template <typename R>

@@ -487,6 +487,7 @@ struct StepPipe {
 
 struct pmgpu_plan {
   int prec;
+  int green_mode = 0;  // 0: pmlib_poisson_setup's kernel; 1: the ppf validation program's spectral kernel
   StepPipe pipe;
   pmgpu_patch patch;
   pmgpu_topo topo;
@@ -838,7 +839,7 @@ static std::string green_key(const pmgpu_plan *pl) {
   cudaGetDevice(&dev);
   char b[512];
   const pmgpu_patch &p = pl->patch;
-  snprintf(b, sizeof(b), "%d|%d|%a,%a,%a|%d,%d,%d|%d,%d,%d|%d,%d,%d,%d|%d,%d,%a", dev, pl->prec, p.dx[0], p.dx[1],
+  snprintf(b, sizeof(b), "%d|%d|%d|%a,%a,%a|%d,%d,%d|%d,%d,%d|%d,%d,%d,%d|%d,%d,%a", dev, pl->green_mode, pl->prec,
            p.dx[2], pl->g.M[0], pl->g.M[1], pl->g.M[2], p.bound_cond[0], p.bound_cond[1], p.bound_cond[2], p.ncell[0],
            p.ncell[1], p.ncell[2], p.nghost, pl->par.poisson_order, pl->par.poisson_kernel,
            pl->par.regularisation_radius);
@@ -945,7 +946,22 @@ template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller)
                      ((double)G.M[0] * (double)G.M[1] * (double)G.M[2]);
     const unsigned nb_real = (unsigned)std::min<size_t>((npts + 255) / 256, 148 * 64);
     const unsigned nb_oct = (unsigned)std::min<size_t>((noct + 255) / 256, 148 * 64);
-    if (gp.kernel == 1) {
+    if (pl->green_mode == 1) {
+      // the spectral kernel of the ppf validation program: the y-transformed spectrum
+      // (kx, ky natural wavenumbers, z positions) is written directly, then z only
+      const unsigned nb_y = (unsigned)std::min<size_t>((nspec + 255) / 256, 148 * 64);
+      k_green_ppf<<<nb_y, 256>>>(gp, G.H, G.Hp, tmp.ry_ok ? tmp.yk.as<int>() : nullptr, gY.as<double2>());
+      PM_LAUNCHED();
+      if (!cuda_ok(cudaGetLastError(), caller)) break;
+      if (zpass<double, 1>(gg, gY.as<double2>(), gY.as<double2>(), Z_FORWARD, 0, 0, G.M[1], 0, caller)) break;
+      if (!cuda_ok(cudaStreamSynchronize(0), caller)) break;
+      if (own->ensure(sizeof(R) * noct, caller)) break;
+      attach_green(pl, own);
+      k_green_octant<R><<<nb_oct, 256>>>(gY.as<double2>(), G.M[1], G.H, G.Hp, pl->gM1, pl->gM2, f, yinv.as<int>(),
+                                         zinv.as<int>(), pl->green.as<R>());
+      PM_LAUNCHED();
+      if (!cuda_ok(cudaGetLastError(), caller)) break;
+    } else if (gp.kernel == 1) {
       k_green_real<<<nb_real, 256>>>(gp, gr.as<double>());
       PM_LAUNCHED();
       if (!cuda_ok(cudaGetLastError(), caller)) break;
@@ -1438,7 +1454,7 @@ int pmgpu_interp_mesh_particle_f32(const pmgpu_topo *topo, const pmgpu_params *p
 // ------------------------------------------------------------------ Poisson
 // plan creation; the caller holds g_mu
 static int create_plan(const pmgpu_patch *patch, const pmgpu_topo *cuboid, const pmgpu_params *par, int precision,
-                       pmgpu_plan **plan, const char *caller) {
+                       pmgpu_plan **plan, const char *caller, int green_mode = 0) {
   if (!plan || !patch || !cuboid) {
     set_error(caller, "missing argument.");
     return -1;
@@ -1490,6 +1506,7 @@ static int create_plan(const pmgpu_patch *patch, const pmgpu_topo *cuboid, const
   pl->g.N2 = pl->g.M[0] / 2;
   pl->g.allper = allper;
   pl->eps = par->regularisation_radius * mdx;
+  pl->green_mode = green_mode;
   const int rc = (precision == PMGPU_FP64) ? plan_tables<double>(pl, caller) : plan_tables<float>(pl, caller);
   if (rc) {
     delete pl;
@@ -1503,6 +1520,29 @@ int pmgpu_poisson_setup(const pmgpu_patch *patch, const pmgpu_topo *cuboid, cons
                         int precision, pmgpu_plan **plan) {
   std::lock_guard<std::mutex> lk(g_mu);
   return create_plan(patch, cuboid, par, precision, plan, "pmlib_poisson_setup");
+}
+
+int pmgpu_poisson_setup_ppf(const pmgpu_patch *patch, const pmgpu_topo *cuboid, const pmgpu_params *par,
+                            int precision, pmgpu_plan **plan) {
+  const char *caller = "pmlib_poisson_setup";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!patch || !par || !plan) {
+    set_error(caller, "missing argument.");
+    return -1;
+  }
+  if (!(patch->bound_cond[0] != 0 && patch->bound_cond[1] != 0 && patch->bound_cond[2] == 0)) {
+    set_error(caller, "The spectral kernel needs periodic x and y and a free z.");
+    return -1;
+  }
+  if (par->poisson_kernel == 2) {  // poisson_setup_ppf.f: no velocity kernel
+    set_error(caller, "Velocity kernel is not implemented.");
+    return -1;
+  }
+  if (par->poisson_order == 100) {
+    set_error(caller, "Integration kernel unknown - change POISSON ORDER.");
+    return -1;
+  }
+  return create_plan(patch, cuboid, par, precision, plan, caller, 1);
 }
 
 void pmgpu_plan_destroy(pmgpu_plan *plan) {

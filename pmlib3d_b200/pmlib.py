@@ -154,6 +154,15 @@ def pmlib_poisson_setup(patch: Patch, topo: Topo, params: Params, precision: int
     return ierr, (Plan(h, precision, topo) if ierr == 0 else None)
 
 
+def poisson_setup_ppf(patch: Patch, topo: Topo, params: Params, precision: int = FP64):
+    """pmlib_poisson_setup with the spectral kernel of the periodic-periodic-free
+    validation program (validation/poisson_ppf/sources/poisson/poisson_setup_ppf.f)
+    -> (ierr, Plan)."""
+    h = C.c_void_p()
+    ierr = lib().pmgpu_poisson_setup_ppf(C.byref(patch), C.byref(topo), C.byref(params), precision, C.byref(h))
+    return ierr, (Plan(h, precision, topo) if ierr == 0 else None)
+
+
 def pmlib_poisson_solve(plan: Plan, vort, vel, vecpot=None, reg_vort=False, reproj=False,
                         calc_vecpot=False) -> int:
     """source/poisson/pmlib_poisson_solve.f:15-34: vel (and vecpot) written, vort

@@ -572,3 +572,42 @@ def test_step_many_matches_single_steps():
         assert P.step_many(plan, [p for p, _ in src], [v for _, v in src], outs) == 0, P.last_error()
         for o, r in zip(outs, ref):
             assert np.array_equal(o, r)
+
+
+PPF_CASES = [
+    ("ppf", (-1, -1, -0.5), (1, 1, 0.5), (0.125, 0.125, 0.0625), (1, 1, 0), 4),
+    ("ppf-noncubic", (-1, -0.75, -0.75), (1, 0.75, 0.75), (0.125, 0.125, 0.125), (1, 1, 0), 4),
+]
+
+
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", PPF_CASES)
+@pytest.mark.parametrize("order", [0, 2, 6, 10])
+def test_ppf_spectral_kernel(name, xmin, xmax, dx, bc, ng, order):
+    """The periodic-periodic-free validation program's spectral Green's function
+    (poisson_setup_ppf.f) against the oracle's restatement: FP64 to 1e-10 (the
+    kernel's 1 - erf terms lose relative digits where erf is near 1, amplified by
+    exp(s rho); tested at 1e-10), FP32 to 1e-5, with reprojection."""
+    po, to, qo, pg, tg, qg = setup_pair(xmin, xmax, dx, bc, ng, interp=3, order=order)
+    w = gaussian_field(to, seed=19, noise=0.01)
+    ierr, pk = O.poisson_setup_ppf(po, qo)
+    assert ierr == 0
+    wo = w.copy()
+    ierr, vel_o, _ = O.poisson_solve(po, to, qo, pk, wo, reproj=True)
+    assert ierr == 0
+    for prec, tol in ((P.FP64, 1e-10), (P.FP32, 1e-5)):
+        dt = np.float64 if prec == P.FP64 else np.float32
+        ierr, plan = P.poisson_setup_ppf(pg, tg, qg, prec)
+        assert ierr == 0, P.last_error()
+        vel = np.zeros(w.shape, dt)
+        wg = w.astype(dt)
+        assert P.pmlib_poisson_solve(plan, wg, vel, reproj=True) == 0
+        assert rel_l2(vel, vel_o) < tol, (prec, rel_l2(vel, vel_o))
+        assert rel_l2(wg, wo) < tol
+
+
+def test_ppf_spectral_kernel_errors(capfd):
+    po, to, qo, pg, tg, qg = setup_pair(*CASES[0][1:], order=6)  # fff: not periodic in x and y
+    assert P.poisson_setup_ppf(pg, tg, qg, P.FP64)[0] == -1
+    po, to, qo, pg, tg, qg = setup_pair(*PPF_CASES[0][1:], order=6, kernel=2)
+    assert P.poisson_setup_ppf(pg, tg, qg, P.FP64)[0] == -1
+    assert "Velocity kernel is not implemented." in capfd.readouterr().out
