@@ -13,6 +13,7 @@
 !   pmlib_poisson_solve(patch,topo_all,mesh,ierr,reg_vort,reproj,calc_vecpot)
 !   pmlib_regularise(patch,topo_all,mesh,reg_order,filter_width,ierr)
 !   pmlib_particles_advance(patch,topo,part,itimestage,dtime,ierr,euler_vort)
+!   pmlib_output_mesh(outdir,tag,patch,topo,mesh,ierr)
 !   pmlib_gpu_finalise()                 (frees the plan; call from pmlib_finalise)
 !
 ! They read the same module globals as the originals (pmlib_poisson_order,
@@ -150,6 +151,15 @@ MODULE pmlib_gpu_c
       TYPE(C_PTR), VALUE :: pos, vort, vel, dvort, vel_rk, dvort_rk
       INTEGER(C_INT) :: npart_out
     END FUNCTION
+    INTEGER(C_INT) FUNCTION pmgpu_output_mesh(outdir, tag, patch, topo, precision, mesh_vort, &
+        mesh_vel, device) BIND(C, NAME='pmgpu_output_mesh')
+      IMPORT
+      CHARACTER(KIND=C_CHAR), DIMENSION(*) :: outdir, tag
+      TYPE(pmgpu_patch) :: patch
+      TYPE(pmgpu_topo) :: topo
+      INTEGER(C_INT), VALUE :: precision, device
+      TYPE(C_PTR), VALUE :: mesh_vort, mesh_vel
+    END FUNCTION
   END INTERFACE
 END MODULE pmlib_gpu_c
 
@@ -165,7 +175,8 @@ MODULE pmlib_gpu_drop_in
   IMPLICIT NONE
   PRIVATE
   PUBLIC :: pmlib_interp_particle_mesh, pmlib_interp_mesh_particle, pmlib_poisson_setup, &
-          & pmlib_poisson_solve, pmlib_regularise, pmlib_particles_advance, pmlib_gpu_finalise
+          & pmlib_poisson_solve, pmlib_regularise, pmlib_particles_advance, pmlib_output_mesh, &
+          & pmlib_gpu_finalise
 
   TYPE(C_PTR), SAVE :: gpu_plan = C_NULL_PTR
   LOGICAL, PARAMETER :: single = MK .NE. KIND(1D0)
@@ -388,6 +399,25 @@ CONTAINS
     DEALLOCATE(part%dvort)
     ALLOCATE(part%dvort(pmlib_ndim, nout))
   END SUBROUTINE pmlib_particles_advance
+
+  ! source/output/pmlib_output_mesh.f:5-189 (one rank): the .pvti and .vti files of
+  ! mesh%vort and mesh%vel, written by the library's host code
+  SUBROUTINE pmlib_output_mesh(outdir, tag, patch, topo, mesh, ierr)
+    CHARACTER(LEN=*), INTENT(IN) :: outdir, tag
+    TYPE(class_patch), INTENT(IN) :: patch
+    TYPE(class_topology), DIMENSION(:), POINTER :: topo
+    TYPE(class_mesh), INTENT(IN) :: mesh
+    INTEGER, INTENT(OUT) :: ierr
+    TYPE(pmgpu_patch) :: p
+    TYPE(pmgpu_topo) :: t
+    INTEGER(C_INT) :: prec
+    p = c_patch(patch)
+    t = c_topo(topo(mpi_rank))
+    prec = PMGPU_FP64
+    IF (single) prec = PMGPU_FP32
+    ierr = pmgpu_output_mesh(TRIM(outdir)//C_NULL_CHAR, TRIM(tag)//C_NULL_CHAR, p, t, prec, &
+         & first4(mesh%vort), first4(mesh%vel), 0_C_INT)
+  END SUBROUTINE pmlib_output_mesh
 
   SUBROUTINE pmlib_gpu_finalise()
     IF (C_ASSOCIATED(gpu_plan)) CALL pmgpu_plan_destroy(gpu_plan)
