@@ -331,9 +331,9 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const unsigned *__r
 // every run.  A cell layer is final once the last bin layer that reaches it has
 // been added.
 constexpr int DEP_TX = 32;
-constexpr int DEP_TY = 8;
+constexpr int DEP_TY = 16;
 constexpr int DEP_THREADS = DEP_TX * DEP_TY;
-constexpr int DEP_LB = 4;
+constexpr int DEP_LB = 3;
 
 template <int W> struct WStride { static constexpr int v = W == 4 ? 4 : 8; };
 
@@ -370,7 +370,7 @@ template <> __device__ __forceinline__ void sts4<double>(double *p, double a, do
 }
 
 template <typename R, int W, int NV>
-__global__ void __launch_bounds__(DEP_THREADS) k_deposit(PartGeom<R> g, const R *__restrict__ pos,
+__global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(PartGeom<R> g, const R *__restrict__ pos,
                                                          const R *__restrict__ val, int vstride,
                                                          const unsigned *__restrict__ start,
                                                          const int *__restrict__ perm, R *__restrict__ mesh,
@@ -378,6 +378,7 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit(PartGeom<R> g, const R 
   constexpr int BX = DEP_TX + W - 1, BY = DEP_TY + W - 1, WS = WStride<W>::v;
   constexpr int NA = W + DEP_LB - 1;   // accumulator layers
   constexpr int NROW = DEP_LB * BY;    // bin rows of one batch
+  static_assert(NROW <= 64, "one warp scans the bin rows of a batch");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // x and y weights weight-major (threads reading consecutive particles hit
   // consecutive banks), z weights and values particle-major for 16-byte loads; the
