@@ -294,3 +294,42 @@ def test_penalisation_errors():
         P.penalisation_solve_dev(plan, pplan32, *(t.data_ptr() for t in d))
     with pytest.raises(RuntimeError, match="pmlib_fd_order"):
         P.penalisation_solve_dev(plan, pplan, *(t.data_ptr() for t in d), fd_order=3)
+
+
+@pytest.mark.parametrize("interp", [3, 4])
+def test_vortex_stage_matches_separate_calls(interp):
+    """pmgpu_vortex_stage_dev (bin-ordered M2P of both fields, then the stage update)
+    agrees with the separate public entry points (P2M, solve, right-hand side, M2P of
+    both fields, pmlib_particles_advance), particles outside every bin included."""
+    import torch
+    from tests.helpers import jittered_particles
+    po, to, qo, pg, tg, qg = setup_pair((-1, -1, -0.5), (1, 1, 0.5), (0.125, 0.125, 0.0625), (1, 1, 0), 4,
+                                        interp=interp, order=6)
+    pos, val = jittered_particles(to, seed=6, jitter=0.1)
+    pos[:7] += np.array([0.0, 0.0, 3.0])  # far outside the z range: no bin, dropped by the map
+    n = len(pos)
+    tg.npart = n
+    rng = np.random.default_rng(2)
+    vr, dr = 0.01 * rng.standard_normal((n, 3)), 0.01 * rng.standard_normal((n, 3))
+    ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP64)
+    d = [torch.from_numpy(a.copy()).cuda() for a in (pos, val, vr, dr)]
+    u = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    dw = torch.zeros_like(u)
+    ierr, m = P.vortex_stage_dev(plan, 3, 2, 0.02, 4, 1e-3, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(),
+                                 d[3].data_ptr(), n, u.data_ptr(), dw.data_ptr())
+    assert ierr == 0, P.last_error()
+    # the same stage from the separate entry points on host arrays
+    mesh = np.zeros(O.topo_shape(to))
+    assert P.pmlib_interp_particle_mesh(tg, qg, pos, val, mesh, clear=True) == 0
+    vel = np.zeros_like(mesh)
+    assert P.pmlib_poisson_solve(plan, mesh.copy(), vel) == 0
+    dv = np.zeros_like(mesh)
+    assert P.part_deriv_vorticity(tg, 4, 1e-3, mesh, vel, dv) == 0
+    pu, pdw = np.zeros((n, 3)), np.zeros((n, 3))
+    assert P.pmlib_interp_mesh_particle(tg, qg, pos, mesh_dvort=dv, mesh_vel=vel, part_dvort=pdw, part_vel=pu) == 0
+    assert rel_l2(u.cpu().numpy(), pu) < 1e-13 and rel_l2(dw.cpu().numpy(), pdw) < 1e-12
+    a = [pos.copy(), val.copy(), pu.copy(), pdw.copy(), vr.copy(), dr.copy()]
+    ierr, m2 = P.pmlib_particles_advance(pg, copy.deepcopy(tg), 3, 2, 0.02, a[0], a[1], a[2], a[3], a[4], a[5])
+    assert ierr == 0 and m2 == m and m == n - 7
+    for i, j in ((0, 0), (1, 1), (2, 4), (3, 5)):
+        assert np.allclose(d[i][:m].cpu().numpy(), a[j][:m], rtol=0, atol=1e-12), i
