@@ -185,7 +185,11 @@ __device__ __forceinline__ void z_multiply(const SolveGeom<R> &g, typename cplx_
   const int iy = min(y, g.M[1] - y);
   const int tks = __ffs(TK) - 1;  // TK is a power of two
   const R *kzt = kzs ? kzs : g.kzt;
-  for (int t = threadIdx.x; t < N * TK; t += blockDim.x) {
+  // a thread's points are taken U at a time: the Green's function values and
+  // wavenumbers of all U are loaded before any is used, so that their global-memory
+  // latencies overlap
+  const bool pre = NC == 3 && zmode != Z_REGULARISE && !g.allper && !g.kernel2;
+  auto point = [&](int t, R kxp, R Gp) {
     const int q = t >> tks, kk = t - (q << tks);
     const int z = zpos ? zpos[q] : q;
     const int kx_i = k0 + kk;
@@ -193,9 +197,9 @@ __device__ __forceinline__ void z_multiply(const SolveGeom<R> &g, typename cplx_
     if (kx_i >= g.H) {
 #pragma unroll
       for (int c = 0; c < NC; c++) v[c] = mk(R(0), R(0));
-      continue;
+      return;
     }
-    const R kx = g.kxt[kx_i], kz = kzt[z];
+    const R kx = kxp, kz = kzt[z];
     const R kxc = (2 * kx_i == g.M[0]) ? R(0) : kx;
     const R kzc = (2 * z == g.M[2]) ? R(0) : kz;
     const R kmag = kx * kx + ky * ky + kz * kz;
@@ -203,7 +207,7 @@ __device__ __forceinline__ void z_multiply(const SolveGeom<R> &g, typename cplx_
       const R zt = zeta_filter<R>(g.order, g.eps2pi * sqrt(kmag)) * g.scale;
 #pragma unroll
       for (int c = 0; c < NC; c++) v[c] = cscale(v[c], zt);
-      continue;
+      return;
     }
     if constexpr (NC == 3) {
       R zt = R(1);
@@ -245,14 +249,13 @@ __device__ __forceinline__ void z_multiply(const SolveGeom<R> &g, typename cplx_
           v[1] = o2;
           v[2] = o3;
         }
-        continue;
+        return;
       }
       R G;
       if (g.allper) {
         G = (kmag > R(0)) ? zt / (twopi * twopi * kmag) * g.scale : R(0);
       } else {
-        const int iz = min(z, g.M[2] - z);
-        G = g.green[((size_t)iz * g.gM1 + iy) * g.H + kx_i];
+        G = Gp;
       }
       const C w1 = v[0], w2 = v[1], w3 = v[2];
       if (zmode == Z_VEL) {
@@ -282,6 +285,33 @@ __device__ __forceinline__ void z_multiply(const SolveGeom<R> &g, typename cplx_
         v[1] = o2;
         v[2] = o3;
       }
+    }
+  };
+  constexpr int U = 4;
+  const int total = N * TK;
+  for (int t0 = threadIdx.x; t0 < total; t0 += U * blockDim.x) {
+    R kxv[U], Gv[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * (int)blockDim.x;
+      kxv[u] = R(0);
+      Gv[u] = R(0);
+      if (t < total) {
+        const int q = t >> tks, kk = t - (q << tks);
+        const int kx_i = k0 + kk;
+        if (kx_i < g.H) {
+          kxv[u] = g.kxt[kx_i];
+          if (pre) {
+            const int z = zpos ? zpos[q] : q;
+            Gv[u] = g.green[((size_t)min(z, g.M[2] - z) * g.gM1 + iy) * g.H + kx_i];
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int t = t0 + u * (int)blockDim.x;
+      if (t < total) point(t, kxv[u], Gv[u]);
     }
   }
 }
