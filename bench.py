@@ -414,11 +414,35 @@ def main():
             raise RuntimeError(P.last_error())
         torch.cuda.synchronize()
         dt = max_over_ranks(time.perf_counter() - t0)
+        # the copies alone (same bytes, same pinned buffers, uploads on one stream and
+        # the download on another, no step): the PCIe ceiling of the pipelined rate
+        dpos, dvort, dvel = (torch.empty_like(pos32) for _ in range(3))
+        cu, cd = torch.cuda.Stream(), torch.cuda.Stream()
+
+        def copies_only():
+            with torch.cuda.stream(cu):
+                dpos.copy_(hp[0], non_blocking=True)
+                dvort.copy_(hv[0], non_blocking=True)
+            with torch.cuda.stream(cd):
+                hu[0].copy_(dvel, non_blocking=True)
+
+        copies_only()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            copies_only()
+        torch.cuda.synchronize()
+        dtc = max_over_ranks(time.perf_counter() - t0)
+        del dpos, dvort, dvel
         e2e = {"value": world * ke / dt, "unit": "steps/s", "h2d_bytes_per_step": 24 * n,
                "d2h_bytes_per_step": 12 * n, "steps": ke,
                "api": "pmgpu_step_many (host pointers, pinned; copies of neighbouring steps overlap each step)",
                "single_step": {"value": world * ke / dt1, "unit": "steps/s",
-                               "api": "pmgpu_step (one call per step, copies and GPU work in sequence)"}}
+                               "api": "pmgpu_step (one call per step, copies and GPU work in sequence)"},
+               "copy_bound": {"value": world * ke / dtc, "unit": "steps/s",
+                              "h2d_gbs": 24 * n * ke / dtc / 1e9,
+                              "what": "the same H2D and D2H bytes per step with no step, uploads and download "
+                                      "on two streams: the rate the pipelined path cannot exceed"}}
 
     # ---- one full stage of the vortex client's RK3 step (P2M, solve, right-hand side,
     # M2P of velocity and right-hand side, stage update with the particle map)

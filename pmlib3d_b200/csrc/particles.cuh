@@ -643,16 +643,49 @@ template <typename R, int W>
 __global__ void __launch_bounds__(M2P_THREADS) k_m2p_tile(PartGeom<R> g, const R *__restrict__ pos,
                                                           const unsigned *__restrict__ start,
                                                           const int *__restrict__ perm, const R *__restrict__ f,
-                                                          R *__restrict__ o) {
+                                                          R *__restrict__ o, int3 org) {
   constexpr int off = Stencil<W>::off;
   constexpr int CX = M2P_TX + W - 1, CY = M2P_TY + W - 1, CZ = M2P_TZ + W - 1, NR = M2P_TY * M2P_TZ;
   constexpr int PLANE = CZ * CY * CX;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R *cells = reinterpret_cast<R *>(smem_raw);  // [3][CZ][CY][CX]
   __shared__ int rs[NR + 1], rg[NR];
-  const int x0 = blockIdx.x * M2P_TX, y0 = blockIdx.y * M2P_TY, z0 = blockIdx.z * M2P_TZ;
+  // tile origin in bins; org (<= 0) puts the tile edges on the first interior bin, so
+  // that one particle per cell fills whole 32-bin rows (warp-aligned, no empty tiles)
+  const int x0 = blockIdx.x * M2P_TX + org.x, y0 = blockIdx.y * M2P_TY + org.y, z0 = blockIdx.z * M2P_TZ + org.z;
   const int cx0 = x0 - (W - 1), cy0 = y0 - (W - 1), cz0 = z0 - (W - 1);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  // ---- particle ranges of the bin rows (two rows a lane, NR <= 64)
+  static_assert(NR <= 64, "one warp scans the bin rows of a tile");
+  if (threadIdx.x < 32) {
+    int len[2] = {0, 0};
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int r = 2 * lane + h;
+      int gs = 0;
+      if (r < NR) {
+        const int by = y0 + r % M2P_TY, bz = z0 + r / M2P_TY;
+        if (by >= 0 && bz >= 0 && by < g.nb[1] && bz < g.nb[2]) {
+          const unsigned rb = (unsigned)g.nb[0] * ((unsigned)by + (unsigned)g.nb[1] * (unsigned)bz);
+          gs = (int)start[rb + (unsigned)max(x0, 0)];
+          len[h] = (int)start[rb + (unsigned)min(x0 + M2P_TX, g.nb[0])] - gs;
+        }
+        rg[r] = gs;
+      }
+    }
+    int x = len[0] + len[1];
+#pragma unroll
+    for (int o2 = 1; o2 < 32; o2 <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o2);
+      if (lane >= o2) x += y;
+    }
+    const int ex = x - len[0] - len[1];
+    if (2 * lane < NR) rs[2 * lane] = ex;
+    if (2 * lane + 1 < NR) rs[2 * lane + 1] = ex + len[0];
+    if (lane == 31) rs[NR] = x;
+  }
+  __syncthreads();
+  if (rs[NR] == 0) return;  // no particle in the tile: nothing to stage
   // ---- stage the cells: one warp per cell row; lane offsets are the same in every row
   {
     constexpr int NE = (CX * 3 + 31) / 32;
@@ -680,35 +713,6 @@ __global__ void __launch_bounds__(M2P_THREADS) k_m2p_tile(PartGeom<R> g, const R
       for (int k = 0; k < NE; k++)
         if (dof[k] >= 0) dst[dof[k]] = v[k];
     }
-  }
-  // ---- particle ranges of the bin rows (two rows a lane, NR <= 64)
-  static_assert(NR <= 64, "one warp scans the bin rows of a tile");
-  if (threadIdx.x < 32) {
-    int len[2] = {0, 0};
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const int r = 2 * lane + h;
-      int gs = 0;
-      if (r < NR) {
-        const int by = y0 + r % M2P_TY, bz = z0 + r / M2P_TY;
-        if (by < g.nb[1] && bz < g.nb[2]) {
-          const unsigned rb = (unsigned)g.nb[0] * ((unsigned)by + (unsigned)g.nb[1] * (unsigned)bz);
-          gs = (int)start[rb + x0];
-          len[h] = (int)start[rb + (unsigned)min(x0 + M2P_TX, g.nb[0])] - gs;
-        }
-        rg[r] = gs;
-      }
-    }
-    int x = len[0] + len[1];
-#pragma unroll
-    for (int o2 = 1; o2 < 32; o2 <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, x, o2);
-      if (lane >= o2) x += y;
-    }
-    const int ex = x - len[0] - len[1];
-    if (2 * lane < NR) rs[2 * lane] = ex;
-    if (2 * lane + 1 < NR) rs[2 * lane + 1] = ex + len[0];
-    if (lane == 31) rs[NR] = x;
   }
   __syncthreads();
   const int total = rs[NR];

@@ -694,8 +694,15 @@ static int run_m2p_sorted_w(const pmgpu_topo *t, const R *pos, const unsigned *s
   PartGeom<R> g = part_geom<R>(t, W);
   const size_t sm = m2p_tile_smem<R, W>();
   CK(cudaFuncSetAttribute(k_m2p_tile<R, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
-  dim3 grid((g.nb[0] + M2P_TX - 1) / M2P_TX, (g.nb[1] + M2P_TY - 1) / M2P_TY, (g.nb[2] + M2P_TZ - 1) / M2P_TZ);
-  { KTimer kt_(KC_M2P, st); k_m2p_tile<R, W><<<grid, M2P_THREADS, sm, st>>>(g, pos, start, perm, f, o); }
+  // tile edges on the bin of interior cell 1 (bin 1 - blo) along each axis
+  auto org = [&](int e, int T) {
+    const int r = (1 - g.blo[e]) % T;
+    return r ? r - T : 0;
+  };
+  const int3 o3 = make_int3(org(0, M2P_TX), org(1, M2P_TY), org(2, M2P_TZ));
+  dim3 grid((g.nb[0] - o3.x + M2P_TX - 1) / M2P_TX, (g.nb[1] - o3.y + M2P_TY - 1) / M2P_TY,
+            (g.nb[2] - o3.z + M2P_TZ - 1) / M2P_TZ);
+  { KTimer kt_(KC_M2P, st); k_m2p_tile<R, W><<<grid, M2P_THREADS, sm, st>>>(g, pos, start, perm, f, o, o3); }
   PM_LAUNCHED();
   const int nblk = std::min((n + 127) / 128, 148 * 8);
   { KTimer kt_(KC_M2P, st);
