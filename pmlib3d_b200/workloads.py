@@ -11,6 +11,12 @@ configurations with their shapes and value distributions:
   omega.  16.7 M particles.
 * ``rings128`` / ``rings192``: the same field on 128^3 / 192^3 cells (scaling,
   test and profiling points).
+* ``ppf512``: 512 x 512 x 256 cells, h = 1/256 on [-1,1]^2 x [-0.5,0.5], periodic
+  along x and y, free along z; two coaxial rings about the z axis (R = 0.5,
+  sigma = 0.08) in the planes z = -+0.15 with opposite circulation, plus 1 % Gaussian
+  noise on omega.  The rings lie across the periodic plane and travel along the free
+  axis; at z = -+0.15 their 4 sigma support stays inside the free extent.  67.1 M
+  particles.
 * ``batched96`` (:func:`batch_specs`): 96 independent patches, cells per axis
   log-uniform in [32, 192], boundary types drawn from {fff, ppf, pff} (periodic
   counts rounded to even), h = 1/64, each holding a Gaussian blob
@@ -47,6 +53,11 @@ class Workload:
     interp: int            # 3 = M4'
     pos: np.ndarray        # (np, 3) float64
     vort: np.ndarray       # (np, 3) float64
+    ncell: tuple = ()      # cells per axis (n, n, n) unless given
+
+    def __post_init__(self):
+        if not self.ncell:
+            self.ncell = (self.n,) * 3
 
     @property
     def npart(self) -> int:
@@ -67,9 +78,28 @@ def _ring_vorticity(pos, x0, R, sigma, sign):
     return out
 
 
+def _ring_vorticity_z(pos, z0, R, sigma, sign):
+    """omega = sign * exp(-(d/sigma)^2) e_theta around the z axis, zero beyond 4 sigma."""
+    x, y = pos[:, 0], pos[:, 1]
+    dz = pos[:, 2] - z0
+    rho = np.sqrt(x * x + y * y)
+    d = np.sqrt((rho - R) ** 2 + dz * dz)
+    w = np.where(d < 4.0 * sigma, sign * np.exp(-(d / sigma) ** 2), 0.0)
+    rs = np.where(rho > 0, rho, 1.0)
+    out = np.zeros_like(pos)
+    out[:, 0] = -w * y / rs
+    out[:, 1] = w * x / rs
+    return out
+
+
 def _lattice(n, xmin, h, rng, jitter=0.1):
-    c = xmin + (np.arange(n, dtype=np.float64) + 0.5) * h
-    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    return _lattice_box((n, n, n), (xmin,) * 3, h, rng, jitter)
+
+
+def _lattice_box(ncell, xmin, h, rng, jitter=0.1):
+    """Cell centres of an ncell[0] x ncell[1] x ncell[2] box (x fastest), jittered."""
+    cx, cy, cz = (xmin[d] + (np.arange(ncell[d], dtype=np.float64) + 0.5) * h for d in range(3))
+    z, y, x = np.meshgrid(cz, cy, cx, indexing="ij")
     pos = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=-1)
     pos += rng.uniform(-jitter * h, jitter * h, size=pos.shape)
     return pos
@@ -90,6 +120,16 @@ def make(name: str) -> Workload:
         pos = _lattice(n, -1.0, h, rng)
         vort = _ring_vorticity(pos, -0.2, 0.5, 0.08, 1.0) + _ring_vorticity(pos, 0.2, 0.5, 0.08, -1.0)
         vort += 0.01 * np.abs(vort).max() * rng.standard_normal(vort.shape)
+    elif name == "ppf512":
+        ncell, h, cid = (512, 512, 256), 1.0 / 256, 2
+        rng = np.random.Generator(np.random.Philox(SEED + cid))
+        xmin, xmax = (-1.0, -1.0, -0.5), (1.0, 1.0, 0.5)
+        pos = _lattice_box(ncell, xmin, h, rng)
+        vort = _ring_vorticity_z(pos, -0.15, 0.5, 0.08, 1.0) + _ring_vorticity_z(pos, 0.15, 0.5, 0.08, -1.0)
+        vort += 0.01 * np.abs(vort).max() * rng.standard_normal(vort.shape)
+        return Workload(name=name, n=ncell[0], xmin=xmin, xmax=xmax, dx=(h,) * 3, bound_cond=(1, 1, 0),
+                        nghost=4, order=6, radius=2.0, interp=3, pos=np.ascontiguousarray(pos),
+                        vort=np.ascontiguousarray(vort), ncell=ncell)
     else:
         raise ValueError(f"unknown workload {name}")
     return Workload(name=name, n=n, xmin=(-1.0,) * 3, xmax=(1.0,) * 3, dx=(h,) * 3, bound_cond=(0, 0, 0),
