@@ -205,6 +205,145 @@ def run_batched(P, Wl, torch, steps, warmup, count=96, rank=0, world=1):
             "scaling": "strong: patches shared out over the ranks by bytes" if world > 1 else "single GPU"}
 
 
+def run_ppf512(P, Wl, torch, steps, warmup, stream, max_over_ranks, barrier):
+    """The 512 x 512 x 256 periodic-periodic-free step (67.1 M particles): FP32 form and
+    FP64 plain path on the same inputs, inputs resident in HBM, CUDA events on the
+    launching stream; FP32 against FP64 on the last step."""
+    w = Wl.make("ppf512")
+    n = w.npart
+    P.fft_tune(True)
+    patch = P.make_patch(w.xmin, w.xmax, w.dx, bound_cond=w.bound_cond, nghost=w.nghost)
+    ierr, topo = P.pmlib_topology_cuboid(patch, w.interp)
+    params = P.make_params(order=w.order, kernel=1, radius=w.radius, interp=w.interp)
+    ierr32, plan32 = P.pmlib_poisson_setup(patch, topo, params, P.FP32)
+    ierr64, plan64 = P.pmlib_poisson_setup(patch, topo, params, P.FP64)
+    P.fft_tune(False)
+    assert ierr32 == 0 and ierr64 == 0, P.last_error()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    pos64 = torch.from_numpy(w.pos).to(dev)
+    vort64 = torch.from_numpy(w.vort).to(dev)
+    del w.pos, w.vort
+    pos32, vort32 = pos64.float().contiguous(), vort64.float().contiguous()
+    vel32, vel64 = torch.empty_like(pos32), torch.empty_like(pos64)
+    sptr = stream.cuda_stream
+
+    def run(plan, pos, vort, vel, k):
+        for i in range(warmup + k):
+            if i == warmup:
+                torch.cuda.synchronize()
+                barrier()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            if P.step_dev(plan, pos.data_ptr(), vort.data_ptr(), n, vel.data_ptr(), sptr) != 0:
+                raise RuntimeError(P.last_error())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1)) / k
+
+    ms32 = run(plan32, pos32, vort32, vel32, steps)
+    k64 = max(3, steps // 2)
+    ms64 = run(plan64, pos64, vort64, vel64, k64)
+    d = vel32.double() - vel64
+    rel_l2 = float(torch.sqrt((d * d).sum() / (vel64 * vel64).sum()).item())
+    max_err = float((d.abs().max() / vel64.abs().max()).item())
+    pen = (512, 512, 264)  # transform input extents: periodic axes N, free axis N + 2 nghost
+    V = pen[0] * pen[1] * pen[2]
+    step_bytes = Wl.solve_bytes((512, 512, 528), pen, 4) + 2 * (24 * n + 12 * V)
+    for p in (plan32, plan64):
+        p.close()
+    return {"value": 1000.0 / ms32, "unit": "steps/s", "ms_per_step": ms32, "steps": steps,
+            "fp64_plain": {"value": 1000.0 / ms64, "unit": "steps/s", "ms_per_step": ms64, "steps": k64},
+            "fp32_speedup_vs_fp64": ms64 / ms32, "particles_per_s": n * 1000.0 / ms32,
+            "accuracy": {"rel_l2_fp32_vs_fp64": rel_l2, "max_rel_err": max_err},
+            "model_bytes_per_step_fp32": step_bytes, "achieved_gbs_fp32": step_bytes / (ms32 / 1e3) / 1e9,
+            "workload": "ppf512: 512 x 512 x 256 cells, h = 1/256 on [-1,1]^2 x [-0.5,0.5], periodic x, y, free z, "
+                        f"two coaxial rings about z (R 0.5, sigma 0.08, z = -+0.15) + 1% noise, {n} particles, "
+                        "order 6 Green's function with periodic images, eps = 2h, M4'; FFT 512 x 512 x 528",
+            "api": "pmgpu_step_dev (device arrays, P2M + solve + M2P)"}
+
+
+def run_penal512(P, torch, stream, max_over_ranks, reps=2):
+    """The penalised sphere at 512^3: one penalised solve of an impulsively started
+    sphere (zero vorticity, uniform inflow U = (1, 0, 0)), FP32 form against the FP64
+    plain path.  Sphere D = 0.25 at the centre of [-1,1]^3 (free), mask
+    chi = (1 - tanh((r - r0) / h)) / 2 (a 2h-wide transition), Brinkman parameter
+    lambda = 1e4 at CFL 0.5 (dt = 0.5 h / U) folded into the mask as the implicit
+    factor lambda dt chi / (1 + lambda dt chi); 10 passes (tolerance 0) on the box
+    with a 5-cell buffer, then the main solve."""
+    n, h = 512, 2.0 / 512
+    r0, nbuff, lam, U = 0.125, 5, 1.0e4, 1.0
+    dt = 0.5 * h / U
+    dev = torch.device("cuda", torch.cuda.current_device())
+    patch = P.make_patch((-1.0,) * 3, (1.0,) * 3, (h,) * 3, bound_cond=(0, 0, 0), nghost=4)
+    ierr, topo = P.pmlib_topology_cuboid(patch, 3)
+    params = P.make_params(order=6, kernel=1, radius=2.0, interp=3)
+    lo = [round((-r0 + 1.0) / h - nbuff) * h - 1.0 for _ in range(3)]
+    hi = [round((r0 + 1.0) / h + nbuff) * h - 1.0 for _ in range(3)]
+    bpatch = P.make_patch(lo, hi, (h,) * 3, bound_cond=(0, 0, 0), nghost=4)
+    ierr, btopo = P.pmlib_topology_cuboid(bpatch, 3)
+    bx = []
+    for d in range(3):
+        i = torch.arange(1 - btopo.nghost[2 * d], btopo.ncell[d] + btopo.nghost[2 * d + 1] + 1,
+                         dtype=torch.float64, device=dev)
+        bx.append(btopo.xmin[d] + (i - 0.5) * btopo.dx[d])
+    bz, by, bxx = torch.meshgrid(bx[2], bx[1], bx[0], indexing="ij")
+    r = torch.sqrt(bxx ** 2 + by ** 2 + bz ** 2)
+    chi = 0.5 * (1.0 - torch.tanh((r - r0) / h))
+    chi = (lam * dt * chi / (1.0 + lam * dt * chi)).unsqueeze(-1).contiguous()
+    shape = tuple(topo.ncell[2 - d] + topo.nghost[4 - 2 * d] + topo.nghost[5 - 2 * d] for d in range(3)) + (3,)
+    sptr = stream.cuda_stream
+    out = {}
+    for name, prec, dtype in (("fp32", P.FP32, torch.float32), ("fp64", P.FP64, torch.float64)):
+        P.fft_tune(True)
+        ierr, plan = P.pmlib_poisson_setup(patch, topo, params, prec)
+        ierr2, bplan = P.pmlib_poisson_setup(bpatch, btopo, params, prec)
+        P.fft_tune(False)
+        assert ierr == 0 and ierr2 == 0, P.last_error()
+        solid = chi.to(dtype).contiguous()
+        svel = torch.zeros(solid.shape[:3] + (3,), dtype=dtype, device=dev)
+        pw = torch.zeros(shape, dtype=dtype, device=dev)
+        pu = torch.zeros_like(pw)
+
+        def once():
+            pw.zero_()
+            pu.zero_()
+            pu[..., 0] = U
+            return P.penalisation_solve_dev(plan, bplan, solid.data_ptr(), svel.data_ptr(), pw.data_ptr(),
+                                            pu.data_ptr(), relaxation=1.0, tolerance=0.0, max_iter=10, dtime=dt,
+                                            fd_order=4, vel_inf=(U, 0.0, 0.0), stream=sptr)
+
+        once()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            force, npass, res = once()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[name] = {"ms_per_solve": max_over_ranks(e0.elapsed_time(e1)) / reps, "passes": npass,
+                     "force": force, "residuals": list(res),
+                     "max_vorticity": float(pw.abs().max().item())}
+        if name == "fp32":
+            w32, u32 = pw.double(), pu.double()
+        else:
+            dw, du = w32 - pw, u32 - pu
+            out["rel_l2_vort_fp32_vs_fp64"] = float(torch.sqrt((dw * dw).sum() / (pw * pw).sum()).item())
+            out["rel_l2_vel_fp32_vs_fp64"] = float(torch.sqrt((du * du).sum() / (pu * pu).sum()).item())
+            del w32, u32, dw, du
+        plan.close()
+        bplan.close()
+        del pw, pu, solid, svel
+        torch.cuda.empty_cache()
+    f32, f64 = out["fp32"]["force"][0], out["fp64"]["force"][0]
+    out["drag_rel_diff_fp32_vs_fp64"] = abs(f32 - f64) / max(abs(f64), 1e-300)
+    out["box_cells"] = list(btopo.ncell)
+    out["workload"] = ("penal512: 512^3 cells on [-1,1]^3 (free), impulsively started sphere D = 0.25 at the "
+                       "centre in U = (1,0,0), tanh mask (2h transition), lambda = 1e4 at CFL 0.5 (dt = h/2) as "
+                       "the implicit Brinkman factor, 10 box passes (FD 4) + the main solve; drag = force[0]")
+    out["api"] = "pmgpu_penalisation_solve_dev (device arrays; the host tests the residual after every pass)"
+    return out
+
+
 def run_served(P, torch, rates=(100.0, 300.0, 1000.0), count=60, budget_gb=24.0):
     """Served stream at swept Poisson arrival rates (FP32 form): solves/s, p50/p99."""
     from pmlib3d_b200 import serve as S
@@ -243,6 +382,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched and served measurements")
     ap.add_argument("--no-stage", action="store_true", help="skip the full vortex-stage measurement")
     ap.add_argument("--no-penal", action="store_true", help="skip the penalisation measurement")
+    ap.add_argument("--no-ppf512", action="store_true", help="skip the 512 x 512 x 256 ppf step")
+    ap.add_argument("--no-penal512", action="store_true", help="skip the 512^3 penalised sphere")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -531,6 +672,21 @@ def main():
                  "api": "pmgpu_penalisation_solve_dev (the host tests the residual after every pass)"}
         bplan.close()
 
+    # ---- the 512 x 512 x 256 periodic-periodic-free step (every rank: replicas)
+    ppf = None
+    if not args.no_ppf512:
+        ppf = run_ppf512(P, Wl, torch, max(4, args.steps // 2), args.warmup, stream, max_over_ranks, barrier)
+        if world > 1:
+            ppf["value"] *= world
+            ppf["fp64_plain"]["value"] *= world
+            ppf["particles_per_s"] *= world
+        torch.cuda.empty_cache()
+
+    # ---- the penalised sphere at 512^3, FP32 against FP64 (every rank: replicas)
+    penal512 = None
+    if not args.no_penal512:
+        penal512 = run_penal512(P, torch, stream, max_over_ranks)
+
     # ---- batched uneven patches (every rank: replicas) and the served stream (rank 0)
     batched = served = None
     if not args.no_batched:
@@ -566,7 +722,8 @@ def main():
             "accuracy": {"rel_l2_fp32_vs_fp64": rel_l2, "max_rel_err": max_err},
             "roofline": roofline, "kernels": kernels, "gpu_launches": launches32,
             "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "batched": batched, "served": served,
-            "vortex_stage": stage, "penalisation": penal,
+            "vortex_stage": stage, "penalisation": penal, "ppf512": ppf,
+            "penal512": penal512,
         }
         print(json.dumps(line), flush=True)
     for p in (plan32, plan64):

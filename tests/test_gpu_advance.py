@@ -283,6 +283,44 @@ def test_penalisation_fp32():
     assert rel_l2(d[3].cpu().numpy(), vo) < 1e-5
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_penalisation_smooth_mask_impulsive_start(prec):
+    """The penalised-sphere start state: zero vorticity, uniform inflow, a tanh mask
+    with the implicit Brinkman factor lambda dt chi / (1 + lambda dt chi) (lambda 1e4,
+    dt = h / 2), ten passes; drag and fields against the oracle."""
+    import torch
+    main, box = PENAL_CASES[0][1:]
+    po, to, qo, pg, tg, qg, ppo, tpo, ppg, tpg, solid, svel, w, vel = _penal_setup(main, box)
+    h = main[2][0]
+    ext = [tpo.ncell[d] + tpo.nghost[2 * d] + tpo.nghost[2 * d + 1] for d in range(3)]
+    ax = [tpo.xmin[d] + (np.arange(ext[d]) - tpo.nghost[2 * d] + 0.5) * tpo.dx[d] for d in range(3)]
+    z, y, x = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+    chi = 0.5 * (1.0 - np.tanh((np.sqrt(x * x + y * y + z * z) - 0.25) / h))
+    dt = 0.5 * h
+    solid = np.ascontiguousarray((1e4 * dt * chi / (1.0 + 1e4 * dt * chi))[..., None])
+    svel = np.zeros_like(svel)
+    w = np.zeros_like(w)
+    vel = np.zeros_like(vel)
+    vel[..., 0] = 1.0
+    kw = dict(tol=0.0, max_iter=10, dtime=dt, fd_order=4, vel_inf=(1.0, 0.0, 0.0))
+    wo, vo = w.copy(), vel.copy()
+    ierr, fo, no, ro = O.penalisation_solve(po, to, qo, ppo, tpo, solid, svel, wo, vo, relax=1.0, **kw)
+    assert ierr == 0 and no == 10 and abs(fo[0]) > 0
+    pr, dty, tol = (P.FP64, np.float64, 1e-12) if prec == "fp64" else (P.FP32, np.float32, 1e-5)
+    ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, pr)
+    assert ierr == 0
+    ierr, pplan = P.pmlib_poisson_setup(ppg, tpg, qg, pr)
+    assert ierr == 0, P.last_error()
+    d = [torch.from_numpy(a.astype(dty)).cuda() for a in (solid, svel, w, vel)]
+    fg, ng, rg = P.penalisation_solve_dev(plan, pplan, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(),
+                                          d[3].data_ptr(), relaxation=1.0, tolerance=0.0, max_iter=10,
+                                          dtime=dt, fd_order=4, vel_inf=(1.0, 0.0, 0.0))
+    assert ng == 10
+    assert abs(fg[0] - fo[0]) <= tol * 10 * abs(fo[0]), (fg, fo)
+    assert rel_l2(d[2].cpu().numpy(), wo) < tol
+    assert rel_l2(d[3].cpu().numpy(), vo) < tol
+
+
 def test_penalisation_errors():
     po, to, qo, pg, tg, qg, ppo, tpo, ppg, tpg, solid, svel, w, vel = _penal_setup(*PENAL_CASES[0][1:])
     import torch
