@@ -423,6 +423,33 @@ def test_step_fp64_and_fp32(name, xmin, xmax, dx, bc, ng):
     assert rel_l2(up32, up_o) < TOL32
 
 
+def test_ring64_step_full_size():
+    """The CPU-runnable single step at its full size: 64^3 cells on [-1,1]^3 (free),
+    one jittered particle per cell (262144), one vortex ring, order-6 Green's
+    function with eps = 2h, M4'.  FP64 and FP32 steps through the host-array call
+    against the oracle's P2M -> solve -> M2P."""
+    from pmlib3d_b200 import workloads as Wl
+    w = Wl.make("ring64")
+    po, to, qo, pg, tg, qg = setup_pair(w.xmin, w.xmax, w.dx, w.bound_cond, w.nghost, interp=w.interp,
+                                        order=w.order, radius=w.radius)
+    to.npart = w.npart
+    mo = np.zeros(O.topo_shape(to))
+    assert O.interp_particle_mesh(to, 3, w.pos, w.vort, mo) == 0
+    vel_o, _, _ = oracle_solve(po, to, qo, mo)
+    ierr, up_o = O.interp_mesh_particle(to, 3, vel_o, w.pos)
+    assert ierr == 0 and np.abs(up_o).max() > 1e-2
+    ierr, plan = P.pmlib_poisson_setup(pg, tg, qg, P.FP64)
+    assert ierr == 0
+    up = np.zeros_like(w.pos)
+    assert P.step(plan, w.pos, w.vort, up) == 0
+    assert rel_l2(up, up_o) < TOL64
+    ierr, plan32 = P.pmlib_poisson_setup(pg, tg, qg, P.FP32)
+    assert ierr == 0
+    up32 = np.zeros(w.pos.shape, np.float32)
+    assert P.step(plan32, w.pos.astype(np.float32), w.vort.astype(np.float32), up32) == 0
+    assert rel_l2(up32, up_o) < TOL32
+
+
 @pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", [CASES[0], CASES[2]])
 @pytest.mark.parametrize("interp", [3, 4])
 def test_step_stray_particles(name, xmin, xmax, dx, bc, ng, interp):
