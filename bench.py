@@ -87,6 +87,12 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def workload_desc(w):
+    """The config.workload string of both arms (same workload, same words)."""
+    return (f"{w.name}: {w.n}^3 cells, free-free-free, two coaxial rings + 1% noise, {w.npart} particles, "
+            f"order 6 Green's function, eps = 2h, M4'")
+
+
 # ------------------------------------------------------------------ CPU oracle (baseline / reference arm)
 def oracle_setup(w, threads):
     from oracle import oracle as O
@@ -101,46 +107,23 @@ def oracle_setup(w, threads):
     return O, po, t, par, pk
 
 
-def oracle_step(O, po, t, par, pk, w, frac):
-    O.set_sample(frac)
+def oracle_step(O, po, t, par, pk, w):
+    """One whole oracle step (P2M, solve, M2P) on the full workload; returns
+    (seconds, particle velocities)."""
     mesh = np.zeros(O.topo_shape(t))
     t0 = time.perf_counter()
     O.interp_particle_mesh(t, w.interp, w.pos, w.vort, mesh)
     ierr, vel, _ = O.poisson_solve(po, t, par, pk, mesh)
     ierr, up = O.interp_mesh_particle(t, w.interp, vel, w.pos)
     dt = time.perf_counter() - t0
-    O.set_sample(1.0)
-    return dt
-
-
-def pick_fraction(O, po, t, par, pk, w, target_s):
-    """Sample fraction of the particles and FFT lines whose oracle step takes about
-    target_s.  Two calibration steps at 1/64 and 1/16 of the work fit t(f) = a + b f:
-    `a` is the part of a step that does not shrink with the sample (the solve's
-    full-size work arrays), `b` the cost of all of the sampled work.  Returns
-    (f, a, b); a full step takes about a + b."""
-    f0, f1 = 1.0 / 64, 1.0 / 16
-    d0 = oracle_step(O, po, t, par, pk, w, f0)
-    d1 = oracle_step(O, po, t, par, pk, w, f1)
-    b = max((d1 - d0) / (f1 - f0), 1e-6)
-    a = max(d0 - b * f0, 0.0)
-    f = min(1.0, max(f0, (target_s - a) / b))
-    return f, a, b
-
-
-def full_step_time(dt, f, a):
-    """Time of a whole step from one sampled step of fraction f: the fixed part a
-    once, the sampled part scaled by 1/f (the step itself when f = 1)."""
-    if f >= 1.0:
-        return dt
-    return a + max(dt - a, 0.0) / f
+    return dt, up
 
 
 def run_reference(args):
     """--impl reference: the reference's algorithm on the host cores.  The Fortran/MPI
     reference cannot be built on these machines (no gfortran, MPI or FFTW), so this
-    times the C restatement of its plain path (oracle/), with all host threads, each
-    step a uniform sample of the full-size workload."""
+    times the C restatement of its plain path (oracle/), with all host threads, over
+    whole steps of the full-size workload (no sampling)."""
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
@@ -148,24 +131,19 @@ def run_reference(args):
     w = Wl.make(args.config)
     threads = os.cpu_count() or 1
     O, po, t, par, pk = oracle_setup(w, threads)
-    budget = 150.0  # seconds for the whole run
-    f, a, b = pick_fraction(O, po, t, par, pk, w, budget / max(1, args.steps + args.warmup))
     for _ in range(args.warmup):
-        oracle_step(O, po, t, par, pk, w, f)
+        oracle_step(O, po, t, par, pk, w)
     tot = 0.0
     for _ in range(args.steps):
-        tot += full_step_time(oracle_step(O, po, t, par, pk, w, f), f, a)
+        tot += oracle_step(O, po, t, par, pk, w)[0]
     value = args.steps / tot
-    sample = (f"each step: oracle P2M + solve + M2P over the first {f:.4f} of the particles and of the "
-              f"FFT lines of the full {w.n}^3 workload; whole-step time = a + (sampled time - a) / fraction "
-              f"with a = {a:.2f} s the per-step cost that does not shrink with the sample (calibrated at "
-              f"1/64 and 1/16: a full step ~{a + b:.1f} s on {threads} threads)")
+    sample = (f"whole steps: oracle P2M + solve + M2P over all {w.npart} particles of the full {w.n}^3 workload "
+              f"({tot / args.steps:.2f} s a step on {threads} threads)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Philox)",
-            "config": {"workload": f"{w.name}: {w.n}^3 fff, two coaxial rings + 1% noise, {w.npart} particles, "
-                                   f"order 6, eps = 2h, M4'", "parallelism": "host threads"},
+            "config": {"workload": workload_desc(w), "parallelism": "host threads"},
             "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -520,9 +498,11 @@ def main():
             continue
         kernels[k] = {"ms_per_step": kms / nprof, "launches_per_step": cnt / nprof}
         if k in mb:
-            kernels[k]["model_bytes_per_launch"] = mb[k]
-            kernels[k]["achieved_gbs"] = mb[k] / (kms / cnt / 1e3) / 1e9
-    modeled = {k: v for k, v in kernels.items() if "model_bytes_per_launch" in v}
+            # the model's bytes are those of the whole step's work of this kernel class
+            # (M2P: the tiled launch and the launch for particles outside every bin)
+            kernels[k]["model_bytes_per_step"] = mb[k]
+            kernels[k]["achieved_gbs"] = mb[k] / (kms / nprof / 1e3) / 1e9
+    modeled = {k: v for k, v in kernels.items() if "model_bytes_per_step" in v}
     dom = max(modeled, key=lambda k: modeled[k]["ms_per_step"])
     peaks = {}
     pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -538,7 +518,8 @@ def main():
     achieved = kernels[dom]["achieved_gbs"]
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
-                "algorithmic_bytes_per_launch": mb[dom]}
+                "algorithmic_bytes_per_launch": mb[dom] / kernels[dom]["launches_per_step"],
+                "launches_per_step": kernels[dom]["launches_per_step"]}
 
     # ---- end to end through the C ABI with host buffers (H2D + step + D2H per step)
     e2e = None
@@ -707,32 +688,36 @@ def main():
             served = run_served(P, torch)
         barrier()
 
-    # ---- CPU baseline: the oracle on this box's host cores (rank 0, one GPU only)
-    cpu = None
+    # ---- CPU baseline: the oracle on this box's host cores (rank 0, one GPU only), one
+    # whole step on the same inputs; its velocities pin the FP64 and FP32 GPU steps
+    cpu = oracle_acc = None
     if not args.no_cpu_baseline and world == 1 and rank == 0:
         threads = os.cpu_count() or 1
         O, po, t, par, pk = oracle_setup(w, threads)
-        f, a, b = pick_fraction(O, po, t, par, pk, w, 15.0)
-        dt = oracle_step(O, po, t, par, pk, w, f)
-        cpu = {"value": 1.0 / full_step_time(dt, f, a), "unit": "steps/s", "cores": threads, "kind": "port",
-               "sample": f"oracle (C restatement of the reference's plain FP64 path) P2M + solve + M2P over "
-                         f"the first {f:.4f} of the particles and FFT lines of the full workload, {dt:.1f} s; "
-                         f"whole-step time = a + (time - a) / fraction with a = {a:.2f} s the per-step cost "
-                         f"that does not shrink with the sample (calibrated at 1/64 and 1/16)"}
+        dt, up = oracle_step(O, po, t, par, pk, w)
+        cpu = {"value": 1.0 / dt, "unit": "steps/s", "cores": threads, "kind": "port",
+               "sample": f"one whole step: oracle (C restatement of the reference's plain FP64 path) P2M + solve + "
+                         f"M2P over all {n} particles of the full workload, {dt:.2f} s"}
+        ref = torch.from_numpy(up).to(dev)
+        oracle_acc = {}
+        for name, v in (("fp64", vel64), ("fp32", vel32)):
+            d = v.double() - ref
+            oracle_acc[f"rel_l2_{name}_vs_oracle"] = float(torch.sqrt((d * d).sum() / (ref * ref).sum()).item())
+            oracle_acc[f"max_rel_err_{name}_vs_oracle"] = float((d.abs().max() / ref.abs().max()).item())
+        del ref, d
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox)",
-            "config": {"workload": f"{w.name}: {w.n}^3 cells, free-free-free, two coaxial rings + 1% noise, "
-                                   f"{n} particles, order 6 Green's function, eps = 2h, M4'",
+            "config": {"workload": workload_desc(w),
                        "grid": f"N={w.n}, nghost={w.nghost}, FFT M={2 * (w.n + 2 * w.nghost)}",
                        "parallelism": f"replicas x{world}", "l2": L2_NOTE},
             "fft_schedules": [e for e in P.fft_tuned() if e["length"] in (2 * (w.n + 2 * w.nghost),)],
             "fp64_plain": {"value": value64, "unit": "steps/s", "ms_per_step": ms64 / k64},
             "particles_per_s": value * n, "fp32_speedup_vs_fp64": value / value64,
-            "accuracy": {"rel_l2_fp32_vs_fp64": rel_l2, "max_rel_err": max_err},
+            "accuracy": {"rel_l2_fp32_vs_fp64": rel_l2, "max_rel_err": max_err, **(oracle_acc or {})},
             "roofline": roofline, "kernels": kernels, "gpu_launches": launches32,
             "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "batched": batched, "served": served,
             "vortex_stage": stage, "penalisation": penal, "ppf512": ppf,

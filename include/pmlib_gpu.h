@@ -101,6 +101,20 @@ int pmgpu_interp_mesh_particle_f32(const pmgpu_topo *topo, const pmgpu_params *p
                                    const float *mesh_vel, const float *pos, int npart,
                                    float *part_vort, float *part_dvort, float *part_vel);
 
+/* The particle order pmgpu_interp_particle_mesh deposits from (no counterpart in the
+ * reference, whose particle loop runs in index order,
+ * source/interpolation/pmlib_interp_particle_mesh.f:137-483).  For xpart(3, npart)
+ * (double, or float with precision PMGPU_FP32) it returns each particle's bin key
+ * (base cell NINT((x - xmin) / dx), :153-155, flattened over the bin box of
+ * (nx' + W - 1)(ny' + W - 1)(nz' + W - 1) bins, x fastest; the bin count itself for a
+ * particle the deposition skips), the stable order of the particles by key (ties in
+ * index order: each cell receives its contributions in ascending particle index, as
+ * in the reference) and the bin starts (bin count + 1 entries).  Any output may be
+ * NULL.  For inspection and tests. */
+int pmgpu_p2m_sort_order(const pmgpu_topo *topo, const pmgpu_params *par, int precision,
+                         const void *xpart, int npart, unsigned *keys, int *order,
+                         unsigned *bin_start);
+
 /* ---- Poisson solver (source/pmlib_poisson.f:5-30) ---- */
 
 /* pmlib_poisson_setup, source/poisson/pmlib_poisson_setup.f:5-19.  `precision` is

@@ -86,6 +86,8 @@ def lib():
         L.pmo_interp_particle_mesh.argtypes = [C.POINTER(Topo), C.c_int, dp, dp, C.c_int, C.c_int,
                                                dp, C.c_int, C.c_int, C.c_int]
         L.pmo_interp_mesh_particle.argtypes = [C.POINTER(Topo), C.c_int, dp, dp, dp, C.c_int]
+        L.pmo_p2m_bins.argtypes = [C.POINTER(Topo), C.c_int, dp, C.c_int, ip, ip]
+        L.pmo_p2m_bins_f32.argtypes = [C.POINTER(Topo), C.c_int, C.POINTER(C.c_float), C.c_int, ip, ip]
         L.pmo_fft_line.argtypes = [dp, dp, C.c_int]
         L.pmo_ifft_line.argtypes = [dp, dp, C.c_int]
         L.pmo_kernel_dims.argtypes = [C.POINTER(Patch), C.POINTER(Params), ip, ip]
@@ -190,6 +192,38 @@ def interp_particle_mesh(t, order, xpart, part, mesh, clear=True, clear_ghost=Fa
     return lib().pmo_interp_particle_mesh(C.byref(t), order, _p(xpart), _p(part), nvar,
                                           part.shape[0], _p(mesh), mesh.shape[-1], int(clear),
                                           int(clear_ghost))
+
+
+def p2m_sort(t, order, xpart):
+    """The deposition order of the reference's P2M restated as a sort: each particle's
+    bin key (base cell NINT((x - xmin) / dx) per axis, pmlib_interp_particle_mesh.f:
+    153-155, flattened x fastest over the bin box that starts W - 1 - off cells below
+    the first cuboid point; the bin count for particles that add nothing, :172-177,
+    :229-246) and the particles stably sorted by key, so each cell sees its
+    contributions in ascending particle index as in the reference's particle loop.
+    float32 positions follow the single-precision build.  Returns (keys, order)."""
+    n = xpart.shape[0]
+    base = np.zeros((n, 3), np.int32)
+    flag = np.zeros(n, np.int32)
+    ip = C.POINTER(C.c_int)
+    if xpart.dtype == np.float32:
+        x = np.ascontiguousarray(xpart)
+        ierr = lib().pmo_p2m_bins_f32(C.byref(t), order, x.ctypes.data_as(C.POINTER(C.c_float)), n,
+                                      base.ctypes.data_as(ip), flag.ctypes.data_as(ip))
+    else:
+        ierr = lib().pmo_p2m_bins(C.byref(t), order, _p(np.ascontiguousarray(xpart)), n,
+                                  base.ctypes.data_as(ip), flag.ctypes.data_as(ip))
+    assert ierr == 0
+    W, off = (4, 1) if order == 3 else (6, 2)
+    nb, blo = [], []
+    for d in range(3):
+        ext = t.ncell[d] + t.nghost[2 * d] + t.nghost[2 * d + 1]
+        nb.append(ext + W - 1)
+        blo.append(1 - t.nghost[2 * d] - (W - 1 - off))
+    b = base.astype(np.int64) - np.array(blo, np.int64)
+    keys = b[:, 0] + nb[0] * (b[:, 1] + nb[1] * b[:, 2])
+    keys = np.where(flag != 0, keys, nb[0] * nb[1] * nb[2]).astype(np.uint32)
+    return keys, np.argsort(keys, kind="stable").astype(np.int32)
 
 
 def interp_mesh_particle(t, order, mesh, pos):

@@ -379,6 +379,61 @@ int pmo_interp_particle_mesh(const pmo_topo *t, int order, const double *xpart,
   return 0;
 }
 
+/* The per-particle index arithmetic of P2M without the deposit: the base cell
+ * NINT((x - xmin) * (1/dx)) of every particle (interp_particle_mesh.f:153-155) and
+ * whether the particle adds anything to the mesh: its stencil meets the cuboid
+ * (:172-177) and it is not outside [xmin, xmax] across a periodic face, where all
+ * its weights are zeroed (:229-246).  base is (3, npart), flag (npart). */
+int pmo_p2m_bins(const pmo_topo *t, int order, const double *xpart, int npart, int *base, int *flag) {
+  if (order != 3 && order != 4) return -1;
+  const int W = (order == 3) ? 4 : 6, off = (order == 3) ? 1 : 2;
+  double c_1_d[3];
+  for (int e = 0; e < 3; e++) c_1_d[e] = 1.0 / t->dx[e];
+  for (int p = 0; p < npart; p++) {
+    const double *x = xpart + (size_t)3 * p;
+    int ok = 1;
+    for (int e = 0; e < 3; e++) {
+      const int b = nint((x[e] - t->xmin[e]) * c_1_d[e]);
+      const int lo = 1 - t->nghost[2 * e], hi = t->ncell[e] + t->nghost[2 * e + 1];
+      if (!(b - off + W - 1 >= lo && b - off <= hi)) ok = 0;
+      if (t->bound_cond[2 * e] != 0 && x[e] < t->xmin[e]) ok = 0;
+      if (t->bound_cond[2 * e + 1] != 0 && x[e] > t->xmax[e]) ok = 0;
+      base[(size_t)3 * p + e] = b;
+    }
+    flag[p] = ok;
+  }
+  return 0;
+}
+
+/* The same in single precision: the reference built with -D__single (REAL(MK) = 4
+ * bytes; source/pmlib_parameters.f:15-31) forms (x - xmin) * (1/dx) in single and
+ * rounds it with NINT. */
+int pmo_p2m_bins_f32(const pmo_topo *t, int order, const float *xpart, int npart, int *base, int *flag) {
+  if (order != 3 && order != 4) return -1;
+  const int W = (order == 3) ? 4 : 6, off = (order == 3) ? 1 : 2;
+  float c_1_d[3], xmin[3], xmax[3];
+  for (int e = 0; e < 3; e++) {
+    c_1_d[e] = 1.0f / (float)t->dx[e];
+    xmin[e] = (float)t->xmin[e];
+    xmax[e] = (float)t->xmax[e];
+  }
+  for (int p = 0; p < npart; p++) {
+    const float *x = xpart + (size_t)3 * p;
+    int ok = 1;
+    for (int e = 0; e < 3; e++) {
+      const float s = (x[e] - xmin[e]) * c_1_d[e];
+      const int b = (int)lroundf(s);
+      const int lo = 1 - t->nghost[2 * e], hi = t->ncell[e] + t->nghost[2 * e + 1];
+      if (!(b - off + W - 1 >= lo && b - off <= hi)) ok = 0;
+      if (t->bound_cond[2 * e] != 0 && x[e] < xmin[e]) ok = 0;
+      if (t->bound_cond[2 * e + 1] != 0 && x[e] > xmax[e]) ok = 0;
+      base[(size_t)3 * p + e] = b;
+    }
+    flag[p] = ok;
+  }
+  return 0;
+}
+
 /* source/interpolation/pmlib_interp_mesh_particle.f:76-409 (M4') and :412-1266 (M6*).
  * M4' keeps the reference's use of 1/dx(1) for the y and z offsets (:115-116). */
 int pmo_interp_mesh_particle(const pmo_topo *t, int order, const double *mesh,

@@ -70,6 +70,8 @@ int pmo_interp_particle_mesh(const pmo_topo *topo, int order, const double *xpar
                              const double *part, int nvar, int npart,
                              double *mesh, int nvar_mesh, int clear, int clear_ghost);
 
+int pmo_p2m_bins(const pmo_topo *topo, int order, const double *xpart, int npart, int *base, int *flag);
+int pmo_p2m_bins_f32(const pmo_topo *topo, int order, const float *xpart, int npart, int *base, int *flag);
 int pmo_interp_mesh_particle(const pmo_topo *topo, int order, const double *mesh,
                              const double *pos, double *out, int npart);
 

@@ -25,7 +25,7 @@ EXPORTS = (
     "pmgpu_particles_advance", "pmgpu_particles_advance_f32", "pmgpu_particles_advance_dev",
     "pmgpu_vortex_stage_dev", "pmgpu_fft_set_schedule", "pmgpu_step_many", "pmgpu_penalisation_solve_dev",
     "pmgpu_output_mesh", "pmgpu_output_pvti", "pmgpu_output_topology", "pmgpu_output_particles",
-    "pmgpu_input_particles", "pmgpu_poisson_setup_ppf",
+    "pmgpu_input_particles", "pmgpu_poisson_setup_ppf", "pmgpu_p2m_sort_order",
 )
 
 
@@ -72,6 +72,7 @@ def lib():
         "pmgpu_topology_cuboid": [PP, C.c_int, TP],
         "pmgpu_interp_particle_mesh": [TP, QP, dp, dp, C.c_int, C.c_int, dp, C.c_int, C.c_int, C.c_int],
         "pmgpu_interp_particle_mesh_f32": [TP, QP, fp, fp, C.c_int, C.c_int, fp, C.c_int, C.c_int, C.c_int],
+        "pmgpu_p2m_sort_order": [TP, QP, C.c_int, vp, C.c_int, C.POINTER(C.c_uint), ip, C.POINTER(C.c_uint)],
         "pmgpu_interp_mesh_particle": [TP, QP, dp, dp, dp, dp, C.c_int, dp, dp, dp],
         "pmgpu_interp_mesh_particle_f32": [TP, QP, fp, fp, fp, fp, C.c_int, fp, fp, fp],
         "pmgpu_poisson_setup": [PP, TP, QP, C.c_int, C.POINTER(vp)],

@@ -45,12 +45,22 @@ def _obj(unit: str) -> str:
     return os.path.join(BUILD, os.path.splitext(os.path.basename(unit))[0] + ".o")
 
 
+def _deps(unit: str) -> list:
+    """The unit and the project headers it includes (nvcc -M), all headers if that fails."""
+    r = subprocess.run([nvcc(), "-std=c++17", "-M", unit], capture_output=True, text=True)
+    if r.returncode != 0:
+        return [unit, *HEADERS]
+    words = r.stdout.replace("\\\n", " ").split()
+    own = {os.path.realpath(h) for h in HEADERS}
+    return [unit] + [w for w in words if os.path.realpath(w) in own]
+
+
 def _stale(unit: str) -> bool:
     o = _obj(unit)
     if not os.path.exists(o):
         return True
     t = os.path.getmtime(o)
-    return any(os.path.getmtime(f) > t for f in [unit, *HEADERS] if os.path.exists(f))
+    return any(os.path.getmtime(f) > t for f in _deps(unit) if os.path.exists(f))
 
 
 def up_to_date() -> bool:

@@ -586,12 +586,12 @@ struct PartScratchRefs {
   DevBuf *key, *val, *key2, *val2, *counts, *start, *spart, *hist;
 };
 
-// P2M on device arrays.  clear_mode: 0 add, 1 clear, 2 clear ghosts.  On return
-// *perm_out (if given) points at the sorted particle order.
+// Bin keys and the stable sort of the particles by bin (the first half of P2M): on
+// return s.key holds every particle's bin key (nbins for particles P2M skips) and
+// s.val2 the sorted order, s.start the bin starts (nbins + 1 entries).
 template <typename R>
-static int run_p2m(const pmgpu_topo *t, int order, const R *pos, const R *val, int nvar, int n, R *mesh,
-                   int nvar_mesh, int clear_mode, PartScratchRefs s, cudaStream_t st, const int **perm_out,
-                   const char *caller) {
+static int run_bin_sort(const pmgpu_topo *t, int order, const R *pos, int n, PartScratchRefs s, cudaStream_t st,
+                        const char *caller) {
   const int W = (order == 3) ? 4 : 6;
   PartGeom<R> g = part_geom<R>(t, W);
   const unsigned long long nb_total = (unsigned long long)g.nb[0] * g.nb[1] * g.nb[2];
@@ -631,6 +631,19 @@ static int run_p2m(const pmgpu_topo *t, int order, const R *pos, const R *val, i
     PM_LAUNCHED();
     CKL(caller);
   }
+  return 0;
+}
+
+// P2M on device arrays.  clear_mode: 0 add, 1 clear, 2 clear ghosts.  On return
+// *perm_out (if given) points at the sorted particle order.
+template <typename R>
+static int run_p2m(const pmgpu_topo *t, int order, const R *pos, const R *val, int nvar, int n, R *mesh,
+                   int nvar_mesh, int clear_mode, PartScratchRefs s, cudaStream_t st, const int **perm_out,
+                   const char *caller) {
+  if (run_bin_sort<R>(t, order, pos, n, s, st, caller)) return -1;
+  const int W = (order == 3) ? 4 : 6;
+  PartGeom<R> g = part_geom<R>(t, W);
+  const int *perm = s.val2->as<int>();
   // deposition, components in groups of at most three
   const int zc = (W == 4) ? 32 : 30;
   dim3 grid((g.ext[0] + DEP_TX - 1) / DEP_TX, (g.ext[1] + DEP_TY - 1) / DEP_TY, (g.ext[2] + zc - 1) / zc);
@@ -847,9 +860,9 @@ static std::string green_key(const pmgpu_plan *pl) {
   char b[512];
   const pmgpu_patch &p = pl->patch;
   snprintf(b, sizeof(b), "%d|%d|%d|%a,%a,%a|%d,%d,%d|%d,%d,%d|%d,%d,%d,%d|%d,%d,%a", dev, pl->green_mode, pl->prec,
-           p.dx[2], pl->g.M[0], pl->g.M[1], pl->g.M[2], p.bound_cond[0], p.bound_cond[1], p.bound_cond[2], p.ncell[0],
-           p.ncell[1], p.ncell[2], p.nghost, pl->par.poisson_order, pl->par.poisson_kernel,
-           pl->par.regularisation_radius);
+           p.dx[0], p.dx[1], p.dx[2], pl->g.M[0], pl->g.M[1], pl->g.M[2], p.bound_cond[0], p.bound_cond[1],
+           p.bound_cond[2], p.ncell[0], p.ncell[1], p.ncell[2], p.nghost, pl->par.poisson_order,
+           pl->par.poisson_kernel, pl->par.regularisation_radius);
   return std::string(b);
 }
 
@@ -1412,6 +1425,37 @@ int pmgpu_interp_particle_mesh_f32(const pmgpu_topo *topo, const pmgpu_params *p
                                    const float *part, int nvar, int npart, float *mesh, int nvar_mesh, int clear,
                                    int clear_ghost) {
   return p2m_host<float>(topo, par, xpart, part, nvar, npart, mesh, nvar_mesh, clear, clear_ghost);
+}
+
+// The bin keys and sorted particle order P2M deposits from (host arrays out)
+template <typename R>
+static int p2m_order_host(const pmgpu_topo *t, const pmgpu_params *par, const R *xpart, int npart, unsigned *keys,
+                          int *order, unsigned *bin_start) {
+  const char *caller = "pmgpu_p2m_sort_order";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (npart < 0) {
+    set_error(caller, "Discrepancy in number of particles");
+    return -1;
+  }
+  if (check_interp(par, caller) || ensure_device(caller)) return -1;
+  Scratch &s = scratch();
+  if (s.a.ensure(sizeof(R) * 3 * (size_t)std::max(npart, 1), caller)) return -1;
+  if (npart > 0) CK(cudaMemcpy(s.a.p, xpart, sizeof(R) * 3 * (size_t)npart, cudaMemcpyHostToDevice), caller);
+  PartScratchRefs r{&s.key, &s.val, &s.key2, &s.val2, &s.counts, &s.start, &s.spart, &s.hist};
+  if (run_bin_sort<R>(t, par->interpolation_order, s.a.as<R>(), npart, r, 0, caller)) return -1;
+  const PartGeom<R> g = part_geom<R>(t, par->interpolation_order == 3 ? 4 : 6);
+  if (npart > 0 && keys) CK(cudaMemcpy(keys, s.key.p, sizeof(unsigned) * npart, cudaMemcpyDeviceToHost), caller);
+  if (npart > 0 && order) CK(cudaMemcpy(order, s.val2.p, sizeof(int) * npart, cudaMemcpyDeviceToHost), caller);
+  if (bin_start)
+    CK(cudaMemcpy(bin_start, s.start.p, sizeof(unsigned) * ((size_t)g.nbins + 1), cudaMemcpyDeviceToHost), caller);
+  return 0;
+}
+
+int pmgpu_p2m_sort_order(const pmgpu_topo *topo, const pmgpu_params *par, int precision, const void *xpart,
+                         int npart, unsigned *keys, int *order, unsigned *bin_start) {
+  if (precision == PMGPU_FP32)
+    return p2m_order_host<float>(topo, par, static_cast<const float *>(xpart), npart, keys, order, bin_start);
+  return p2m_order_host<double>(topo, par, static_cast<const double *>(xpart), npart, keys, order, bin_start);
 }
 
 template <typename R>

@@ -114,6 +114,27 @@ def pmlib_interp_particle_mesh(topo: Topo, params: Params, xpart, part, mesh, cl
              part.shape[0], _ptr(mesh, dt), mesh.shape[-1], int(bool(clear)), int(bool(clear_ghost)))
 
 
+def p2m_sort_order(topo: Topo, params: Params, xpart):
+    """The bin keys, the stable particle order and the bin starts the deposition of
+    `xpart` (float64, or float32 for the FP32 form) works from; raises on error."""
+    dt = xpart.dtype
+    n = xpart.shape[0]
+    W = 4 if params.interpolation_order == 3 else 6
+    nb = 1
+    for d in range(3):
+        nb *= topo.ncell[d] + topo.nghost[2 * d] + topo.nghost[2 * d + 1] + W - 1
+    keys = np.zeros(n, np.uint32)
+    order = np.zeros(n, np.int32)
+    start = np.zeros(nb + 1, np.uint32)
+    u32 = C.POINTER(C.c_uint)
+    rc = lib().pmgpu_p2m_sort_order(C.byref(topo), C.byref(params), FP32 if dt == np.float32 else FP64,
+                                    xpart.ctypes.data_as(C.c_void_p), n, keys.ctypes.data_as(u32),
+                                    order.ctypes.data_as(C.POINTER(C.c_int)), start.ctypes.data_as(u32))
+    if rc != 0:
+        raise RuntimeError(last_error())
+    return keys, order, start
+
+
 def pmlib_interp_mesh_particle(topo: Topo, params: Params, pos, mesh_vort=None, mesh_dvort=None,
                                mesh_vel=None, part_vort=None, part_dvort=None, part_vel=None) -> int:
     """source/interpolation/pmlib_interp_mesh_particle.f:5-24: the vort / dvort / vel

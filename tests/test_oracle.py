@@ -106,3 +106,49 @@ def test_si_function():
     assert abs(O.si(5.0) - 1.549931244944674) < 1e-14
     assert abs(O.si(10.0) - 1.658347594218874) < 1e-14
     assert abs(O.si(200.0) - pi / 2) < 1e-2
+
+
+def _nint_exact(t: float) -> int:
+    """Fortran NINT (half away from zero) on the exact value of a double."""
+    from decimal import ROUND_HALF_UP, Decimal
+    return int(Decimal(t).to_integral_value(rounding=ROUND_HALF_UP))
+
+
+@pytest.mark.parametrize("interp", [3, 4])
+def test_p2m_sort_restatement(interp):
+    """The oracle's bin keys and sort order (the deposition order of the reference's
+    P2M, pmlib_interp_particle_mesh.f:153-155,172-177,229-246) against a pure-Python
+    restatement: exact decimal rounding of (x - xmin) * (1/dx), the skip rules, and a
+    sort of (key, index) pairs."""
+    po = O.make_patch((0.0, -1.0, -0.5), (1.0, 1.0, 0.5), (0.0625, 0.125, 0.0625), bound_cond=(1, 0, 0), nghost=4)
+    ierr, t = O.topology_cuboid(po, interp)
+    rng = np.random.default_rng(4)
+    half = [0.0625 * (i + 0.5) for i in range(-6, 20)]
+    pos = np.concatenate([rng.uniform(-1.4, 1.4, (400, 3)),
+                          np.array([[h, 0.125 * (j - 8.5), 0.03125] for j, h in enumerate(half)]),
+                          np.array([[0.0, 0.0, 0.0], [-0.0, 1.0, -0.5], [1.0, -1.0, 0.5],
+                                    [np.nextafter(1.0, 2.0), 0.0, 0.0], [np.nextafter(0.0, -1.0), 0.0, 0.0],
+                                    [0.49999999999999994, 0.0, 0.0]])])
+    pos = np.ascontiguousarray(pos)
+    keys, order = O.p2m_sort(t, interp, pos)
+    W, off = (4, 1) if interp == 3 else (6, 2)
+    ext = [t.ncell[d] + t.nghost[2 * d] + t.nghost[2 * d + 1] for d in range(3)]
+    nb = [e + W - 1 for e in ext]
+    blo = [1 - t.nghost[2 * d] - (W - 1 - off) for d in range(3)]
+    want = []
+    for p in range(pos.shape[0]):
+        ok, b = True, []
+        for e in range(3):
+            x = float(pos[p, e])
+            bi = _nint_exact((x - t.xmin[e]) * (1.0 / t.dx[e]))
+            lo, hi = 1 - t.nghost[2 * e], t.ncell[e] + t.nghost[2 * e + 1]
+            if not (bi - off + W - 1 >= lo and bi - off <= hi):
+                ok = False
+            if t.bound_cond[2 * e] and x < t.xmin[e]:
+                ok = False
+            if t.bound_cond[2 * e + 1] and x > t.xmax[e]:
+                ok = False
+            b.append(bi - blo[e])
+        want.append(b[0] + nb[0] * (b[1] + nb[1] * b[2]) if ok else nb[0] * nb[1] * nb[2])
+    assert keys.tolist() == want
+    assert order.tolist() == [i for _, i in sorted(zip(want, range(len(want))))]
