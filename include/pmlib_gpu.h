@@ -158,6 +158,22 @@ int pmgpu_regularise_f32(pmgpu_plan *plan, float *mesh, int nvar, int reg_order,
 int pmgpu_poisson_setup_ppf(const pmgpu_patch *patch, const pmgpu_topo *cuboid,
                             const pmgpu_params *par, int precision, pmgpu_plan **plan);
 
+/* pmlib_poisson_setup with the mixed-space Green's function of the
+ * periodic-free-free validation program
+ * (validation/poisson_pff/sources/poisson/poisson_setup_pff.f:7-860): for patches
+ * periodic in x and free in y and z, kernel 1.  The kernel holds the periodic axis in
+ * Fourier space and y, z in real space, (1/2 pi) K0(2 pi |k_x| r) / dx with
+ * r = sqrt(y^2 + z^2) (order 0; K0 as the program's BESSEL_K0, :890-1078), and is
+ * transformed along y and z.  The program's orders 2-10 assign no kernel values, so
+ * their kernel is zero and so is the velocity.  At k_x = 0 the program's K0(0) is
+ * 1e30: with kx0 = PMGPU_PFF_AS_WRITTEN that plane is kept as written (a solve is
+ * then finite only for a field without k_x = 0 content); with PMGPU_PFF_LOG2D the
+ * plane holds the two-dimensional free-space kernel -(1/2 pi) ln(r) / dx (zero at
+ * r = 0), the k_x -> 0 limit less a constant that does not change the velocity. */
+enum { PMGPU_PFF_AS_WRITTEN = 0, PMGPU_PFF_LOG2D = 1 };
+int pmgpu_poisson_setup_pff(const pmgpu_patch *patch, const pmgpu_topo *cuboid,
+                            const pmgpu_params *par, int precision, int kx0, pmgpu_plan **plan);
+
 /* Replaces the deallocation of mesh%pkernel_fft (source/pmlib_finalise.f:63).  The
  * plan's device memory returns to the device's stream-ordered pool without
  * synchronising the device, so call it only when no work that uses the plan is still
@@ -371,6 +387,12 @@ int pmgpu_input_particles(const char *file, double trunc, int precision, int max
 const char *pmgpu_last_error(void);
 /* number of this library's kernels launched since the last reset */
 long long pmgpu_launch_count(int reset);
+/* For tests of a caller's error handling (no counterpart in the reference): the
+ * library's device allocation after the next `after` ones fails as if the device
+ * were out of memory (the entry point that needed it returns -1 with the message
+ * "[0000](caller) : out of memory"); after < 0 turns it off.  Buffers already held
+ * are not touched, so the next calls allocate again. */
+int pmgpu_inject_alloc_failure(long long after);
 /* per-kernel-class device timing: when enabled every launch is bracketed by CUDA
  * events on its own stream.  Classes are numbered 0..n-1; pmgpu_timing_get returns
  * -1 past the last one. */

@@ -105,6 +105,9 @@ def lib():
                                              C.POINTER(Patch), C.POINTER(Topo), dp, dp, C.c_double, C.c_double,
                                              C.c_int, C.c_double, C.c_int, C.c_int, dp, dp, dp, dp, ip, dp]
         L.pmo_poisson_setup_ppf.argtypes = [C.POINTER(Patch), C.POINTER(Params), dp]
+        L.pmo_poisson_setup_pff.argtypes = [C.POINTER(Patch), C.POINTER(Params), C.c_int, dp]
+        L.pmo_bessel_k0.argtypes = [C.c_double]
+        L.pmo_bessel_k0.restype = C.c_double
         L.pmo_si.argtypes = [C.c_double]
         L.pmo_si.restype = C.c_double
         _lib = L
@@ -329,3 +332,19 @@ def poisson_setup_ppf(patch, par):
     buf = np.zeros(2 * M[0] * M[1] * M[2])
     ierr = lib().pmo_poisson_setup_ppf(C.byref(patch), C.byref(par), _p(buf))
     return ierr, buf.view(np.complex128).reshape(M[2], M[1], M[0], 1)
+
+
+def poisson_setup_pff(patch, par, kx0=0):
+    """The periodic-free-free validation program's mixed-space kernel transformed
+    along y and z, in the layout of poisson_setup: (ierr, pkernel_fft (Mz, My, Mx, 1)).
+    kx0: 0 = the k_x = 0 plane as the program writes it, 1 = the two-dimensional
+    free-space kernel there."""
+    M, nk = kernel_dims(patch, par)
+    buf = np.zeros(2 * M[0] * M[1] * M[2])
+    ierr = lib().pmo_poisson_setup_pff(C.byref(patch), C.byref(par), int(kx0), _p(buf))
+    return ierr, buf.view(np.complex128).reshape(M[2], M[1], M[0], 1)
+
+
+def bessel_k0(z: float) -> float:
+    """K0 as the periodic-free-free validation program evaluates it."""
+    return lib().pmo_bessel_k0(float(z))

@@ -1733,3 +1733,138 @@ int pmo_poisson_setup_ppf(const pmo_patch *pa, const pmo_params *par, double *pk
   cb_free(&w);
   return 0;
 }
+
+/* ------------------------------------------------------------------------- */
+/* K0(z) for real z >= 0 as the periodic-free-free validation program evaluates it
+ * (its BESSEL_K0, validation/poisson_pff/sources/poisson/poisson_setup_pff.f:890-1078,
+ * the I0 / K0 branches of Zhang and Jin's CIK01 for a real argument): I0 by its power
+ * series up to |z| = 18 (terms until the last adds less than 1e-15 relative), by the
+ * asymptotic series (A&S 9.7.1, 12 / 9 / 7 terms below 35 / 50 / beyond) above; K0 by
+ * the series -(ln(z/2) + gamma) I0 + sum (z^2/4)^k / (k!)^2 H_k up to |z| = 9, and by
+ * the asymptotic form of I0 K0 (10 terms) divided by I0 above; K0(0) is the routine's
+ * 1e30.  The cross-term test of the K0 series starts from a zero previous sum. */
+double pmo_bessel_k0(double z) {
+  static const double a[12] = {0.125, 7.03125e-02, 7.32421875e-02, 1.1215209960938e-01, 2.2710800170898e-01,
+                               5.7250142097473e-01, 1.7277275025845, 6.0740420012735, 2.4380529699556e+01,
+                               1.1001714026925e+02, 5.5133589612202e+02, 3.0380905109224e+03};
+  static const double a1[10] = {0.125, 0.2109375, 1.0986328125, 1.1775970458984e+01, 2.1461706161499e+02,
+                                5.9511522710323e+03, 2.3347645606175e+05, 1.2312234987631e+07,
+                                8.401390346421e+08, 7.2031420482627e+10};
+  const double pi = 3.141592653589793;
+  const double a0 = fabs(z);
+  if (a0 == 0.0) return 1.0e30;
+  const double z2 = z * z, z1 = a0;
+  double bi0;
+  if (a0 <= 18.0) {
+    double cr = 1.0;
+    bi0 = 1.0;
+    for (int k = 1; k <= 50; k++) {
+      cr = 0.25 * cr * z2 / (double)(k * k);
+      bi0 = bi0 + cr;
+      if (fabs(cr / bi0) < 1.0e-15) break;
+    }
+  } else {
+    const int k0 = a0 < 35.0 ? 12 : (a0 < 50.0 ? 9 : 7);
+    const double ca = exp(z1) / sqrt(2.0 * pi * z1);
+    const double zr = 1.0 / z1;
+    double zk = 1.0;
+    bi0 = 1.0;
+    for (int k = 1; k <= k0; k++) {
+      zk = zk * zr;
+      bi0 = bi0 + a[k - 1] * zk;
+    }
+    bi0 = ca * bi0;
+  }
+  double bk0;
+  if (a0 <= 9.0) {
+    const double ct = -log(0.5 * z1) - 0.5772156649015329;
+    double cs = 0.0, w0 = 0.0, cr = 1.0, cw = 0.0;
+    for (int k = 1; k <= 50; k++) {
+      w0 = w0 + 1.0 / (double)k;
+      cr = 0.25 * cr / (double)(k * k) * z2;
+      cs = cs + cr * (w0 + ct);
+      if (fabs((cs - cw) / cs) < 1.0e-15) break;
+      cw = cs;
+    }
+    bk0 = ct + cs;
+  } else {
+    const double cb = 0.5 / z1, zr2 = 1.0 / z2;
+    double zk = 1.0;
+    bk0 = 1.0;
+    for (int k = 1; k <= 10; k++) {
+      zk = zk * zr2;
+      bk0 = bk0 + a1[k - 1] * zk;
+    }
+    bk0 = cb * bk0 / bi0;
+  }
+  return bk0;
+}
+
+/* The mixed-space Green's function of the periodic-free-free validation program
+ * (validation/poisson_pff/sources/poisson/poisson_setup_pff.f:244-360, one rank): on
+ * the kernel grid x holds wavenumbers (natural order, the formula of :296-302) and
+ * y, z positions centred on zero; order 0 is (1/2 pi) K0(2 pi |k_x| r) / dx with
+ * r = sqrt(y^2 + z^2) (:310-321), zero at r = 0 and where 2 pi |k_x| r >= 500; then
+ * transformed along y and z (fft_shift, :825-827).  Orders 2-10 of the program
+ * assign nothing in their loops (:373-777), so their kernel is zero.
+ * kx0 selects the k_x = 0 plane: 0 = as written (K0(0) is the routine's 1e30, so the
+ * plane holds 1e30 / (2 pi dx) wherever r > 0: a solve is finite only for fields with
+ * no k_x = 0 content); 1 = the two-dimensional free-space kernel -(1/2 pi) ln(r) / dx
+ * (the k_x -> 0 limit of the same kernel less its divergent constant, which adds a
+ * uniform vector potential and leaves the velocity unchanged), zero at r = 0.
+ * pkf gets the layout of pmo_poisson_setup: (Mz, My, Mx) complex, x fastest. */
+int pmo_poisson_setup_pff(const pmo_patch *pa, const pmo_params *par, int kx0, double *pkf) {
+  const char *caller = "pmlib_poisson_setup";
+  if (!(pa->bound_cond[0] == 1 && pa->bound_cond[1] == 0 && pa->bound_cond[2] == 0)) {
+    pm_write(caller, "The spectral kernel needs a periodic x and free y and z.");
+    return -1;
+  }
+  if (par->poisson_kernel != 1) {
+    pm_write(caller, "Velocity kernel is not implemented.");
+    return -1;
+  }
+  const int o = par->poisson_order;
+  if (o != 0 && o != 2 && o != 4 && o != 6 && o != 8 && o != 10) {
+    pm_write(caller, "Integration kernel unknown - change POISSON ORDER.");
+    return -1;
+  }
+  if (kx0 != 0 && kx0 != 1) {
+    pm_write(caller, "Unknown treatment of the kx = 0 plane.");
+    return -1;
+  }
+  int M[3], nk;
+  pmo_kernel_dims(pa, par, M, &nk);
+  const double PI = acos(-1.0);
+  double dx[3];
+  for (int e = 0; e < 3; e++) dx[e] = pa->dx[e];
+  const double c_1_2pi = 0.5 / PI;
+  const double ymin = -(0.5 * (double)M[1] + 0.5) * dx[1], zmin = -(0.5 * (double)M[2] + 0.5) * dx[2];
+  int lo[3] = {1, 1, 1};
+  cbox w = cb_alloc(lo, M, 1);
+  for (int k = 1; k <= M[2]; k++) {
+    const double pz = zmin + ((double)(k - 1) + 0.5) * dx[2];
+    for (int j = 1; j <= M[1]; j++) {
+      const double py = ymin + ((double)(j - 1) + 0.5) * dx[1];
+      const double r = sqrt(py * py + pz * pz);
+      for (int i = 1; i <= M[0]; i++) {
+        const double ki = wavenumber(i, 0, M[0], -0.5 / dx[0], 1.0 / ((double)M[0] * dx[0]), 0.5 / dx[0]);
+        double g = 0.0;
+        if (o == 0 && r != 0.0) {
+          const double zarg = r * 2.0 * PI * fabs(ki);
+          if (ki == 0.0 && kx0 == 1) g = -c_1_2pi * log(r) / dx[0];
+          else if (zarg < 500.0) g = c_1_2pi * pmo_bessel_k0(zarg) / dx[0];
+        }
+        const size_t q = cb_idx(&w, 0, i - 1, j - 1, k - 1);
+        w.d[q] = g;
+        w.d[q + 1] = 0.0;
+      }
+    }
+  }
+  if (cb_fft_axis(&w, 1, 0, 1, "pmlib_fft") || cb_fft_axis(&w, 2, 0, 1, "pmlib_fft")) {
+    cb_free(&w);
+    return -1;
+  }
+  memcpy(pkf, w.d, sizeof(double) * 2 * (size_t)M[0] * M[1] * M[2]);
+  cb_free(&w);
+  return 0;
+}

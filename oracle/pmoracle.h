@@ -124,6 +124,8 @@ int pmo_poisson_setup_ppf(const pmo_patch *patch, const pmo_params *par, double 
 
 /* helper: sine integral used by the order-100 kernel */
 double pmo_si(double x);
+double pmo_bessel_k0(double z);
+int pmo_poisson_setup_pff(const pmo_patch *patch, const pmo_params *par, int kx0, double *pkernel_fft);
 
 #ifdef __cplusplus
 }

@@ -26,6 +26,7 @@ EXPORTS = (
     "pmgpu_vortex_stage_dev", "pmgpu_fft_set_schedule", "pmgpu_step_many", "pmgpu_penalisation_solve_dev",
     "pmgpu_output_mesh", "pmgpu_output_pvti", "pmgpu_output_topology", "pmgpu_output_particles",
     "pmgpu_input_particles", "pmgpu_poisson_setup_ppf", "pmgpu_p2m_sort_order",
+    "pmgpu_poisson_setup_pff", "pmgpu_inject_alloc_failure",
 )
 
 
@@ -77,6 +78,7 @@ def lib():
         "pmgpu_interp_mesh_particle_f32": [TP, QP, fp, fp, fp, fp, C.c_int, fp, fp, fp],
         "pmgpu_poisson_setup": [PP, TP, QP, C.c_int, C.POINTER(vp)],
         "pmgpu_poisson_setup_ppf": [PP, TP, QP, C.c_int, C.POINTER(vp)],
+        "pmgpu_poisson_setup_pff": [PP, TP, QP, C.c_int, C.c_int, C.POINTER(vp)],
         "pmgpu_poisson_solve": [vp, dp, dp, dp, C.c_int, C.c_int, C.c_int],
         "pmgpu_poisson_solve_f32": [vp, fp, fp, fp, C.c_int, C.c_int, C.c_int],
         "pmgpu_regularise": [vp, dp, C.c_int, C.c_int, C.c_double],
@@ -92,6 +94,7 @@ def lib():
         "pmgpu_timing_get": [C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(C.c_longlong)],
         "pmgpu_interp_particle_mesh_noalloc": [TP, QP, vp, vp, C.c_int, C.c_int, vp, C.c_int, C.c_int, C.c_int, vp],
         "pmgpu_fft_engine": [C.c_int],
+        "pmgpu_inject_alloc_failure": [C.c_longlong],
         "pmgpu_poisson_solve_dev": [vp, vp, vp, vp, C.c_int, C.c_int, C.c_int, vp],
         "pmgpu_batch_create": [C.c_int, PP, TP, QP, C.c_int, C.POINTER(vp)],
         "pmgpu_batch_solve": [vp, C.POINTER(vp), C.POINTER(vp), vp],

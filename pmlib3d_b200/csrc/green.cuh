@@ -288,6 +288,99 @@ __global__ void k_green_ppf(GreenParams gp, int H, int Hp, const int *__restrict
   }
 }
 
+// K0(z), z >= 0, as the periodic-free-free validation program evaluates it (its
+// BESSEL_K0, the I0 / K0 branches of Zhang and Jin's CIK01 for a real argument,
+// poisson_setup_pff.f:890-1078): I0 by its power series up to z = 18 and by the
+// asymptotic series (A&S 9.7.1; 12 / 9 / 7 terms below 35 / 50 / beyond) above; K0
+// by -(ln(z/2) + gamma) I0 + sum (z^2/4)^k / (k!)^2 H_k up to z = 9 and by the
+// asymptotic form of I0 K0 (10 terms) over I0 above; K0(0) = 1e30 as in the routine.
+// The same truncations are kept so that values agree with the program's to rounding.
+__device__ __forceinline__ double dev_bessel_k0(double z) {
+  const double a0 = fabs(z);
+  if (a0 == 0.0) return 1.0e30;
+  const double z2 = z * z, z1 = a0;
+  double bi0 = 1.0;
+  if (a0 <= 18.0) {
+    double cr = 1.0;
+    for (int k = 1; k <= 50; k++) {
+      cr = 0.25 * cr * z2 / (double)(k * k);
+      bi0 = bi0 + cr;
+      if (fabs(cr / bi0) < 1.0e-15) break;
+    }
+  } else {
+    const double a[12] = {0.125, 7.03125e-02, 7.32421875e-02, 1.1215209960938e-01, 2.2710800170898e-01,
+                          5.7250142097473e-01, 1.7277275025845, 6.0740420012735, 2.4380529699556e+01,
+                          1.1001714026925e+02, 5.5133589612202e+02, 3.0380905109224e+03};
+    const int k0 = a0 < 35.0 ? 12 : (a0 < 50.0 ? 9 : 7);
+    const double ca = exp(z1) / sqrt(2.0 * 3.141592653589793 * z1);
+    const double zr = 1.0 / z1;
+    double zk = 1.0;
+    for (int k = 1; k <= k0; k++) {
+      zk = zk * zr;
+      bi0 = bi0 + a[k - 1] * zk;
+    }
+    bi0 = ca * bi0;
+  }
+  if (a0 <= 9.0) {
+    const double ct = -log(0.5 * z1) - 0.5772156649015329;
+    double cs = 0.0, w0 = 0.0, cr = 1.0, cw = 0.0;
+    for (int k = 1; k <= 50; k++) {
+      w0 = w0 + 1.0 / (double)k;
+      cr = 0.25 * cr / (double)(k * k) * z2;
+      cs = cs + cr * (w0 + ct);
+      if (fabs((cs - cw) / cs) < 1.0e-15) break;
+      cw = cs;
+    }
+    return ct + cs;
+  }
+  const double a1[10] = {0.125, 0.2109375, 1.0986328125, 1.1775970458984e+01, 2.1461706161499e+02,
+                         5.9511522710323e+03, 2.3347645606175e+05, 1.2312234987631e+07, 8.401390346421e+08,
+                         7.2031420482627e+10};
+  const double cb = 0.5 / z1, zr2 = 1.0 / z2;
+  double zk = 1.0, bk0 = 1.0;
+  for (int k = 1; k <= 10; k++) {
+    zk = zk * zr2;
+    bk0 = bk0 + a1[k - 1] * zk;
+  }
+  return cb * bk0 / bi0;
+}
+
+// The mixed-space kernel of the periodic-free-free validation program
+// (poisson_setup_pff.f:244-360) in the x-transformed layout spec[z][y][kx] (kx < Hp):
+// x holds the periodic axis's wavenumbers (natural order, the formula of :296-302),
+// y and z the shifted positions of the doubled free axes, so that transforms along y
+// and z complete it.  Order 0 is (1/2 pi) K0(2 pi |k_x| r) / dx, r = sqrt(y^2 + z^2),
+// zero at r = 0 and where 2 pi |k_x| r >= 500; the program's orders 2-10 assign
+// nothing, so their kernel is zero.  kx0 = 1 replaces the k_x = 0 plane (the
+// routine's K0(0) = 1e30) with the two-dimensional kernel -(1/2 pi) ln(r) / dx.
+__global__ void k_green_pff(GreenParams gp, int kx0, int H, int Hp, double2 *__restrict__ spec) {
+  const double PI = 3.14159265358979323846;
+  const double c_1_2pi = 0.5 / PI;
+  const size_t total = (size_t)gp.M[2] * gp.M[1] * Hp;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int kx = (int)(t % Hp);
+    const int y = (int)((t / Hp) % gp.M[1]);
+    const int z = (int)(t / ((size_t)Hp * gp.M[1]));
+    double g = 0.0;
+    if (kx < H && gp.order == 0) {
+      const int i = kx + 1;  // 1-based index along the periodic axis
+      const double kmin = -0.5 / gp.dx[0], dk = 1.0 / ((double)gp.M[0] * gp.dx[0]), ksmp = 0.5 / gp.dx[0];
+      const double ki = (2 * i <= gp.M[0]) ? kmin + (double)(i - 1) * dk + ksmp : kmin + (double)(i - 1) * dk - ksmp;
+      const int hy = gp.M[1] / 2, hz = gp.M[2] / 2;
+      const int jy = y < hy ? y + hy + 1 : y - hy + 1, kz = z < hz ? z + hz + 1 : z - hz + 1;
+      const double py = gp.xmin[1] + ((double)(jy - 1) + 0.5) * gp.dx[1];
+      const double pz = gp.xmin[2] + ((double)(kz - 1) + 0.5) * gp.dx[2];
+      const double r = sqrt(py * py + pz * pz);
+      if (r != 0.0) {
+        const double zarg = r * 2.0 * PI * fabs(ki);
+        if (ki == 0.0 && kx0 == 1) g = -c_1_2pi * log(r) / gp.dx[0];
+        else if (zarg < 500.0) g = c_1_2pi * dev_bessel_k0(zarg) / gp.dx[0];
+      }
+    }
+    spec[t] = make_double2(g, 0.0);
+  }
+}
+
 // octant of the real spectrum, scaled by dx dy dz / (Mx My Mz), in the plan precision;
 // yrow / zrow: frequency -> row of the transformed spectrum along y / z
 template <typename R>

@@ -130,6 +130,10 @@ static int ensure_device(const char *caller) {
 // the pool): allocating or freeing never synchronises the whole device, so plans can
 // be created and destroyed while other streams run.  A buffer is freed in order on
 // the legacy stream; its owner frees it only when no work using it is in flight.
+// Injected allocation failure (pmgpu_inject_alloc_failure): the allocation that
+// brings the countdown to zero reports cudaErrorMemoryAllocation; -1 = off.
+static long long g_fail_alloc = -1;
+
 struct DevBuf {
   void *p = nullptr;
   size_t cap = 0;
@@ -148,6 +152,7 @@ struct DevBuf {
     p = nullptr;
     cap = 0;
     size_t b = std::max<size_t>(bytes, 256);
+    if (g_fail_alloc >= 0 && g_fail_alloc-- == 0) CK(cudaErrorMemoryAllocation, caller);
     if (stream_ordered) {
       CK(cudaMallocAsync(&p, b, 0), caller);
       CK(cudaStreamSynchronize(0), caller);  // usable from every stream from here on
@@ -487,7 +492,8 @@ struct StepPipe {
 
 struct pmgpu_plan {
   int prec;
-  int green_mode = 0;  // 0: pmlib_poisson_setup's kernel; 1: the ppf validation program's spectral kernel
+  int green_mode = 0;  // 0: pmlib_poisson_setup's kernel; 1 / 2: the ppf / pff validation programs' kernels
+  int pff_kx0 = 0;     // pff: treatment of the k_x = 0 plane (0 as written, 1 two-dimensional kernel)
   StepPipe pipe;
   pmgpu_patch patch;
   pmgpu_topo topo;
@@ -859,7 +865,8 @@ static std::string green_key(const pmgpu_plan *pl) {
   cudaGetDevice(&dev);
   char b[512];
   const pmgpu_patch &p = pl->patch;
-  snprintf(b, sizeof(b), "%d|%d|%d|%a,%a,%a|%d,%d,%d|%d,%d,%d|%d,%d,%d,%d|%d,%d,%a", dev, pl->green_mode, pl->prec,
+  snprintf(b, sizeof(b), "%d|%d.%d|%d|%a,%a,%a|%d,%d,%d|%d,%d,%d|%d,%d,%d,%d|%d,%d,%a", dev, pl->green_mode,
+           pl->pff_kx0, pl->prec,
            p.dx[0], p.dx[1], p.dx[2], pl->g.M[0], pl->g.M[1], pl->g.M[2], p.bound_cond[0], p.bound_cond[1],
            p.bound_cond[2], p.ncell[0], p.ncell[1], p.ncell[2], p.nghost, pl->par.poisson_order,
            pl->par.poisson_kernel, pl->par.regularisation_radius);
@@ -966,7 +973,23 @@ template <typename R> static int setup_green(pmgpu_plan *pl, const char *caller)
                      ((double)G.M[0] * (double)G.M[1] * (double)G.M[2]);
     const unsigned nb_real = (unsigned)std::min<size_t>((npts + 255) / 256, 148 * 64);
     const unsigned nb_oct = (unsigned)std::min<size_t>((noct + 255) / 256, 148 * 64);
-    if (pl->green_mode == 1) {
+    if (pl->green_mode == 2) {
+      // the mixed-space kernel of the pff validation program: the x-transformed layout
+      // (kx natural wavenumbers, y and z positions) is written directly, then y and z
+      const unsigned nb_x = (unsigned)std::min<size_t>((nspec + 255) / 256, 148 * 64);
+      k_green_pff<<<nb_x, 256>>>(gp, pl->pff_kx0, G.H, G.Hp, gX.as<double2>());
+      PM_LAUNCHED();
+      if (!cuda_ok(cudaGetLastError(), caller)) break;
+      if (ypass<double, 1>(gg, gX.as<double2>(), gY.as<double2>(), 0, 0, caller)) break;
+      if (zpass<double, 1>(gg, gY.as<double2>(), gY.as<double2>(), Z_FORWARD, 0, 0, G.M[1], 0, caller)) break;
+      if (!cuda_ok(cudaStreamSynchronize(0), caller)) break;
+      if (own->ensure(sizeof(R) * noct, caller)) break;
+      attach_green(pl, own);
+      k_green_octant<R><<<nb_oct, 256>>>(gY.as<double2>(), G.M[1], G.H, G.Hp, pl->gM1, pl->gM2, f, yinv.as<int>(),
+                                         zinv.as<int>(), pl->green.as<R>());
+      PM_LAUNCHED();
+      if (!cuda_ok(cudaGetLastError(), caller)) break;
+    } else if (pl->green_mode == 1) {
       // the spectral kernel of the ppf validation program: the y-transformed spectrum
       // (kx, ky natural wavenumbers, z positions) is written directly, then z only
       const unsigned nb_y = (unsigned)std::min<size_t>((nspec + 255) / 256, 148 * 64);
@@ -1295,6 +1318,12 @@ long long pmgpu_launch_count(int reset) {
 
 int pmgpu_parameters_check(const pmgpu_params *par) { return check_params(par); }
 
+int pmgpu_inject_alloc_failure(long long after) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_fail_alloc = after < 0 ? -1 : after;
+  return 0;
+}
+
 void pmgpu_timing_enable(int on) {
   std::lock_guard<std::mutex> lk(g_mu);
   timing_collect();
@@ -1504,6 +1533,7 @@ int pmgpu_interp_mesh_particle_f32(const pmgpu_topo *topo, const pmgpu_params *p
 
 // ------------------------------------------------------------------ Poisson
 // plan creation; the caller holds g_mu
+static int g_pff_kx0 = 0;  // k_x = 0 treatment handed from pmgpu_poisson_setup_pff to create_plan (under g_mu)
 static int create_plan(const pmgpu_patch *patch, const pmgpu_topo *cuboid, const pmgpu_params *par, int precision,
                        pmgpu_plan **plan, const char *caller, int green_mode = 0) {
   if (!plan || !patch || !cuboid) {
@@ -1558,6 +1588,7 @@ static int create_plan(const pmgpu_patch *patch, const pmgpu_topo *cuboid, const
   pl->g.allper = allper;
   pl->eps = par->regularisation_radius * mdx;
   pl->green_mode = green_mode;
+  pl->pff_kx0 = green_mode == 2 ? g_pff_kx0 : 0;
   const int rc = (precision == PMGPU_FP64) ? plan_tables<double>(pl, caller) : plan_tables<float>(pl, caller);
   if (rc) {
     delete pl;
@@ -1594,6 +1625,36 @@ int pmgpu_poisson_setup_ppf(const pmgpu_patch *patch, const pmgpu_topo *cuboid, 
     return -1;
   }
   return create_plan(patch, cuboid, par, precision, plan, caller, 1);
+}
+
+int pmgpu_poisson_setup_pff(const pmgpu_patch *patch, const pmgpu_topo *cuboid, const pmgpu_params *par,
+                            int precision, int kx0, pmgpu_plan **plan) {
+  const char *caller = "pmlib_poisson_setup";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!patch || !par || !plan) {
+    set_error(caller, "missing argument.");
+    return -1;
+  }
+  if (!(patch->bound_cond[0] != 0 && patch->bound_cond[1] == 0 && patch->bound_cond[2] == 0)) {
+    set_error(caller, "The spectral kernel needs a periodic x and free y and z.");
+    return -1;
+  }
+  if (par->poisson_kernel == 2) {  // poisson_setup_pff.f: no velocity kernel
+    set_error(caller, "Velocity kernel is not implemented.");
+    return -1;
+  }
+  if (par->poisson_order == 100) {
+    set_error(caller, "Integration kernel unknown - change POISSON ORDER.");
+    return -1;
+  }
+  if (kx0 != PMGPU_PFF_AS_WRITTEN && kx0 != PMGPU_PFF_LOG2D) {
+    set_error(caller, "Unknown treatment of the kx = 0 plane.");
+    return -1;
+  }
+  g_pff_kx0 = kx0;
+  const int rc = create_plan(patch, cuboid, par, precision, plan, caller, 2);
+  g_pff_kx0 = 0;
+  return rc;
 }
 
 void pmgpu_plan_destroy(pmgpu_plan *plan) {

@@ -60,6 +60,12 @@ def timing_reset() -> None:
     lib().pmgpu_timing_reset()
 
 
+def inject_alloc_failure(after: int) -> None:
+    """The library's device allocation after the next `after` ones fails as if the
+    device were out of memory (after < 0: off).  For tests of error handling."""
+    lib().pmgpu_inject_alloc_failure(int(after))
+
+
 def timing_read() -> dict:
     """{kernel class: (total ms, launches)} accumulated since the last reset."""
     out = {}
@@ -181,6 +187,20 @@ def poisson_setup_ppf(patch: Patch, topo: Topo, params: Params, precision: int =
     -> (ierr, Plan)."""
     h = C.c_void_p()
     ierr = lib().pmgpu_poisson_setup_ppf(C.byref(patch), C.byref(topo), C.byref(params), precision, C.byref(h))
+    return ierr, (Plan(h, precision, topo) if ierr == 0 else None)
+
+
+PFF_AS_WRITTEN, PFF_LOG2D = 0, 1
+
+
+def poisson_setup_pff(patch: Patch, topo: Topo, params: Params, precision: int = FP64, kx0: int = PFF_AS_WRITTEN):
+    """pmlib_poisson_setup with the mixed-space kernel of the periodic-free-free
+    validation program (validation/poisson_pff/sources/poisson/poisson_setup_pff.f)
+    -> (ierr, Plan).  kx0: the k_x = 0 plane as the program writes it
+    (PFF_AS_WRITTEN) or the two-dimensional free-space kernel (PFF_LOG2D)."""
+    h = C.c_void_p()
+    ierr = lib().pmgpu_poisson_setup_pff(C.byref(patch), C.byref(topo), C.byref(params), precision, int(kx0),
+                                         C.byref(h))
     return ierr, (Plan(h, precision, topo) if ierr == 0 else None)
 
 

@@ -638,3 +638,73 @@ def test_ppf_spectral_kernel_errors(capfd):
     po, to, qo, pg, tg, qg = setup_pair(*PPF_CASES[0][1:], order=6, kernel=2)
     assert P.poisson_setup_ppf(pg, tg, qg, P.FP64)[0] == -1
     assert "Velocity kernel is not implemented." in capfd.readouterr().out
+
+
+PFF_CASES = [
+    ("pff", (0, -1, -1), (1, 1, 1), (1 / 16, 1 / 16, 1 / 16), (1, 0, 0), 4),
+    ("pff-noncubic", (0, -0.75, -0.5), (1.5, 0.75, 0.5), (0.125, 0.0625, 0.0625), (1, 0, 0), 4),
+]
+
+
+def _square_wave(to, bits=12):
+    """Vorticity without k_x = 0 content in any summation order: +q(y, z) on the first
+    half of the periodic x extent, -q on the second, q quantised to `bits` bits."""
+    axes = []
+    for d in range(3):
+        i = np.arange(1 - to.nghost[2 * d], to.ncell[d] + to.nghost[2 * d + 1] + 1, dtype=np.float64)
+        axes.append(to.xmin[d] + (i - 0.5) * to.dx[d])
+    z, y, x = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
+    s = np.where(x < 0.5 * (to.xmin[0] + to.xmax[0]), 1.0, -1.0)
+    w = np.zeros(z.shape + (3,))
+    for c, (cy, cz) in enumerate(((0.1, 0.0), (-0.2, 0.15), (0.0, -0.25))):
+        w[..., c] = s * np.round(np.exp(-((y - cy) ** 2 + (z - cz) ** 2) / 0.1) * 2 ** bits) / 2 ** bits
+    return np.ascontiguousarray(w)
+
+
+@pytest.mark.parametrize("name,xmin,xmax,dx,bc,ng", PFF_CASES)
+@pytest.mark.parametrize("kx0", [P.PFF_AS_WRITTEN, P.PFF_LOG2D])
+def test_pff_spectral_kernel(name, xmin, xmax, dx, bc, ng, kx0):
+    """The periodic-free-free validation program's mixed-space Green's function
+    (poisson_setup_pff.f, order 0: K0 along the periodic axis's wavenumbers) against
+    the oracle's restatement, with its k_x = 0 plane as written (a field without
+    k_x = 0 content, so the plane's 1e30 never acts) or as the two-dimensional
+    free-space kernel (a general field): FP64 to 1e-12, FP32 to 1e-5, with
+    reprojection."""
+    po, to, qo, pg, tg, qg = setup_pair(xmin, xmax, dx, bc, ng, interp=3, order=0)
+    w = _square_wave(to) if kx0 == P.PFF_AS_WRITTEN else gaussian_field(to, seed=23, noise=0.01)
+    ierr, pk = O.poisson_setup_pff(po, qo, kx0)
+    assert ierr == 0
+    wo = w.copy()
+    ierr, vel_o, _ = O.poisson_solve(po, to, qo, pk, wo, reproj=True)
+    assert ierr == 0 and np.all(np.isfinite(vel_o)) and np.abs(vel_o).max() > 1e-3
+    for prec, tol in ((P.FP64, 1e-12), (P.FP32, 1e-5)):
+        dt = np.float64 if prec == P.FP64 else np.float32
+        ierr, plan = P.poisson_setup_pff(pg, tg, qg, prec, kx0)
+        assert ierr == 0, P.last_error()
+        vel = np.zeros(w.shape, dt)
+        wg = w.astype(dt)
+        assert P.pmlib_poisson_solve(plan, wg, vel, reproj=True) == 0
+        assert rel_l2(vel, vel_o) < tol, (prec, rel_l2(vel, vel_o))
+        assert rel_l2(wg, wo) < tol
+        plan.close()
+
+
+def test_pff_higher_orders_give_zero_velocity():
+    """The program's orders 2-10 assign no kernel values, so the velocity is zero."""
+    po, to, qo, pg, tg, qg = setup_pair(*PFF_CASES[0][1:], interp=3, order=6)
+    ierr, plan = P.poisson_setup_pff(pg, tg, qg, P.FP64)
+    assert ierr == 0, P.last_error()
+    w = gaussian_field(to, seed=24)
+    vel = np.full_like(w, 7.0)
+    assert P.pmlib_poisson_solve(plan, w.copy(), vel) == 0
+    assert not np.any(vel)
+
+
+def test_pff_spectral_kernel_errors(capfd):
+    po, to, qo, pg, tg, qg = setup_pair(*CASES[0][1:], order=0)  # fff: x not periodic
+    assert P.poisson_setup_pff(pg, tg, qg, P.FP64)[0] == -1
+    po, to, qo, pg, tg, qg = setup_pair(*PFF_CASES[0][1:], order=0, kernel=2)
+    assert P.poisson_setup_pff(pg, tg, qg, P.FP64)[0] == -1
+    assert "Velocity kernel is not implemented." in capfd.readouterr().out
+    po, to, qo, pg, tg, qg = setup_pair(*PFF_CASES[0][1:], order=0)
+    assert P.poisson_setup_pff(pg, tg, qg, P.FP64, kx0=5)[0] == -1

@@ -152,3 +152,91 @@ def test_p2m_sort_restatement(interp):
         want.append(b[0] + nb[0] * (b[1] + nb[1] * b[2]) if ok else nb[0] * nb[1] * nb[2])
     assert keys.tolist() == want
     assert order.tolist() == [i for _, i in sorted(zip(want, range(len(want))))]
+
+
+def test_bessel_k0_restatement():
+    """K0 as the periodic-free-free validation program evaluates it (its BESSEL_K0)
+    against scipy's k0: the routine's series and asymptotic branches, with the
+    accuracy they have (the K0 series loses digits to cancellation towards z = 9)."""
+    import scipy.special as sp
+    for lo, hi, tol in ((1e-8, 2.0, 1e-14), (2.0, 5.0, 5e-12), (5.0, 12.0, 2e-8), (12.0, 20.0, 1e-10),
+                        (20.0, 499.0, 1e-12)):
+        for z in np.geomspace(lo, hi, 400):
+            assert abs(O.bessel_k0(z) - sp.k0(z)) <= tol * sp.k0(z), z
+    assert O.bessel_k0(0.0) == 1e30
+
+
+def _pff_setup(n, kx0, order=0, ncx=8):
+    h = 2.0 / n
+    po = O.make_patch((0.0, -1.0, -1.0), (ncx * h, 1.0, 1.0), (h, h, h), bound_cond=(1, 0, 0), nghost=4)
+    ierr, t = O.topology_cuboid(po, 3)
+    assert ierr == 0
+    qo = O.make_params(order=order, kernel=1, radius=2.0, interp=3)
+    ierr, pk = O.poisson_setup_pff(po, qo, kx0)
+    assert ierr == 0
+    return po, t, qo, pk
+
+
+def _cuboid_axes(t):
+    ax = []
+    for d in range(3):
+        i = np.arange(1 - t.nghost[2 * d], t.ncell[d] + t.nghost[2 * d + 1] + 1, dtype=np.float64)
+        ax.append(t.xmin[d] + (i - 0.5) * t.dx[d])
+    return np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+
+
+def test_pff_log2d_vortex_tube():
+    """The two-dimensional treatment of the k_x = 0 plane of the pff kernel: a
+    Lamb-Oseen tube along the periodic axis (all of it at k_x = 0) gets the analytic
+    velocity Gamma / (2 pi r) (1 - exp(-r^2 / sigma^2)) e_theta, converging at about
+    second order as h falls (the kernel is sampled at cell centres, zero at r = 0)."""
+    errs = []
+    for n in (32, 64):
+        po, t, qo, pk = _pff_setup(n, kx0=1)
+        z, y, x = _cuboid_axes(t)
+        r2 = y * y + z * z
+        sig = 0.2
+        w = np.zeros(z.shape + (3,))
+        w[..., 0] = np.exp(-r2 / sig ** 2) / (np.pi * sig ** 2)
+        ierr, vel, _ = O.poisson_solve(po, t, qo, pk, w)
+        assert ierr == 0
+        with np.errstate(invalid="ignore", divide="ignore"):
+            ut = np.where(r2 > 0, (1 - np.exp(-r2 / sig ** 2)) / (2 * np.pi * r2), 0.0)
+        ref = np.stack([np.zeros_like(ut), -ut * z, ut * y], -1)
+        g = [t.nghost[2 * d] for d in range(3)]
+        sl = (slice(g[2], -g[2]), slice(g[1], -g[1]), slice(g[0], -g[0]))
+        d = vel[sl] - ref[sl]
+        errs.append(np.sqrt(np.sum(d * d) / np.sum(ref[sl] ** 2)))
+    assert errs[0] < 0.1 and errs[1] < 0.03 and errs[1] < errs[0] / 2.5, errs
+
+
+def _square_wave_field(t, bits=12):
+    """A field without k_x = 0 content in any summation order: +q(y, z) on the first
+    half of the periodic x extent and -q on the second, q quantised to `bits` bits so
+    that every partial sum is exact."""
+    z, y, x = _cuboid_axes(t)
+    s = np.where(x < 0.5 * (t.xmin[0] + t.xmax[0]), 1.0, -1.0)
+    out = np.zeros(z.shape + (3,))
+    for c, (cy, cz) in enumerate(((0.1, 0.0), (-0.2, 0.15), (0.0, -0.25))):
+        q = np.exp(-((y - cy) ** 2 + (z - cz) ** 2) / 0.1)
+        out[..., c] = s * np.round(q * 2 ** bits) / 2 ** bits
+    return np.ascontiguousarray(out)
+
+
+def test_pff_as_written_equals_log2d_without_kx0_content():
+    """With no k_x = 0 content the program's own k_x = 0 plane (K0(0) = 1e30) never
+    acts, so both treatments give the same velocity, bit for bit, and it is finite."""
+    po, t, qo, pk0 = _pff_setup(32, kx0=0)
+    _, _, _, pk1 = _pff_setup(32, kx0=1)
+    w = _square_wave_field(t)
+    ierr, v0, _ = O.poisson_solve(po, t, qo, pk0, w.copy())
+    ierr, v1, _ = O.poisson_solve(po, t, qo, pk1, w.copy())
+    assert np.all(np.isfinite(v0)) and np.abs(v0).max() > 1e-3
+    assert np.array_equal(v0, v1)
+
+
+def test_pff_higher_orders_are_empty():
+    """The program's orders 2-10 assign no kernel values: the kernel is zero."""
+    for order in (2, 6, 10):
+        _, _, _, pk = _pff_setup(16, kx0=0, order=order)
+        assert not np.any(pk)
