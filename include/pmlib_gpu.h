@@ -266,12 +266,14 @@ int pmgpu_fft_set_schedule(int length, int precision, int axis, const int *radic
  * must not risk the implicit synchronisation of cudaMalloc / cudaFree.  Same
  * arguments and result as pmgpu_interp_particle_mesh (FP64), but every array is a
  * device pointer and the work runs on `stream`; the call allocates nothing.  Its
- * scratch is one static device array of about 8.6 MB that every GPU loading the
- * library holds until the process exits; a call is limited to 262144 particles and
- * 524288 bins ((nx'+3)(ny'+3)(nz'+3) for M4', +5 per axis for M6*; larger inputs are
- * rejected with ierr = -1).  The first call on a device looks up the array's device
- * address, so make it before any CUDA stream capture.  All calls share the array:
- * calls that overlap on the GPU (different streams or threads) race. */
+ * scratch is one static device array of about 8.4 MB that every GPU holds from the
+ * library's first call on it (any entry point: that call looks up the array's device
+ * address and the driver reserves it then) until the process exits, so make that
+ * first call before reserving the device's memory for your own pool and before any
+ * CUDA stream capture.  A call is limited to 262144 particles and 524288 bins
+ * ((nx'+3)(ny'+3)(nz'+3) for M4', +5 per axis for M6*; larger inputs are rejected with
+ * ierr = -1).  All calls share the array: calls that overlap on the GPU (different
+ * streams or threads) race. */
 int pmgpu_interp_particle_mesh_noalloc(const pmgpu_topo *topo, const pmgpu_params *par,
                                        const double *d_xpart, const double *d_part, int nvar,
                                        int npart, double *d_mesh, int nvar_mesh, int clear,

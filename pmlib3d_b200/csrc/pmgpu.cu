@@ -91,10 +91,13 @@ static bool g_dev_ready[128];
 // plans made while set use the out-of-place Stockham passes along y and z only
 static int g_force_stockham = 0;
 
+static int noalloc_reserve(int dev, const char *caller);
+
 static int ensure_device(const char *caller) {
   int dev = 0;
   CK(cudaGetDevice(&dev), caller);
   if (dev >= 0 && dev < 128 && g_dev_ready[dev]) return 0;
+  if (noalloc_reserve(dev, caller)) return -1;
   static float t32[CS_R][CS_M][2];
   static double t64[CS_R][CS_M][2];
   const long double twopi = 2.0L * acosl(-1.0L);
@@ -1976,19 +1979,33 @@ int pmgpu_remesh(const pmgpu_topo *topo, const double *mesh_vort, const double *
 // reserved the GPU's memory up front (a fixed-budget pool or another runtime owning
 // the allocator), or a loop that must not risk the implicit synchronisation and
 // failure modes of cudaMalloc / cudaFree.  This variant of the deposition keeps all
-// of its scratch (bin keys, particle order, bin counts and starts, sort histograms)
-// in one static device array that the library reserves when it is loaded on a GPU,
-// and takes only device pointers from the caller.
+// of its scratch (bin keys, particle order, bin counts and starts, the list of
+// crowded bins) in one static device array, and takes only device pointers from the
+// caller.  The module loads lazily, so the array exists on a device only once code
+// of this file has been used there: the library's first call on a device (any entry
+// point) looks up its address, which makes the driver reserve it then.
 namespace pmgpu {
 constexpr size_t NOALLOC_MAX_PART = size_t(1) << 18;  // particles per call
 constexpr size_t NOALLOC_MAX_BINS = size_t(1) << 19;  // (nx' + 3)(ny' + 3)(nz' + 3) for M4'
 constexpr size_t NA_PART_BYTES = NOALLOC_MAX_PART * 4;
 constexpr size_t NA_BIN_BYTES = (NOALLOC_MAX_BINS + 256) * 4;
-constexpr size_t NA_HIST_BYTES = (65536 + 256) * 4;  // 1024 digits x 64 sort tiles, + 1
+// the overflow list of the stable fix-up: a count and the bins that hold more than
+// FIX_SMALL particles, at most NOALLOC_MAX_PART / (FIX_SMALL + 1) of them
+constexpr size_t NA_HIST_BYTES = ((NOALLOC_MAX_PART / (FIX_SMALL + 1) + 2) * 4 + 255) / 256 * 256;
 constexpr size_t NA_SPART_BYTES = size_t(1) << 12;
 constexpr size_t NOALLOC_BYTES = 4 * NA_PART_BYTES + 2 * NA_BIN_BYTES + NA_HIST_BYTES + NA_SPART_BYTES;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 static void *g_noalloc_addr[128];
+
+// once per device, with that device current: the host-side symbol is only a
+// stand-in, the kernels need the device address of the array
+static int noalloc_reserve(int dev, const char *caller) {
+  if (dev < 0 || dev >= 128 || g_noalloc_addr[dev]) return 0;
+  void *ptr = nullptr;
+  CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch), caller);
+  g_noalloc_addr[dev] = ptr;
+  return 0;
+}
 }  // namespace pmgpu
 
 int pmgpu_interp_particle_mesh_noalloc(const pmgpu_topo *topo, const pmgpu_params *par, const double *d_xpart,
@@ -2028,13 +2045,7 @@ int pmgpu_interp_particle_mesh_noalloc(const pmgpu_topo *topo, const pmgpu_param
     set_error(caller, "device index out of range.");
     return -1;
   }
-  if (!g_noalloc_addr[dev]) {
-    // once per device, with that device current: the host-side symbol is only a
-    // stand-in, the kernels need the device address of the array
-    void *ptr = nullptr;
-    CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch), caller);
-    g_noalloc_addr[dev] = ptr;
-  }
+  if (noalloc_reserve(dev, caller)) return -1;
   unsigned char *base = reinterpret_cast<unsigned char *>(g_noalloc_addr[dev]);
   DevBuf key, val, key2, val2, counts, start, spart, hist;
   DevBuf *views[] = {&key, &val, &key2, &val2};

@@ -13,6 +13,7 @@
 !   pmlib_poisson_solve(patch,topo_all,mesh,ierr,reg_vort,reproj,calc_vecpot)
 !   pmlib_regularise(patch,topo_all,mesh,reg_order,filter_width,ierr)
 !   pmlib_particles_advance(patch,topo,part,itimestage,dtime,ierr,euler_vort)
+!   pmlib_remesh(patch,topo,mesh,part,min_vort,min_dvort,ierr,dvort,vel,mask,incl_ghost)
 !   pmlib_output_mesh(outdir,tag,patch,topo,mesh,ierr)
 !   pmlib_gpu_finalise()                 (frees the plan; call from pmlib_finalise)
 !
@@ -176,7 +177,7 @@ MODULE pmlib_gpu_drop_in
   PRIVATE
   PUBLIC :: pmlib_interp_particle_mesh, pmlib_interp_mesh_particle, pmlib_poisson_setup, &
           & pmlib_poisson_solve, pmlib_regularise, pmlib_particles_advance, pmlib_output_mesh, &
-          & pmlib_gpu_finalise
+          & pmlib_remesh, pmlib_gpu_finalise
 
   TYPE(C_PTR), SAVE :: gpu_plan = C_NULL_PTR
   LOGICAL, PARAMETER :: single = MK .NE. KIND(1D0)
@@ -399,6 +400,82 @@ CONTAINS
     DEALLOCATE(part%dvort)
     ALLOCATE(part%dvort(pmlib_ndim, nout))
   END SUBROUTINE pmlib_particles_advance
+
+  ! source/remesh/pmlib_remesh.f:5-233: one particle at the centre of every kept cell
+  ! in k-j-i order.  A first call counts the cells, the particle arrays are reallocated
+  ! to that count as the reference reallocates them (:63-144), a second call fills
+  ! them.  The criterion reads mesh%dvort whether or not dvort is requested (:178-181);
+  ! part%dvort and part%vel get the mesh values only when requested (zero otherwise),
+  ! vel_rk and dvort_rk are zeroed.  A __single build goes through FP64 copies.
+  SUBROUTINE pmlib_remesh(patch, topo, mesh, part, min_vort, min_dvort, ierr, dvort, vel, mask, incl_ghost)
+    TYPE(class_patch), INTENT(IN) :: patch
+    TYPE(class_topology), DIMENSION(:), POINTER, INTENT(INOUT) :: topo
+    TYPE(class_mesh), INTENT(IN) :: mesh
+    TYPE(class_particles), INTENT(INOUT) :: part
+    REAL(MK), INTENT(IN) :: min_vort, min_dvort
+    INTEGER, INTENT(OUT) :: ierr
+    LOGICAL, INTENT(IN), OPTIONAL :: dvort, vel, mask, incl_ghost
+    TYPE(pmgpu_topo) :: t
+    INTEGER(C_INT) :: fg, n, nout
+    LOGICAL :: fd, fv, fm
+    INTEGER(C_SIGNED_CHAR), DIMENSION(:,:,:), ALLOCATABLE, TARGET :: cmask
+    REAL(C_DOUBLE), DIMENSION(:,:,:,:), ALLOCATABLE, TARGET :: w, dw, u
+    REAL(C_DOUBLE), DIMENSION(:,:), ALLOCATABLE, TARGET :: pp, pw, pdw, pu
+    TYPE(C_PTR) :: cm, cdw, cu
+    fd = .FALSE.; fv = .FALSE.; fm = .FALSE.
+    IF (PRESENT(dvort)) fd = dvort
+    IF (PRESENT(vel)) fv = vel
+    IF (PRESENT(mask)) fm = mask
+    fg = 0
+    IF (PRESENT(incl_ghost)) fg = flag(.TRUE., incl_ghost)
+    t = c_topo(topo(mpi_rank))
+    ALLOCATE(w(SIZE(mesh%vort,1), SIZE(mesh%vort,2), SIZE(mesh%vort,3), SIZE(mesh%vort,4)))
+    w = REAL(mesh%vort, C_DOUBLE)
+    cdw = C_NULL_PTR
+    IF (ASSOCIATED(mesh%dvort)) THEN
+      ALLOCATE(dw(SIZE(mesh%dvort,1), SIZE(mesh%dvort,2), SIZE(mesh%dvort,3), SIZE(mesh%dvort,4)))
+      dw = REAL(mesh%dvort, C_DOUBLE)
+      cdw = C_LOC(dw)
+    END IF
+    cu = C_NULL_PTR
+    IF (fv) THEN
+      ALLOCATE(u(SIZE(mesh%vel,1), SIZE(mesh%vel,2), SIZE(mesh%vel,3), SIZE(mesh%vel,4)))
+      u = REAL(mesh%vel, C_DOUBLE)
+      cu = C_LOC(u)
+    END IF
+    cm = C_NULL_PTR
+    IF (fm) THEN
+      ALLOCATE(cmask(SIZE(mesh%patch_mask,1), SIZE(mesh%patch_mask,2), SIZE(mesh%patch_mask,3)))
+      cmask = 0_C_SIGNED_CHAR
+      WHERE (mesh%patch_mask) cmask = 1_C_SIGNED_CHAR
+      cm = C_LOC(cmask)
+    END IF
+    n = 0
+    ierr = pmgpu_remesh(t, C_LOC(w), cdw, cu, cm, REAL(min_vort, C_DOUBLE), REAL(min_dvort, C_DOUBLE), fg, &
+         & 0_C_INT, C_NULL_PTR, C_NULL_PTR, C_NULL_PTR, C_NULL_PTR, n)
+    IF (ierr .NE. 0) RETURN
+    ALLOCATE(pp(3, MAX(n, 1)), pw(3, MAX(n, 1)), pdw(3, MAX(n, 1)), pu(3, MAX(n, 1)))
+    ierr = pmgpu_remesh(t, C_LOC(w), cdw, cu, cm, REAL(min_vort, C_DOUBLE), REAL(min_dvort, C_DOUBLE), fg, &
+         & n, C_LOC(pp), C_LOC(pw), C_LOC(pdw), C_LOC(pu), nout)
+    IF (ierr .NE. 0) RETURN
+    IF (ASSOCIATED(part%pos)) DEALLOCATE(part%pos)
+    IF (ASSOCIATED(part%vel)) DEALLOCATE(part%vel)
+    IF (ASSOCIATED(part%vort)) DEALLOCATE(part%vort)
+    IF (ASSOCIATED(part%dvort)) DEALLOCATE(part%dvort)
+    IF (ASSOCIATED(part%vel_rk)) DEALLOCATE(part%vel_rk)
+    IF (ASSOCIATED(part%dvort_rk)) DEALLOCATE(part%dvort_rk)
+    ALLOCATE(part%pos(pmlib_ndim, nout), part%vort(pmlib_nvort, nout), part%vel(pmlib_ndim, nout), &
+           & part%dvort(pmlib_nvort, nout), part%vel_rk(pmlib_ndim, nout), part%dvort_rk(pmlib_nvort, nout))
+    part%pos = REAL(pp(:, 1:nout), MK)
+    part%vort = REAL(pw(:, 1:nout), MK)
+    part%vel = 0.0_MK
+    IF (fv) part%vel = REAL(pu(:, 1:nout), MK)
+    part%dvort = 0.0_MK
+    IF (fd) part%dvort = REAL(pdw(:, 1:nout), MK)
+    part%vel_rk = 0.0_MK
+    part%dvort_rk = 0.0_MK
+    topo(mpi_rank)%npart = nout
+  END SUBROUTINE pmlib_remesh
 
   ! source/output/pmlib_output_mesh.f:5-189 (one rank): the .pvti and .vti files of
   ! mesh%vort and mesh%vel, written by the library's host code

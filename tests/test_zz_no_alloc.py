@@ -59,3 +59,36 @@ def test_noalloc_rejects_inputs_beyond_its_limit():
                                               dmesh.data_ptr(), 3, clear=True)
     assert rc == -1
     assert "allocation-free deposition is limited" in P.last_error()
+
+
+def test_noalloc_call_allocates_nothing():
+    """After a first call, a call changes neither the device's free memory nor what
+    the device's default (stream-ordered) memory pool has in use: nothing is
+    allocated, by the library or any runtime routine it calls."""
+    import torch
+    from cuda.bindings import runtime as rt
+    tg, qg, pos, val = _case((-1, -1, -1), (1, 1, 1), (0.125,) * 3, (0, 0, 0), 4, 3, 25)
+    dpos = torch.from_numpy(pos).cuda()
+    dval = torch.from_numpy(val).cuda()
+    dmesh = torch.zeros(P.topo_shape(tg), dtype=torch.float64, device="cuda")
+    dev = torch.cuda.current_device()
+
+    def pool_used():
+        err, pool = rt.cudaDeviceGetDefaultMemPool(dev)
+        assert err == rt.cudaError_t.cudaSuccess
+        err, used = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent)
+        assert err == rt.cudaError_t.cudaSuccess
+        return int(used)
+
+    def call():
+        rc = P.pmlib_interp_particle_mesh_noalloc(tg, qg, dpos.data_ptr(), dval.data_ptr(), 3, pos.shape[0],
+                                                  dmesh.data_ptr(), 3, clear=True)
+        assert rc == 0, P.last_error()
+        torch.cuda.synchronize()
+
+    call()
+    free0, used0 = torch.cuda.mem_get_info()[0], pool_used()
+    call()
+    call()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert pool_used() == used0
