@@ -151,10 +151,12 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ batched and served solves
-def run_batched(P, Wl, torch, steps, warmup, count=96, rank=0, world=1):
+def run_batched(P, Wl, torch, steps, warmup, count=96, rank=0, world=1, fused=True):
     """96 patches of uneven sizes and boundary types (FP32 form), one batch solve per
     step replayed from a CUDA graph; solves/s and the 5-pass model bytes per second.
-    With several ranks the patches are shared out by bytes (each rank solves its part)."""
+    fused: each pass family of all patches in one persistent launch (else every patch's
+    passes on internal streams).  With several ranks the patches are shared out by
+    bytes (each rank solves its part)."""
     from pmlib3d_b200 import shard
     specs_all = Wl.batch_specs(count)
     owner = shard.assign([float(np.prod([c + 8 for c in s["ncell"]])) for s in specs_all], world)
@@ -173,8 +175,14 @@ def run_batched(P, Wl, torch, steps, warmup, count=96, rank=0, world=1):
         M = [Pp[d] if per[d] else 2 * Pp[d] for d in range(3)]
         nbytes += Wl.solve_bytes(M, Pp, 4)
     t0 = time.perf_counter()
-    b = P.Batch(patches, topos, par, P.FP32)
+    old_mode = P.batch_mode(fused)
+    try:
+        b = P.Batch(patches, topos, par, P.FP32)
+    finally:
+        P.batch_mode(old_mode)
     setup_s = time.perf_counter() - t0
+    mode = ("persistent launch per pass family (x fwd, y fwd, z, y inv, x inv, ghost fill) over a work list of "
+            "(patch, tile) items" if b.fused else "every patch's own passes on 8 internal streams")
     vel = [torch.empty_like(w) for w in vort]
     wp, up = [w.data_ptr() for w in vort], [u.data_ptr() for u in vel]
     st = torch.cuda.Stream()
@@ -196,7 +204,7 @@ def run_batched(P, Wl, torch, steps, warmup, count=96, rank=0, world=1):
                         f"h = 1/64, FP32 form, FP64 Green's set-up",
             "solves_per_s": count / (ms / 1e3), "ms_per_batch": ms, "cells": cells,
             "model_bytes_per_rank": nbytes, "achieved_gbs_per_rank": nbytes / (ms / 1e3) / 1e9,
-            "setup_s": setup_s, "graph": "captured CUDA graph, 8 internal streams",
+            "setup_s": setup_s, "graph": "captured CUDA graph", "mode": mode,
             "scaling": "strong: patches shared out over the ranks by bytes" if world > 1 else "single GPU"}
 
 
@@ -684,6 +692,9 @@ def main():
     batched = served = None
     if not args.no_batched:
         batched = run_batched(P, Wl, torch, max(3, args.steps // 2), args.warmup, rank=rank, world=world)
+        streams = run_batched(P, Wl, torch, max(3, args.steps // 2), args.warmup, rank=rank, world=world,
+                              fused=False)
+        batched["per_patch_streams"] = {k: streams[k] for k in ("solves_per_s", "ms_per_batch", "mode")}
         if rank == 0:
             served = run_served(P, torch)
         barrier()

@@ -209,7 +209,8 @@ int pmgpu_remesh(const pmgpu_topo *topo, const double *mesh_vort, const double *
                  double min_dvort, int incl_ghost, int max_part, double *pos, double *part_vort,
                  double *part_dvort, double *part_vel, int *npart);
 
-/* ---- batches of independent solves (no counterpart in the reference) ----
+/* ---- batches of independent solves (no counterpart in the reference; the
+ * multi-patch caller is validation/multipatch/sources/multipatch.f:447) ----
  * A batch holds one plan per patch (patches of any sizes and boundary types, the same
  * kernel parameters and precision); Green's spectra of identical grids are shared.
  * pmgpu_batch_solve queues the velocity solve of every patch (d_vort[i] -> d_vel[i],
@@ -225,6 +226,15 @@ int pmgpu_batch_size(const pmgpu_batch *batch);
 /* the plan of patch i (owned by the batch) */
 pmgpu_plan *pmgpu_batch_plan(pmgpu_batch *batch, int i);
 void pmgpu_batch_destroy(pmgpu_batch *batch);
+/* Batches made while the mode is 1 (the default) run each pass family (x forward,
+ * y forward, the fused z pass, y inverse, x inverse, then the periodic ghost fill
+ * per axis) of all their patches as one persistent launch whose CTAs walk a work list
+ * of (patch, tile) items; with 0, or when a patch needs the Stockham fallback, or for
+ * more than 1024 patches, every patch runs its own passes on internal streams.  The
+ * results are the same either way, bit for bit.  pmgpu_batch_mode returns the
+ * previous mode; pmgpu_batch_fused tells which way a batch runs (1 = batched passes). */
+int pmgpu_batch_mode(int fused);
+int pmgpu_batch_fused(const pmgpu_batch *batch);
 
 /* Selects the line-FFT engine of plans created afterwards (no counterpart in the
  * reference): 0 = in-place register passes wherever the y / z lengths factor into

@@ -26,7 +26,7 @@ EXPORTS = (
     "pmgpu_vortex_stage_dev", "pmgpu_fft_set_schedule", "pmgpu_step_many", "pmgpu_penalisation_solve_dev",
     "pmgpu_output_mesh", "pmgpu_output_pvti", "pmgpu_output_topology", "pmgpu_output_particles",
     "pmgpu_input_particles", "pmgpu_poisson_setup_ppf", "pmgpu_p2m_sort_order",
-    "pmgpu_poisson_setup_pff", "pmgpu_inject_alloc_failure",
+    "pmgpu_poisson_setup_pff", "pmgpu_inject_alloc_failure", "pmgpu_batch_mode", "pmgpu_batch_fused",
 )
 
 
@@ -101,6 +101,8 @@ def lib():
         "pmgpu_batch_size": [vp],
         "pmgpu_batch_plan": [vp, C.c_int],
         "pmgpu_batch_destroy": [vp],
+        "pmgpu_batch_mode": [C.c_int],
+        "pmgpu_batch_fused": [vp],
         "pmgpu_fft_tune": [C.c_int],
         "pmgpu_fft_tuned": [C.c_int, ip, ip, ip, ip, ip, dp],
         "pmgpu_fft_set_schedule": [C.c_int, C.c_int, C.c_int, ip, C.c_int],

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <vector>
 
 #include "../../include/pmlib_gpu.h"
 #include "common.cuh"
@@ -102,6 +103,27 @@ static inline int pick_rb(int n2, int P0, int Hp, int nc, size_t csize, size_t r
   return 0;
 }
 
+// ---- batches of patches: one launch per pass family (x forward, y forward, z pass,
+// y inverse, x inverse) over the tiles of every patch, then the periodic ghost fill
+// per axis.  The descriptors are built on the host once (batch_layout) and live in
+// device memory; a solve passes the patches' arrays by value (BatchIo).
+struct BatchPassInfo {
+  size_t desc_off;  // byte offset of the pass's descriptors
+  int nitems, chunk, wide;
+  size_t smem;
+};
+struct BatchGhostInfo {
+  size_t desc_off;
+  int npatch;
+  long long total;
+};
+struct BatchLayout {
+  int npatch = 0;
+  BatchPassInfo pass[5];
+  BatchGhostInfo ghost[3];
+  size_t bytes = 0;  // descriptor bytes
+};
+
 // ---- FFT passes (passes.cuh, instantiated per precision and component count)
 // x then y forward: real cuboid (component stride cs) -> X -> Y
 template <typename R, int NC>
@@ -117,6 +139,17 @@ int inv_yx(SolveGeom<R> &g, const pmgpu_topo *topo, typename cplx_t<R>::type *Y,
            cudaStream_t st, const char *caller, int cs = NC, bool ghosts = true);
 
 // one pass along y (forward X -> Y, or inverse Y -> X)
+// fills `desc` (host bytes) and `lay` for the velocity solve of n patches of
+// geometries g[i] with work spectra X[i], Y[i] (run_solve's layout); -1 if a patch
+// needs a pass the batched kernels do not run (the Stockham fallback)
+template <typename R, int NC>
+int batch_layout(int n, const SolveGeom<R> *g, typename cplx_t<R>::type *const *X,
+                 typename cplx_t<R>::type *const *Y, const pmgpu_topo *const *topo, std::vector<unsigned char> &desc,
+                 BatchLayout &lay, const char *caller);
+// queues the batched solve: d_desc holds the descriptors, counters 5 zeroed words
+template <typename R, int NC>
+int batch_launch(const BatchLayout &lay, const void *d_desc, unsigned *counters, const void *const *vort,
+                 void *const *vel, cudaStream_t st, const char *caller);
 template <typename R, int NC>
 int ypass(SolveGeom<R> &g, const typename cplx_t<R>::type *X, typename cplx_t<R>::type *Y, int inverse,
           cudaStream_t st, const char *caller);

@@ -2,3 +2,4 @@
 #include "passes.cuh"
 
 PMGPU_INSTANTIATE_PASSES(float, 3, f32_3)
+PMGPU_INSTANTIATE_BATCH(float, 3)

@@ -2,3 +2,4 @@
 #include "passes.cuh"
 
 PMGPU_INSTANTIATE_PASSES(double, 3, f64_3)
+PMGPU_INSTANTIATE_BATCH(double, 3)

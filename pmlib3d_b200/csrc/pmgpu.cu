@@ -2090,9 +2090,17 @@ int pmgpu_fft_engine(int engine) {
 // onto the least loaded stream, so small solves overlap on the device; the whole
 // batch is captured once into a CUDA graph and replayed while the caller passes the
 // same arrays on the same stream.
+static int g_batch_fuse = 1;  // batches made while set run the batched passes
+
 struct pmgpu_batch {
   int prec = 0;
   std::vector<pmgpu_plan *> plans;
+  // the batched passes: one launch per pass family over the tiles of every patch
+  // (unless a patch needs the Stockham fallback or there are more than BATCH_MAX
+  // patches: then each patch runs its own passes on the internal streams)
+  bool fused = false;
+  pmgpu::BatchLayout lay;
+  DevBuf desc, counters;
   std::vector<int> lane;  // internal stream of each patch
   std::vector<cudaStream_t> aux;
   std::vector<cudaEvent_t> ev;  // [0] fork, [1 + k] join of stream k
@@ -2107,13 +2115,47 @@ struct pmgpu_batch {
     for (cudaEvent_t e : ev) cudaEventDestroy(e);
     for (cudaStream_t s : aux) cudaStreamDestroy(s);
     for (pmgpu_plan *p : plans) delete p;
+    desc.release();
+    counters.release();
   }
 };
 
 namespace pmgpu {
-// queue every patch's solve: fork the internal streams off `st`, join them back
+// sets up the batched passes: every plan's work spectra, then the descriptors of
+// the five pass families in device memory; leaves b->fused false when a patch needs
+// a pass the batched kernels do not run
+template <typename R> static int batch_fuse(pmgpu_batch *b, const char *caller) {
+  typedef typename cplx_t<R>::type C;
+  const int n = (int)b->plans.size();
+  std::vector<SolveGeom<R>> geo(n);
+  std::vector<C *> X(n), Y(n);
+  std::vector<const pmgpu_topo *> topo(n);
+  for (int i = 0; i < n; i++) {
+    pmgpu_plan *pl = b->plans[i];
+    geo[i] = solve_geom<R>(pl);
+    const size_t nX = (size_t)geo[i].P[1] * geo[i].P[2] * geo[i].Hp * 3;
+    const size_t nY = (size_t)geo[i].M[1] * geo[i].P[2] * geo[i].Hp * 3;
+    if (pl->X.ensure(sizeof(C) * nX, caller) || pl->Y.ensure(sizeof(C) * nY, caller)) return -1;
+    X[i] = pl->X.as<C>();
+    Y[i] = pl->Y.as<C>();
+    topo[i] = &pl->topo;
+  }
+  std::vector<unsigned char> host;
+  if (batch_layout<R, 3>(n, geo.data(), X.data(), Y.data(), topo.data(), host, b->lay, caller)) return 0;
+  if (b->desc.ensure(host.size(), caller) || b->counters.ensure(5 * sizeof(unsigned), caller)) return -1;
+  CK(cudaMemcpy(b->desc.p, host.data(), host.size(), cudaMemcpyHostToDevice), caller);
+  b->fused = true;
+  return 0;
+}
+
+// queue every patch's solve: the batched passes, or each patch's own passes with the
+// internal streams forked off `st` and joined back
 static int batch_enqueue(pmgpu_batch *b, void *const *d_vort, void *const *d_vel, cudaStream_t st,
                          const char *caller) {
+  if (b->fused)
+    return b->prec == PMGPU_FP64
+               ? batch_launch<double, 3>(b->lay, b->desc.p, b->counters.as<unsigned>(), d_vort, d_vel, st, caller)
+               : batch_launch<float, 3>(b->lay, b->desc.p, b->counters.as<unsigned>(), d_vort, d_vel, st, caller);
   CK(cudaEventRecord(b->ev[0], st), caller);
   for (cudaStream_t s : b->aux) CK(cudaStreamWaitEvent(s, b->ev[0], 0), caller);
   for (size_t i = 0; i < b->plans.size(); i++) {
@@ -2182,8 +2224,24 @@ int pmgpu_batch_create(int npatch, const pmgpu_patch *patches, const pmgpu_topo 
       delete b;
       return -1;
     }
+  if (g_batch_fuse) {
+    const int rc = precision == PMGPU_FP64 ? batch_fuse<double>(b, caller) : batch_fuse<float>(b, caller);
+    if (rc) {
+      delete b;
+      return -1;
+    }
+  }
   *batch = b;
   return 0;
+}
+
+int pmgpu_batch_fused(const pmgpu_batch *b) { return b && b->fused ? 1 : 0; }
+
+int pmgpu_batch_mode(int fused) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int old = g_batch_fuse;
+  g_batch_fuse = fused ? 1 : 0;
+  return old;
 }
 
 int pmgpu_batch_solve(pmgpu_batch *b, void *const *d_vort, void *const *d_vel, void *stream) {

@@ -387,68 +387,180 @@ __global__ void __launch_bounds__(PASS_THREADS, 1) k_lines(SolveGeom<R> g, LineT
 // one CTA's loads overlap another's transforms.
 constexpr int RL_THREADS = 256;
 
+// shared memory of a line pass: tables of the geometry, then the tile buffer
+template <typename R> struct RlSmem {
+  typename cplx_t<R>::type *tw, *chirp, *bpos;
+  int *zpos;
+  R *kzs;
+  typename RVec<R>::V *buf;
+};
+
+// carves the shared memory of a line pass of geometry g and stages its tables (the
+// caller synchronises before the first tile)
+template <typename R>
+__device__ __forceinline__ RlSmem<R> rl_setup(const SolveGeom<R> &g, const LineTiles &lt, int axis, int lmode,
+                                              unsigned char *smem_raw) {
+  typedef typename cplx_t<R>::type C;
+  typedef typename RVec<R>::V V;
+  const RegPlan &pl = (axis == 1) ? g.ry : g.rz;
+  const int m = pl.n, nl = lt.n;
+  const bool blue = pl.bl != 0;
+  RlSmem<R> s;
+  unsigned char *sp = smem_raw;
+  s.tw = reinterpret_cast<C *>(sp);
+  sp += ((size_t)m * sizeof(C) + 15) & ~(size_t)15;
+  s.zpos = reinterpret_cast<int *>(sp);
+  sp += ((size_t)nl * sizeof(int) + 15) & ~(size_t)15;
+  s.kzs = reinterpret_cast<R *>(sp);
+  sp += ((size_t)nl * sizeof(R) + 15) & ~(size_t)15;
+  s.chirp = reinterpret_cast<C *>(sp);
+  s.bpos = s.chirp + nl;
+  if (blue) sp += ((size_t)(nl + m) * sizeof(C) + 15) & ~(size_t)15;
+  s.buf = reinterpret_cast<V *>(sp);
+  const C *twg = (axis == 1) ? g.rtwy : g.rtwz;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) s.tw[i] = twg[i];
+  if (lmode == L_Z)
+    for (int i = threadIdx.x; i < nl; i += blockDim.x) {
+      s.zpos[i] = g.zk[i];
+      s.kzs[i] = g.kzt[i];
+    }
+  if (blue) {
+    const C *cg = (axis == 1) ? g.rchy : g.rchz, *bg = (axis == 1) ? g.rby : g.rbz;
+    for (int i = threadIdx.x; i < nl; i += blockDim.x) s.chirp[i] = cg[i];
+    for (int i = threadIdx.x; i < m; i += blockDim.x) s.bpos[i] = bg[i];
+  }
+  return s;
+}
+
+// one tile of a line pass (ends with a barrier)
+template <typename R, int NC, bool WIDE>
+__device__ __forceinline__ void rl_tile(const SolveGeom<R> &g, const LineTiles &lt, const typename cplx_t<R>::type *in,
+                                        typename cplx_t<R>::type *out, int axis, int lmode, int zmode, int reproj,
+                                        int use_zeta, const RlSmem<R> &s, int tile) {
+  typedef typename cplx_t<R>::type C;
+  constexpr int G = RVec<R>::G;
+  const RegPlan &pl = (axis == 1) ? g.ry : g.rz;
+  const int nl = lt.n, TK = lt.TK, L = NC * TK, LG = L / G;
+  const bool blue = pl.bl != 0;
+  const int o = tile / lt.nkt, kt = tile - o * lt.nkt;
+  PhaseGlobal gl;
+  gl.in = in + (o * lt.in_os + (long long)kt * TK) * NC;
+  gl.out = out + (o * lt.out_os + (long long)kt * TK) * NC;
+  gl.rs_in = lt.in_rs * NC;
+  gl.rs_out = lt.out_rs * NC;
+  gl.rows_in = lt.rows_in;
+  gl.rows_out = lt.rows_out;
+  if (lmode == L_FWD) {
+    if (blue) bfft<R, false>(pl, s.buf, LG, lt.dLG, s.tw, s.chirp, s.bpos, true, true, gl, lt.rows_in, nl);
+    else rfft_fwd<R, WIDE>(pl, s.buf, LG, lt.dLG, s.tw, true, true, gl);
+  } else if (lmode == L_INV) {
+    if (blue) bfft<R, true>(pl, s.buf, LG, lt.dLG, s.tw, s.chirp, s.bpos, true, true, gl, nl, lt.rows_out);
+    else rfft_inv<R, WIDE>(pl, s.buf, LG, lt.dLG, s.tw, true, true, gl);
+  } else {
+    if (blue) bfft<R, false>(pl, s.buf, LG, lt.dLG, s.tw, s.chirp, s.bpos, true, false, gl, lt.rows_in, nl);
+    else rfft_fwd<R, WIDE>(pl, s.buf, LG, lt.dLG, s.tw, true, false, gl);
+    z_multiply<R, NC>(g, reinterpret_cast<C *>(s.buf), L, TK, kt * TK, g.yk ? g.yk[o] : o, zmode, reproj, use_zeta,
+                      blue ? nullptr : s.zpos, s.kzs);
+    __syncthreads();
+    if (blue) bfft<R, true>(pl, s.buf, LG, lt.dLG, s.tw, s.chirp, s.bpos, false, true, gl, nl, lt.rows_out);
+    else rfft_inv<R, WIDE>(pl, s.buf, LG, lt.dLG, s.tw, false, true, gl);
+  }
+}
+
 template <typename R, int NC, bool WIDE = false>
 __global__ void __launch_bounds__(RL_THREADS, WIDE ? 2 : RMinBlocks<R>::v) k_rlines(SolveGeom<R> g, LineTiles lt,
                                                           const typename cplx_t<R>::type *in,
                                                           typename cplx_t<R>::type *out, int axis, int lmode,
                                                           int zmode, int reproj, int use_zeta) {
-  typedef typename cplx_t<R>::type C;
-  typedef typename RVec<R>::V V;
-  constexpr int G = RVec<R>::G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const RegPlan &pl = (axis == 1) ? g.ry : g.rz;
-  const int m = pl.n, nl = lt.n, TK = lt.TK, L = NC * TK, LG = L / G;  // m: transform length
-  const bool blue = pl.bl != 0;
-  unsigned char *sp = smem_raw;
-  C *tw = reinterpret_cast<C *>(sp);
-  sp += ((size_t)m * sizeof(C) + 15) & ~(size_t)15;
-  int *zpos = reinterpret_cast<int *>(sp);
-  sp += ((size_t)nl * sizeof(int) + 15) & ~(size_t)15;
-  R *kzs = reinterpret_cast<R *>(sp);
-  sp += ((size_t)nl * sizeof(R) + 15) & ~(size_t)15;
-  C *chirp = reinterpret_cast<C *>(sp);
-  C *bpos = chirp + nl;
-  if (blue) sp += ((size_t)(nl + m) * sizeof(C) + 15) & ~(size_t)15;
-  V *buf = reinterpret_cast<V *>(sp);
-  {
-    const C *twg = (axis == 1) ? g.rtwy : g.rtwz;
-    for (int i = threadIdx.x; i < m; i += blockDim.x) tw[i] = twg[i];
-    if (lmode == L_Z)
-      for (int i = threadIdx.x; i < nl; i += blockDim.x) {
-        zpos[i] = g.zk[i];
-        kzs[i] = g.kzt[i];
-      }
-    if (blue) {
-      const C *cg = (axis == 1) ? g.rchy : g.rchz, *bg = (axis == 1) ? g.rby : g.rbz;
-      for (int i = threadIdx.x; i < nl; i += blockDim.x) chirp[i] = cg[i];
-      for (int i = threadIdx.x; i < m; i += blockDim.x) bpos[i] = bg[i];
-    }
-  }
+  const RlSmem<R> s = rl_setup<R>(g, lt, axis, lmode, smem_raw);
   __syncthreads();
   const int ntiles = lt.nouter * lt.nkt;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int o = tile / lt.nkt, kt = tile - o * lt.nkt;
-    PhaseGlobal gl;
-    gl.in = in + (o * lt.in_os + (long long)kt * TK) * NC;
-    gl.out = out + (o * lt.out_os + (long long)kt * TK) * NC;
-    gl.rs_in = lt.in_rs * NC;
-    gl.rs_out = lt.out_rs * NC;
-    gl.rows_in = lt.rows_in;
-    gl.rows_out = lt.rows_out;
-    if (lmode == L_FWD) {
-      if (blue) bfft<R, false>(pl, buf, LG, lt.dLG, tw, chirp, bpos, true, true, gl, lt.rows_in, nl);
-      else rfft_fwd<R, WIDE>(pl, buf, LG, lt.dLG, tw, true, true, gl);
-    } else if (lmode == L_INV) {
-      if (blue) bfft<R, true>(pl, buf, LG, lt.dLG, tw, chirp, bpos, true, true, gl, nl, lt.rows_out);
-      else rfft_inv<R, WIDE>(pl, buf, LG, lt.dLG, tw, true, true, gl);
-    } else {
-      if (blue) bfft<R, false>(pl, buf, LG, lt.dLG, tw, chirp, bpos, true, false, gl, lt.rows_in, nl);
-      else rfft_fwd<R, WIDE>(pl, buf, LG, lt.dLG, tw, true, false, gl);
-      z_multiply<R, NC>(g, reinterpret_cast<C *>(buf), L, TK, kt * TK, g.yk ? g.yk[o] : o, zmode, reproj, use_zeta,
-                        blue ? nullptr : zpos, kzs);
-      __syncthreads();
-      if (blue) bfft<R, true>(pl, buf, LG, lt.dLG, tw, chirp, bpos, false, true, gl, nl, lt.rows_out);
-      else rfft_inv<R, WIDE>(pl, buf, LG, lt.dLG, tw, false, true, gl);
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    rl_tile<R, NC, WIDE>(g, lt, in, out, axis, lmode, zmode, reproj, use_zeta, s, tile);
+}
+
+// ---------------------------------------------------------------- batches of patches
+// A batched pass runs one pass family (x forward, y forward, the fused z pass, y
+// inverse or x inverse) of every patch of a batch in one launch.  Every patch has a
+// descriptor (its geometry and the pass's tiles and arrays) and a range of work
+// items, one per tile.  CTAs take chunks of consecutive items from a counter in
+// global memory (zeroed before the launch) and load a patch's descriptor and tables
+// into shared memory when the patch changes.  Each tile is transformed by the same
+// code as in the pass of a single plan, so a patch's result is bit-identical to
+// its solve alone.
+template <typename R> struct PassDesc {
+  SolveGeom<R> g;
+  LineTiles lt;     // line passes: the tiles of this patch's lines
+  const void *in;   // pass input (x forward: the patch's vorticity)
+  void *out;        // pass output (x inverse: the patch's velocity)
+  int RB, cs;       // x passes: rows per tile, component stride of the real field
+  int vec16;        // x forward: rows are staged in 16-byte chunks
+  int first;        // first work item of the patch
+  FastDiv dLG;      // x passes: division by the line vectors of a tile
+  int ntiles, pad;
+};
+struct BatchWork {
+  const void *desc;   // PassDesc<R>[npatch]
+  int npatch, nitems, chunk, pad;
+  unsigned *counter;  // zero at the launch
+};
+// the caller's arrays of a batched solve, one per patch (x forward: vorticity, x
+// inverse and ghost fill: velocity), passed by value with the launch
+constexpr int BATCH_MAX = 1024;
+struct BatchIo {
+  const void *p[BATCH_MAX];
+};
+
+// the CTA's next chunk of work items [i0, i1); false when none is left
+__device__ __forceinline__ bool batch_next(const BatchWork &bw, int &i0, int &i1) {
+  __shared__ int s_next;
+  __syncthreads();
+  if (threadIdx.x == 0) s_next = (int)atomicAdd(bw.counter, (unsigned)bw.chunk);
+  __syncthreads();
+  i0 = s_next;
+  i1 = min(i0 + bw.chunk, bw.nitems);
+  return i0 < bw.nitems;
+}
+
+// the patch that holds work item `item`, and a copy of its descriptor in shared
+// memory when it is not the current one (all threads; ends with a barrier when it
+// loads).  Returns true when the patch changed.
+template <typename R>
+__device__ __forceinline__ bool batch_patch(const BatchWork &bw, int item, PassDesc<R> &sd, int &cur) {
+  const PassDesc<R> *d = reinterpret_cast<const PassDesc<R> *>(bw.desc);
+  if (cur >= 0 && item >= sd.first && item < sd.first + sd.ntiles) return false;
+  int lo = 0, hi = bw.npatch - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (d[mid].first <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  __syncthreads();  // everyone is done with the previous descriptor
+  const unsigned *src = reinterpret_cast<const unsigned *>(d + lo);
+  unsigned *dst = reinterpret_cast<unsigned *>(&sd);
+  for (int i = threadIdx.x; i < (int)(sizeof(PassDesc<R>) / 4); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  cur = lo;
+  return true;
+}
+
+template <typename R, int NC, bool WIDE = false>
+__global__ void __launch_bounds__(RL_THREADS, WIDE ? 2 : RMinBlocks<R>::v) k_rlines_batch(BatchWork bw, int axis,
+                                                                int lmode, int zmode, int reproj, int use_zeta) {
+  typedef typename cplx_t<R>::type C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ PassDesc<R> sd;
+  RlSmem<R> s;
+  int cur = -1, i0, i1;
+  while (batch_next(bw, i0, i1)) {
+    for (int it = i0; it < i1; it++) {
+      if (batch_patch<R>(bw, it, sd, cur)) {
+        s = rl_setup<R>(sd.g, sd.lt, axis, lmode, smem_raw);
+        __syncthreads();
+      }
+      rl_tile<R, NC, WIDE>(sd.g, sd.lt, reinterpret_cast<const C *>(sd.in), reinterpret_cast<C *>(sd.out), axis,
+                           lmode, zmode, reproj, use_zeta, s, it - sd.first);
     }
   }
 }
@@ -458,222 +570,325 @@ __global__ void __launch_bounds__(RL_THREADS, WIDE ? 2 : RMinBlocks<R>::v) k_rli
 // with the transform done in place by the register engine: the packed line has
 // its second half zero (not read), and the digit-reversed spectrum is addressed
 // through the frequency -> position table.
+template <typename R> struct RxSmem {
+  typename cplx_t<R>::type *tw, *ext, *chirp, *bpos;
+  int *xpos;
+  void *stage;  // raw rows (forward: reals, inverse: spectrum rows)
+  typename RVec<R>::V *buf;
+};
+
+// carves the shared memory of an x pass of geometry g with RB rows per tile and
+// stages its tables; inverse: the staged rows are spectrum rows of Hp complex
+template <typename R, int NC>
+__device__ __forceinline__ RxSmem<R> rx_setup(const SolveGeom<R> &g, int RB, bool inverse, unsigned char *smem_raw) {
+  typedef typename cplx_t<R>::type C;
+  typedef typename RVec<R>::V V;
+  const RegPlan &pl = g.rx;
+  const bool blue = pl.bl != 0;
+  const int N = blue ? pl.bn : pl.n, m = pl.n, H = g.H;
+  RxSmem<R> s;
+  unsigned char *sp = smem_raw;
+  s.tw = reinterpret_cast<C *>(sp);
+  sp += ((size_t)m * sizeof(C) + 15) & ~(size_t)15;
+  s.ext = reinterpret_cast<C *>(sp);
+  sp += ((size_t)H * sizeof(C) + 15) & ~(size_t)15;
+  s.xpos = reinterpret_cast<int *>(sp);
+  sp += ((size_t)N * sizeof(int) + 15) & ~(size_t)15;
+  s.chirp = reinterpret_cast<C *>(sp);
+  s.bpos = s.chirp + N;
+  if (blue) sp += ((size_t)(N + m) * sizeof(C) + 15) & ~(size_t)15;
+  s.stage = sp;
+  if (inverse) sp += (size_t)RB * g.Hp * NC * sizeof(C);
+  else sp += ((size_t)RB * g.P[0] * NC * sizeof(R) + 15) & ~(size_t)15;
+  s.buf = reinterpret_cast<V *>(sp);
+  for (int i = threadIdx.x; i < m; i += blockDim.x) s.tw[i] = g.rtwx[i];
+  for (int i = threadIdx.x; i < N; i += blockDim.x) s.xpos[i] = g.xpos[i];
+  for (int i = threadIdx.x; i < H; i += blockDim.x) s.ext[i] = g.rextx[i];
+  if (blue) {
+    for (int i = threadIdx.x; i < N; i += blockDim.x) s.chirp[i] = g.rchx[i];
+    for (int i = threadIdx.x; i < m; i += blockDim.x) s.bpos[i] = g.rbx[i];
+  }
+  return s;
+}
+
+// x forward: raw rows of tile `tile` into the stage (cp.async, committed)
+template <typename R, int NC>
+__device__ __forceinline__ void rxf_load(const SolveGeom<R> &g, const R *__restrict__ in, int RB, int cs, int vec16,
+                                         const RxSmem<R> &s, int tile) {
+  const int P0 = g.P[0];
+  const int nrows = g.P[1] * g.P[2];
+  R *Sr = reinterpret_cast<R *>(s.stage);
+  const int row0 = tile * RB;
+  for (int rr = 0; rr < RB; rr++) {
+    const int row = row0 + rr;
+    if (row >= nrows) break;
+    const int y = row % g.P[1], z = row / g.P[1];
+    const R *src = in + (((size_t)(z + g.off[2]) * g.ext[1] + (y + g.off[1])) * g.ext[0] + g.off[0]) * cs;
+    R *dst = Sr + (size_t)rr * P0 * NC;
+    if (vec16) {
+      const int nch = (P0 * NC * (int)sizeof(R)) / 16;
+      for (int c = threadIdx.x; c < nch; c += blockDim.x)
+        cp_async16(reinterpret_cast<char *>(dst) + 16 * c, reinterpret_cast<const char *>(src) + 16 * c);
+    } else {
+      for (int e = threadIdx.x; e < P0 * NC; e += blockDim.x) {
+        const int x = e / NC, c = e - x * NC;
+        if (sizeof(R) == 8) cp_async8(dst + e, src + (size_t)x * cs + c);
+        else cp_async4(dst + e, src + (size_t)x * cs + c);
+      }
+    }
+  }
+  cp_async_commit();
+}
+
+// x forward of a staged tile (the caller waited for its copies and synchronised);
+// `prefetch` runs once the stage has been read.  Ends with a barrier.
+template <typename R, int NC, typename Prefetch>
+__device__ __forceinline__ void rxf_tile(const SolveGeom<R> &g, typename cplx_t<R>::type *__restrict__ X, int RB,
+                                         const FastDiv &dLG, const RxSmem<R> &s, int tile, Prefetch prefetch) {
+  typedef typename cplx_t<R>::type C;
+  constexpr int G = RVec<R>::G;
+  const RegPlan &pl = g.rx;
+  const bool blue = pl.bl != 0;
+  const int N = blue ? pl.bn : pl.n, L = NC * RB, LG = L / G, H = g.H;
+  const int P0 = g.P[0];
+  const int nrows = g.P[1] * g.P[2];
+  const int npk = (P0 + 1) / 2;  // packed points that hold data
+  const R *Sr = reinterpret_cast<const R *>(s.stage);
+  C *Bc = reinterpret_cast<C *>(s.buf);
+  const int row0 = tile * RB;
+  for (int t = threadIdx.x; t < RB * npk; t += blockDim.x) {
+    const int rr = t / npk, m = t - rr * npk;
+    const R *xr = Sr + (size_t)rr * P0 * NC;
+    const int x0 = 2 * m, x1 = 2 * m + 1;
+    const bool ok = row0 + rr < nrows;
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      const R a = ok ? xr[x0 * NC + c] : R(0);
+      const R b = (ok && x1 < P0) ? xr[x1 * NC + c] : R(0);
+      Bc[m * L + rr * NC + c] = mk(a, b);
+    }
+  }
+  __syncthreads();
+  prefetch();
+  PhaseGlobal gl;
+  gl.in = nullptr;
+  gl.out = nullptr;
+  gl.rs_in = gl.rs_out = 0;
+  gl.rows_in = gl.rows_out = N;
+  if (blue) bfft<R, false>(pl, s.buf, LG, dLG, s.tw, s.chirp, s.bpos, false, false, gl, npk, N);
+  else rfft_fwd<R>(pl, s.buf, LG, dLG, s.tw, false, false, gl, npk);
+  for (int t = threadIdx.x; t < RB * g.Hp; t += blockDim.x) {
+    const int rr = t / g.Hp, k = t - rr * g.Hp;
+    const int row = row0 + rr;
+    if (row >= nrows) continue;
+    C o[NC];
+    if (k < H) {
+      const int kk = (k == N) ? 0 : k;
+      const int km = (k == 0 || k == N) ? 0 : N - k;
+      const int pk = s.xpos[kk], pm = s.xpos[km];
+      const C w = s.ext[k];
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        const C zk = Bc[pk * L + rr * NC + c];
+        const C zn = cconj(Bc[pm * L + rr * NC + c]);
+        const C a = cadd(zk, zn), bb = csub(zk, zn);
+        const C wb = cmul(w, bb);
+        o[c] = mk(R(0.5) * (a.x + wb.y), R(0.5) * (a.y - wb.x));  // (a - i W^k b) / 2
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < NC; c++) o[c] = mk(R(0), R(0));
+    }
+#pragma unroll
+    for (int c = 0; c < NC; c++) X[((size_t)row * g.Hp + k) * NC + c] = o[c];
+  }
+  __syncthreads();
+}
+
 template <typename R, int NC>
 __global__ void __launch_bounds__(RL_THREADS, RMinBlocks<R>::v) k_rxfwd(SolveGeom<R> g, const R *__restrict__ in,
                                                          typename cplx_t<R>::type *__restrict__ X, int RB, int cs,
                                                          int vec16, FastDiv dLG) {
-  typedef typename cplx_t<R>::type C;
-  typedef typename RVec<R>::V V;
-  constexpr int G = RVec<R>::G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const RegPlan &pl = g.rx;
-  const bool blue = pl.bl != 0;
-  const int N = blue ? pl.bn : pl.n, m = pl.n, L = NC * RB, LG = L / G, H = g.H;
-  const int P0 = g.P[0];
-  unsigned char *sp = smem_raw;
-  C *tw = reinterpret_cast<C *>(sp);
-  sp += ((size_t)m * sizeof(C) + 15) & ~(size_t)15;
-  C *ext = reinterpret_cast<C *>(sp);
-  sp += ((size_t)H * sizeof(C) + 15) & ~(size_t)15;
-  int *xpos = reinterpret_cast<int *>(sp);
-  sp += ((size_t)N * sizeof(int) + 15) & ~(size_t)15;
-  C *chirp = reinterpret_cast<C *>(sp);
-  C *bpos = chirp + N;
-  if (blue) sp += ((size_t)(N + m) * sizeof(C) + 15) & ~(size_t)15;
-  R *Sr = reinterpret_cast<R *>(sp);
-  sp += ((size_t)RB * P0 * NC * sizeof(R) + 15) & ~(size_t)15;
-  V *buf = reinterpret_cast<V *>(sp);
-  C *Bc = reinterpret_cast<C *>(buf);
-  for (int i = threadIdx.x; i < m; i += blockDim.x) tw[i] = g.rtwx[i];
-  for (int i = threadIdx.x; i < N; i += blockDim.x) xpos[i] = g.xpos[i];
-  for (int i = threadIdx.x; i < H; i += blockDim.x) ext[i] = g.rextx[i];
-  if (blue) {
-    for (int i = threadIdx.x; i < N; i += blockDim.x) chirp[i] = g.rchx[i];
-    for (int i = threadIdx.x; i < m; i += blockDim.x) bpos[i] = g.rbx[i];
-  }
+  const RxSmem<R> s = rx_setup<R, NC>(g, RB, false, smem_raw);
   const int nrows = g.P[1] * g.P[2];
   const int ntiles = (nrows + RB - 1) / RB;
-  const int npk = (P0 + 1) / 2;  // packed points that hold data
-  auto load = [&](int tile) {
-    const int row0 = tile * RB;
-    for (int rr = 0; rr < RB; rr++) {
-      const int row = row0 + rr;
-      if (row >= nrows) break;
-      const int y = row % g.P[1], z = row / g.P[1];
-      const R *src = in + (((size_t)(z + g.off[2]) * g.ext[1] + (y + g.off[1])) * g.ext[0] + g.off[0]) * cs;
-      R *dst = Sr + (size_t)rr * P0 * NC;
-      if (vec16) {
-        const int nch = (P0 * NC * (int)sizeof(R)) / 16;
-        for (int c = threadIdx.x; c < nch; c += blockDim.x)
-          cp_async16(reinterpret_cast<char *>(dst) + 16 * c, reinterpret_cast<const char *>(src) + 16 * c);
-      } else {
-        for (int e = threadIdx.x; e < P0 * NC; e += blockDim.x) {
-          const int x = e / NC, c = e - x * NC;
-          if (sizeof(R) == 8) cp_async8(dst + e, src + (size_t)x * cs + c);
-          else cp_async4(dst + e, src + (size_t)x * cs + c);
-        }
-      }
-    }
-    cp_async_commit();
-  };
   int tile = blockIdx.x;
-  if (tile < ntiles) load(tile);
+  if (tile < ntiles) rxf_load<R, NC>(g, in, RB, cs, vec16, s, tile);
   for (; tile < ntiles; tile += gridDim.x) {
     cp_async_wait_all();
     __syncthreads();
-    const int row0 = tile * RB;
-    for (int t = threadIdx.x; t < RB * npk; t += blockDim.x) {
-      const int rr = t / npk, m = t - rr * npk;
-      const R *xr = Sr + (size_t)rr * P0 * NC;
-      const int x0 = 2 * m, x1 = 2 * m + 1;
-      const bool ok = row0 + rr < nrows;
-#pragma unroll
-      for (int c = 0; c < NC; c++) {
-        const R a = ok ? xr[x0 * NC + c] : R(0);
-        const R b = (ok && x1 < P0) ? xr[x1 * NC + c] : R(0);
-        Bc[m * L + rr * NC + c] = mk(a, b);
-      }
-    }
-    __syncthreads();
     const int next = tile + gridDim.x;
-    if (next < ntiles) load(next);
-    PhaseGlobal gl;
-    gl.in = nullptr;
-    gl.out = nullptr;
-    gl.rs_in = gl.rs_out = 0;
-    gl.rows_in = gl.rows_out = N;
-    if (blue) bfft<R, false>(pl, buf, LG, dLG, tw, chirp, bpos, false, false, gl, npk, N);
-    else rfft_fwd<R>(pl, buf, LG, dLG, tw, false, false, gl, npk);
-    for (int t = threadIdx.x; t < RB * g.Hp; t += blockDim.x) {
-      const int rr = t / g.Hp, k = t - rr * g.Hp;
-      const int row = row0 + rr;
-      if (row >= nrows) continue;
-      C o[NC];
-      if (k < H) {
-        const int kk = (k == N) ? 0 : k;
-        const int km = (k == 0 || k == N) ? 0 : N - k;
-        const int pk = xpos[kk], pm = xpos[km];
-        const C w = ext[k];
-#pragma unroll
-        for (int c = 0; c < NC; c++) {
-          const C zk = Bc[pk * L + rr * NC + c];
-          const C zn = cconj(Bc[pm * L + rr * NC + c]);
-          const C a = cadd(zk, zn), bb = csub(zk, zn);
-          const C wb = cmul(w, bb);
-          o[c] = mk(R(0.5) * (a.x + wb.y), R(0.5) * (a.y - wb.x));  // (a - i W^k b) / 2
-        }
-      } else {
-#pragma unroll
-        for (int c = 0; c < NC; c++) o[c] = mk(R(0), R(0));
-      }
-#pragma unroll
-      for (int c = 0; c < NC; c++) X[((size_t)row * g.Hp + k) * NC + c] = o[c];
-    }
-    __syncthreads();
+    rxf_tile<R, NC>(g, X, RB, dLG, s, tile, [&]() {
+      if (next < ntiles) rxf_load<R, NC>(g, in, RB, cs, vec16, s, next);
+    });
   }
   cp_async_wait_all();
+}
+
+template <typename R, int NC>
+__global__ void __launch_bounds__(RL_THREADS, RMinBlocks<R>::v) k_rxfwd_batch(BatchWork bw, BatchIo io) {
+  typedef typename cplx_t<R>::type C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ PassDesc<R> sd;
+  RxSmem<R> s;
+  int cur = -1, i0, i1, staged = -1;
+  while (batch_next(bw, i0, i1)) {
+    for (int it = i0; it < i1; it++) {
+      if (cur >= 0 && (it < sd.first || it >= sd.first + sd.ntiles)) {
+        cp_async_wait_all();  // no copy into the old layout may still be in flight
+        staged = -1;
+      }
+      if (batch_patch<R>(bw, it, sd, cur)) {
+        s = rx_setup<R, NC>(sd.g, sd.RB, false, smem_raw);
+        __syncthreads();
+      }
+      const R *in = reinterpret_cast<const R *>(io.p[cur]);
+      if (staged != it) rxf_load<R, NC>(sd.g, in, sd.RB, sd.cs, sd.vec16, s, it - sd.first);
+      cp_async_wait_all();
+      __syncthreads();
+      const int next = it + 1;
+      const bool pre = next < i1 && next < sd.first + sd.ntiles;
+      rxf_tile<R, NC>(sd.g, reinterpret_cast<C *>(sd.out), sd.RB, sd.dLG, s, it - sd.first, [&]() {
+        if (pre) rxf_load<R, NC>(sd.g, in, sd.RB, sd.cs, sd.vec16, s, next - sd.first);
+      });
+      staged = pre ? next : -1;
+    }
+  }
+  cp_async_wait_all();
+}
+
+// x inverse: spectrum rows of tile `tile` into the stage (cp.async, committed)
+template <typename R, int NC>
+__device__ __forceinline__ void rxi_load(const SolveGeom<R> &g, const typename cplx_t<R>::type *__restrict__ X, int RB,
+                                         const RxSmem<R> &s, int tile) {
+  typedef typename cplx_t<R>::type C;
+  const size_t rowc = (size_t)g.Hp * NC;
+  const int nrows = g.P[1] * g.P[2];
+  const int row0 = tile * RB;
+  const int nr = min(RB, nrows - row0);
+  const size_t nch = (size_t)nr * rowc * sizeof(C) / 16;
+  const char *src = reinterpret_cast<const char *>(X + (size_t)row0 * rowc);
+  for (size_t c = threadIdx.x; c < nch; c += blockDim.x)
+    cp_async16(reinterpret_cast<char *>(s.stage) + 16 * c, src + 16 * c);
+  cp_async_commit();
+}
+
+// x inverse of a staged tile (the caller waited for its copies and synchronised);
+// `prefetch` runs once the stage has been read.  Ends with a barrier.
+template <typename R, int NC, typename Prefetch>
+__device__ __forceinline__ void rxi_tile(const SolveGeom<R> &g, R *__restrict__ outp, int RB, int cs,
+                                         const FastDiv &dLG, const RxSmem<R> &s, int tile, Prefetch prefetch) {
+  typedef typename cplx_t<R>::type C;
+  constexpr int G = RVec<R>::G;
+  const RegPlan &pl = g.rx;
+  const bool blue = pl.bl != 0;
+  const int N = blue ? pl.bn : pl.n, L = NC * RB, LG = L / G;
+  const size_t rowc = (size_t)g.Hp * NC;
+  const int nrows = g.P[1] * g.P[2];
+  const C *Sc = reinterpret_cast<const C *>(s.stage);
+  C *Bc = reinterpret_cast<C *>(s.buf);
+  const int row0 = tile * RB;
+  for (int t = threadIdx.x; t < RB * N; t += blockDim.x) {
+    const int rr = t / N, m = t - rr * N;
+    const C w = cconj(s.ext[m]);
+    const bool ok = row0 + rr < nrows;
+    const int pm = s.xpos[m];
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      C z = mk(R(0), R(0));
+      if (ok) {
+        C xm = Sc[rr * rowc + (size_t)m * NC + c];
+        C xn = Sc[rr * rowc + (size_t)(N - m) * NC + c];
+        if (m == 0) {
+          xm.y = R(0);
+          xn.y = R(0);
+        }  // DC and Nyquist are real
+        const C a = cadd(xm, cconj(xn));
+        const C b = csub(xm, cconj(xn));
+        const C wb = cmul(w, b);
+        z = mk(a.x - wb.y, a.y + wb.x);  // a + i W^{-m} b
+      }
+      Bc[pm * L + rr * NC + c] = z;
+    }
+  }
+  __syncthreads();
+  prefetch();
+  PhaseGlobal gl;
+  gl.in = nullptr;
+  gl.out = nullptr;
+  gl.rs_in = gl.rs_out = 0;
+  gl.rows_in = gl.rows_out = N;
+  const int P0 = g.P[0];
+  const int nout = (P0 + 1) / 2;
+  if (blue) bfft<R, true>(pl, s.buf, LG, dLG, s.tw, s.chirp, s.bpos, false, false, gl, N, nout);
+  else rfft_inv<R>(pl, s.buf, LG, dLG, s.tw, false, false, gl);
+  for (int t = threadIdx.x; t < RB * nout; t += blockDim.x) {
+    const int rr = t / nout, m = t - rr * nout;
+    const int row = row0 + rr;
+    if (row >= nrows) continue;
+    const int y = row % g.P[1], z = row / g.P[1];
+    R *dst = outp + (((size_t)(z + g.off[2]) * g.ext[1] + (y + g.off[1])) * g.ext[0] + g.off[0]) * cs;
+    const int x0 = 2 * m, x1 = 2 * m + 1;
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      const C v = Bc[m * L + rr * NC + c];
+      dst[(size_t)x0 * cs + c] = v.x;
+      if (x1 < P0) dst[(size_t)x1 * cs + c] = v.y;
+    }
+  }
+  __syncthreads();
 }
 
 template <typename R, int NC>
 __global__ void __launch_bounds__(RL_THREADS, RMinBlocks<R>::v) k_rxinv(SolveGeom<R> g,
                                                          const typename cplx_t<R>::type *__restrict__ X,
                                                          R *__restrict__ outp, int RB, int cs, FastDiv dLG) {
-  typedef typename cplx_t<R>::type C;
-  typedef typename RVec<R>::V V;
-  constexpr int G = RVec<R>::G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const RegPlan &pl = g.rx;
-  const bool blue = pl.bl != 0;
-  const int N = blue ? pl.bn : pl.n, m = pl.n, L = NC * RB, LG = L / G, H = g.H;
-  const size_t rowc = (size_t)g.Hp * NC;  // complex per X row
-  unsigned char *sp = smem_raw;
-  C *tw = reinterpret_cast<C *>(sp);
-  sp += ((size_t)m * sizeof(C) + 15) & ~(size_t)15;
-  C *ext = reinterpret_cast<C *>(sp);
-  sp += ((size_t)H * sizeof(C) + 15) & ~(size_t)15;
-  int *xpos = reinterpret_cast<int *>(sp);
-  sp += ((size_t)N * sizeof(int) + 15) & ~(size_t)15;
-  C *chirp = reinterpret_cast<C *>(sp);
-  C *bpos = chirp + N;
-  if (blue) sp += ((size_t)(N + m) * sizeof(C) + 15) & ~(size_t)15;
-  C *Sc = reinterpret_cast<C *>(sp);
-  sp += (size_t)RB * rowc * sizeof(C);
-  V *buf = reinterpret_cast<V *>(sp);
-  C *Bc = reinterpret_cast<C *>(buf);
-  for (int i = threadIdx.x; i < m; i += blockDim.x) tw[i] = g.rtwx[i];
-  for (int i = threadIdx.x; i < N; i += blockDim.x) xpos[i] = g.xpos[i];
-  for (int i = threadIdx.x; i < H; i += blockDim.x) ext[i] = g.rextx[i];
-  if (blue) {
-    for (int i = threadIdx.x; i < N; i += blockDim.x) chirp[i] = g.rchx[i];
-    for (int i = threadIdx.x; i < m; i += blockDim.x) bpos[i] = g.rbx[i];
-  }
+  const RxSmem<R> s = rx_setup<R, NC>(g, RB, true, smem_raw);
   const int nrows = g.P[1] * g.P[2];
   const int ntiles = (nrows + RB - 1) / RB;
-  auto load = [&](int tile) {
-    const int row0 = tile * RB;
-    const int nr = min(RB, nrows - row0);
-    const size_t nch = (size_t)nr * rowc * sizeof(C) / 16;
-    const char *src = reinterpret_cast<const char *>(X + (size_t)row0 * rowc);
-    for (size_t c = threadIdx.x; c < nch; c += blockDim.x)
-      cp_async16(reinterpret_cast<char *>(Sc) + 16 * c, src + 16 * c);
-    cp_async_commit();
-  };
   int tile = blockIdx.x;
-  if (tile < ntiles) load(tile);
+  if (tile < ntiles) rxi_load<R, NC>(g, X, RB, s, tile);
   for (; tile < ntiles; tile += gridDim.x) {
     cp_async_wait_all();
     __syncthreads();
-    const int row0 = tile * RB;
-    for (int t = threadIdx.x; t < RB * N; t += blockDim.x) {
-      const int rr = t / N, m = t - rr * N;
-      const C w = cconj(ext[m]);
-      const bool ok = row0 + rr < nrows;
-      const int pm = xpos[m];
-#pragma unroll
-      for (int c = 0; c < NC; c++) {
-        C z = mk(R(0), R(0));
-        if (ok) {
-          C xm = Sc[rr * rowc + (size_t)m * NC + c];
-          C xn = Sc[rr * rowc + (size_t)(N - m) * NC + c];
-          if (m == 0) {
-            xm.y = R(0);
-            xn.y = R(0);
-          }  // DC and Nyquist are real
-          const C a = cadd(xm, cconj(xn));
-          const C b = csub(xm, cconj(xn));
-          const C wb = cmul(w, b);
-          z = mk(a.x - wb.y, a.y + wb.x);  // a + i W^{-m} b
-        }
-        Bc[pm * L + rr * NC + c] = z;
-      }
-    }
-    __syncthreads();
     const int next = tile + gridDim.x;
-    if (next < ntiles) load(next);
-    PhaseGlobal gl;
-    gl.in = nullptr;
-    gl.out = nullptr;
-    gl.rs_in = gl.rs_out = 0;
-    gl.rows_in = gl.rows_out = N;
-    const int P0 = g.P[0];
-    const int nout = (P0 + 1) / 2;
-    if (blue) bfft<R, true>(pl, buf, LG, dLG, tw, chirp, bpos, false, false, gl, N, nout);
-    else rfft_inv<R>(pl, buf, LG, dLG, tw, false, false, gl);
-    for (int t = threadIdx.x; t < RB * nout; t += blockDim.x) {
-      const int rr = t / nout, m = t - rr * nout;
-      const int row = row0 + rr;
-      if (row >= nrows) continue;
-      const int y = row % g.P[1], z = row / g.P[1];
-      R *dst = outp + (((size_t)(z + g.off[2]) * g.ext[1] + (y + g.off[1])) * g.ext[0] + g.off[0]) * cs;
-      const int x0 = 2 * m, x1 = 2 * m + 1;
-#pragma unroll
-      for (int c = 0; c < NC; c++) {
-        const C v = Bc[m * L + rr * NC + c];
-        dst[(size_t)x0 * cs + c] = v.x;
-        if (x1 < P0) dst[(size_t)x1 * cs + c] = v.y;
+    rxi_tile<R, NC>(g, outp, RB, cs, dLG, s, tile, [&]() {
+      if (next < ntiles) rxi_load<R, NC>(g, X, RB, s, next);
+    });
+  }
+  cp_async_wait_all();
+}
+
+template <typename R, int NC>
+__global__ void __launch_bounds__(RL_THREADS, RMinBlocks<R>::v) k_rxinv_batch(BatchWork bw, BatchIo io) {
+  typedef typename cplx_t<R>::type C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ PassDesc<R> sd;
+  RxSmem<R> s;
+  int cur = -1, i0, i1, staged = -1;
+  while (batch_next(bw, i0, i1)) {
+    for (int it = i0; it < i1; it++) {
+      if (cur >= 0 && (it < sd.first || it >= sd.first + sd.ntiles)) {
+        cp_async_wait_all();
+        staged = -1;
       }
+      if (batch_patch<R>(bw, it, sd, cur)) {
+        s = rx_setup<R, NC>(sd.g, sd.RB, true, smem_raw);
+        __syncthreads();
+      }
+      const C *X = reinterpret_cast<const C *>(sd.in);
+      if (staged != it) rxi_load<R, NC>(sd.g, X, sd.RB, s, it - sd.first);
+      cp_async_wait_all();
+      __syncthreads();
+      const int next = it + 1;
+      const bool pre = next < i1 && next < sd.first + sd.ntiles;
+      rxi_tile<R, NC>(sd.g, (R *)io.p[cur], sd.RB, sd.cs, sd.dLG, s, it - sd.first, [&]() {
+        if (pre) rxi_load<R, NC>(sd.g, X, sd.RB, s, next - sd.first);
+      });
+      staged = pre ? next : -1;
     }
-    __syncthreads();
   }
   cp_async_wait_all();
 }
@@ -871,26 +1086,57 @@ __global__ void __launch_bounds__(PASS_THREADS, 1) k_xinv(SolveGeom<R> g, const 
 // ---------------------------------------------------------------- periodic ghosts
 // ghost fill after the inverse transform (source/fourier/pmlib_fourier_ifft.f:247-253):
 // along a periodic axis the ghosts copy the interior one period away.
+// ghost point t of the (ngl + ngh) x e[o1] x e[o2] strips along `axis`
+template <typename R>
+__device__ __forceinline__ void ghost_fill_point(R *__restrict__ mesh, int ex, int ey, int ez, int nv, int axis, int N,
+                                                 int ngl, int ngh, long long t) {
+  const int e[3] = {ex, ey, ez};
+  const int ng = ngl + ngh;
+  const int o1 = axis == 0 ? 1 : 0, o2 = axis == 2 ? 1 : 2;
+  const int s = (int)(t % ng);
+  const long long r = t / ng;
+  const int a = (int)(r % e[o1]), b = (int)(r / e[o1]);
+  int dstc = (s < ngl) ? s : ngl + N + (s - ngl);
+  int srcc = (s < ngl) ? dstc + N : dstc - N;
+  int id[3], is[3];
+  id[o1] = a; id[o2] = b; id[axis] = dstc;
+  is[o1] = a; is[o2] = b; is[axis] = srcc;
+  const size_t di = (((size_t)id[2] * ey + id[1]) * ex + id[0]) * nv;
+  const size_t si = (((size_t)is[2] * ey + is[1]) * ex + is[0]) * nv;
+  for (int c = 0; c < nv; c++) mesh[di + c] = mesh[si + c];
+}
+
 template <typename R>
 __global__ void k_ghost_fill(R *__restrict__ mesh, int ex, int ey, int ez, int nv, int axis, int N,
                              int ngl, int ngh) {
   const int e[3] = {ex, ey, ez};
-  const int ng = ngl + ngh;
   const int o1 = axis == 0 ? 1 : 0, o2 = axis == 2 ? 1 : 2;
-  const long long total = (long long)ng * e[o1] * e[o2];
+  const long long total = (long long)(ngl + ngh) * e[o1] * e[o2];
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x)
+    ghost_fill_point<R>(mesh, ex, ey, ez, nv, axis, N, ngl, ngh, t);
+}
+
+// the ghost fill along one axis of every patch of a batch that is periodic there:
+// patch i's ghost points are items [first, first + total) of one index space
+struct GhostDesc {
+  long long first, total;
+  int patch, ext[3], nv, N, ngl, ngh;
+};
+template <typename R>
+__global__ void k_ghost_fill_batch(const GhostDesc *__restrict__ d, int npatch, long long total, int axis,
+                                   BatchIo io) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
-    const int s = (int)(t % ng);
-    const long long r = t / ng;
-    const int a = (int)(r % e[o1]), b = (int)(r / e[o1]);
-    int dstc = (s < ngl) ? s : ngl + N + (s - ngl);
-    int srcc = (s < ngl) ? dstc + N : dstc - N;
-    int id[3], is[3];
-    id[o1] = a; id[o2] = b; id[axis] = dstc;
-    is[o1] = a; is[o2] = b; is[axis] = srcc;
-    const size_t di = (((size_t)id[2] * ey + id[1]) * ex + id[0]) * nv;
-    const size_t si = (((size_t)is[2] * ey + is[1]) * ex + is[0]) * nv;
-    for (int c = 0; c < nv; c++) mesh[di + c] = mesh[si + c];
+    int lo = 0, hi = npatch - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (d[mid].first <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const GhostDesc &q = d[lo];
+    ghost_fill_point<R>((R *)io.p[q.patch], q.ext[0], q.ext[1], q.ext[2], q.nv, axis, q.N, q.ngl, q.ngh,
+                        t - q.first);
   }
 }
 

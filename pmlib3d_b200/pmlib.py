@@ -265,10 +265,18 @@ def pmlib_poisson_solve_dev(plan: Plan, d_vort: int, d_vel: int, d_vecpot: int =
                                          int(bool(calc_vecpot)), C.c_void_p(stream or None))
 
 
+def batch_mode(fused: bool) -> bool:
+    """Batches made afterwards run batched passes (True, the default: one launch per
+    pass family over every patch's tiles) or each patch's own passes on internal
+    streams (False); returns the previous mode."""
+    return bool(lib().pmgpu_batch_mode(int(bool(fused))))
+
+
 class Batch:
     """Independent velocity solves of patches of uneven sizes and boundary types
-    (pmgpu_batch_*): one plan per patch, solves overlapping on the device, replayed
-    from a captured CUDA graph after the first two calls on a stream."""
+    (pmgpu_batch_*): one plan per patch, each pass family of all patches in one
+    persistent launch, replayed from a captured CUDA graph after the first two calls
+    on a stream."""
 
     def __init__(self, patches, topos, params: Params, precision: int):
         n = len(patches)
@@ -280,6 +288,11 @@ class Batch:
         self.handle = h
         self.n = n
         self.precision = precision
+
+    @property
+    def fused(self) -> bool:
+        """True when the batch runs the batched passes."""
+        return bool(lib().pmgpu_batch_fused(self.handle))
 
     def plan(self, i: int) -> "Plan":
         """A non-owning view of patch i's plan (valid while the batch lives)."""

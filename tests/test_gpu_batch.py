@@ -28,8 +28,11 @@ def _batch_inputs(count, seed, nmin=12, nmax=40):
     return specs, patches, topos, fields
 
 
+@pytest.mark.parametrize("fused", [True, False])
 @pytest.mark.parametrize("prec", [P.FP32, P.FP64])
-def test_batch_matches_single_solves(prec):
+def test_batch_matches_single_solves(prec, fused):
+    """Batched passes (one launch per pass family over all patches) and per-patch
+    passes on internal streams: both bit-identical to each patch solved alone."""
     import torch
     specs, patches, topos, fields = _batch_inputs(7, seed=40)
     par = P.make_params(order=6, kernel=1, radius=2.0, interp=3)
@@ -45,7 +48,12 @@ def test_batch_matches_single_solves(prec):
         torch.cuda.synchronize()
         alone.append(u.cpu())
         plan.close()
-    b = P.Batch(patches, topos, par, prec)
+    old = P.batch_mode(fused)
+    try:
+        b = P.Batch(patches, topos, par, prec)
+    finally:
+        P.batch_mode(old)
+    assert b.fused == fused
     vel = [torch.full_like(w, 7.0) for w in vort]
     s = torch.cuda.Stream()
     with torch.cuda.stream(s):
@@ -97,3 +105,45 @@ def test_batch_errors():
     par = P.make_params(order=6, kernel=3, radius=2.0, interp=3)  # unknown kernel
     with pytest.raises(RuntimeError):
         P.Batch(patches, topos, par, P.FP32)
+
+
+@pytest.mark.parametrize("prec", [P.FP32, P.FP64])
+def test_batched_passes_full_size_mix(prec):
+    """The 96-patch workload's first 24 patches at full size (cells per axis in
+    [32, 192] before pmlib_patch_adjust; fff, ppf and pff, periodic ghosts filled):
+    the batched passes give each patch the same bits as its own plan's solve, on a
+    direct call, on the capturing call and on a replay."""
+    import torch
+    specs = Wl.batch_specs(96)[:24]
+    par = P.make_params(order=6, kernel=1, radius=2.0, interp=3)
+    dt = torch.float32 if prec == P.FP32 else torch.float64
+    patches, topos, vort, alone = [], [], [], []
+    for s_ in specs:
+        pa = P.make_patch(s_["xmin"], s_["xmax"], s_["dx"], bound_cond=s_["bound_cond"], nghost=4)
+        assert P.pmlib_patch_adjust(pa) == 0
+        ierr, t = P.pmlib_topology_cuboid(pa, 3)
+        patches.append(pa)
+        topos.append(t)
+        w = Wl.blob_field(t, s_["axis"], xp=torch).to(dt).contiguous()
+        vort.append(w)
+        ierr, plan = P.pmlib_poisson_setup(pa, t, par, prec)
+        assert ierr == 0
+        u = torch.zeros_like(w)
+        assert P.pmlib_poisson_solve_dev(plan, w.data_ptr(), u.data_ptr()) == 0
+        torch.cuda.synchronize()
+        alone.append(u.cpu())
+        plan.close()
+    b = P.Batch(patches, topos, par, prec)
+    assert b.fused
+    vel = [torch.zeros_like(w) for w in vort]
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        for call in range(3):
+            for v in vel:
+                v.fill_(3.0)
+            assert b.solve([w.data_ptr() for w in vort], [v.data_ptr() for v in vel], s.cuda_stream) == 0, \
+                P.last_error()
+            s.synchronize()
+            for i in range(len(vel)):
+                assert torch.equal(vel[i].cpu(), alone[i]), (call, i, specs[i]["bc"])
+    b.close()
