@@ -367,6 +367,44 @@ int pmgpu_penalisation_solve_dev(pmgpu_plan *plan, pmgpu_plan *penal_plan, const
                                  const double vel_inf[3], void *d_vort, void *d_vel, double force[3],
                                  int *niter, double residuals[3], void *stream);
 
+/* One stage of the penalisation client's time loop (no counterpart as one procedure in
+ * the reference: the stage of vortex_codes/vortex_penalisation/source/main.f:343-492,
+ * one rank, without repatching, diagnostics or output) on device arrays:
+ *   P2M of the particle vorticity (cleared); the solve, reprojected when `reproject`
+ *   or on the first stage of the first step (the vorticity is then replaced, as the
+ *   client pulls it back); vel_inf added; on the first stage the iterative
+ *   penalisation (pmgpu_penalisation_solve_dev; skipped when penal_plan is NULL);
+ *   the vorticity right-hand side (part_deriv_vorticity, fd_order, visc); on the first
+ *   stage of a remeshing step or of the first step pmlib_remesh from the mesh
+ *   (thresholds remesh_trunc on |vort| and remesh_trunc / dtime on |dvort|, velocity
+ *   and right-hand side copied, vel_rk and dvort_rk zeroed), otherwise M2P of the
+ *   velocity and the right-hand side; then pmlib_particles_advance (stage update and
+ *   particle map, euler_vort off).
+ * Particle arrays (3, max_part) of the plan's precision hold npart particles on entry
+ * and *npart_out on return (the remesh may change the count: more than max_part is an
+ * error).  force, niter and residuals are the penalisation's (zero on later stages);
+ * force[0] is the drag along x.  Synchronises `stream` (the counts come back). */
+typedef struct {
+  int time_order;       /* pmlib_time_integration_order (1-3) */
+  int itimestage;       /* 1-based stage */
+  double dtime;
+  int fd_order;         /* finite differences of the right-hand side and the penalisation: 2 or 4 */
+  double visc;
+  int reproject;        /* the client's reproject flag */
+  int regularise_vort;  /* the client's regularise_vort flag */
+  int first_step;       /* itime == 0 */
+  int remesh;           /* MOD(itime, iremesh) == 0 */
+  double remesh_trunc;
+  double relaxation, tolerance;
+  int max_iter;
+  double vel_inf[3];
+} pmgpu_penal_stage_args;
+int pmgpu_penalisation_stage_dev(pmgpu_plan *plan, pmgpu_plan *penal_plan, const void *d_solid,
+                                 const void *d_solid_vel, const pmgpu_penal_stage_args *args,
+                                 void *d_pos, void *d_vort, void *d_vel_rk, void *d_dvort_rk, int npart,
+                                 int max_part, void *d_part_vel, void *d_part_dvort, int *npart_out,
+                                 double force[3], int *niter, double residuals[3], void *stream);
+
 /* ---- files around the step (host code; `device` = 1 when the arrays live on the GPU) ---- */
 
 /* pmlib_output_mesh (source/output/pmlib_output_mesh.f:5-189), one rank: writes

@@ -27,6 +27,7 @@ EXPORTS = (
     "pmgpu_output_mesh", "pmgpu_output_pvti", "pmgpu_output_topology", "pmgpu_output_particles",
     "pmgpu_input_particles", "pmgpu_poisson_setup_ppf", "pmgpu_p2m_sort_order",
     "pmgpu_poisson_setup_pff", "pmgpu_inject_alloc_failure", "pmgpu_batch_mode", "pmgpu_batch_fused",
+    "pmgpu_penalisation_stage_dev",
 )
 
 
@@ -109,6 +110,8 @@ def lib():
         "pmgpu_step_many": [vp, C.c_int, C.POINTER(vp), C.POINTER(vp), ip, C.POINTER(vp)],
         "pmgpu_penalisation_solve_dev": [vp, vp, vp, vp, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
                                          C.c_int, dp, vp, vp, dp, ip, dp, vp],
+        "pmgpu_penalisation_stage_dev": [vp, vp, vp, vp, vp, vp, vp, vp, vp, C.c_int, C.c_int, vp, vp, ip, dp, ip,
+                                         dp, vp],
         "pmgpu_output_mesh": [C.c_char_p, C.c_char_p, PP, TP, C.c_int, vp, vp, C.c_int],
         "pmgpu_output_pvti": [C.c_char_p, C.c_char_p, PP, C.c_int, ip, ip],
         "pmgpu_output_topology": [C.c_char_p, PP, C.c_int, TP],

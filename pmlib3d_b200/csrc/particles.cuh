@@ -535,6 +535,16 @@ __global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(PartGeom<R> g, const
   }
 }
 
+// a constant vector added to every point of a (3, n) field (the client's free-stream
+// velocity, vortex_codes/vortex_penalisation/source/main.f:425-437)
+template <typename R> __global__ void k_add_vec3(R *__restrict__ f, size_t n, R a, R b, R c) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+    f[3 * t] = f[3 * t] + a;
+    f[3 * t + 1] = f[3 * t + 1] + b;
+    f[3 * t + 2] = f[3 * t + 2] + c;
+  }
+}
+
 // periodic ghost reverse-add of P2M, one axis (pmlib_mesh_map_ghost.f:119-207 with
 // pmlib_comm_unpack.f:269-273): both strips [1-ngl, ngh] and [N-ngl+1, N+ngh]
 // receive the sum of the two, from the values before the exchange.
@@ -827,9 +837,10 @@ __global__ void k_diag_final(const double *__restrict__ part, int nblk, double *
 
 // ------------------------------------------------------------------ remesh
 // source/remesh/pmlib_remesh.f:84-226: a particle per kept cell, cells in k-j-i order
-__global__ void k_remesh_flag(PartGeom<double> g, const double *__restrict__ vort,
-                              const double *__restrict__ dvort, const unsigned char *__restrict__ mask,
-                              double min_vort, double min_dvort, int incl_ghost, unsigned *__restrict__ flag) {
+template <typename R>
+__global__ void k_remesh_flag(PartGeom<R> g, const R *__restrict__ vort, const R *__restrict__ dvort,
+                              const unsigned char *__restrict__ mask, R min_vort, R min_dvort, int incl_ghost,
+                              unsigned *__restrict__ flag) {
   const size_t total = (size_t)g.ext[0] * g.ext[1] * g.ext[2];
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
     const int i = (int)(t % g.ext[0]) + g.lo[0];
@@ -842,11 +853,11 @@ __global__ void k_remesh_flag(PartGeom<double> g, const double *__restrict__ vor
                       (incl_ghost && ii[e] > g.nint[e] && g.bchi[e] == 0);
       place = place && in;
     }
-    const double *v = vort + 3 * t;
-    const double s = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-    double ds = 0.0;
+    const R *v = vort + 3 * t;
+    const R s = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    R ds = R(0);
     if (dvort) {
-      const double *dv = dvort + 3 * t;
+      const R *dv = dvort + 3 * t;
       ds = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
     }
     if (place && (s > min_vort || ds > min_dvort)) place = mask ? (mask[t] != 0) : true;
@@ -855,11 +866,11 @@ __global__ void k_remesh_flag(PartGeom<double> g, const double *__restrict__ vor
   }
 }
 
-__global__ void k_remesh_fill(PartGeom<double> g, const double *__restrict__ vort,
-                              const double *__restrict__ dvort, const double *__restrict__ vel,
-                              const unsigned *__restrict__ flag, const unsigned *__restrict__ slot,
-                              double *__restrict__ pos, double *__restrict__ pv, double *__restrict__ pdv,
-                              double *__restrict__ pvel) {
+template <typename R>
+__global__ void k_remesh_fill(PartGeom<R> g, const R *__restrict__ vort, const R *__restrict__ dvort,
+                              const R *__restrict__ vel, const unsigned *__restrict__ flag,
+                              const unsigned *__restrict__ slot, R *__restrict__ pos, R *__restrict__ pv,
+                              R *__restrict__ pdv, R *__restrict__ pvel) {
   const size_t total = (size_t)g.ext[0] * g.ext[1] * g.ext[2];
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
     if (!flag[t]) continue;
@@ -867,10 +878,10 @@ __global__ void k_remesh_fill(PartGeom<double> g, const double *__restrict__ vor
                        (int)(t / ((size_t)g.ext[0] * g.ext[1])) + g.lo[2]};
     const size_t q = 3 * (size_t)slot[t];
     for (int e = 0; e < 3; e++) {
-      pos[q + e] = g.xmin[e] + ((double)(ii[e] - 1) + 0.5) * g.dx[e];
+      pos[q + e] = g.xmin[e] + ((R)(ii[e] - 1) + R(0.5)) * g.dx[e];
       pv[q + e] = vort[3 * t + e];
-      if (pdv) pdv[q + e] = dvort ? dvort[3 * t + e] : 0.0;
-      if (pvel) pvel[q + e] = vel ? vel[3 * t + e] : 0.0;
+      if (pdv) pdv[q + e] = dvort ? dvort[3 * t + e] : R(0);
+      if (pvel) pvel[q + e] = vel ? vel[3 * t + e] : R(0);
     }
   }
 }

@@ -1943,8 +1943,8 @@ int pmgpu_remesh(const pmgpu_topo *topo, const double *mesh_vort, const double *
   }
   const int nblk = (int)std::min<size_t>((nc + 255) / 256, 148 * 32);
   CK(cudaMemset(s.counts.p, 0, sizeof(unsigned) * (nc + 1)), caller);
-  k_remesh_flag<<<nblk, 256>>>(g, s.c.as<double>(), ddv, dmask, min_vort, min_dvort, incl_ghost,
-                               s.counts.as<unsigned>());
+  k_remesh_flag<double><<<nblk, 256>>>(g, s.c.as<double>(), ddv, dmask, min_vort, min_dvort, incl_ghost,
+                                       s.counts.as<unsigned>());
   PM_LAUNCHED();
   CKL(caller);
   if (exclusive_scan(s.counts.as<unsigned>(), s.start.as<unsigned>(), nc + 1, s.spart, 0, caller)) return -1;
@@ -1959,8 +1959,8 @@ int pmgpu_remesh(const pmgpu_topo *topo, const double *mesh_vort, const double *
   const size_t np3 = 3 * (size_t)std::max<unsigned>(total, 1);
   if (s.f.ensure(sizeof(double) * np3 * 4, caller)) return -1;
   double *dpos = s.f.as<double>(), *dpv = dpos + np3, *dpdv = dpv + np3, *dpvel = dpdv + np3;
-  k_remesh_fill<<<nblk, 256>>>(g, s.c.as<double>(), ddv, dvel, s.counts.as<unsigned>(), s.start.as<unsigned>(),
-                               dpos, dpv, dpdv, dpvel);
+  k_remesh_fill<double><<<nblk, 256>>>(g, s.c.as<double>(), ddv, dvel, s.counts.as<unsigned>(),
+                                       s.start.as<unsigned>(), dpos, dpv, dpdv, dpvel);
   PM_LAUNCHED();
   CKL(caller);
   if (total > 0) {
@@ -2965,4 +2965,135 @@ int pmgpu_penalisation_solve_dev(pmgpu_plan *plan, pmgpu_plan *penal_plan, const
   return run_penal<float>(plan, penal_plan, (const float *)d_solid, (const float *)d_solid_vel, relaxation, tolerance,
                           max_iter, dtime, fd_order, reproject, vel_inf, (float *)d_vort, (float *)d_vel, force,
                           niter, residuals, st);
+}
+
+// ------------------------------------------------------------------ one stage of the penalisation client
+namespace pmgpu {
+// pmlib_remesh on device fields (source/remesh/pmlib_remesh.f:84-226, one rank): one
+// particle at the centre of every kept cell in k-j-i order into arrays of capacity
+// max_part; the count comes back to the host (the stream is synchronised)
+template <typename R>
+static int run_remesh_dev(pmgpu_plan *pl, const pmgpu_topo *t, const R *vort, const R *dvort, const R *vel,
+                          double min_vort, double min_dvort, int max_part, R *pos, R *pv, R *pdv, R *pvel, int *np,
+                          cudaStream_t st, const char *caller) {
+  const size_t nc = mesh_points(t);
+  PartGeom<R> g = part_geom<R>(t, 4);
+  if (pl->counts.ensure(sizeof(unsigned) * (nc + 1), caller) || pl->start.ensure(sizeof(unsigned) * (nc + 1), caller))
+    return -1;
+  const int nblk = (int)std::min<size_t>((nc + 255) / 256, 148 * 32);
+  CK(cudaMemsetAsync(pl->counts.p, 0, sizeof(unsigned) * (nc + 1), st), caller);
+  k_remesh_flag<R><<<nblk, 256, 0, st>>>(g, vort, dvort, nullptr, (R)min_vort, (R)min_dvort, 0,
+                                         pl->counts.as<unsigned>());
+  PM_LAUNCHED();
+  CKL(caller);
+  if (exclusive_scan(pl->counts.as<unsigned>(), pl->start.as<unsigned>(), nc + 1, pl->spart, st, caller)) return -1;
+  unsigned total = 0;
+  CK(cudaMemcpyAsync(&total, pl->start.as<unsigned>() + nc, sizeof(unsigned), cudaMemcpyDeviceToHost, st), caller);
+  CK(cudaStreamSynchronize(st), caller);
+  if ((long long)total > (long long)max_part) {
+    char msg[160];
+    snprintf(msg, sizeof(msg), "remeshing makes %u particles, more than the arrays hold (%d).", total, max_part);
+    set_error(caller, msg);
+    return -1;
+  }
+  k_remesh_fill<R><<<nblk, 256, 0, st>>>(g, vort, dvort, vel, pl->counts.as<unsigned>(), pl->start.as<unsigned>(),
+                                         pos, pv, pdv, pvel);
+  PM_LAUNCHED();
+  CKL(caller);
+  *np = (int)total;
+  return 0;
+}
+
+// One stage of the penalisation client's time loop (vortex_codes/vortex_penalisation/
+// source/main.f:343-492, one rank, no repatching, diagnostics or output) on the plan's
+// mesh buffers: P2M of the particle vorticity (cleared), the solve (reprojected when
+// the client asks or on the first stage of the first step, the vorticity pulled back
+// then), the free-stream velocity added, the iterative penalisation on the first
+// stage, the vorticity right-hand side, then a remesh from the mesh fields (first
+// stage of a remeshing step or of the first step; thresholds remesh_trunc and
+// remesh_trunc / dtime, velocity and right-hand side copied) or M2P of the velocity
+// and the right-hand side, and the stage update with the particle map.
+template <typename R>
+static int penal_stage(pmgpu_plan *pm, pmgpu_plan *pp, const R *solid, const R *svel, const pmgpu_penal_stage_args &a,
+                       R *pos, R *vort, R *vel_rk, R *dvort_rk, int n, int max_part, R *pvel, R *pdvort, int *nout,
+                       double force[3], int *niter, double resid[3], cudaStream_t st) {
+  const char *caller = "pmgpu_penalisation_stage";
+  const size_t nmp = mesh_points(&pm->topo), nm = nmp * 3;
+  if (pm->mesh_w.ensure(sizeof(R) * nm, caller) || pm->mesh_u.ensure(sizeof(R) * nm, caller) ||
+      pm->mesh_a.ensure(sizeof(R) * nm, caller))
+    return -1;
+  R *w = pm->mesh_w.as<R>(), *u = pm->mesh_u.as<R>(), *dw = pm->mesh_a.as<R>();
+  pmgpu_topo t = pm->topo;
+  t.npart = n;
+  PartScratchRefs r{&pm->key, &pm->val, &pm->key2, &pm->val2, &pm->counts, &pm->start, &pm->spart, &pm->hist};
+  const int *perm = nullptr;
+  if (run_p2m<R>(&t, pm->par.interpolation_order, pos, vort, 3, n, w, 3, 1, r, st, &perm, caller)) return -1;
+  const int first = a.first_step && a.itimestage == 1;
+  const int reproj = a.reproject || first;
+  const int back = reproj || a.regularise_vort;
+  if (run_solve<R>(pm, w, u, back ? w : nullptr, nullptr, a.regularise_vort, reproj, 0, st, caller)) return -1;
+  if (a.vel_inf[0] != 0.0 || a.vel_inf[1] != 0.0 || a.vel_inf[2] != 0.0) {
+    const int nblk = (int)std::min<size_t>((nmp + 255) / 256, 148 * 16);
+    k_add_vec3<R><<<nblk, 256, 0, st>>>(u, nmp, (R)a.vel_inf[0], (R)a.vel_inf[1], (R)a.vel_inf[2]);
+    PM_LAUNCHED();
+    CKL(caller);
+  }
+  force[0] = force[1] = force[2] = 0.0;
+  resid[0] = resid[1] = resid[2] = 0.0;
+  *niter = 0;
+  if (a.itimestage == 1 && pp && solid &&
+      run_penal<R>(pm, pp, solid, svel, a.relaxation, a.tolerance, a.max_iter, a.dtime, a.fd_order, a.reproject,
+                   a.vel_inf, w, u, force, niter, resid, st))
+    return -1;
+  CK(cudaMemsetAsync(dw, 0, sizeof(R) * nm, st), caller);
+  if (run_deriv_vorticity<R>(&t, a.fd_order, a.visc, w, u, dw, st, caller)) return -1;
+  if ((a.remesh || a.first_step) && a.itimestage == 1) {
+    int m = 0;
+    if (run_remesh_dev<R>(pm, &t, w, dw, u, a.remesh_trunc, a.remesh_trunc / a.dtime, max_part, pos, vort, pdvort, pvel,
+                          &m, st, caller))
+      return -1;
+    if (m > 0) {
+      CK(cudaMemsetAsync(vel_rk, 0, sizeof(R) * 3 * (size_t)m, st), caller);
+      CK(cudaMemsetAsync(dvort_rk, 0, sizeof(R) * 3 * (size_t)m, st), caller);
+    }
+    n = m;
+    t.npart = m;
+  } else if (run_m2p_sorted<R>(&t, pm->par.interpolation_order, pos, pm->start.as<unsigned>(), perm, n, dw, pdvort, st,
+                               caller) ||
+             run_m2p_sorted<R>(&t, pm->par.interpolation_order, pos, pm->start.as<unsigned>(), perm, n, u, pvel, st,
+                               caller)) {
+    return -1;
+  }
+  return run_advance<R>(&pm->patch, &t, a.time_order, a.itimestage, a.dtime, 0, pos, vort, pvel, pdvort, vel_rk,
+                        dvort_rk, n, nout, st, caller);
+}
+}  // namespace pmgpu
+
+int pmgpu_penalisation_stage_dev(pmgpu_plan *plan, pmgpu_plan *penal_plan, const void *d_solid,
+                                 const void *d_solid_vel, const pmgpu_penal_stage_args *args, void *d_pos,
+                                 void *d_vort, void *d_vel_rk, void *d_dvort_rk, int npart, int max_part,
+                                 void *d_part_vel, void *d_part_dvort, int *npart_out, double force[3], int *niter,
+                                 double residuals[3], void *stream) {
+  const char *caller = "pmgpu_penalisation_stage";
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!plan || !args || !npart_out || !force || !niter || !residuals || npart < 0 || max_part < npart ||
+      (max_part > 0 && (!d_pos || !d_vort || !d_vel_rk || !d_dvort_rk || !d_part_vel || !d_part_dvort)) ||
+      !(args->dtime != 0.0) || args->itimestage < 1 || args->itimestage > args->time_order) {
+    set_error(caller, "missing or invalid argument.");
+    return -1;
+  }
+  if (penal_plan && (!d_solid || !d_solid_vel || penal_plan->prec != plan->prec || args->max_iter < 1)) {
+    set_error(caller, "missing or invalid penalisation argument.");
+    return -1;
+  }
+  if (ensure_device(caller)) return -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plan->prec == PMGPU_FP64)
+    return penal_stage<double>(plan, penal_plan, (const double *)d_solid, (const double *)d_solid_vel, *args,
+                               (double *)d_pos, (double *)d_vort, (double *)d_vel_rk, (double *)d_dvort_rk, npart,
+                               max_part, (double *)d_part_vel, (double *)d_part_dvort, npart_out, force, niter,
+                               residuals, st);
+  return penal_stage<float>(plan, penal_plan, (const float *)d_solid, (const float *)d_solid_vel, *args,
+                            (float *)d_pos, (float *)d_vort, (float *)d_vel_rk, (float *)d_dvort_rk, npart, max_part,
+                            (float *)d_part_vel, (float *)d_part_dvort, npart_out, force, niter, residuals, st);
 }

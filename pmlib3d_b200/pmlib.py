@@ -480,6 +480,50 @@ def penalisation_solve_dev(plan: Plan, penal_plan: Plan, d_solid: int, d_solid_v
     return list(force), n.value, tuple(res)
 
 
+class PenalStageArgs(C.Structure):
+    """pmgpu_penal_stage_args: the settings of one stage of the penalisation client."""
+
+    _fields_ = [("time_order", C.c_int), ("itimestage", C.c_int), ("dtime", C.c_double), ("fd_order", C.c_int),
+                ("visc", C.c_double), ("reproject", C.c_int), ("regularise_vort", C.c_int),
+                ("first_step", C.c_int), ("remesh", C.c_int), ("remesh_trunc", C.c_double),
+                ("relaxation", C.c_double), ("tolerance", C.c_double), ("max_iter", C.c_int),
+                ("vel_inf", C.c_double * 3)]
+
+
+def penal_stage_args(time_order=2, itimestage=1, dtime=0.01, fd_order=4, visc=0.0, reproject=False,
+                     regularise_vort=False, first_step=False, remesh=False, remesh_trunc=0.0, relaxation=1.0,
+                     tolerance=1e-3, max_iter=20, vel_inf=(1.0, 0.0, 0.0)) -> PenalStageArgs:
+    a = PenalStageArgs()
+    a.time_order, a.itimestage, a.dtime, a.fd_order, a.visc = time_order, itimestage, dtime, fd_order, visc
+    a.reproject, a.regularise_vort, a.first_step, a.remesh = (int(bool(v)) for v in
+                                                              (reproject, regularise_vort, first_step, remesh))
+    a.remesh_trunc, a.relaxation, a.tolerance, a.max_iter = remesh_trunc, relaxation, tolerance, max_iter
+    for d in range(3):
+        a.vel_inf[d] = vel_inf[d]
+    return a
+
+
+def penalisation_stage_dev(plan: Plan, penal_plan, d_solid: int, d_solid_vel: int, args: PenalStageArgs,
+                           d_pos: int, d_vort: int, d_vel_rk: int, d_dvort_rk: int, npart: int, max_part: int,
+                           d_part_vel: int, d_part_dvort: int, stream: int = 0):
+    """One stage of the penalisation client (pmgpu_penalisation_stage_dev) on device
+    arrays of capacity max_part.  Returns (npart, force, passes, residuals); raises on
+    error."""
+    force = (C.c_double * 3)()
+    res = (C.c_double * 3)()
+    n = C.c_int(0)
+    it = C.c_int(0)
+    rc = lib().pmgpu_penalisation_stage_dev(plan.handle, penal_plan.handle if penal_plan is not None else None,
+                                            C.c_void_p(d_solid), C.c_void_p(d_solid_vel), C.byref(args),
+                                            C.c_void_p(d_pos), C.c_void_p(d_vort), C.c_void_p(d_vel_rk),
+                                            C.c_void_p(d_dvort_rk), int(npart), int(max_part),
+                                            C.c_void_p(d_part_vel), C.c_void_p(d_part_dvort), C.byref(n), force,
+                                            C.byref(it), res, C.c_void_p(stream or None))
+    if rc != 0:
+        raise RuntimeError(last_error())
+    return n.value, list(force), it.value, tuple(res)
+
+
 def _prec_of(a) -> int:
     return FP64 if a.dtype == np.float64 else FP32
 
