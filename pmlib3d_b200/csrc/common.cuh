@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cstdio>
 #include <string>
 
@@ -60,7 +61,7 @@ template <> __device__ __forceinline__ float2 cfma_r<float2, float>(float2 s, fl
 #endif
 
 // kernel launch accounting (read by pmgpu_launch_count)
-extern long long g_launches;
+extern std::atomic<long long> g_launches;
 
 // error state shared with the C ABI
 void set_error(const char *caller, const char *msg);

@@ -35,6 +35,10 @@ struct KTimer {
 #define CKL(caller) CK(cudaGetLastError(), caller)
 
 int num_sms();
+// Raises a kernel's maximum dynamic shared memory to `bytes` if it is below: the
+// attribute only grows, and it is set at most once per size increase and device, so
+// launches of the same kernel on other streams are not held up by setting it again.
+int smem_attr(const void *func, size_t bytes, const char *caller);
 
 // shared-memory budget of one persistent pass CTA
 constexpr size_t PASS_SMEM_BUDGET = 220 * 1024;

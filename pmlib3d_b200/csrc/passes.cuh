@@ -69,7 +69,7 @@ static int launch_lines(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typ
       lt.dLG = make_fastdiv((unsigned)(NC * TK / RVec<R>::G));
       const size_t sm = reg_smem(n, mt, NC, TK, sizeof(C));
       auto launch = [&](auto kern) -> int {
-        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+        if (smem_attr((const void *)kern, sm, caller)) return -1;
         int per = 1;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, RL_THREADS, sm) != cudaSuccess || per < 1)
           per = 1;
@@ -103,7 +103,7 @@ static int launch_lines(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typ
   lt.nkt = g.Hp / TK;
   lt.TK = TK;
   const size_t sm = lines_smem(n, NC, TK, sizeof(C), ntw);
-  CK(cudaFuncSetAttribute(k_lines<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+  if (smem_attr((const void *)k_lines<R, NC>, sm, caller)) return -1;
   const int grid = persistent_grid(k_lines<R, NC>, sm, lt.nouter * lt.nkt);
   k_lines<R, NC><<<grid, PASS_THREADS, sm, st>>>(g, lt, in, out, axis, lmode, zmode, reproj, use_zeta);
   PM_LAUNCHED();
@@ -121,7 +121,7 @@ int fwd_xy(SolveGeom<R> &g, const R *in, typename cplx_t<R>::type *X, typename c
     const int RB = pick_rb_reg(g.N2, g.rx.n, g.H, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), false, reg_budget(sizeof(R)));
     if (RB > 0) {
       const size_t sm = rx_smem(g.N2, g.rx.n, g.H, g.P[0], g.Hp, NC, RB, sizeof(C), sizeof(R), false);
-      CK(cudaFuncSetAttribute(k_rxfwd<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+      if (smem_attr((const void *)k_rxfwd<R, NC>, sm, caller)) return -1;
       const int rows = g.P[1] * g.P[2];
       const int ntiles = (rows + RB - 1) / RB;
       int per = 1;
@@ -149,7 +149,7 @@ int fwd_xy(SolveGeom<R> &g, const R *in, typename cplx_t<R>::type *X, typename c
   const size_t sm = tw_bytes(ntwx, sizeof(C)) + stage + 2 * (size_t)NC * RB * g.N2 * sizeof(C);
   const bool vec16 = cs == NC && ((size_t)g.ext[0] * NC * sizeof(R)) % 16 == 0 &&
                      ((size_t)g.off[0] * NC * sizeof(R)) % 16 == 0 && ((size_t)g.P[0] * NC * sizeof(R)) % 16 == 0;
-  CK(cudaFuncSetAttribute(k_xfwd<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+  if (smem_attr((const void *)k_xfwd<R, NC>, sm, caller)) return -1;
   const int rows = g.P[1] * g.P[2];
   const int ntiles = (rows + RB - 1) / RB;
   { KTimer kt_(KC_XFWD, st);
@@ -200,7 +200,7 @@ int inv_yx(SolveGeom<R> &g, const pmgpu_topo *topo, typename cplx_t<R>::type *Y,
   const int RBr = g.rx_ok ? pick_rb_reg(g.N2, g.rx.n, g.H, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), true, reg_budget(sizeof(R))) : 0;
   if (RBr > 0) {
     const size_t sm = rx_smem(g.N2, g.rx.n, g.H, g.P[0], g.Hp, NC, RBr, sizeof(C), sizeof(R), true);
-    CK(cudaFuncSetAttribute(k_rxinv<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+    if (smem_attr((const void *)k_rxinv<R, NC>, sm, caller)) return -1;
     const int ntiles = (rows + RBr - 1) / RBr;
     int per = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rxinv<R, NC>, RL_THREADS, sm) != cudaSuccess || per < 1)
@@ -219,7 +219,7 @@ int inv_yx(SolveGeom<R> &g, const pmgpu_topo *topo, typename cplx_t<R>::type *Y,
     }
     const size_t sm =
         tw_bytes(ntwx, sizeof(C)) + (size_t)RB * g.Hp * NC * sizeof(C) + 2 * (size_t)NC * RB * g.N2 * sizeof(C);
-    CK(cudaFuncSetAttribute(k_xinv<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+    if (smem_attr((const void *)k_xinv<R, NC>, sm, caller)) return -1;
     const int ntiles = (rows + RB - 1) / RB;
     { KTimer kt_(KC_XINV, st);
       k_xinv<R, NC><<<persistent_grid(k_xinv<R, NC>, sm, ntiles), PASS_THREADS, sm, st>>>(g, X, out, RB, cs); }
@@ -406,7 +406,7 @@ int batch_launch(const BatchLayout &lay, const void *d_desc, unsigned *counters,
   };
   auto launch = [&](auto kern, int f, auto... args) -> int {
     const size_t sm = lay.pass[f].smem;
-    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+    if (smem_attr((const void *)kern, sm, caller)) return -1;
     int per = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, RL_THREADS, sm) != cudaSuccess || per < 1) per = 1;
     const int grid = std::max(1, std::min(lay.pass[f].nitems, per * num_sms()));

@@ -18,6 +18,7 @@
 #include <complex>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <memory>
 #include <tuple>
@@ -27,7 +28,7 @@
 
 namespace pmgpu {
 
-long long g_launches = 0;
+std::atomic<long long> g_launches{0};
 
 // ------------------------------------------------------------------ per-kernel timing
 // When enabled, every launch of the library is bracketed by CUDA events on its
@@ -36,6 +37,7 @@ static const char *kc_names[KC_N] = {"bin", "scan", "place", "fixup", "deposit",
                                      "x_fwd", "y_fwd", "z_pass", "y_inv", "x_inv", "ghost_fill", "m2p",
                                      "deriv_vorticity", "advance", "map", "other"};
 static bool g_timing = false;
+static std::mutex g_time_mu;  // the pending events (launches of several threads)
 struct PendingEv {
   int cls;
   cudaEvent_t a, b;
@@ -54,10 +56,12 @@ KTimer::KTimer(int c, cudaStream_t s) : cls(c), st(s) {
 KTimer::~KTimer() {
   if (g_timing && a) {
     cudaEventRecord(b, st);
+    std::lock_guard<std::mutex> lk(g_time_mu);
     g_pending.push_back({cls, a, b});
   }
 }
 static void timing_collect() {
+  std::lock_guard<std::mutex> lk(g_time_mu);
   for (auto &p : g_pending) {
     float ms = 0.f;
     cudaEventSynchronize(p.b);
@@ -70,8 +74,17 @@ static void timing_collect() {
   g_pending.clear();
 }
 
-static char g_err[512] = "";
+// The last error of the calling thread (plan set-up may run on another thread than
+// the solves, see g_setup_mu).
+static thread_local char g_err[512] = "";
+// Entry points serialise on g_mu, except plan creation (pmgpu_poisson_setup*,
+// pmgpu_batch_create) and the schedule table (pmgpu_fft_tune / _tuned /
+// _set_schedule), which serialise on g_setup_mu: a plan can be set up while another
+// thread queues solves of other plans.  The state both sides share is guarded on
+// its own (device set-up, timing events, the launch counter, allocation injection).
 static std::mutex g_mu;
+static std::mutex g_setup_mu;
+static std::mutex g_dev_mu;
 
 // source/pmlib_write.f:40-48 format for rank 0
 void set_error(const char *caller, const char *msg) {
@@ -96,6 +109,7 @@ static int noalloc_reserve(int dev, const char *caller);
 static int ensure_device(const char *caller) {
   int dev = 0;
   CK(cudaGetDevice(&dev), caller);
+  std::lock_guard<std::mutex> lk(g_dev_mu);
   if (dev >= 0 && dev < 128 && g_dev_ready[dev]) return 0;
   if (noalloc_reserve(dev, caller)) return -1;
   static float t32[CS_R][CS_M][2];
@@ -135,7 +149,7 @@ static int ensure_device(const char *caller) {
 // the legacy stream; its owner frees it only when no work using it is in flight.
 // Injected allocation failure (pmgpu_inject_alloc_failure): the allocation that
 // brings the countdown to zero reports cudaErrorMemoryAllocation; -1 = off.
-static long long g_fail_alloc = -1;
+static std::atomic<long long> g_fail_alloc{-1};
 
 struct DevBuf {
   void *p = nullptr;
@@ -155,7 +169,7 @@ struct DevBuf {
     p = nullptr;
     cap = 0;
     size_t b = std::max<size_t>(bytes, 256);
-    if (g_fail_alloc >= 0 && g_fail_alloc-- == 0) CK(cudaErrorMemoryAllocation, caller);
+    if (g_fail_alloc.load() >= 0 && g_fail_alloc.fetch_sub(1) == 0) CK(cudaErrorMemoryAllocation, caller);
     if (stream_ordered) {
       CK(cudaMallocAsync(&p, b, 0), caller);
       CK(cudaStreamSynchronize(0), caller);  // usable from every stream from here on
@@ -452,6 +466,19 @@ static void bluestein_tables(const RegPlan &pl, std::vector<C> &chirp, std::vect
   for (int q = 0; q < m; q++) bpos[q] = mk((R)b[kp[q]].real(), (R)b[kp[q]].imag());
 }
 
+static std::mutex g_attr_mu;
+static std::map<std::pair<int, const void *>, size_t> g_smem_attr;
+int smem_attr(const void *func, size_t bytes, const char *caller) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev), caller);
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  size_t &cur = g_smem_attr[std::make_pair(dev, func)];
+  if (bytes <= cur) return 0;
+  CK(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes), caller);
+  cur = bytes;
+  return 0;
+}
+
 static int g_nsm = 0;
 int num_sms() {
   if (g_nsm == 0) {
@@ -516,6 +543,9 @@ struct pmgpu_plan {
   int tky = 0, tkz = 0;  // tuned kx tiles (0: chosen by shared memory)
   DevBuf rtwx, rtwy, rtwz, yk, zk, rextx, xpos;
   DevBuf rchx, rchy, rchz, rbx, rby, rbz;  // Bluestein chirps and spectra
+  // the register-engine tables above are views of device tables shared by the plans
+  // of the same transform length, precision and schedule; these keep them alive
+  std::vector<std::shared_ptr<DevBuf>> tab_keep;
   DevBuf mesh_w, mesh_u, mesh_a, mesh_b;
   DevBuf h_pos, h_val, h_out;  // device mirrors used by host-pointer calls
   // particle scratch
@@ -666,8 +696,7 @@ static int run_p2m(const pmgpu_topo *t, int order, const R *pos, const R *val, i
     const int *pp = perm;
 #define DEP_CASE(WW, NVV)                                                                                  \
   if (W == WW && nv == NVV) {                                                                              \
-    CK(cudaFuncSetAttribute(k_deposit<R, WW, NVV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), \
-       caller);                                                                                            \
+    if (smem_attr((const void *)k_deposit<R, WW, NVV>, smem, caller)) return -1;                           \
     KTimer kt_(KC_DEPOSIT, st);                                                                            \
     k_deposit<R, WW, NVV><<<grid, DEP_THREADS, smem, st>>>(g, pos, vp, nvar, s.start->as<unsigned>(),      \
                                                                 pp, mp, nvar_mesh, zc, cap, clear_mode);    \
@@ -715,7 +744,7 @@ static int run_m2p_sorted_w(const pmgpu_topo *t, const R *pos, const unsigned *s
                             const R *f, R *o, cudaStream_t st, const char *caller) {
   PartGeom<R> g = part_geom<R>(t, W);
   const size_t sm = m2p_tile_smem<R, W>();
-  CK(cudaFuncSetAttribute(k_m2p_tile<R, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), caller);
+  if (smem_attr((const void *)k_m2p_tile<R, W>, sm, caller)) return -1;
   // tile edges on the bin of interior cell 1 (bin 1 - blo) along each axis
   auto org = [&](int e, int T) {
     const int r = (1 - g.blo[e]) % T;
@@ -1153,55 +1182,110 @@ template <typename R> static int tune_axis(pmgpu_plan *pl, int axis, TunedSchedu
   return best.np > 0 ? 0 : -1;
 }
 
+// Device tables of the register engine, shared by every plan of the same transform
+// length, precision and radix schedule (held by weak references, as the Green's
+// spectra): a plan's set-up computes and uploads only the tables of lengths no live
+// plan has.  Guarded by the set-up lock.
+static std::map<std::string, std::weak_ptr<DevBuf>> g_tab_cache;
+// the most recently used tables stay alive past their last plan (they are small), so
+// that the FP64 transforms of the Green's set-up and plans of recurring lengths reuse
+// them
+// (never destroyed: freeing device memory from static destructors at exit could
+// run after the runtime has unloaded)
+static std::deque<std::shared_ptr<DevBuf>> &g_tab_recent = *new std::deque<std::shared_ptr<DevBuf>>();
+constexpr size_t TAB_RECENT = 512;
+
+static std::string regplan_key(const char *kind, int prec_bytes, int n, int extra, const RegPlan &rp) {
+  char b[160];
+  snprintf(b, sizeof(b), "%s|%d|%d|%d|%d:%d,%d,%d|%d,%d", kind, prec_bytes, n, extra, rp.np, rp.rad[0],
+           rp.np > 1 ? rp.rad[1] : 0, rp.np > 2 ? rp.rad[2] : 0, rp.bl, rp.bn);
+  return std::string(b);
+}
+
+// attaches `view` to the cached device table `key`, made by fill(host vector) and
+// uploaded on a miss
+template <typename T, typename Fill>
+static int shared_table(pmgpu_plan *pl, const std::string &key, DevBuf &view, Fill fill, const char *caller) {
+  std::shared_ptr<DevBuf> sp;
+  auto it = g_tab_cache.find(key);
+  if (it != g_tab_cache.end()) sp = it->second.lock();
+  if (!sp) {
+    std::vector<T> host;
+    fill(host);
+    sp = std::shared_ptr<DevBuf>(new DevBuf(), [](DevBuf *b) {
+      b->release();
+      delete b;
+    });
+    if (sp->ensure(sizeof(T) * std::max<size_t>(host.size(), 1), caller)) return -1;
+    if (!host.empty()) CK(cudaMemcpy(sp->p, host.data(), sizeof(T) * host.size(), cudaMemcpyHostToDevice), caller);
+    g_tab_cache[key] = sp;
+    g_tab_recent.push_back(sp);
+    if (g_tab_recent.size() > TAB_RECENT) g_tab_recent.pop_front();
+  }
+  view.release();
+  view.p = sp->p;
+  view.cap = sp->cap;
+  view.fixed = true;
+  pl->tab_keep.push_back(sp);
+  return 0;
+}
+
 template <typename R> static int reg_tables(pmgpu_plan *pl, const char *caller, bool tune_ok) {
   typedef typename cplx_t<R>::type C;
   pl->rx_ok = pl->ry_ok = pl->rz_ok = 0;
   if (g_force_stockham) return 0;
   const long double twopi = 2.0L * acosl(-1.0L);
+  const int pb = (int)sizeof(R);
   // twiddles w_m^q of a plan's transform length m
-  auto twiddles = [&](int mm) {
-    std::vector<C> tw(mm);
+  auto twiddles = [&](int mm, std::vector<C> &tw) {
+    tw.resize(mm);
     for (int q = 0; q < mm; q++) {
       const long double a = twopi * (long double)q / (long double)mm;
       tw[q] = mk((R)cosl(a), (R)-sinl(a));
     }
-    return tw;
   };
   // Bluestein chirp and spectrum of a plan (nothing for a direct plan)
-  auto upload_blue = [&](const RegPlan &rp, DevBuf &ch, DevBuf &bp) -> int {
+  auto upload_blue = [&](const std::string &key, const RegPlan &rp, DevBuf &ch, DevBuf &bp) -> int {
     if (!rp.bl) return 0;
     std::vector<C> c, b;
-    bluestein_tables<C, R>(rp, c, b);
-    if (ch.ensure(sizeof(C) * c.size(), caller) || bp.ensure(sizeof(C) * b.size(), caller)) return -1;
-    CK(cudaMemcpy(ch.p, c.data(), sizeof(C) * c.size(), cudaMemcpyHostToDevice), caller);
-    CK(cudaMemcpy(bp.p, b.data(), sizeof(C) * b.size(), cudaMemcpyHostToDevice), caller);
-    return 0;
+    bool made = false;
+    auto make = [&]() {
+      if (!made) bluestein_tables<C, R>(rp, c, b);
+      made = true;
+    };
+    if (shared_table<C>(pl, key + "|ch", ch, [&](std::vector<C> &h) { make(); h = c; }, caller)) return -1;
+    return shared_table<C>(pl, key + "|bp", bp, [&](std::vector<C> &h) { make(); h = b; }, caller);
   };
+  pl->tab_keep.clear();
   {
     // x passes: half-length complex transform N = Mx / 2
     RegPlan rp;
     const int N = pl->g.N2, H = pl->g.H, Mx = pl->g.M[0];
     if (make_regplan(N, rp) || make_bluestein(N, rp)) {
-      const std::vector<C> tw = twiddles(rp.n);
-      std::vector<C> ext(H);
-      for (int k = 0; k < H; k++) {
-        const long double a = twopi * (long double)k / (long double)Mx;
-        ext[k] = mk((R)cosl(a), (R)-sinl(a));
-      }
-      std::vector<int> xp(N);
-      if (rp.bl) {
-        for (int q = 0; q < N; q++) xp[q] = q;  // natural order
-      } else {
-        const std::vector<int> kp = regplan_positions(rp);
-        for (int q = 0; q < N; q++) xp[kp[q]] = q;
-      }
-      if (pl->rtwx.ensure(sizeof(C) * tw.size(), caller) || pl->rextx.ensure(sizeof(C) * H, caller) ||
-          pl->xpos.ensure(sizeof(int) * N, caller))
+      const std::string key = regplan_key("x", pb, N, Mx, rp);
+      if (shared_table<C>(pl, key + "|tw", pl->rtwx, [&](std::vector<C> &h) { twiddles(rp.n, h); }, caller) ||
+          shared_table<C>(pl, key + "|ext", pl->rextx,
+                          [&](std::vector<C> &h) {
+                            h.resize(H);
+                            for (int k = 0; k < H; k++) {
+                              const long double a = twopi * (long double)k / (long double)Mx;
+                              h[k] = mk((R)cosl(a), (R)-sinl(a));
+                            }
+                          },
+                          caller) ||
+          shared_table<int>(pl, key + "|pos", pl->xpos,
+                            [&](std::vector<int> &h) {
+                              h.resize(N);
+                              if (rp.bl) {
+                                for (int q = 0; q < N; q++) h[q] = q;  // natural order
+                              } else {
+                                const std::vector<int> kp = regplan_positions(rp);
+                                for (int q = 0; q < N; q++) h[kp[q]] = q;
+                              }
+                            },
+                            caller) ||
+          upload_blue(key, rp, pl->rchx, pl->rbx))
         return -1;
-      CK(cudaMemcpy(pl->rtwx.p, tw.data(), sizeof(C) * tw.size(), cudaMemcpyHostToDevice), caller);
-      CK(cudaMemcpy(pl->rextx.p, ext.data(), sizeof(C) * H, cudaMemcpyHostToDevice), caller);
-      CK(cudaMemcpy(pl->xpos.p, xp.data(), sizeof(int) * N, cudaMemcpyHostToDevice), caller);
-      if (upload_blue(rp, pl->rchx, pl->rbx)) return -1;
       pl->rx = rp;
       pl->rx_ok = 1;
     }
@@ -1218,19 +1302,22 @@ template <typename R> static int reg_tables(pmgpu_plan *pl, const char *caller, 
         (axis == 1 ? pl->tky : pl->tkz) = it->second.tk;
       }
     }
-    const std::vector<C> tw = twiddles(rp.n);
-    std::vector<int> kp(n);
-    if (rp.bl) {
-      for (int q = 0; q < n; q++) kp[q] = q;  // natural order
-    } else {
-      kp = regplan_positions(rp);
-    }
+    const std::string key = regplan_key("l", pb, n, 0, rp);
     DevBuf &tb = axis == 1 ? pl->rtwy : pl->rtwz;
     DevBuf &kb = axis == 1 ? pl->yk : pl->zk;
-    if (tb.ensure(sizeof(C) * tw.size(), caller) || kb.ensure(sizeof(int) * n, caller)) return -1;
-    CK(cudaMemcpy(tb.p, tw.data(), sizeof(C) * tw.size(), cudaMemcpyHostToDevice), caller);
-    CK(cudaMemcpy(kb.p, kp.data(), sizeof(int) * n, cudaMemcpyHostToDevice), caller);
-    if (upload_blue(rp, axis == 1 ? pl->rchy : pl->rchz, axis == 1 ? pl->rby : pl->rbz)) return -1;
+    if (shared_table<C>(pl, key + "|tw", tb, [&](std::vector<C> &h) { twiddles(rp.n, h); }, caller) ||
+        shared_table<int>(pl, key + "|pos", kb,
+                          [&](std::vector<int> &h) {
+                            if (rp.bl) {
+                              h.resize(n);
+                              for (int q = 0; q < n; q++) h[q] = q;  // natural order
+                            } else {
+                              h = regplan_positions(rp);
+                            }
+                          },
+                          caller) ||
+        upload_blue(key, rp, axis == 1 ? pl->rchy : pl->rchz, axis == 1 ? pl->rby : pl->rbz))
+      return -1;
     if (axis == 1) {
       pl->ry = rp;
       pl->ry_ok = 1;
@@ -1262,6 +1349,7 @@ template <typename R> static int apply_tuning(pmgpu_plan *pl, const char *caller
 }
 
 template <typename R> static int plan_tables(pmgpu_plan *pl, const char *caller) {
+  typedef typename cplx_t<R>::type C;
   std::vector<cld> tw;
   if (!make_fft(pl->g.N2, pl->g.M[0], pl->fx, tw) || upload_tw<R>(tw, pl->twx, caller)) return -1;
   if (!make_fft(pl->g.M[1], 0, pl->fy, tw) || upload_tw<R>(tw, pl->twy, caller)) return -1;
@@ -1269,6 +1357,11 @@ template <typename R> static int plan_tables(pmgpu_plan *pl, const char *caller)
   if (upload_wavenumbers<R>(pl, caller)) return -1;
   if (reg_tables<R>(pl, caller, true)) return -1;
   if (setup_green<R>(pl, caller)) return -1;
+  // the work spectra of a three-component solve, so that a plan's first solve (often
+  // queued from another thread than the set-up) allocates nothing
+  const Geometry &G = pl->g;
+  const size_t nX = (size_t)G.P[1] * G.P[2] * G.Hp * 3, nY = (size_t)G.M[1] * G.P[2] * G.Hp * 3;
+  if (pl->X.ensure(sizeof(C) * nX, caller) || pl->Y.ensure(sizeof(C) * nY, caller)) return -1;
   return apply_tuning<R>(pl, caller);
 }
 
@@ -1314,16 +1407,14 @@ static int check_interp(const pmgpu_params *par, const char *caller) {
 const char *pmgpu_last_error(void) { return pmgpu::g_err; }
 
 long long pmgpu_launch_count(int reset) {
-  long long v = pmgpu::g_launches;
-  if (reset) pmgpu::g_launches = 0;
+  const long long v = reset ? pmgpu::g_launches.exchange(0) : pmgpu::g_launches.load();
   return v;
 }
 
 int pmgpu_parameters_check(const pmgpu_params *par) { return check_params(par); }
 
 int pmgpu_inject_alloc_failure(long long after) {
-  std::lock_guard<std::mutex> lk(g_mu);
-  g_fail_alloc = after < 0 ? -1 : after;
+  g_fail_alloc.store(after < 0 ? -1 : after);
   return 0;
 }
 
@@ -1536,7 +1627,7 @@ int pmgpu_interp_mesh_particle_f32(const pmgpu_topo *topo, const pmgpu_params *p
 
 // ------------------------------------------------------------------ Poisson
 // plan creation; the caller holds g_mu
-static int g_pff_kx0 = 0;  // k_x = 0 treatment handed from pmgpu_poisson_setup_pff to create_plan (under g_mu)
+static int g_pff_kx0 = 0;  // k_x = 0 treatment handed from pmgpu_poisson_setup_pff to create_plan (under g_setup_mu)
 static int create_plan(const pmgpu_patch *patch, const pmgpu_topo *cuboid, const pmgpu_params *par, int precision,
                        pmgpu_plan **plan, const char *caller, int green_mode = 0) {
   if (!plan || !patch || !cuboid) {
@@ -1603,14 +1694,14 @@ static int create_plan(const pmgpu_patch *patch, const pmgpu_topo *cuboid, const
 
 int pmgpu_poisson_setup(const pmgpu_patch *patch, const pmgpu_topo *cuboid, const pmgpu_params *par,
                         int precision, pmgpu_plan **plan) {
-  std::lock_guard<std::mutex> lk(g_mu);
+  std::lock_guard<std::mutex> lk(g_setup_mu);
   return create_plan(patch, cuboid, par, precision, plan, "pmlib_poisson_setup");
 }
 
 int pmgpu_poisson_setup_ppf(const pmgpu_patch *patch, const pmgpu_topo *cuboid, const pmgpu_params *par,
                             int precision, pmgpu_plan **plan) {
   const char *caller = "pmlib_poisson_setup";
-  std::lock_guard<std::mutex> lk(g_mu);
+  std::lock_guard<std::mutex> lk(g_setup_mu);
   if (!patch || !par || !plan) {
     set_error(caller, "missing argument.");
     return -1;
@@ -1633,7 +1724,7 @@ int pmgpu_poisson_setup_ppf(const pmgpu_patch *patch, const pmgpu_topo *cuboid, 
 int pmgpu_poisson_setup_pff(const pmgpu_patch *patch, const pmgpu_topo *cuboid, const pmgpu_params *par,
                             int precision, int kx0, pmgpu_plan **plan) {
   const char *caller = "pmlib_poisson_setup";
-  std::lock_guard<std::mutex> lk(g_mu);
+  std::lock_guard<std::mutex> lk(g_setup_mu);
   if (!patch || !par || !plan) {
     set_error(caller, "missing argument.");
     return -1;
@@ -2077,7 +2168,7 @@ int pmgpu_interp_particle_mesh_noalloc(const pmgpu_topo *topo, const pmgpu_param
 }
 
 int pmgpu_fft_engine(int engine) {
-  std::lock_guard<std::mutex> lk(g_mu);
+  std::lock_guard<std::mutex> lk(g_setup_mu);
   const int old = g_force_stockham;
   g_force_stockham = engine == 1 ? 1 : 0;
   return old;
@@ -2180,6 +2271,7 @@ int pmgpu_batch_create(int npatch, const pmgpu_patch *patches, const pmgpu_topo 
                        const pmgpu_params *par, int precision, pmgpu_batch **batch) {
   const char *caller = "pmgpu_batch_create";
   std::lock_guard<std::mutex> lk(g_mu);
+  std::lock_guard<std::mutex> lk2(g_setup_mu);  // it creates plans
   if (!batch || npatch <= 0 || !patches || !cuboids) {
     set_error(caller, "missing argument.");
     return -1;
@@ -2304,14 +2396,14 @@ void pmgpu_batch_destroy(pmgpu_batch *b) {
 }
 
 int pmgpu_fft_tune(int on) {
-  std::lock_guard<std::mutex> lk(g_mu);
+  std::lock_guard<std::mutex> lk(g_setup_mu);
   const int old = g_tune;
   g_tune = on ? 1 : 0;
   return old;
 }
 
 int pmgpu_fft_tuned(int index, int *length, int *precision, int *axis, int *radices, int *tile, double *ms) {
-  std::lock_guard<std::mutex> lk(g_mu);
+  std::lock_guard<std::mutex> lk(g_setup_mu);
   if (index < 0 || index >= (int)g_tuned.size()) return -1;
   auto it = g_tuned.begin();
   std::advance(it, index);
@@ -2327,7 +2419,7 @@ int pmgpu_fft_tuned(int index, int *length, int *precision, int *axis, int *radi
 
 int pmgpu_fft_set_schedule(int length, int precision, int axis, const int *radices, int tile) {
   const char *caller = "pmgpu_fft_set_schedule";
-  std::lock_guard<std::mutex> lk(g_mu);
+  std::lock_guard<std::mutex> lk(g_setup_mu);
   if ((precision != PMGPU_FP32 && precision != PMGPU_FP64) || (axis != 1 && axis != 2) || length < 2) {
     set_error(caller, "length, precision or axis out of range.");
     return -1;

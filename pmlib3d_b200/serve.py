@@ -10,10 +10,13 @@ room.  Every request records arrival, start and completion times; the report giv
 solves/s and p50 / p99 latency (arrival to completion).
 
 The results do not depend on the mix: a request is solved by a plan of its own grid
-with the same kernels and tiles as when it is alone.
+with the same kernels and tiles as when it is alone.  The report splits each
+request's latency into queueing (arrival to set-up), plan set-up, waiting for a
+slot and service, and gives the most solves that ran on the device at one time.
 """
 from __future__ import annotations
 
+import threading
 import time
 from collections import OrderedDict, deque
 from dataclasses import dataclass
@@ -33,11 +36,18 @@ class Request:
     bound_cond: tuple
     vort: object = None       # device tensor (nz', ny', nx', 3) of the plan's precision
     vel: object = None        # filled by the server
-    start: float = None
-    done: float = None
+    setup_start: float = None  # the set-up thread took the request
+    setup_end: float = None    # its plan was ready (reused or new)
+    new_plan: bool = False
+    start: float = None        # its solve was queued on a slot
+    done: float = None         # the server saw the solve finished
+    dev_start_ms: float = None  # device clock (CUDA events) of the solve, from the run's start
+    dev_end_ms: float = None
     topo: object = None
     key: tuple = None
     nbytes: int = 0
+    plan: object = None
+    need: int = 0
 
 
 def grid_key(r: Request):
@@ -78,15 +88,26 @@ def field_bytes(topo, precision: int) -> int:
 class _Slot:
     stream: object
     req: Request = None
-    plan: object = None
-    event: object = None
+    ev0: object = None
+    ev1: object = None
 
 
 class Server:
     """Admission-controlled request loop over `slots` CUDA streams within `budget`
-    bytes of device memory (plans + request buffers)."""
+    bytes of device memory (plans + request buffers).
 
-    def __init__(self, params, precision: int = P.FP32, slots: int = 8, budget: int = 16 << 30, nghost: int = 4):
+    Two host threads: a set-up thread takes the arrived requests in arrival order and
+    gets each a plan (an idle plan of its grid, or a new one once the budget has room,
+    evicting idle plans of other grids first), at most `ahead` requests ahead of the
+    solves; the serving thread queues the solves of prepared requests on free slots
+    (arrival order), retires finished ones and returns their plans and memory.  The
+    library serialises plan set-up on its own lock, so a new grid's set-up runs while
+    solves of other requests are queued and run.  Neither thread spins: each waits on
+    a condition variable (the serving thread with a 0.2 ms limit, to look at the
+    slots' events)."""
+
+    def __init__(self, params, precision: int = P.FP32, slots: int = 8, budget: int = 16 << 30, nghost: int = 4,
+                 ahead: int = None):
         import torch
         self.torch = torch
         self.params = params
@@ -94,14 +115,21 @@ class Server:
         self.nghost = nghost
         self.budget = int(budget)
         self.slots = [_Slot(torch.cuda.Stream()) for _ in range(slots)]
+        self.ahead = ahead if ahead is not None else 2 * slots
         self.idle = OrderedDict()   # key -> list of idle plans (LRU order of keys)
-        self.held = 0               # bytes of all live plans
+        self.held = 0               # bytes of all live plans and of the admitted requests' buffers
         self.plan_size = {}         # id(plan) -> bytes
-        self.inflight_io = 0
-        self.queue = deque()
+        self.cv = threading.Condition()
+        self.pending = deque()      # submitted, not yet taken by the set-up thread
+        self.prepared = deque()     # plans ready, waiting for a slot
         self.finished = []
+        self.inflight = 0
+        self.max_inflight = 0
+        self.max_held = 0
+        self.error = None
+        self.stop = False
 
-    # -------------------------------------------------------------- plans
+    # -------------------------------------------------------------- plans (set-up thread)
     def _topo(self, r: Request):
         pa = P.make_patch(r.xmin, r.xmax, r.dx, bound_cond=r.bound_cond, nghost=self.nghost)
         ierr, t = P.pmlib_topology_cuboid(pa, self.params.interpolation_order)
@@ -121,96 +149,180 @@ class Server:
                 return True
         return False
 
-    def _acquire_plan(self, r: Request):
-        """An idle plan of the request's grid, or a new one if the budget allows
-        (evicting idle plans of other grids first); None if it must wait."""
+    def _prepare(self, r: Request, clock, t0) -> None:
+        """Gets r a plan and reserves its memory; waits (without spinning) for memory
+        held by running requests.  Called with self.cv held; releases it while a new
+        plan is set up."""
         plans = self.idle.get(r.key)
         if plans:
             self.idle.move_to_end(r.key)
-            return plans.pop()
+            r.plan = plans.pop()
+            self.held += r.nbytes
+            self.max_held = max(self.max_held, self.held)
+            return
         need = plan_bytes(r.topo, self.precision, self.params.poisson_kernel)
-        while self.held + self.inflight_io + r.nbytes + need > self.budget:
-            if not self._evict_one():
-                return None
-        pa, t = self._topo(r)
-        ierr, plan = P.pmlib_poisson_setup(pa, t, self.params, self.precision)
+        while self.held + r.nbytes + need > self.budget:
+            if self._evict_one():
+                continue
+            if self.inflight == 0 and not self.prepared:
+                raise RuntimeError(f"request {r.rid} needs more device memory than the budget "
+                                   f"({self.budget / 1e9:.2f} GB)")
+            self.cv.wait()
+            if self.stop:
+                return
+        self.held += need + r.nbytes
+        self.max_held = max(self.max_held, self.held)
+        r.need = need
+        r.new_plan = True
+        self.cv.release()
+        try:
+            pa, t = self._topo(r)
+            ierr, plan = P.pmlib_poisson_setup(pa, t, self.params, self.precision)
+        finally:
+            self.cv.acquire()
         if ierr != 0:
             raise RuntimeError(P.last_error())
         self.plan_size[id(plan)] = need
-        self.held += need
-        return plan
+        r.plan = plan
 
-    def _release_plan(self, key, plan):
-        self.idle.setdefault(key, []).append(plan)
-        self.idle.move_to_end(key)
+    def _setup_loop(self, clock, t0):
+        try:
+            with self.cv:
+                while not self.stop:
+                    if not self.pending or len(self.prepared) >= self.ahead:
+                        if not self.pending and self.submitted_all:
+                            return
+                        self.cv.wait()
+                        continue
+                    r = self.pending[0]
+                    now = clock() - t0
+                    if r.arrival > now:
+                        self.cv.wait(timeout=r.arrival - now)
+                        continue
+                    self.pending.popleft()
+                    r.setup_start = clock() - t0
+                    self._prepare(r, clock, t0)
+                    if self.stop:
+                        return
+                    r.setup_end = clock() - t0
+                    self.prepared.append(r)
+                    self.cv.notify_all()
+        except BaseException as e:  # handed to the serving thread
+            with self.cv:
+                self.error = e
+                self.cv.notify_all()
 
-    # -------------------------------------------------------------- loop
+    # -------------------------------------------------------------- solves (serving thread)
     def submit(self, r: Request):
         pa, t = self._topo(r)
         r.topo = t
         r.key = grid_key(r)
         r.nbytes = field_bytes(t, self.precision)
-        self.queue.append(r)
+        self.pending.append(r)
 
-    def _start(self, slot: _Slot, r: Request, plan, now: float):
+    def _start(self, slot: _Slot, r: Request, now: float, ref):
         torch = self.torch
         with torch.cuda.stream(slot.stream):
             r.vel = torch.empty_like(r.vort)
-            rc = P.pmlib_poisson_solve_dev(plan, r.vort.data_ptr(), r.vel.data_ptr(), stream=slot.stream.cuda_stream)
+            slot.ev0 = torch.cuda.Event(enable_timing=True)
+            slot.ev1 = torch.cuda.Event(enable_timing=True)
+            slot.ev0.record(slot.stream)
+            rc = P.pmlib_poisson_solve_dev(r.plan, r.vort.data_ptr(), r.vel.data_ptr(),
+                                           stream=slot.stream.cuda_stream)
             if rc != 0:
                 raise RuntimeError(P.last_error())
-            ev = torch.cuda.Event()
-            ev.record(slot.stream)
-        slot.req, slot.plan, slot.event = r, plan, ev
+            slot.ev1.record(slot.stream)
+        slot.req = r
         r.start = now
-        self.inflight_io += r.nbytes
+        self.inflight += 1
+        self.max_inflight = max(self.max_inflight, self.inflight)
 
-    def poll(self, now: float):
-        """Retire finished solves, then admit waiting requests in arrival order."""
+    def _retire(self, now: float, ref) -> bool:
+        """Finished solves return their plan and memory; True if any did."""
+        any_done = False
         for slot in self.slots:
-            if slot.req is not None and slot.event.query():
+            if slot.req is not None and slot.ev1.query():
                 r = slot.req
                 r.done = now
-                self.inflight_io -= r.nbytes
-                self._release_plan(r.key, slot.plan)
+                r.dev_start_ms = ref.elapsed_time(slot.ev0)
+                r.dev_end_ms = ref.elapsed_time(slot.ev1)
+                self.held -= r.nbytes
+                self.idle.setdefault(r.key, []).append(r.plan)
+                self.idle.move_to_end(r.key)
+                r.plan = None
                 self.finished.append(r)
-                slot.req = slot.plan = slot.event = None
-        for slot in self.slots:
-            if slot.req is not None or not self.queue:
-                continue
-            r = self.queue[0]
-            if r.arrival > now:
-                break
-            plan = self._acquire_plan(r)
-            if plan is None:
-                if not any(s.req is not None for s in self.slots):
-                    raise RuntimeError(f"request {r.rid} needs more device memory than the budget "
-                                       f"({self.budget / 1e9:.2f} GB)")
-                break  # wait for memory: keep arrival order
-            self.queue.popleft()
-            self._start(slot, r, plan, now)
-
-    def busy(self) -> bool:
-        return bool(self.queue) or any(s.req is not None for s in self.slots)
+                slot.req = slot.ev0 = slot.ev1 = None
+                self.inflight -= 1
+                any_done = True
+        return any_done
 
     def run(self, requests, clock=time.perf_counter):
-        """Serve requests whose `arrival` is relative to the start of the run."""
-        t0 = clock()
+        """Serve requests whose `arrival` is relative to the start of the run.  Plans
+        stay resident between runs (idle, evicted as memory is needed)."""
+        torch = self.torch
+        self.finished = []
+        self.pending.clear()
+        self.prepared.clear()
+        self.max_inflight = 0
+        self.error = None
+        self.stop = False
         for r in sorted(requests, key=lambda q: q.arrival):
             self.submit(r)
-        while self.busy():
-            now = clock() - t0
-            self.poll(now)
-            if self.queue and all(s.req is not None for s in self.slots):
-                time.sleep(0)  # all slots busy: yield
+        self.submitted_all = True
+        n = len(self.pending)
+        ref = torch.cuda.Event(enable_timing=True)
+        ref.record()
+        t0 = clock()
+        worker = threading.Thread(target=self._setup_loop, args=(clock, t0), daemon=True)
+        worker.start()
+        try:
+            with self.cv:
+                while len(self.finished) < n:
+                    if self.error is not None:
+                        raise self.error
+                    now = clock() - t0
+                    if self._retire(now, ref):
+                        self.cv.notify_all()  # memory and plans returned
+                    while self.prepared and any(s.req is None for s in self.slots):
+                        slot = next(s for s in self.slots if s.req is None)
+                        self._start(slot, self.prepared.popleft(), clock() - t0, ref)
+                        self.cv.notify_all()  # room to prepare further ahead
+                    if len(self.finished) < n:
+                        self.cv.wait(timeout=2e-4)
+        finally:
+            with self.cv:
+                self.stop = True
+                self.cv.notify_all()
+            worker.join()
         return self.report(clock() - t0)
 
     def report(self, wall: float) -> dict:
-        lat = np.array([(r.done - r.arrival) * 1e3 for r in self.finished])
-        return {"solves": len(self.finished), "seconds": wall,
-                "solves_per_s": len(self.finished) / wall if wall > 0 else None,
-                "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
-                "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
+        fin = self.finished
+
+        def pct(vals, q):
+            return float(np.percentile(vals, q)) if len(vals) else None
+
+        lat = [(r.done - r.arrival) * 1e3 for r in fin]
+        queue = [(r.setup_start - r.arrival) * 1e3 for r in fin]
+        setup = [(r.setup_end - r.setup_start) * 1e3 for r in fin]
+        wait = [(r.start - r.setup_end) * 1e3 for r in fin]
+        serv = [(r.done - r.start) * 1e3 for r in fin]
+        dev = [r.dev_end_ms - r.dev_start_ms for r in fin]
+        # most solves running on the device at one time (CUDA event intervals)
+        ev = sorted([(r.dev_start_ms, 1) for r in fin] + [(r.dev_end_ms, -1) for r in fin])
+        cur = peak = 0
+        for _, d in ev:
+            cur += d
+            peak = max(peak, cur)
+        split = {}
+        for name, v in (("queue", queue), ("setup", setup), ("wait_slot", wait), ("service", serv),
+                        ("device", dev)):
+            split[name] = {"p50_ms": pct(v, 50), "p99_ms": pct(v, 99), "mean_ms": float(np.mean(v)) if v else None}
+        return {"solves": len(fin), "seconds": wall,
+                "solves_per_s": len(fin) / wall if wall > 0 else None,
+                "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+                "split": split, "new_plans": sum(1 for r in fin if r.new_plan),
+                "max_inflight": self.max_inflight, "max_on_device": peak,
                 "budget_gb": self.budget / 1e9, "slots": len(self.slots)}
 
     def close(self):
