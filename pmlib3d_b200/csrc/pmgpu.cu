@@ -371,6 +371,26 @@ static std::vector<RadixSeq> regplan_candidates_wide(int n) {
   return out;
 }
 
+// The same radices ordered for the fused middle of the z pass: the smallest radix
+// that the registers take last, an even radix first where there is one (the zero half
+// of a padded line is then skipped); any order of the radices is a valid plan.
+static RadixSeq z_order(const RadixSeq &c, int rsize) {
+  RadixSeq q = c;
+  if (c.np < 2) return q;
+  const int lim = rsize == 4 ? 8 : 6;
+  int best = -1;
+  for (int i = 0; i < c.np; i++)
+    if (c.r[i] <= lim && (best < 0 || c.r[i] < c.r[best])) best = i;
+  if (best < 0) return q;
+  int rest[2], nr = 0;
+  for (int i = 0; i < c.np; i++)
+    if (i != best) rest[nr++] = c.r[i];
+  if (nr == 2 && rest[0] % 2 && !(rest[1] % 2)) std::swap(rest[0], rest[1]);
+  for (int i = 0; i < nr; i++) q.r[i] = rest[i];
+  q.r[nr] = c.r[best];
+  return q;
+}
+
 static bool make_regplan(int n, RegPlan &pl) {
   const std::vector<RadixSeq> c = regplan_candidates(n);
   if (c.empty()) return false;
@@ -1110,6 +1130,17 @@ template <typename R> static int tune_axis(pmgpu_plan *pl, int axis, TunedSchedu
   const int n = G.M[axis];
   std::vector<RadixSeq> cands = regplan_candidates(n);
   if (cands.size() > 5) cands.resize(5);
+  if (axis == 2) {
+    // the same radices ordered for the fused middle of the z pass
+    const size_t nc = cands.size();
+    for (size_t i = 0; i < nc; i++) {
+      const RadixSeq q = z_order(cands[i], (int)sizeof(R));
+      bool dup = false;
+      for (const RadixSeq &o : cands)
+        dup = dup || (o.np == q.np && o.r[0] == q.r[0] && o.r[1] == q.r[1] && o.r[2] == q.r[2]);
+      if (!dup) cands.push_back(q);
+    }
+  }
   if (sizeof(R) == 4) {
     std::vector<RadixSeq> w = regplan_candidates_wide(n);
     if (w.size() > 3) w.resize(3);
@@ -1294,13 +1325,24 @@ template <typename R> static int reg_tables(pmgpu_plan *pl, const char *caller, 
     RegPlan rp;
     const int n = pl->g.M[axis];
     if (!make_regplan(n, rp) && !make_bluestein(n, rp)) continue;
+    bool tuned = false;
     if (!rp.bl && tune_ok) {
       // a schedule measured earlier for this length
       auto it = g_tuned.find(std::make_tuple(n, (int)sizeof(R), axis));
       if (it != g_tuned.end()) {
         regplan_from(n, it->second.r, it->second.np, rp);
         (axis == 1 ? pl->tky : pl->tkz) = it->second.tk;
+        tuned = true;
       }
+    }
+    if (!rp.bl && !tuned && axis == 2) {
+      // untuned z plans: the model's radices ordered for the fused middle
+      RadixSeq c;
+      c.np = rp.np;
+      for (int i = 0; i < 3; i++) c.r[i] = i < rp.np ? rp.rad[i] : 0;
+      c.cost = 0.0;
+      const RadixSeq q = z_order(c, (int)sizeof(R));
+      regplan_from(n, q.r, q.np, rp);
     }
     const std::string key = regplan_key("l", pb, n, 0, rp);
     DevBuf &tb = axis == 1 ? pl->rtwy : pl->rtwz;

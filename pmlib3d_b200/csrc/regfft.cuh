@@ -239,8 +239,10 @@ __device__ __forceinline__ void rphase_any(const RegPlan &pl, int p, typename RV
 template <typename R, bool WIDE = false>
 __device__ __forceinline__ void rfft_fwd(const RegPlan &pl, typename RVec<R>::V *buf, int LG, const FastDiv &dLG,
                                          const typename cplx_t<R>::type *tw, bool gfirst, bool glast,
-                                         const PhaseGlobal &gl, int nz0 = -1) {
-  for (int p = 0; p < pl.np; p++) {
+                                         const PhaseGlobal &gl, int nz0 = -1, int pend = -1) {
+  // pend: phases [0, pend) only (the default: all)
+  const int np = pend >= 0 ? pend : pl.np;
+  for (int p = 0; p < np; p++) {
     const bool last = p == pl.np - 1;
     const int nz = p > 0 ? pl.n : gfirst ? gl.rows_in : nz0 >= 0 ? nz0 : pl.n;
     rphase_any<false, R, WIDE>(pl, p, buf, LG, dLG, tw, gfirst && p == 0, glast && last, !last, gl, nz);
@@ -253,8 +255,9 @@ __device__ __forceinline__ void rfft_fwd(const RegPlan &pl, typename RVec<R>::V 
 template <typename R, bool WIDE = false>
 __device__ __forceinline__ void rfft_inv(const RegPlan &pl, typename RVec<R>::V *buf, int LG, const FastDiv &dLG,
                                          const typename cplx_t<R>::type *tw, bool gfirst, bool glast,
-                                         const PhaseGlobal &gl) {
-  for (int p = pl.np - 1; p >= 0; p--) {
+                                         const PhaseGlobal &gl, int pstart = -1) {
+  // pstart: phases pstart, ..., 0 only (the default: all)
+  for (int p = pstart >= 0 ? pstart : pl.np - 1; p >= 0; p--) {
     const bool gs = gfirst && p == pl.np - 1;
     rphase_any<true, R, WIDE>(pl, p, buf, LG, dLG, tw, gs, glast && p == 0, p < pl.np - 1, gl,
                               gs ? gl.rows_in : pl.n);

@@ -170,6 +170,109 @@ __device__ __forceinline__ void tile_rows_store(typename cplx_t<R>::type *out, c
     *reinterpret_cast<float4 *>(dst + r * strideb + c * 16) = *reinterpret_cast<const float4 *>(src + r * rowb + c * 16);
 }
 
+// the spectral multiply at one point (kx index kx_i, row y of the y spectrum, kz
+// index z): the NC values v of the point in place.  kxp: kx wavenumber, Gp: the
+// Green's function value (loaded by the caller for the plain velocity solve)
+template <typename R, int NC>
+__device__ __forceinline__ void z_point(const SolveGeom<R> &g, typename cplx_t<R>::type *v, int kx_i, R kxp, R Gp,
+                                        R ky, R kyc, int y, int iy, int z, R kz, int zmode, int reproj,
+                                        int use_zeta) {
+  typedef typename cplx_t<R>::type C;
+  const R twopi = R(6.283185307179586476925286766559);
+  if (kx_i >= g.H) {
+#pragma unroll
+    for (int c = 0; c < NC; c++) v[c] = mk(R(0), R(0));
+    return;
+  }
+  const R kx = kxp;
+  const R kxc = (2 * kx_i == g.M[0]) ? R(0) : kx;
+  const R kzc = (2 * z == g.M[2]) ? R(0) : kz;
+  const R kmag = kx * kx + ky * ky + kz * kz;
+  if (zmode == Z_REGULARISE) {
+    const R zt = zeta_filter<R>(g.order, g.eps2pi * sqrt(kmag)) * g.scale;
+#pragma unroll
+    for (int c = 0; c < NC; c++) v[c] = cscale(v[c], zt);
+    return;
+  }
+  if constexpr (NC == 3) {
+    R zt = R(1);
+    if (use_zeta) zt = zeta_filter<R>(g.order, g.eps2pi * sqrt(kmag));
+    if (g.kernel2 && !g.allper) {
+      // derivative kernel K (pmlib_poisson_solve.f, kernel 2): component c is
+      // i S_c + (-1)^(k_c) E_c, S_c odd along axis c and even along the others
+      // (stored for |ky|, |kz| with the sign of the odd axis applied here), E_c the
+      // spectrum of the kernel's plane at -M_c/2 dx_c
+      const size_t noct = (size_t)g.gM2 * g.gM1 * g.H;
+      const int iz = min(z, g.M[2] - z);
+      const size_t oc = ((size_t)iz * g.gM1 + iy) * g.H + kx_i;
+      const R *E = g.green + 3 * noct;
+      R sx = g.green[oc], sy = g.green[noct + oc], sz = g.green[2 * noct + oc];
+      if (2 * y > g.M[1]) sy = -sy;
+      if (2 * z > g.M[2]) sz = -sz;
+      R ex = E[(size_t)iz * g.gM1 + iy];
+      R ey = E[(size_t)g.gM2 * g.gM1 + (size_t)iz * g.H + kx_i];
+      R ez = E[(size_t)g.gM2 * (g.gM1 + g.H) + (size_t)iy * g.H + kx_i];
+      if (kx_i & 1) ex = -ex;
+      if (y & 1) ey = -ey;
+      if (z & 1) ez = -ez;
+      const C Kx = mk(ex, sx), Ky = mk(ey, sy), Kz = mk(ez, sz);
+      const C w1 = v[0], w2 = v[1], w3 = v[2];
+      if (zmode == Z_VEL) {
+        v[0] = csub(cmul(Ky, w3), cmul(Kz, w2));
+        v[1] = csub(cmul(Kz, w1), cmul(Kx, w3));
+        v[2] = csub(cmul(Kx, w2), cmul(Ky, w1));
+      } else {  // Z_VORT: zeta w (+ K 2 pi i (k . w), Nyquist components dropped)
+        C o1 = cscale(w1, zt * g.scale), o2 = cscale(w2, zt * g.scale), o3 = cscale(w3, zt * g.scale);
+        if (reproj) {
+          const C da = cadd(cadd(cscale(w1, kxc), cscale(w2, kyc)), cscale(w3, kzc));
+          const C dv = mk(-twopi * da.y, twopi * da.x);
+          o1 = cadd(o1, cmul(Kx, dv));
+          o2 = cadd(o2, cmul(Ky, dv));
+          o3 = cadd(o3, cmul(Kz, dv));
+        }
+        v[0] = o1;
+        v[1] = o2;
+        v[2] = o3;
+      }
+      return;
+    }
+    R G;
+    if (g.allper) {
+      G = (kmag > R(0)) ? zt / (twopi * twopi * kmag) * g.scale : R(0);
+    } else {
+      G = Gp;
+    }
+    const C w1 = v[0], w2 = v[1], w3 = v[2];
+    if (zmode == Z_VEL) {
+      const C c1 = csub(cscale(w3, kyc), cscale(w2, kzc));
+      const C c2 = csub(cscale(w1, kzc), cscale(w3, kxc));
+      const C c3 = csub(cscale(w2, kxc), cscale(w1, kyc));
+      const R f = G * twopi;
+      v[0] = mk(-f * c1.y, f * c1.x);
+      v[1] = mk(-f * c2.y, f * c2.x);
+      v[2] = mk(-f * c3.y, f * c3.x);
+    } else if (zmode == Z_VECPOT) {
+      v[0] = cscale(w1, G);
+      v[1] = cscale(w2, G);
+      v[2] = cscale(w3, G);
+    } else {  // Z_VORT: zeta w (+ reprojection -4 pi^2 G k (k . w), Hermitian part)
+      C o1 = cscale(w1, zt * g.scale), o2 = cscale(w2, zt * g.scale), o3 = cscale(w3, zt * g.scale);
+      if (reproj) {
+        const R nx = kx - kxc, ny = ky - kyc, nz = kz - kzc;
+        const C da = cadd(cadd(cscale(w1, kxc), cscale(w2, kyc)), cscale(w3, kzc));
+        const C dn = cadd(cadd(cscale(w1, nx), cscale(w2, ny)), cscale(w3, nz));
+        const R f = -twopi * twopi * G;
+        o1 = cadd(o1, cscale(cadd(cscale(da, kxc), cscale(dn, nx)), f));
+        o2 = cadd(o2, cscale(cadd(cscale(da, kyc), cscale(dn, ny)), f));
+        o3 = cadd(o3, cscale(cadd(cscale(da, kzc), cscale(dn, nz)), f));
+      }
+      v[0] = o1;
+      v[1] = o2;
+      v[2] = o3;
+    }
+  }
+}
+
 // z-pass spectral multiply of one tile held in buffer V (complex view C).
 // zpos: position -> kz index (nullptr: natural order); kzs: kz wavenumbers (shared
 // copy of g.kzt, or nullptr)
@@ -194,98 +297,7 @@ __device__ __forceinline__ void z_multiply(const SolveGeom<R> &g, typename cplx_
     const int z = zpos ? zpos[q] : q;
     const int kx_i = k0 + kk;
     C *v = Cb + q * L + kk * NC;
-    if (kx_i >= g.H) {
-#pragma unroll
-      for (int c = 0; c < NC; c++) v[c] = mk(R(0), R(0));
-      return;
-    }
-    const R kx = kxp, kz = kzt[z];
-    const R kxc = (2 * kx_i == g.M[0]) ? R(0) : kx;
-    const R kzc = (2 * z == g.M[2]) ? R(0) : kz;
-    const R kmag = kx * kx + ky * ky + kz * kz;
-    if (zmode == Z_REGULARISE) {
-      const R zt = zeta_filter<R>(g.order, g.eps2pi * sqrt(kmag)) * g.scale;
-#pragma unroll
-      for (int c = 0; c < NC; c++) v[c] = cscale(v[c], zt);
-      return;
-    }
-    if constexpr (NC == 3) {
-      R zt = R(1);
-      if (use_zeta) zt = zeta_filter<R>(g.order, g.eps2pi * sqrt(kmag));
-      if (g.kernel2 && !g.allper) {
-        // derivative kernel K (pmlib_poisson_solve.f, kernel 2): component c is
-        // i S_c + (-1)^(k_c) E_c, S_c odd along axis c and even along the others
-        // (stored for |ky|, |kz| with the sign of the odd axis applied here), E_c the
-        // spectrum of the kernel's plane at -M_c/2 dx_c
-        const size_t noct = (size_t)g.gM2 * g.gM1 * g.H;
-        const int iz = min(z, g.M[2] - z);
-        const size_t oc = ((size_t)iz * g.gM1 + iy) * g.H + kx_i;
-        const R *E = g.green + 3 * noct;
-        R sx = g.green[oc], sy = g.green[noct + oc], sz = g.green[2 * noct + oc];
-        if (2 * y > g.M[1]) sy = -sy;
-        if (2 * z > g.M[2]) sz = -sz;
-        R ex = E[(size_t)iz * g.gM1 + iy];
-        R ey = E[(size_t)g.gM2 * g.gM1 + (size_t)iz * g.H + kx_i];
-        R ez = E[(size_t)g.gM2 * (g.gM1 + g.H) + (size_t)iy * g.H + kx_i];
-        if (kx_i & 1) ex = -ex;
-        if (y & 1) ey = -ey;
-        if (z & 1) ez = -ez;
-        const C Kx = mk(ex, sx), Ky = mk(ey, sy), Kz = mk(ez, sz);
-        const C w1 = v[0], w2 = v[1], w3 = v[2];
-        if (zmode == Z_VEL) {
-          v[0] = csub(cmul(Ky, w3), cmul(Kz, w2));
-          v[1] = csub(cmul(Kz, w1), cmul(Kx, w3));
-          v[2] = csub(cmul(Kx, w2), cmul(Ky, w1));
-        } else {  // Z_VORT: zeta w (+ K 2 pi i (k . w), Nyquist components dropped)
-          C o1 = cscale(w1, zt * g.scale), o2 = cscale(w2, zt * g.scale), o3 = cscale(w3, zt * g.scale);
-          if (reproj) {
-            const C da = cadd(cadd(cscale(w1, kxc), cscale(w2, kyc)), cscale(w3, kzc));
-            const C dv = mk(-twopi * da.y, twopi * da.x);
-            o1 = cadd(o1, cmul(Kx, dv));
-            o2 = cadd(o2, cmul(Ky, dv));
-            o3 = cadd(o3, cmul(Kz, dv));
-          }
-          v[0] = o1;
-          v[1] = o2;
-          v[2] = o3;
-        }
-        return;
-      }
-      R G;
-      if (g.allper) {
-        G = (kmag > R(0)) ? zt / (twopi * twopi * kmag) * g.scale : R(0);
-      } else {
-        G = Gp;
-      }
-      const C w1 = v[0], w2 = v[1], w3 = v[2];
-      if (zmode == Z_VEL) {
-        const C c1 = csub(cscale(w3, kyc), cscale(w2, kzc));
-        const C c2 = csub(cscale(w1, kzc), cscale(w3, kxc));
-        const C c3 = csub(cscale(w2, kxc), cscale(w1, kyc));
-        const R f = G * twopi;
-        v[0] = mk(-f * c1.y, f * c1.x);
-        v[1] = mk(-f * c2.y, f * c2.x);
-        v[2] = mk(-f * c3.y, f * c3.x);
-      } else if (zmode == Z_VECPOT) {
-        v[0] = cscale(w1, G);
-        v[1] = cscale(w2, G);
-        v[2] = cscale(w3, G);
-      } else {  // Z_VORT: zeta w (+ reprojection -4 pi^2 G k (k . w), Hermitian part)
-        C o1 = cscale(w1, zt * g.scale), o2 = cscale(w2, zt * g.scale), o3 = cscale(w3, zt * g.scale);
-        if (reproj) {
-          const R nx = kx - kxc, ny = ky - kyc, nz = kz - kzc;
-          const C da = cadd(cadd(cscale(w1, kxc), cscale(w2, kyc)), cscale(w3, kzc));
-          const C dn = cadd(cadd(cscale(w1, nx), cscale(w2, ny)), cscale(w3, nz));
-          const R f = -twopi * twopi * G;
-          o1 = cadd(o1, cscale(cadd(cscale(da, kxc), cscale(dn, nx)), f));
-          o2 = cadd(o2, cscale(cadd(cscale(da, kyc), cscale(dn, ny)), f));
-          o3 = cadd(o3, cscale(cadd(cscale(da, kzc), cscale(dn, nz)), f));
-        }
-        v[0] = o1;
-        v[1] = o2;
-        v[2] = o3;
-      }
-    }
+    z_point<R, NC>(g, v, kx_i, kxp, Gp, ky, kyc, y, iy, z, kzt[z], zmode, reproj, use_zeta);
   };
   constexpr int U = 4;
   const int total = N * TK;
@@ -313,6 +325,93 @@ __device__ __forceinline__ void z_multiply(const SolveGeom<R> &g, typename cplx_
       const int t = t0 + u * (int)blockDim.x;
       if (t < total) point(t, kxv[u], Gv[u]);
     }
+  }
+}
+
+// ---------------------------------------------------------------- fused middle of the z pass
+// Largest last radix of a z plan whose last forward phase, spectral multiply and first
+// inverse phase run in registers (three component lines of RL points a thread).
+__host__ __device__ inline bool z_fusable(const RegPlan &pl, int rsize) {
+  if (pl.bl || pl.np < 2) return false;
+  const int r = pl.rad[pl.np - 1];
+  return r >= 2 && r <= (rsize == 4 ? 8 : 6);
+}
+
+// The z pass's last forward phase, spectral multiply and first inverse phase in
+// registers: a thread takes one block of RL consecutive (digit-reversed) positions of
+// the NC component lines of one kx, runs the RL-point forward DFT of each (the last
+// decimation-in-frequency phase has no twiddles), multiplies every point, runs the
+// inverse DFTs (the first decimation-in-time phase has none either) and writes the
+// block back in place.  The arithmetic is that of the two phases and the multiply
+// done apart, so the result is the same; two shared-memory round trips and two
+// barriers per tile are saved.  Ends with a barrier.
+template <int RL, typename R, int NC>
+__device__ __forceinline__ void z_fused_mid_r(const SolveGeom<R> &g, const RegPlan &pl,
+                                              typename cplx_t<R>::type *Cb, int L, int TK, int k0, int y, int zmode,
+                                              int reproj, int use_zeta, const int *zpos, const R *kzs) {
+  typedef typename cplx_t<R>::type C;
+  const int nblk = pl.n / RL;
+  const R ky = g.kyt[y];
+  const R kyc = (2 * y == g.M[1]) ? R(0) : ky;  // Nyquist component dropped in the curl
+  const int iy = min(y, g.M[1] - y);
+  const bool pre = NC == 3 && zmode != Z_REGULARISE && !g.allper && !g.kernel2;
+  const int tks = __ffs(TK) - 1;  // TK is a power of two
+  const int total = nblk * TK;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int beta = t >> tks, kk = t - (beta << tks);
+    const int kx_i = k0 + kk;
+    C *base = Cb + (size_t)beta * RL * L + kk * NC;
+    int zs[RL];
+    R Gv[RL];
+    const R kxp = kx_i < g.H ? g.kxt[kx_i] : R(0);
+#pragma unroll
+    for (int k = 0; k < RL; k++) {
+      zs[k] = zpos[beta * RL + k];
+      Gv[k] = R(0);
+      if (pre && kx_i < g.H) Gv[k] = g.green[((size_t)min(zs[k], g.M[2] - zs[k]) * g.gM1 + iy) * g.H + kx_i];
+    }
+    C a[NC][RL];
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+#pragma unroll
+      for (int j = 0; j < RL; j++) a[c][j] = base[j * L + c];
+      dft<RL, false>(a[c]);
+    }
+#pragma unroll
+    for (int k = 0; k < RL; k++) {
+      C v[NC];
+#pragma unroll
+      for (int c = 0; c < NC; c++) v[c] = a[c][k];
+      z_point<R, NC>(g, v, kx_i, kxp, Gv[k], ky, kyc, y, iy, zs[k], kzs[zs[k]], zmode, reproj, use_zeta);
+#pragma unroll
+      for (int c = 0; c < NC; c++) a[c][k] = v[c];
+    }
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      dft<RL, true>(a[c]);
+#pragma unroll
+      for (int j = 0; j < RL; j++) base[j * L + c] = a[c][j];
+    }
+  }
+  __syncthreads();
+}
+
+template <typename R, int NC>
+__device__ __forceinline__ void z_fused_mid(const SolveGeom<R> &g, const RegPlan &pl, typename cplx_t<R>::type *Cb,
+                                            int L, int TK, int k0, int y, int zmode, int reproj, int use_zeta,
+                                            const int *zpos, const R *kzs) {
+  switch (pl.rad[pl.np - 1]) {
+    case 2: z_fused_mid_r<2, R, NC>(g, pl, Cb, L, TK, k0, y, zmode, reproj, use_zeta, zpos, kzs); break;
+    case 3: z_fused_mid_r<3, R, NC>(g, pl, Cb, L, TK, k0, y, zmode, reproj, use_zeta, zpos, kzs); break;
+    case 4: z_fused_mid_r<4, R, NC>(g, pl, Cb, L, TK, k0, y, zmode, reproj, use_zeta, zpos, kzs); break;
+    case 5: z_fused_mid_r<5, R, NC>(g, pl, Cb, L, TK, k0, y, zmode, reproj, use_zeta, zpos, kzs); break;
+    case 6: z_fused_mid_r<6, R, NC>(g, pl, Cb, L, TK, k0, y, zmode, reproj, use_zeta, zpos, kzs); break;
+    default:
+      if constexpr (sizeof(R) == 4) {
+        if (pl.rad[pl.np - 1] == 7) z_fused_mid_r<7, R, NC>(g, pl, Cb, L, TK, k0, y, zmode, reproj, use_zeta, zpos, kzs);
+        else z_fused_mid_r<8, R, NC>(g, pl, Cb, L, TK, k0, y, zmode, reproj, use_zeta, zpos, kzs);
+      }
+      break;
   }
 }
 
@@ -456,6 +555,11 @@ __device__ __forceinline__ void rl_tile(const SolveGeom<R> &g, const LineTiles &
   } else if (lmode == L_INV) {
     if (blue) bfft<R, true>(pl, s.buf, LG, lt.dLG, s.tw, s.chirp, s.bpos, true, true, gl, nl, lt.rows_out);
     else rfft_inv<R, WIDE>(pl, s.buf, LG, lt.dLG, s.tw, true, true, gl);
+  } else if (!blue && NC == 3 && z_fusable(pl, (int)sizeof(R))) {
+    rfft_fwd<R, WIDE>(pl, s.buf, LG, lt.dLG, s.tw, true, false, gl, -1, pl.np - 1);
+    z_fused_mid<R, NC>(g, pl, reinterpret_cast<C *>(s.buf), L, TK, kt * TK, g.yk ? g.yk[o] : o, zmode, reproj,
+                       use_zeta, s.zpos, s.kzs);
+    rfft_inv<R, WIDE>(pl, s.buf, LG, lt.dLG, s.tw, false, true, gl, pl.np - 2);
   } else {
     if (blue) bfft<R, false>(pl, s.buf, LG, lt.dLG, s.tw, s.chirp, s.bpos, true, false, gl, lt.rows_in, nl);
     else rfft_fwd<R, WIDE>(pl, s.buf, LG, lt.dLG, s.tw, true, false, gl);
