@@ -382,6 +382,8 @@ def main():
                     help="profile: only the FP32 warm-up and timed steps (for ncu captures)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"],
                     help="precision of --mode profile")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="the model's radix schedules instead of the autotuner's (profiling)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched and served measurements")
     ap.add_argument("--no-stage", action="store_true", help="skip the full vortex-stage measurement")
     ap.add_argument("--no-penal", action="store_true", help="skip the penalisation measurement")
@@ -416,7 +418,7 @@ def main():
 
     w = Wl.make(args.config)
     n = w.npart
-    P.fft_tune(True)  # schedules (radix sequence, kx tile) measured when the plans are made
+    P.fft_tune(not args.no_tune)  # schedules (radix sequence, kx tile) measured when the plans are made
     patch = P.make_patch(w.xmin, w.xmax, w.dx, bound_cond=w.bound_cond, nghost=w.nghost)
     ierr, topo = P.pmlib_topology_cuboid(patch, w.interp)
     params = P.make_params(order=w.order, kernel=1, radius=w.radius, interp=w.interp)
