@@ -384,6 +384,8 @@ def main():
                     help="precision of --mode profile")
     ap.add_argument("--no-tune", action="store_true",
                     help="the model's radix schedules instead of the autotuner's (profiling)")
+    ap.add_argument("--no-specialised", action="store_true",
+                    help="line passes on the run-time register engine only (no compile-time-plan kernels)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched and served measurements")
     ap.add_argument("--no-stage", action="store_true", help="skip the full vortex-stage measurement")
     ap.add_argument("--no-penal", action="store_true", help="skip the penalisation measurement")
@@ -418,6 +420,7 @@ def main():
 
     w = Wl.make(args.config)
     n = w.npart
+    P.fft_specialised(not args.no_specialised)
     P.fft_tune(not args.no_tune)  # schedules (radix sequence, kx tile) measured when the plans are made
     patch = P.make_patch(w.xmin, w.xmax, w.dx, bound_cond=w.bound_cond, nghost=w.nghost)
     ierr, topo = P.pmlib_topology_cuboid(patch, w.interp)

@@ -242,6 +242,13 @@ int pmgpu_batch_fused(const pmgpu_batch *batch);
  * the same results to round-off; returns the previous setting. */
 int pmgpu_fft_engine(int engine);
 
+/* Lets the y / z line passes of 3-component fields run kernels compiled for their
+ * plan (length, radices and kx tile known to the compiler) where one exists: 1 =
+ * on (default), 0 = the run-time register engine only (no counterpart in the
+ * reference).  The results are bit-identical either way; returns the previous
+ * setting. */
+int pmgpu_fft_specialised(int on);
+
 /* Global particle diagnostics accumulated in FP64 for FP32 or FP64 particle arrays
  * (device pointers, (3, npart) component fastest), the quantities of
  * vortex_codes/vortex_structures/source/diagnostics/diagnostics_knot.f:75-175:

@@ -18,7 +18,7 @@ EXPORTS = (
     "pmgpu_regularise", "pmgpu_regularise_f32", "pmgpu_plan_destroy",
     "pmgpu_step", "pmgpu_step_dev", "pmgpu_remesh", "pmgpu_last_error", "pmgpu_launch_count",
     "pmgpu_timing_enable", "pmgpu_timing_reset", "pmgpu_timing_get",
-    "pmgpu_interp_particle_mesh_noalloc", "pmgpu_fft_engine", "pmgpu_poisson_solve_dev",
+    "pmgpu_interp_particle_mesh_noalloc", "pmgpu_fft_engine", "pmgpu_fft_specialised", "pmgpu_poisson_solve_dev",
     "pmgpu_batch_create", "pmgpu_batch_solve", "pmgpu_batch_size", "pmgpu_batch_plan", "pmgpu_batch_destroy",
     "pmgpu_fft_tune", "pmgpu_fft_tuned", "pmgpu_particle_diagnostics",
     "pmgpu_deriv_vorticity", "pmgpu_deriv_vorticity_f32", "pmgpu_deriv_vorticity_dev",
@@ -95,6 +95,7 @@ def lib():
         "pmgpu_timing_get": [C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(C.c_longlong)],
         "pmgpu_interp_particle_mesh_noalloc": [TP, QP, vp, vp, C.c_int, C.c_int, vp, C.c_int, C.c_int, C.c_int, vp],
         "pmgpu_fft_engine": [C.c_int],
+        "pmgpu_fft_specialised": [C.c_int],
         "pmgpu_inject_alloc_failure": [C.c_longlong],
         "pmgpu_poisson_solve_dev": [vp, vp, vp, vp, C.c_int, C.c_int, C.c_int, vp],
         "pmgpu_batch_create": [C.c_int, PP, TP, QP, C.c_int, C.POINTER(vp)],

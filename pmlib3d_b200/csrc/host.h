@@ -163,5 +163,11 @@ int upload_cs_f32_1(const void *t32, const void *t64);
 int upload_cs_f32_3(const void *t32, const void *t64);
 int upload_cs_f64_1(const void *t32, const void *t64);
 int upload_cs_f64_3(const void *t32, const void *t64);
+int upload_cs_ct_f32(const void *t32, const void *t64);
+int upload_cs_ct_f64(const void *t32, const void *t64);
+
+// launches of the y / z line passes take a compile-time-plan kernel when one is
+// compiled for the plan and kx tile (0: always the run-time engine)
+extern int g_fft_ct;
 
 }  // namespace pmgpu

@@ -38,6 +38,15 @@ static int rl_pick_tk(const SolveGeom<R> &g, int axis, size_t slack, bool &wide)
   return TK;
 }
 
+// a line-pass kernel (k_rlines and its compile-time-plan instances)
+template <typename R>
+using LinesKernel = void (*)(SolveGeom<R>, LineTiles, const typename cplx_t<R>::type *, typename cplx_t<R>::type *,
+                             int, int, int, int, int);
+// the compile-time-plan kernel of 3-component lines for plan rp and kx tile TK
+// (nullptr: none compiled); defined in passes_ct_*.cu
+LinesKernel<float> ct_lines_f32(const RegPlan &rp, int TK);
+LinesKernel<double> ct_lines_f64(const RegPlan &rp, int TK);
+
 template <typename R, int NC>
 static int launch_lines(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typename cplx_t<R>::type *out, int axis,
                         int lmode, int zmode, int reproj, int use_zeta, int rows_in, int rows_out, long long in_os,
@@ -79,6 +88,14 @@ static int launch_lines(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typ
         CKL(caller);
         return 0;
       };
+      if constexpr (NC == 3) {
+        if (g_fft_ct) {
+          LinesKernel<R> ck;
+          if constexpr (sizeof(R) == 4) ck = ct_lines_f32(rp, TK);
+          else ck = ct_lines_f64(rp, TK);
+          if (ck) return launch(ck);
+        }
+      }
       if constexpr (sizeof(R) == 4) {
         if (wide) return launch(k_rlines<R, NC, true>);
       }

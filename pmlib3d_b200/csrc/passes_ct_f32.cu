@@ -1,0 +1,25 @@
+// passes_ct_f32.cu -- compile-time-plan y / z line passes for float fields of 3
+// components: the plans and kx tiles of the common grid lengths (the free-axis
+// lengths 2 (2^k + 8) of 2^k cells with four ghost layers, and powers of two), with
+// the radix orders the schedule tuner chooses between.  Other plans run the
+// run-time engine.
+#include "passes.cuh"
+
+namespace pmgpu {
+
+#define PMGPU_CT(N, A, B, C, T)                                                                              \
+  if (ct_match<CtPlan<N, A, B, C>>(rp) && TK == T)                                                           \
+    return k_rlines_ct<float, 3, (A > 17 || B > 17 || C > 17), N, A, B, C, T>;
+
+LinesKernel<float> ct_lines_f32(const RegPlan &rp, int TK) {
+  PMGPU_CT(528, 24, 22, 1, 8)
+  PMGPU_CT(528, 22, 24, 1, 8)
+  PMGPU_CT(528, 12, 11, 4, 8)
+  return nullptr;
+}
+
+#undef PMGPU_CT
+
+int upload_cs_ct_f32(const void *t32, const void *t64) { return upload_cs_local(t32, t64); }
+
+}  // namespace pmgpu

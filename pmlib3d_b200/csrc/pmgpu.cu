@@ -124,7 +124,7 @@ static int ensure_device(const char *caller) {
       t32[R][m][1] = (float)sinl(a);
     }
   if (upload_cs_f32_1(t32, t64) || upload_cs_f32_3(t32, t64) || upload_cs_f64_1(t32, t64) ||
-      upload_cs_f64_3(t32, t64)) {
+      upload_cs_f64_3(t32, t64) || upload_cs_ct_f32(t32, t64) || upload_cs_ct_f64(t32, t64)) {
     set_error(caller, "could not upload the DFT constant tables.");
     return -1;
   }
@@ -2213,6 +2213,17 @@ int pmgpu_fft_engine(int engine) {
   std::lock_guard<std::mutex> lk(g_setup_mu);
   const int old = g_force_stockham;
   g_force_stockham = engine == 1 ? 1 : 0;
+  return old;
+}
+
+namespace pmgpu {
+int g_fft_ct = 1;
+}
+
+int pmgpu_fft_specialised(int on) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int old = g_fft_ct;
+  g_fft_ct = on ? 1 : 0;
   return old;
 }
 

@@ -266,6 +266,121 @@ __device__ __forceinline__ void rfft_inv(const RegPlan &pl, typename RVec<R>::V 
 }
 
 // ---------------------------------------------------------------------------
+// Compile-time plans.  The phases of rphase / rfft_fwd / rfft_inv with the length,
+// the radices and the line vectors of a tile known to the compiler: the block and
+// stride arithmetic becomes multiplication by constants, the shared-memory offsets
+// of a butterfly's points become immediates, no plan field is read at run time and
+// the phase loop unrolls.  The arithmetic (the DFT codelets, the twiddles and their
+// order) is that of the run-time engine, so the results are bit-identical.
+constexpr int REG_THREADS = 256;  // threads of the CTAs that run the compile-time phases
+
+template <int N_, int R0_, int R1_, int R2_ = 1> struct CtPlan {
+  static constexpr int n = N_;
+  static constexpr int np = R2_ > 1 ? 3 : (R1_ > 1 ? 2 : 1);
+  __host__ __device__ static constexpr int rad(int p) { return p == 0 ? R0_ : p == 1 ? R1_ : R2_; }
+  __host__ __device__ static constexpr int blk(int p) { return p == 0 ? N_ : p == 1 ? N_ / R0_ : N_ / (R0_ * R1_); }
+  __host__ __device__ static constexpr int str(int p) { return blk(p) / rad(p); }
+  __host__ __device__ static constexpr int twm(int p) { return N_ / blk(p); }
+  static_assert(R0_ * R1_ * R2_ == N_, "the radices multiply to the length");
+};
+
+// the run-time plan `pl` is the compile-time plan P
+template <typename P> __host__ __device__ inline bool ct_match(const RegPlan &pl) {
+  if (pl.bl || pl.n != P::n || pl.np != P::np) return false;
+  for (int p = 0; p < P::np; p++)
+    if (pl.rad[p] != P::rad(p)) return false;
+  return true;
+}
+
+// phase p of plan P over a tile of LG line vectors (rphase with constants)
+template <typename P, int p, bool INV, typename R, int LG, bool GSRC, bool GDST>
+__device__ __forceinline__ void rphase_ct(typename RVec<R>::V *buf, const typename cplx_t<R>::type *__restrict__ tw,
+                                          const PhaseGlobal &gl, int nz) {
+  typedef typename cplx_t<R>::type C;
+  typedef typename RVec<R>::V V;
+  constexpr int G = RVec<R>::G;
+  constexpr int RAD = P::rad(p), s = P::str(p), B = P::blk(p), tm = P::twm(p);
+  constexpr bool twid = p < P::np - 1;
+  constexpr unsigned total = (unsigned)(P::n / RAD) * (unsigned)LG;
+  static_assert(G == 1, "one complex point per vector");
+  const V *gin = reinterpret_cast<const V *>(gl.in);
+  V *gout = reinterpret_cast<V *>(gl.out);
+  const long long vri = gl.rs_in, vro = gl.rs_out;
+#pragma unroll 1
+  for (unsigned u = threadIdx.x; u < total; u += REG_THREADS) {
+    const unsigned b = u / (unsigned)LG;
+    const int g = (int)(u - b * (unsigned)LG);
+    const unsigned beta = b / (unsigned)s;
+    const int r = (int)(b - beta * (unsigned)s);
+    const int pos0 = (int)beta * B + r;
+    C a[RAD];
+    if constexpr (GSRC) {
+      const V *src = gin + (long long)pos0 * vri + g;
+#pragma unroll
+      for (int j = 0; j < RAD; j++) {
+        V v = zero_vec<R>();
+        if (pos0 + s * j < nz) v = ldg_vec<R>(src + (long long)(s * j) * vri);
+        a[j] = v;
+      }
+    } else {
+      const V *src = buf + pos0 * LG + g;
+      if (nz >= P::n) {
+#pragma unroll
+        for (int j = 0; j < RAD; j++) a[j] = src[s * j * LG];
+      } else {
+#pragma unroll
+        for (int j = 0; j < RAD; j++) a[j] = pos0 + s * j < nz ? src[s * j * LG] : zero_vec<R>();
+      }
+    }
+    if constexpr (INV && twid) {
+      const int tb = tm * r;
+#pragma unroll
+      for (int j = 1; j < RAD; j++) a[j] = cmulc(a[j], tw[tb * j]);
+    }
+    dft<RAD, INV>(a);
+    if constexpr (!INV && twid) {
+      const int tb = tm * r;
+#pragma unroll
+      for (int k = 1; k < RAD; k++) a[k] = cmul(a[k], tw[tb * k]);
+    }
+    if constexpr (GDST) {
+      V *dst = gout + (long long)pos0 * vro + g;
+#pragma unroll
+      for (int k = 0; k < RAD; k++)
+        if (pos0 + s * k < gl.rows_out) dst[(long long)(s * k) * vro] = a[k];
+    } else {
+      V *dst = buf + pos0 * LG + g;
+#pragma unroll
+      for (int k = 0; k < RAD; k++) dst[s * k * LG] = a[k];
+    }
+  }
+}
+
+// forward phases p .. PEND - 1 of plan P (rfft_fwd); each ends with a barrier
+template <typename P, typename R, int LG, bool GFIRST, bool GLAST, int PEND, int p = 0>
+__device__ __forceinline__ void rfft_fwd_ct(typename RVec<R>::V *buf, const typename cplx_t<R>::type *tw,
+                                            const PhaseGlobal &gl) {
+  if constexpr (p < PEND) {
+    const int nz = (GFIRST && p == 0) ? gl.rows_in : P::n;
+    rphase_ct<P, p, false, R, LG, GFIRST && p == 0, GLAST && p == P::np - 1>(buf, tw, gl, nz);
+    __syncthreads();
+    rfft_fwd_ct<P, R, LG, GFIRST, GLAST, PEND, p + 1>(buf, tw, gl);
+  }
+}
+
+// inverse phases p = PSTART .. 0 of plan P (rfft_inv); each ends with a barrier
+template <typename P, typename R, int LG, bool GFIRST, bool GLAST, int p>
+__device__ __forceinline__ void rfft_inv_ct(typename RVec<R>::V *buf, const typename cplx_t<R>::type *tw,
+                                            const PhaseGlobal &gl) {
+  if constexpr (p >= 0) {
+    constexpr bool gs = GFIRST && p == P::np - 1;
+    rphase_ct<P, p, true, R, LG, gs, GLAST && p == 0>(buf, tw, gl, gs ? gl.rows_in : P::n);
+    __syncthreads();
+    rfft_inv_ct<P, R, LG, GFIRST, GLAST, p - 1>(buf, tw, gl);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Bluestein (chirp-z) transform of lines of length n with a plan of length m >= 2n-1:
 //   X[k] = c[k] sum_j (x[j] c[j]) conj(c[k - j]),   c[j] = exp(-i pi j^2 / n),
 // a circular convolution of length m: forward transform of the chirped input (zero

@@ -345,18 +345,21 @@ __host__ __device__ inline bool z_fusable(const RegPlan &pl, int rsize) {
 // block back in place.  The arithmetic is that of the two phases and the multiply
 // done apart, so the result is the same; two shared-memory round trips and two
 // barriers per tile are saved.  Ends with a barrier.
-template <int RL, typename R, int NC>
+// NCT, TKC: the transform length and the kx tile when known at compile time (0: read
+// from pl and TK)
+template <int RL, typename R, int NC, int NCT = 0, int TKC = 0>
 __device__ __forceinline__ void z_fused_mid_r(const SolveGeom<R> &g, const RegPlan &pl,
                                               typename cplx_t<R>::type *Cb, int L, int TK, int k0, int y, int zmode,
                                               int reproj, int use_zeta, const int *zpos, const R *kzs) {
   typedef typename cplx_t<R>::type C;
-  const int nblk = pl.n / RL;
+  const int nblk = NCT ? NCT / RL : pl.n / RL;
   const R ky = g.kyt[y];
   const R kyc = (2 * y == g.M[1]) ? R(0) : ky;  // Nyquist component dropped in the curl
   const int iy = min(y, g.M[1] - y);
   const bool pre = NC == 3 && zmode != Z_REGULARISE && !g.allper && !g.kernel2;
-  const int tks = __ffs(TK) - 1;  // TK is a power of two
-  const int total = nblk * TK;
+  const int tks = TKC ? (TKC == 1 ? 0 : TKC == 2 ? 1 : TKC == 4 ? 2 : TKC == 8 ? 3 : 4) : __ffs(TK) - 1;  // TK: 2^k
+  if (TKC) L = NC * TKC;
+  const int total = nblk * (TKC ? TKC : TK);
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
     const int beta = t >> tks, kk = t - (beta << tks);
     const int kx_i = k0 + kk;
@@ -582,6 +585,65 @@ __global__ void __launch_bounds__(RL_THREADS, WIDE ? 2 : RMinBlocks<R>::v) k_rli
   const int ntiles = lt.nouter * lt.nkt;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
     rl_tile<R, NC, WIDE>(g, lt, in, out, axis, lmode, zmode, reproj, use_zeta, s, tile);
+}
+
+// ---------------------------------------------------------------- compile-time line passes
+// rl_tile for a plan P (no Bluestein) and a kx tile TK known at compile time: the
+// same phases, multiply and fused middle, so the results equal those of rl_tile bit
+// for bit.
+template <typename P, typename R> __host__ __device__ constexpr bool ct_z_fusable() {
+  return P::np >= 2 && P::rad(P::np - 1) >= 2 && P::rad(P::np - 1) <= (sizeof(R) == 4 ? 8 : 6);
+}
+
+template <typename R, int NC, typename P, int TK>
+__device__ __forceinline__ void rl_tile_ct(const SolveGeom<R> &g, const LineTiles &lt,
+                                           const typename cplx_t<R>::type *in, typename cplx_t<R>::type *out,
+                                           int lmode, int zmode, int reproj, int use_zeta, const RlSmem<R> &s,
+                                           int tile) {
+  typedef typename cplx_t<R>::type C;
+  constexpr int L = NC * TK, LG = L / RVec<R>::G;
+  const int o = tile / lt.nkt, kt = tile - o * lt.nkt;
+  PhaseGlobal gl;
+  gl.in = in + (o * lt.in_os + (long long)kt * TK) * NC;
+  gl.out = out + (o * lt.out_os + (long long)kt * TK) * NC;
+  gl.rs_in = lt.in_rs * NC;
+  gl.rs_out = lt.out_rs * NC;
+  gl.rows_in = lt.rows_in;
+  gl.rows_out = lt.rows_out;
+  if (lmode == L_FWD) {
+    rfft_fwd_ct<P, R, LG, true, true, P::np>(s.buf, s.tw, gl);
+  } else if (lmode == L_INV) {
+    rfft_inv_ct<P, R, LG, true, true, P::np - 1>(s.buf, s.tw, gl);
+  } else {
+    const int y = g.yk ? g.yk[o] : o;
+    if constexpr (NC == 3 && ct_z_fusable<P, R>()) {
+      rfft_fwd_ct<P, R, LG, true, false, P::np - 1>(s.buf, s.tw, gl);
+      z_fused_mid_r<P::rad(P::np - 1), R, NC, P::n, TK>(g, RegPlan(), reinterpret_cast<C *>(s.buf), L, TK, kt * TK,
+                                                        y, zmode, reproj, use_zeta, s.zpos, s.kzs);
+      rfft_inv_ct<P, R, LG, false, true, P::np - 2>(s.buf, s.tw, gl);
+    } else {
+      rfft_fwd_ct<P, R, LG, true, false, P::np>(s.buf, s.tw, gl);
+      z_multiply<R, NC>(g, reinterpret_cast<C *>(s.buf), L, TK, kt * TK, y, zmode, reproj, use_zeta, s.zpos,
+                        s.kzs);
+      __syncthreads();
+      rfft_inv_ct<P, R, LG, false, true, P::np - 1>(s.buf, s.tw, gl);
+    }
+  }
+}
+
+// k_rlines for the compile-time plan (N; R0, R1, R2) and kx tile TK
+template <typename R, int NC, bool WIDE, int N, int R0, int R1, int R2, int TK>
+__global__ void __launch_bounds__(RL_THREADS, WIDE ? 2 : RMinBlocks<R>::v) k_rlines_ct(SolveGeom<R> g, LineTiles lt,
+                                                          const typename cplx_t<R>::type *in,
+                                                          typename cplx_t<R>::type *out, int axis, int lmode,
+                                                          int zmode, int reproj, int use_zeta) {
+  static_assert(RL_THREADS == REG_THREADS, "the compile-time phases stride by REG_THREADS");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const RlSmem<R> s = rl_setup<R>(g, lt, axis, lmode, smem_raw);
+  __syncthreads();
+  const int ntiles = lt.nouter * lt.nkt;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    rl_tile_ct<R, NC, CtPlan<N, R0, R1, R2>, TK>(g, lt, in, out, lmode, zmode, reproj, use_zeta, s, tile);
 }
 
 // ---------------------------------------------------------------- batches of patches

@@ -366,6 +366,13 @@ def fft_engine(engine: int) -> int:
     return lib().pmgpu_fft_engine(int(engine))
 
 
+def fft_specialised(on: bool) -> int:
+    """Lets the y / z line passes run the kernels compiled for their plan where one
+    exists (default on); off: the run-time register engine only.  The results are
+    bit-identical either way.  Returns the previous setting."""
+    return lib().pmgpu_fft_specialised(1 if on else 0)
+
+
 def step(plan: Plan, pos, part_vort, part_vel) -> int:
     """One vortex step through host arrays: P2M (clear), unbounded solve and curl,
     M2P of the velocity into ``part_vel``."""

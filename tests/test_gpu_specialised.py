@@ -1,0 +1,64 @@
+"""Compile-time-plan line passes against the run-time register engine.
+
+The y / z passes of 3-component fields run kernels compiled for their plan (length,
+radices, kx tile) where one exists; they do the arithmetic of the run-time engine
+in the same order, so the solves agree to round-off (the compiler may fuse a
+different multiply and add of an expression in the two builds).  The grids have y
+and z lines of 528 points (256 cells, four ghost layers, free), the length of the
+256^3 step, and the schedules are set to the compiled plans.
+"""
+import numpy as np
+import pytest
+
+from pmlib3d_b200 import pmlib as P
+from tests.helpers import gaussian_field
+
+pytestmark = pytest.mark.gpu
+
+# (precision, y schedule, z schedule), tile 8
+CASES = [
+    (P.FP32, (24, 22), (12, 11, 4)),
+    (P.FP32, (24, 22), (22, 24)),
+    (P.FP64, (12, 11, 4), (12, 11, 4)),
+    (P.FP64, (12, 11, 4), (8, 6, 11)),
+]
+
+
+def _solve(prec, sched, specialised, w, reproj):
+    old = P.fft_specialised(specialised)
+    try:
+        for axis, rad in sched.items():
+            assert P.fft_set_schedule(528, prec, axis, rad, 8) == 0, P.last_error()
+        patch = P.make_patch((-0.0625, -1.0, -1.0), (0.0625, 1.0, 1.0), (1.0 / 128,) * 3,
+                             bound_cond=(0, 0, 0), nghost=4)
+        ierr, topo = P.pmlib_topology_cuboid(patch, 3)
+        assert ierr == 0
+        params = P.make_params(order=6, kernel=1, radius=2.0, interp=3)
+        ierr, plan = P.pmlib_poisson_setup(patch, topo, params, prec)
+        assert ierr == 0, P.last_error()
+        dt = np.float32 if prec == P.FP32 else np.float64
+        wg = w.astype(dt)
+        vel = np.zeros(w.shape, dt)
+        assert P.pmlib_poisson_solve(plan, wg, vel, reproj=reproj) == 0, P.last_error()
+        plan.close()
+        return vel, wg, topo
+    finally:
+        P.fft_specialised(old)
+        for axis in sched:
+            P.fft_set_schedule(528, prec, axis, None)
+
+
+@pytest.mark.parametrize("prec,ysched,zsched", CASES)
+@pytest.mark.parametrize("reproj", [False, True])
+def test_specialised_equals_runtime_engine(prec, ysched, zsched, reproj):
+    sched = {1: ysched, 2: zsched}
+    patch = P.make_patch((-0.0625, -1.0, -1.0), (0.0625, 1.0, 1.0), (1.0 / 128,) * 3, bound_cond=(0, 0, 0), nghost=4)
+    ierr, topo = P.pmlib_topology_cuboid(patch, 3)
+    w = gaussian_field(topo, seed=5, noise=0.05)
+    v1, w1, t1 = _solve(prec, sched, True, w, reproj)
+    v0, w0, _ = _solve(prec, sched, False, w, reproj)
+    assert np.abs(v1).max() > 0
+    tol = 2e-6 if prec == P.FP32 else 1e-14
+    for a, b in ((v1, v0), (w1, w0)):
+        d = np.linalg.norm((a.astype(np.float64) - b).ravel()) / np.linalg.norm(b.astype(np.float64).ravel())
+        assert d < tol, d
