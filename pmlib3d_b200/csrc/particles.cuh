@@ -12,6 +12,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "fft.cuh"  // cp.async helpers
 
 namespace pmgpu {
 
@@ -320,27 +321,63 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const unsigned *__r
 }
 
 // ------------------------------------------------------------------ deposition (gather)
-// A CTA owns TX x TY cell columns and a chunk of ZC cell layers, and marches up the
-// bin layers, DEP_LB at a time.  For each batch of bin layers it stages the
-// particles of the (TX+W-1) x (TY+W-1) bins of every layer that reach its columns
-// in shared memory with their weights, and each thread adds them to a rolling
-// window of W + DEP_LB - 1 cell layers held in registers.  The W bins of one bin
-// row that reach a cell column are consecutive in the sorted order, so a thread
-// walks one contiguous range of staged particles per bin row.  Per cell the order
-// is fixed (bin layer, bin row, bin, particle index), so the result is the same on
-// every run.  A cell layer is final once the last bin layer that reaches it has
-// been added.
+// Every cell gathers the particles of the W x W x W bins that reach it, so no
+// floating-point atomics are needed and the sum order per cell is fixed (bin layer,
+// bin row, bin, particle index): the same result on every run.
+//
+// Work split.  The cuboid is cut into tiles of TW x TH cell columns of equal size
+// (TW <= 32, TH <= CY); all (tile, cell layer) pairs, tile by tile and layer by
+// layer, are divided into consecutive shares of equal cost, one per CTA (a persistent grid of one CTA per SM).  A
+// CTA's share is one or a few segments: a tile and a range of cell layers.  For a
+// segment the CTA marches up the bin layers that reach its cell layers.
+//
+// Roles.  A CTA has NCW consumer warps and two groups of NPG producer warps.  The
+// producers stage one bin layer at a time in shared memory: the bin starts of the
+// (32+W-1) x (CY+W-1) bins of the layer that reach the tile, and for each of their
+// particles a record (values, bin x), its z weights, x weights and zero-padded y
+// weights.  The consumers add the staged particles to a rolling window of W cell
+// layers held in registers; each consumer thread owns two cell columns adjacent
+// along y.  The two producer groups take alternate bin layers, each into its own
+// buffer, handed over by named barriers (FULL_g: group g arrives, consumers wait;
+// EMPTY_g: consumers arrive, group g waits): a group's global loads for layer k + 2
+// overlap the consumers' sums over layers k and k + 1.  A bin layer with more
+// particles than a buffer holds is staged in several chunks, taken by both sides in
+// the same order.
+//
+// Consumer visits.  The W bins of one bin row that reach a cell column are
+// consecutive in the sorted order, so a thread walks one contiguous range of
+// staged particles per bin row; its W + 1 ranges (bin rows 2 ty .. 2 ty + W) are
+// walked as one flattened loop, and every visit adds to both columns of the pair
+// (the weight of a row that does not reach one of them is a stored zero).  A cell
+// layer is final once the last bin layer that reaches it has been added.
 constexpr int DEP_TX = 32;
-constexpr int DEP_TY = 16;
-constexpr int DEP_THREADS = DEP_TX * DEP_TY;
-constexpr int DEP_LB = 3;
 
-template <int W> struct WStride { static constexpr int v = W == 4 ? 4 : 8; };
+template <typename R, int W> struct DepCfg;
+// ncw consumer warps, two producer groups of npg warps, staging capacity per buffer
+template <> struct DepCfg<float, 4> { static constexpr int ncw = 14, npg = 4, cap = 1152, ws = 4; };
+template <> struct DepCfg<float, 6> { static constexpr int ncw = 12, npg = 2, cap = 1024, ws = 8; };
+template <> struct DepCfg<double, 4> { static constexpr int ncw = 6, npg = 2, cap = 640, ws = 4; };
+template <> struct DepCfg<double, 6> { static constexpr int ncw = 6, npg = 2, cap = 512, ws = 8; };
 
-// shared-memory bytes of k_deposit for `cap` staged particles
-template <typename R, int W> __host__ __device__ constexpr size_t deposit_smem(int cap) {
-  return (size_t)cap * (3 * WStride<W>::v + 4) * sizeof(R) +
-         sizeof(int) * (DEP_LB * (DEP_TY + W - 1) * (DEP_TX + W) + DEP_LB * (DEP_TY + W - 1) + 2);
+template <typename R, int W> __host__ __device__ constexpr int dep_threads() {
+  return 32 * (DepCfg<R, W>::ncw + 2 * DepCfg<R, W>::npg);
+}
+template <typename R, int W> __host__ __device__ constexpr int dep_cells_y() { return 2 * DepCfg<R, W>::ncw; }
+
+// one staging buffer: records [cap][4], z weights [cap][ws], x weights [W][cap],
+// y weights [W + 2][cap] (rows 0 and W + 1 zero), bin starts [BYB][BX + 1], staged
+// row offsets [BYB + 2]
+template <typename R, int W> __host__ __device__ constexpr size_t dep_buf_vals() {
+  return (size_t)DepCfg<R, W>::cap * (4 + DepCfg<R, W>::ws + W + (W + 2));
+}
+template <typename R, int W> __host__ __device__ constexpr size_t dep_buf_ints() {
+  return (size_t)(dep_cells_y<R, W>() + W - 1) * (DEP_TX + W) + (dep_cells_y<R, W>() + W - 1) + 2;
+}
+template <typename R, int W> __host__ __device__ constexpr size_t dep_buf_bytes() {
+  return (dep_buf_vals<R, W>() * sizeof(R) + dep_buf_ints<R, W>() * sizeof(int) + 15) / 16 * 16;
+}
+template <typename R, int W> __host__ __device__ constexpr size_t deposit_smem() {
+  return 2 * dep_buf_bytes<R, W>() + 16 * sizeof(int);
 }
 
 // an int carried in a value slot (bit pattern)
@@ -369,169 +406,367 @@ template <> __device__ __forceinline__ void sts4<double>(double *p, double a, do
   *reinterpret_cast<double2 *>(p + 2) = make_double2(c, d);
 }
 
+// accumulators of a column pair: FP32 as packed pairs (one FFMA2 adds to both
+// columns), FP64 as two scalars
+template <typename R> struct PairAcc;
+template <> struct PairAcc<float> {
+  float2 a;
+  __device__ __forceinline__ void zero() { a = make_float2(0.f, 0.f); }
+  __device__ __forceinline__ void fma(float2 w, float v) { a = __ffma2_rn(w, make_float2(v, v), a); }
+  __device__ __forceinline__ float lo() const { return a.x; }
+  __device__ __forceinline__ float hi() const { return a.y; }
+};
+template <> struct PairAcc<double> {
+  double x, y;
+  __device__ __forceinline__ void zero() { x = 0.0; y = 0.0; }
+  __device__ __forceinline__ void fma(double2 w, double v) { x = __fma_rn(w.x, v, x); y = __fma_rn(w.y, v, y); }
+  __device__ __forceinline__ double lo() const { return x; }
+  __device__ __forceinline__ double hi() const { return y; }
+};
+template <typename R> struct Pair2;
+template <> struct Pair2<float> { using T = float2; };
+template <> struct Pair2<double> { using T = double2; };
+__device__ __forceinline__ float2 pmul(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
+__device__ __forceinline__ double2 pmul(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+
+// one value copied asynchronously from global to shared memory
+template <typename R> __device__ __forceinline__ void cp_async_val(R *sdst, const R *gsrc);
+template <> __device__ __forceinline__ void cp_async_val<float>(float *sdst, const float *gsrc) { cp_async4(sdst, gsrc); }
+template <> __device__ __forceinline__ void cp_async_val<double>(double *sdst, const double *gsrc) {
+  cp_async8(sdst, gsrc);
+}
+
+// named CTA barriers: barrier.sync waits until `n` threads (a multiple of 32) have
+// arrived, barrier.arrive counts the calling threads without waiting (their
+// shared-memory writes before it are visible to the threads that wait)
+__device__ __forceinline__ void nb_sync(int id, int n) {
+  __syncwarp();
+  asm volatile("barrier.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+__device__ __forceinline__ void nb_arrive(int id, int n) {
+  __syncwarp();
+  asm volatile("barrier.arrive %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+constexpr int DEP_BAR_FULL = 1, DEP_BAR_EMPTY = 3, DEP_BAR_PROD = 5;  // + group (0, 1)
+
+// The (tile, cell layer) position where share s starts.  A tile layer costs its
+// cells plus a fixed part (the staging round trip and hand-over of a bin layer),
+// counted as a quarter of a full tile.
+struct DepPos { int t, z; };
+__device__ __forceinline__ long long dep_layer_cost(int t, int ntx, int ext0, int ext1, int tw, int th) {
+  const int tx = t % ntx, ty = t / ntx;
+  return (long long)min(tw, ext0 - tx * tw) * min(th, ext1 - ty * th) + (tw * th) / 4;
+}
+__device__ inline DepPos dep_share_start(long long s, long long nshare, int ntx, int nt, int ext0, int ext1, int ext2,
+                                         int tw, int th) {
+  long long total = 0;
+  for (int t = 0; t < nt; t++) total += dep_layer_cost(t, ntx, ext0, ext1, tw, th) * ext2;
+  const long long P = s * total / nshare;
+  long long cum = 0;
+  for (int t = 0; t < nt; t++) {
+    const long long a = dep_layer_cost(t, ntx, ext0, ext1, tw, th);
+    const long long w = a * ext2;
+    if (P < cum + w) return DepPos{t, (int)((P - cum) / a)};
+    cum += w;
+  }
+  return DepPos{nt, 0};
+}
+
+template <typename R, int W> struct DepBuf {
+  R *recs, *wzs, *wxs, *wyp;
+  int *sraw, *rowo;
+  __device__ __forceinline__ DepBuf(unsigned char *base) {
+    constexpr int CAP = DepCfg<R, W>::cap, WS = DepCfg<R, W>::ws;
+    recs = reinterpret_cast<R *>(base);
+    wzs = recs + (size_t)4 * CAP;
+    wxs = wzs + (size_t)WS * CAP;
+    wyp = wxs + (size_t)W * CAP;
+    sraw = reinterpret_cast<int *>(wyp + (size_t)(W + 2) * CAP);
+    rowo = sraw + (dep_cells_y<R, W>() + W - 1) * (DEP_TX + W);
+  }
+};
+
 template <typename R, int W, int NV>
-__global__ void __launch_bounds__(DEP_THREADS, 2) k_deposit(PartGeom<R> g, const R *__restrict__ pos,
-                                                         const R *__restrict__ val, int vstride,
-                                                         const unsigned *__restrict__ start,
-                                                         const int *__restrict__ perm, R *__restrict__ mesh,
-                                                         int mstride, int ZC, int cap, int clear_mode) {
-  constexpr int BX = DEP_TX + W - 1, BY = DEP_TY + W - 1, WS = WStride<W>::v;
-  constexpr int NA = W + DEP_LB - 1;   // accumulator layers
-  constexpr int NROW = DEP_LB * BY;    // bin rows of one batch
-  static_assert(NROW <= 64, "one warp scans the bin rows of a batch");
+__global__ void __launch_bounds__(dep_threads<R, W>(), 1)
+    k_deposit(PartGeom<R> g, const R *__restrict__ pos, const R *__restrict__ val, int vstride,
+              const unsigned *__restrict__ start, const int *__restrict__ perm, R *__restrict__ mesh, int mstride,
+              int clear_mode, int TW, int TH) {
+  using P2 = typename Pair2<R>::T;
+  constexpr int CAP = DepCfg<R, W>::cap, WS = DepCfg<R, W>::ws;
+  constexpr int NCW = DepCfg<R, W>::ncw, NPG = DepCfg<R, W>::npg;
+  constexpr int NPT = 32 * NPG;            // threads of one producer group
+  constexpr int NBAR = 32 * (NCW + NPG);   // consumers + one group
+  constexpr int CY = dep_cells_y<R, W>();
+  constexpr int BX = DEP_TX + W - 1, BYB = CY + W - 1;
+  constexpr int NSR = BYB * (BX + 1);      // bin starts per layer
+  constexpr int KSR = (NSR + NPT - 1) / NPT;
+  static_assert(BYB <= 64, "one warp scans the bin rows of a layer");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  // x and y weights weight-major (threads reading consecutive particles hit
-  // consecutive banks), z weights and values particle-major for 16-byte loads; the
-  // value vector's last slot carries the particle's bin x within the tile
-  R *wxs = reinterpret_cast<R *>(smem_raw);  // [WS][cap]
-  R *wys = wxs + (size_t)WS * cap;           // [WS][cap]
-  R *wzs = wys + (size_t)WS * cap;           // [cap][WS]
-  R *vs = wzs + (size_t)WS * cap;            // [cap][4]
-  int *sraw = reinterpret_cast<int *>(vs + (size_t)4 * cap);  // [NROW][BX+1] start of bin (row clamp)
-  int *rowo = sraw + NROW * (BX + 1);                        // [NROW+1] staged offset of each row
+  int *share = reinterpret_cast<int *>(smem_raw + 2 * dep_buf_bytes<R, W>());  // [4] first and end position
 
-  const int tx = threadIdx.x % DEP_TX, ty = threadIdx.x / DEP_TX;
-  const int x0 = blockIdx.x * DEP_TX, y0 = blockIdx.y * DEP_TY;
-  const int zc0 = blockIdx.z * ZC, zc1 = min(zc0 + ZC, g.ext[2]);
-  const int cx = x0 + tx, cy = y0 + ty;
-  const bool active = cx < g.ext[0] && cy < g.ext[1];
+  // tiles of TW x TH cells (TW <= 32, TH <= CY, equal sizes chosen by the host)
+  const int ntx = (g.ext[0] + TW - 1) / TW, nty = (g.ext[1] + TH - 1) / TH, nt = ntx * nty;
+  const int BXr = TW + W - 1, BYr = TH + W - 1;  // bins per row and bin rows that reach a tile
+  if (threadIdx.x == 0) {
+    const DepPos a = dep_share_start(blockIdx.x, gridDim.x, ntx, nt, g.ext[0], g.ext[1], g.ext[2], TW, TH);
+    const DepPos b = dep_share_start(blockIdx.x + 1, gridDim.x, ntx, nt, g.ext[0], g.ext[1], g.ext[2], TW, TH);
+    share[0] = a.t; share[1] = a.z; share[2] = b.t; share[3] = b.z;
+  }
+  __syncthreads();
+  const int ta = share[0], za = share[1], tb = share[2], zb = share[3];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-  // acc[s] is cell layer bz0 - (W - 1) + s while the batch starting at bin layer
-  // bz0 is added; after the batch the first nl layers are final and the window
-  // shifts by nl
-  R acc[NA][NV];
-#pragma unroll
-  for (int s = 0; s < NA; s++)
-#pragma unroll
-    for (int c = 0; c < NV; c++) acc[s][c] = R(0);
-
-  const int bz_end = zc1 + W - 2;  // last bin layer (inclusive)
-  for (int bz0 = zc0; bz0 <= bz_end; bz0 += DEP_LB) {
-    const int nl = min(DEP_LB, bz_end - bz0 + 1);
-    // ---- bin starts of the batch's rows (clamped to the row end)
-    for (int i = threadIdx.x; i < NROW * (BX + 1); i += blockDim.x) {
-      const int row = i / (BX + 1), bx = i - row * (BX + 1);
-      const int l = row / BY, r = row - l * BY;
-      const int by = y0 + r, bz = bz0 + l;
-      int v = 0;
-      if (l < nl && by < g.nb[1] && bz < g.nb[2] && x0 < g.nb[0]) {
-        const unsigned rb = (unsigned)g.nb[0] * ((unsigned)by + (unsigned)g.nb[1] * (unsigned)bz);
-        v = (int)start[rb + (unsigned)min(x0 + bx, g.nb[0])];
-      }
-      sraw[i] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      // exclusive prefix of the row lengths, two rows per lane (NROW <= 64)
-      const int lane = threadIdx.x;
-      const int r0 = 2 * lane, r1 = 2 * lane + 1;
-      const int l0 = r0 < NROW ? sraw[r0 * (BX + 1) + BX] - sraw[r0 * (BX + 1)] : 0;
-      const int l1 = r1 < NROW ? sraw[r1 * (BX + 1) + BX] - sraw[r1 * (BX + 1)] : 0;
-      int x = l0 + l1;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-      }
-      const int ex = x - l0 - l1;
-      if (r0 <= NROW) rowo[r0] = ex;
-      if (r1 <= NROW) rowo[r1] = ex + l0;
-    }
-    __syncthreads();
-    const int total = rowo[NROW];
-    for (int c0 = 0; c0 < total; c0 += cap) {
-      const int c1 = min(total, c0 + cap);
-      // ---- stage particles [c0, c1) with their weights
-      for (int q = c0 + threadIdx.x; q < c1; q += blockDim.x) {
-        int lo = 0, hi = NROW - 1;  // last row with rowo[row] <= q
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (rowo[mid] <= q) lo = mid;
-          else hi = mid - 1;
-        }
-        const int gi = sraw[lo * (BX + 1)] + (q - rowo[lo]);
-        const int p = perm[gi];
-        const int i = q - c0;
-        R wv[3][WS];
-        long long bxi = 0;
-#pragma unroll
-        for (int e = 0; e < 3; e++) {
-          const R x = pos[(size_t)3 * p + e];
-          const long long b = base_index(x, g.xmin[e], g.c1dx[e]);
-          if (e == 0) bxi = b;
-          weights<R, W>(cell_offset<R>(x, g.xmin[e], g.dx[e], b, g.c1dx[e]), wv[e]);
-#pragma unroll
-          for (int t = W; t < WS; t++) wv[e][t] = R(0);
-        }
-#pragma unroll
-        for (int t = 0; t < W; t++) {
-          wxs[t * cap + i] = wv[0][t];
-          wys[t * cap + i] = wv[1][t];
-        }
-#pragma unroll
-        for (int t = 0; t < WS; t += 4) sts4<R>(wzs + i * WS + t, wv[2][t], wv[2][t + 1], wv[2][t + 2], wv[2][t + 3]);
-        R vv[4] = {R(0), R(0), R(0), R(0)};
-#pragma unroll
-        for (int c = 0; c < NV; c++) vv[c] = val[(size_t)vstride * p + c];
-        vv[3] = int_bits<R>((int)(bxi - g.blo[0]) - x0);
-        sts4<R>(vs + i * 4, vv[0], vv[1], vv[2], vv[3]);
-      }
-      __syncthreads();
-      if (active) {
-#pragma unroll
-        for (int l = 0; l < DEP_LB; l++) {
-          if (l < nl) {
-#pragma unroll 1
-            for (int ry = 0; ry < W; ry++) {
-              const int row = l * BY + ty + ry;  // bin row of the batch
-              const int sy = W - 1 - ry;         // stencil position of this cell row
-              const int *sr = sraw + row * (BX + 1);
-              const int b0 = sr[0];
-              const int lo = max(rowo[row] + sr[tx] - b0, c0);
-              const int hi = min(rowo[row] + sr[tx + W] - b0, c1);
-              const R *wyrow = wys + sy * cap - c0;
-              const R *wxtx = wxs + (W - 1 + tx) * cap - c0;  // wx[W - 1 - (bx - tx)] = wxtx[q - bx cap]
-#pragma unroll 1
-              for (int q = lo; q < hi; q++) {
-                const int i = q - c0;
-                R wz[WS], v[4];
-                lds4<R>(vs + i * 4, v);
-                lds4<R>(wzs + i * WS, wz);
-                if constexpr (WS == 8) lds4<R>(wzs + i * WS + 4, wz + 4);
-                const int bx = bits_int<R>(v[3]);
-                const R wxy = wxtx[q - bx * cap] * wyrow[q];
-#pragma unroll
-                for (int sz = 0; sz < W; sz++) {
-                  const R w = wxy * wz[sz];
-#pragma unroll
-                  for (int c = 0; c < NV; c++) acc[l + sz][c] += w * v[c];
-                }
+  if (warp >= NCW) {
+    // ======================================================== producers
+    const int grp = (warp - NCW) / NPG;            // bin layers L with L % 2 == grp
+    const int pt = threadIdx.x - 32 * (NCW + grp * NPG);
+    const int pw = pt >> 5;
+    DepBuf<R, W> B(smem_raw + grp * dep_buf_bytes<R, W>());
+    int L = 0;  // running bin-layer count of this CTA (both roles count alike)
+    int m = 0;  // chunks staged by this group
+    for (int t = ta; t <= tb && t < nt; t++) {
+      const int z0 = (t == ta) ? za : 0, z1 = (t == tb) ? zb : g.ext[2];
+      if (z0 >= z1) continue;
+      const int x0 = (t % ntx) * TW, y0 = (t / ntx) * TH;
+      for (int bz = z0; bz <= z1 + W - 2; bz++, L++) {
+        if ((L & 1) != grp) continue;
+        const bool zin = bz < g.nb[2] && x0 < g.nb[0];
+        int c0 = 0, total = 0;
+        do {
+          if (m >= 1) nb_sync(DEP_BAR_EMPTY + grp, NBAR);  // consumers are done with this buffer
+          // ---- bin starts of the layer's rows (clamped to the row end), copied
+          // asynchronously so that all of a thread's loads are in flight together
+#pragma unroll 4
+          for (int k = 0; k < KSR; k++) {
+            const int i = pt + k * NPT;
+            const int row = i / (BX + 1), bx = i - row * (BX + 1);
+            const int by = y0 + row;
+            if (i < NSR) {
+              if (zin && row < BYr && by < g.nb[1]) {
+                const unsigned rb = (unsigned)g.nb[0] * ((unsigned)by + (unsigned)g.nb[1] * (unsigned)bz);
+                cp_async4(B.sraw + i, start + rb + (unsigned)min(x0 + min(bx, BXr), g.nb[0]));
+              } else {
+                B.sraw[i] = 0;
               }
+            }
+          }
+          cp_async_commit();
+          cp_async_wait_all();
+          nb_sync(DEP_BAR_PROD + grp, NPT);
+          if (pw == 0) {
+            // exclusive prefix of the row lengths, two rows per lane (BYB <= 64)
+            int len[2];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const int row = 2 * lane + h;
+              len[h] = row < BYB ? B.sraw[row * (BX + 1) + BX] - B.sraw[row * (BX + 1)] : 0;
+            }
+            int x = len[0] + len[1];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+              const int y = __shfl_up_sync(0xffffffffu, x, o);
+              if (lane >= o) x += y;
+            }
+            const int ex = x - len[0] - len[1];
+            if (2 * lane <= BYB) B.rowo[2 * lane] = ex;
+            if (2 * lane + 1 <= BYB) B.rowo[2 * lane + 1] = ex + len[0];
+          }
+          nb_sync(DEP_BAR_PROD + grp, NPT);
+          total = B.rowo[BYB];
+          const int c1 = min(total, c0 + CAP);
+          // ---- stage particles [c0, c1).  Pass 1: each particle's index (row search
+          // and sorted order), then asynchronous copies of its position into its
+          // z-weight slots and of its values into its record, eight particles' loads
+          // in flight at a time and all copies of the thread outstanding together.
+          constexpr int U = 8;
+          for (int qb = c0 + pt; qb < c1; qb += U * NPT) {
+            int pp[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+              const int q = qb + u * NPT;
+              pp[u] = -1;
+              if (q < c1) {
+                int a = 0, bb = BYB - 1;  // last row with rowo[row] <= q
+                while (a < bb) {
+                  const int mid = (a + bb + 1) >> 1;
+                  if (B.rowo[mid] <= q) a = mid;
+                  else bb = mid - 1;
+                }
+                pp[u] = perm[B.sraw[a * (BX + 1)] + (q - B.rowo[a])];
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+              if (pp[u] < 0) continue;
+              const int i = qb + u * NPT - c0;
+#pragma unroll
+              for (int e = 0; e < 3; e++) cp_async_val<R>(B.wzs + (size_t)i * WS + e, pos + (size_t)3 * pp[u] + e);
+#pragma unroll
+              for (int c = 0; c < NV; c++) cp_async_val<R>(B.recs + (size_t)i * 4 + c, val + (size_t)vstride * pp[u] + c);
+            }
+          }
+          cp_async_commit();
+          cp_async_wait_all();
+          // Pass 2: weights from the staged positions (a thread reads only the copies
+          // it issued itself)
+#pragma unroll 2
+          for (int q = c0 + pt; q < c1; q += NPT) {
+            const int i = q - c0;
+            R wv[3][WS];
+            long long bxi = 0;
+#pragma unroll
+            for (int e = 0; e < 3; e++) {
+              const R x = B.wzs[(size_t)i * WS + e];
+              const long long b2 = base_index(x, g.xmin[e], g.c1dx[e]);
+              if (e == 0) bxi = b2;
+              weights<R, W>(cell_offset<R>(x, g.xmin[e], g.dx[e], b2, g.c1dx[e]), wv[e]);
+#pragma unroll
+              for (int tt = W; tt < WS; tt++) wv[e][tt] = R(0);
+            }
+#pragma unroll
+            for (int tt = 0; tt < W; tt++) {
+              B.wxs[tt * CAP + i] = wv[0][tt];
+              B.wyp[(tt + 1) * CAP + i] = wv[1][tt];
+            }
+            B.wyp[i] = R(0);
+            B.wyp[(W + 1) * CAP + i] = R(0);
+#pragma unroll
+            for (int tt = 0; tt < WS; tt += 4)
+              sts4<R>(B.wzs + i * WS + tt, wv[2][tt], wv[2][tt + 1], wv[2][tt + 2], wv[2][tt + 3]);
+            const int bx = (int)(bxi - g.blo[0]) - x0;
+            B.recs[(size_t)i * 4 + 3] = int_bits<R>(-bx * CAP);
+          }
+          nb_arrive(DEP_BAR_FULL + grp, NBAR);
+          m++;
+          c0 += CAP;
+        } while (c0 < total);
+      }
+    }
+    // drain: wait for the consumers' last hand-back so that every arrive on the
+    // EMPTY barrier has its matching wait
+    if (m >= 1) nb_sync(DEP_BAR_EMPTY + grp, NBAR);
+    return;
+  }
+
+  // ========================================================== consumers
+  const int tx = lane, ty = warp;
+  int L = 0;
+  for (int t = ta; t <= tb && t < nt; t++) {
+    const int z0 = (t == ta) ? za : 0, z1 = (t == tb) ? zb : g.ext[2];
+    if (z0 >= z1) continue;
+    const int x0 = (t % ntx) * TW, y0 = (t / ntx) * TH;
+    const int cx = x0 + tx, cy = y0 + 2 * ty;
+    const bool active = tx < TW && cx < g.ext[0] && 2 * ty < TH && cy < g.ext[1];
+    // acc[s] is cell layer bz - (W - 1) + s of the columns (cx, cy) and (cx, cy + 1)
+    // while bin layer bz is added
+    PairAcc<R> acc[W][NV];
+#pragma unroll
+    for (int s = 0; s < W; s++)
+#pragma unroll
+      for (int c = 0; c < NV; c++) acc[s][c].zero();
+    for (int bz = z0; bz <= z1 + W - 2; bz++, L++) {
+      const int b = L & 1;
+      DepBuf<R, W> B(smem_raw + b * dep_buf_bytes<R, W>());
+      int c0 = 0, total = 0;
+      do {
+        nb_sync(DEP_BAR_FULL + b, NBAR);
+        total = B.rowo[BYB];
+        const int c1 = min(total, c0 + CAP);
+        if (active && c1 > c0) {
+          // this thread's W + 1 particle ranges (staged order), bin rows 2 ty .. 2 ty + W
+          // (2 ty + W <= BYB - 1: every row exists), clamped to [c0, c1); one loop per
+          // row with the row's y-weight offsets as constants, staged data addressed by
+          // byte offsets from the shared-memory base
+          const unsigned char *sb = smem_raw + b * dep_buf_bytes<R, W>();
+          constexpr unsigned O_WZ = 4u * CAP * sizeof(R), O_WX = O_WZ + (unsigned)WS * CAP * sizeof(R);
+          constexpr unsigned O_WY = O_WX + (unsigned)W * CAP * sizeof(R);
+#pragma unroll
+          for (int r = 0; r <= W; r++) {
+            const int *sr = B.sraw + (2 * ty + r) * (BX + 1);
+            const int l = B.rowo[2 * ty + r] + sr[tx] - sr[0];
+            const int q0 = max(l, c0) - c0, q1 = min(l + sr[tx + W] - sr[tx], c1) - c0;
+            // row r: y weights of the pair are wyp[W - r] and wyp[W + 1 - r]
+            const unsigned char *prec = sb + (size_t)q0 * 4 * sizeof(R);
+            const unsigned char *pwz = sb + O_WZ + (size_t)q0 * WS * sizeof(R);
+            const unsigned char *pwy = sb + O_WY + (unsigned)(W - r) * CAP * sizeof(R) + (size_t)q0 * sizeof(R);
+            const unsigned char *pwx = sb + O_WX + (unsigned)(W - 1 + tx) * CAP * sizeof(R) + (size_t)q0 * sizeof(R);
+            // two particles per iteration (their loads in flight together), then the
+            // odd one
+            auto visit = [&](const R *v, const R *wz, R wx, R wy0, R wy1) {
+              P2 wxy;
+              wxy.x = wx * wy0;
+              wxy.y = wx * wy1;
+#pragma unroll
+              for (int sz = 0; sz < W; sz++) {
+                const P2 w = pmul(wxy, wz[sz]);
+#pragma unroll
+                for (int c = 0; c < NV; c++) acc[sz][c].fma(w, v[c]);
+              }
+            };
+            int q = q0;
+#pragma unroll 1
+            for (; q + 1 < q1; q += 2) {
+              R v[2][4], wz[2][WS];
+#pragma unroll
+              for (int h = 0; h < 2; h++) {
+                lds4<R>(reinterpret_cast<const R *>(prec) + 4 * h, v[h]);
+                lds4<R>(reinterpret_cast<const R *>(pwz) + WS * h, wz[h]);
+                if constexpr (WS == 8) lds4<R>(reinterpret_cast<const R *>(pwz) + WS * h + 4, wz[h] + 4);
+              }
+              R wx[2], wy0[2], wy1[2];
+#pragma unroll
+              for (int h = 0; h < 2; h++) {
+                wx[h] = *reinterpret_cast<const R *>(pwx + (ptrdiff_t)(bits_int<R>(v[h][3]) + h) * (ptrdiff_t)sizeof(R));
+                wy0[h] = *reinterpret_cast<const R *>(pwy + h * sizeof(R));
+                wy1[h] = *reinterpret_cast<const R *>(pwy + (CAP + h) * sizeof(R));
+              }
+              visit(v[0], wz[0], wx[0], wy0[0], wy1[0]);
+              visit(v[1], wz[1], wx[1], wy0[1], wy1[1]);
+              prec += 8 * sizeof(R);
+              pwz += 2 * WS * sizeof(R);
+              pwy += 2 * sizeof(R);
+              pwx += 2 * sizeof(R);
+            }
+            if (q < q1) {
+              R v[4], wz[WS];
+              lds4<R>(reinterpret_cast<const R *>(prec), v);
+              lds4<R>(reinterpret_cast<const R *>(pwz), wz);
+              if constexpr (WS == 8) lds4<R>(reinterpret_cast<const R *>(pwz) + 4, wz + 4);
+              const R wx = *reinterpret_cast<const R *>(pwx + (ptrdiff_t)bits_int<R>(v[3]) * (ptrdiff_t)sizeof(R));
+              visit(v, wz, wx, *reinterpret_cast<const R *>(pwy), *reinterpret_cast<const R *>(pwy + CAP * sizeof(R)));
+            }
+          }
+        }
+        nb_arrive(DEP_BAR_EMPTY + b, NBAR);
+        c0 += CAP;
+      } while (c0 < total);
+      // ---- cell layer bz - (W - 1) is complete
+      const int cz = bz - (W - 1);
+      if (active && cz >= z0 && cz < z1) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int yy = cy + h;
+          if (2 * ty + h < TH && yy < g.ext[1]) {
+            const size_t m = (((size_t)cz * g.ext[1] + yy) * g.ext[0] + cx) * mstride;
+            const int ii = cx + g.lo[0], jj = yy + g.lo[1], kk = cz + g.lo[2];
+            const bool ghost = ii < 1 || ii > g.nint[0] || jj < 1 || jj > g.nint[1] || kk < 1 || kk > g.nint[2];
+            const bool overwrite = clear_mode == 1 || (clear_mode == 2 && ghost);
+#pragma unroll
+            for (int c = 0; c < NV; c++) {
+              const R a = h ? acc[0][c].hi() : acc[0][c].lo();
+              mesh[m + c] = overwrite ? a : mesh[m + c] + a;
             }
           }
         }
       }
-      __syncthreads();
+#pragma unroll
+      for (int s = 0; s < W; s++)
+#pragma unroll
+        for (int c = 0; c < NV; c++) {
+          if (s + 1 < W) acc[s][c] = acc[s + 1][c];
+          else acc[s][c].zero();
+        }
     }
-    // ---- cell layers bz0 - (W - 1) .. + nl - 1 are complete
-#pragma unroll
-    for (int l = 0; l < DEP_LB; l++) {
-      const int cz = bz0 - (W - 1) + l;
-      if (l < nl && active && cz >= zc0 && cz < zc1) {
-        const size_t m = (((size_t)cz * g.ext[1] + cy) * g.ext[0] + cx) * mstride;
-        const int ii = cx + g.lo[0], jj = cy + g.lo[1], kk = cz + g.lo[2];
-        const bool ghost = ii < 1 || ii > g.nint[0] || jj < 1 || jj > g.nint[1] || kk < 1 || kk > g.nint[2];
-        const bool overwrite = clear_mode == 1 || (clear_mode == 2 && ghost);
-#pragma unroll
-        for (int c = 0; c < NV; c++) mesh[m + c] = overwrite ? acc[l][c] : mesh[m + c] + acc[l][c];
-      }
-    }
-    if (nl == DEP_LB) {
-#pragma unroll
-      for (int s = 0; s < NA; s++)
-#pragma unroll
-        for (int c = 0; c < NV; c++) acc[s][c] = (s + DEP_LB < NA) ? acc[s + DEP_LB][c] : R(0);
-    }  // a shorter batch is the last one
   }
 }
 

@@ -693,6 +693,28 @@ static int run_bin_sort(const pmgpu_topo *t, int order, const R *pos, int n, Par
   return 0;
 }
 
+// One deposition launch: a persistent grid of one CTA per SM (fewer for small
+// grids), each taking an equal share of the cells.
+template <typename R, int W, int NV>
+static int launch_deposit(const PartGeom<R> &g, const R *pos, const R *vp, int vstride, PartScratchRefs s,
+                          const int *perm, R *mp, int mstride, int clear_mode, cudaStream_t st, const char *caller) {
+  const size_t smem = deposit_smem<R, W>();
+  const int threads = dep_threads<R, W>();
+  if (smem_attr((const void *)k_deposit<R, W, NV>, smem, caller)) return -1;
+  // tiles of equal size: as many as 32 x CY tiles would need, cells spread evenly
+  const int CY = dep_cells_y<R, W>();
+  const long long ntx = (g.ext[0] + DEP_TX - 1) / DEP_TX, nty = (g.ext[1] + CY - 1) / CY;
+  const int tw = (int)((g.ext[0] + ntx - 1) / ntx), th = (int)((g.ext[1] + nty - 1) / nty);
+  const long long units = ntx * nty * g.ext[2];
+  const int grid = (int)std::max<long long>(1, std::min<long long>(num_sms(), units));
+  KTimer kt_(KC_DEPOSIT, st);
+  k_deposit<R, W, NV><<<grid, threads, smem, st>>>(g, pos, vp, vstride, s.start->as<unsigned>(), perm, mp, mstride,
+                                                    clear_mode, tw, th);
+  PM_LAUNCHED();
+  CKL(caller);
+  return 0;
+}
+
 // P2M on device arrays.  clear_mode: 0 add, 1 clear, 2 clear ghosts.  On return
 // *perm_out (if given) points at the sorted particle order.
 template <typename R>
@@ -704,27 +726,16 @@ static int run_p2m(const pmgpu_topo *t, int order, const R *pos, const R *val, i
   PartGeom<R> g = part_geom<R>(t, W);
   const int *perm = s.val2->as<int>();
   // deposition, components in groups of at most three
-  const int zc = (W == 4) ? 32 : 30;
-  dim3 grid((g.ext[0] + DEP_TX - 1) / DEP_TX, (g.ext[1] + DEP_TY - 1) / DEP_TY, (g.ext[2] + zc - 1) / zc);
   for (int c0 = 0; c0 < nvar;) {
     const int nv = (nvar - c0 >= 3) ? 3 : 1;
-    int cap = (sizeof(R) == 4) ? 1024 : 512;
-    if (W == 6) cap = cap * 3 / 4;
-    const size_t smem = (W == 4) ? deposit_smem<R, 4>(cap) : deposit_smem<R, 6>(cap);
     const R *vp = val + c0;
     R *mp = mesh + c0;
-    const int *pp = perm;
-#define DEP_CASE(WW, NVV)                                                                                  \
-  if (W == WW && nv == NVV) {                                                                              \
-    if (smem_attr((const void *)k_deposit<R, WW, NVV>, smem, caller)) return -1;                           \
-    KTimer kt_(KC_DEPOSIT, st);                                                                            \
-    k_deposit<R, WW, NVV><<<grid, DEP_THREADS, smem, st>>>(g, pos, vp, nvar, s.start->as<unsigned>(),      \
-                                                                pp, mp, nvar_mesh, zc, cap, clear_mode);    \
-    PM_LAUNCHED();                                                                                         \
-  }
-    DEP_CASE(4, 1) DEP_CASE(4, 3) DEP_CASE(6, 1) DEP_CASE(6, 3)
-#undef DEP_CASE
-    CKL(caller);
+    int rc = 0;
+    if (W == 4) rc = (nv == 3) ? launch_deposit<R, 4, 3>(g, pos, vp, nvar, s, perm, mp, nvar_mesh, clear_mode, st, caller)
+                               : launch_deposit<R, 4, 1>(g, pos, vp, nvar, s, perm, mp, nvar_mesh, clear_mode, st, caller);
+    else rc = (nv == 3) ? launch_deposit<R, 6, 3>(g, pos, vp, nvar, s, perm, mp, nvar_mesh, clear_mode, st, caller)
+                        : launch_deposit<R, 6, 1>(g, pos, vp, nvar, s, perm, mp, nvar_mesh, clear_mode, st, caller);
+    if (rc) return -1;
     c0 += nv;
   }
   // components beyond nvar in the mesh are left alone; a wider mesh is an error upstream
