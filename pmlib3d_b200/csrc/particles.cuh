@@ -374,10 +374,15 @@ template <typename R, int W> __host__ __device__ constexpr size_t dep_buf_ints()
   return (size_t)(dep_cells_y<R, W>() + W - 1) * (DEP_TX + W) + (dep_cells_y<R, W>() + W - 1) + 2;
 }
 template <typename R, int W> __host__ __device__ constexpr size_t dep_buf_bytes() {
-  return (dep_buf_vals<R, W>() * sizeof(R) + dep_buf_ints<R, W>() * sizeof(int) + 15) / 16 * 16;
+  return (dep_buf_vals<R, W>() * sizeof(R) + 15) / 16 * 16;
 }
+template <typename R, int W> __host__ __device__ constexpr size_t dep_slot_bytes() {
+  return (dep_buf_ints<R, W>() * sizeof(int) + 15) / 16 * 16;
+}
+// two staging buffers, four bin-start tables (two per producer group, alternating), the
+// CTA's share
 template <typename R, int W> __host__ __device__ constexpr size_t deposit_smem() {
-  return 2 * dep_buf_bytes<R, W>() + 16 * sizeof(int);
+  return 2 * dep_buf_bytes<R, W>() + 4 * dep_slot_bytes<R, W>() + 16 * sizeof(int);
 }
 
 // an int carried in a value slot (bit pattern)
@@ -472,16 +477,17 @@ __device__ inline DepPos dep_share_start(long long s, long long nshare, int ntx,
   return DepPos{nt, 0};
 }
 
+// staging buffer of producer group `grp` and its bin-start table `par`
 template <typename R, int W> struct DepBuf {
   R *recs, *wzs, *wxs, *wyp;
   int *sraw, *rowo;
-  __device__ __forceinline__ DepBuf(unsigned char *base) {
+  __device__ __forceinline__ DepBuf(unsigned char *smem, int grp, int par) {
     constexpr int CAP = DepCfg<R, W>::cap, WS = DepCfg<R, W>::ws;
-    recs = reinterpret_cast<R *>(base);
+    recs = reinterpret_cast<R *>(smem + grp * dep_buf_bytes<R, W>());
     wzs = recs + (size_t)4 * CAP;
     wxs = wzs + (size_t)WS * CAP;
     wyp = wxs + (size_t)W * CAP;
-    sraw = reinterpret_cast<int *>(wyp + (size_t)(W + 2) * CAP);
+    sraw = reinterpret_cast<int *>(smem + 2 * dep_buf_bytes<R, W>() + (2 * grp + par) * dep_slot_bytes<R, W>());
     rowo = sraw + (dep_cells_y<R, W>() + W - 1) * (DEP_TX + W);
   }
 };
@@ -502,7 +508,7 @@ __global__ void __launch_bounds__(dep_threads<R, W>(), 1)
   constexpr int KSR = (NSR + NPT - 1) / NPT;
   static_assert(BYB <= 64, "one warp scans the bin rows of a layer");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  int *share = reinterpret_cast<int *>(smem_raw + 2 * dep_buf_bytes<R, W>());  // [4] first and end position
+  int *share = reinterpret_cast<int *>(smem_raw + 2 * dep_buf_bytes<R, W>() + 4 * dep_slot_bytes<R, W>());
 
   // tiles of TW x TH cells (TW <= 32, TH <= CY, equal sizes chosen by the host)
   const int ntx = (g.ext[0] + TW - 1) / TW, nty = (g.ext[1] + TH - 1) / TH, nt = ntx * nty;
@@ -521,7 +527,6 @@ __global__ void __launch_bounds__(dep_threads<R, W>(), 1)
     const int grp = (warp - NCW) / NPG;            // bin layers L with L % 2 == grp
     const int pt = threadIdx.x - 32 * (NCW + grp * NPG);
     const int pw = pt >> 5;
-    DepBuf<R, W> B(smem_raw + grp * dep_buf_bytes<R, W>());
     int L = 0;  // running bin-layer count of this CTA (both roles count alike)
     int m = 0;  // chunks staged by this group
     for (int t = ta; t <= tb && t < nt; t++) {
@@ -533,7 +538,9 @@ __global__ void __launch_bounds__(dep_threads<R, W>(), 1)
         const bool zin = bz < g.nb[2] && x0 < g.nb[0];
         int c0 = 0, total = 0;
         do {
-          if (m >= 1) nb_sync(DEP_BAR_EMPTY + grp, NBAR);  // consumers are done with this buffer
+          // this chunk's bin-start table was last read for the group's chunk m - 2,
+          // which the consumers have handed back: it is filled before the buffer is free
+          DepBuf<R, W> B(smem_raw, grp, m & 1);
           // ---- bin starts of the layer's rows (clamped to the row end), copied
           // asynchronously so that all of a thread's loads are in flight together
 #pragma unroll 4
@@ -579,8 +586,8 @@ __global__ void __launch_bounds__(dep_threads<R, W>(), 1)
           // z-weight slots and of its values into its record, eight particles' loads
           // in flight at a time and all copies of the thread outstanding together.
           constexpr int U = 8;
-          for (int qb = c0 + pt; qb < c1; qb += U * NPT) {
-            int pp[U];
+          int pp[U];
+          auto indices = [&](int qb) {
 #pragma unroll
             for (int u = 0; u < U; u++) {
               const int q = qb + u * NPT;
@@ -595,6 +602,12 @@ __global__ void __launch_bounds__(dep_threads<R, W>(), 1)
                 pp[u] = perm[B.sraw[a * (BX + 1)] + (q - B.rowo[a])];
               }
             }
+          };
+          // the first batch's indices are loaded before the buffer is free
+          indices(c0 + pt);
+          if (m >= 1) nb_sync(DEP_BAR_EMPTY + grp, NBAR);  // consumers are done with this buffer
+          for (int qb = c0 + pt; qb < c1; qb += U * NPT) {
+            if (qb != c0 + pt) indices(qb);
 #pragma unroll
             for (int u = 0; u < U; u++) {
               if (pp[u] < 0) continue;
@@ -651,6 +664,7 @@ __global__ void __launch_bounds__(dep_threads<R, W>(), 1)
   // ========================================================== consumers
   const int tx = lane, ty = warp;
   int L = 0;
+  int mc0 = 0, mc1 = 0;  // chunks taken from each producer group (their bin-start tables alternate)
   for (int t = ta; t <= tb && t < nt; t++) {
     const int z0 = (t == ta) ? za : 0, z1 = (t == tb) ? zb : g.ext[2];
     if (z0 >= z1) continue;
@@ -666,9 +680,10 @@ __global__ void __launch_bounds__(dep_threads<R, W>(), 1)
       for (int c = 0; c < NV; c++) acc[s][c].zero();
     for (int bz = z0; bz <= z1 + W - 2; bz++, L++) {
       const int b = L & 1;
-      DepBuf<R, W> B(smem_raw + b * dep_buf_bytes<R, W>());
       int c0 = 0, total = 0;
       do {
+        const int mcb = b ? mc1 : mc0;
+        DepBuf<R, W> B(smem_raw, b, mcb & 1);
         nb_sync(DEP_BAR_FULL + b, NBAR);
         total = B.rowo[BYB];
         const int c1 = min(total, c0 + CAP);
@@ -738,6 +753,8 @@ __global__ void __launch_bounds__(dep_threads<R, W>(), 1)
           }
         }
         nb_arrive(DEP_BAR_EMPTY + b, NBAR);
+        if (b) mc1++;
+        else mc0++;
         c0 += CAP;
       } while (c0 < total);
       // ---- cell layer bz - (W - 1) is complete

@@ -52,23 +52,32 @@ def test_served_results_equal_alone(precision):
 def test_served_work_overlaps_on_device():
     """Bursts of requests on four slots with plans resident from a first burst of the
     same grids: at least two solves run on the device at the same time (their CUDA
-    event intervals overlap), and every result is the same as the request alone."""
+    event intervals overlap), and every result is the same as the request alone.
+    Whether two intervals overlap depends on how fast the host queues the solves
+    against how long each runs, so the resident burst is repeated (up to three times)
+    until one shows the overlap; every burst's results are checked."""
     import torch
     params = P.make_params(order=6, kernel=1, radius=2.0, interp=3)
     srv = S.Server(params, precision=P.FP32, slots=4, budget=8 << 30)
     first = S.request_stream(8, rate=1e6, seed=5, nmin=96, nmax=128)
     assert srv.run(first)["solves"] == 8
-    reqs = S.request_stream(8, rate=1e6, seed=5, nmin=96, nmax=128)  # the same grids, new fields
-    for r in reqs:
-        r.vort = (r.vort * 0.25).contiguous()
-    rep = srv.run(reqs)
-    assert rep["solves"] == 8 and rep["new_plans"] == 0
-    assert rep["max_inflight"] >= 2 and rep["max_on_device"] >= 2, rep
-    pairs = sum(1 for a in srv.finished for b in srv.finished
-                if a.rid < b.rid and a.dev_start_ms < b.dev_end_ms and b.dev_start_ms < a.dev_end_ms)
-    assert pairs >= 1
-    for r in srv.finished:
-        assert torch.equal(r.vel, _alone(r, params, P.FP32)), r.rid
+    overlapped = False
+    reports = []
+    for attempt in range(3):
+        reqs = S.request_stream(8, rate=1e6, seed=5, nmin=96, nmax=128)  # the same grids, new fields
+        for r in reqs:
+            r.vort = (r.vort * (0.25 + 0.25 * attempt)).contiguous()
+        rep = srv.run(reqs)
+        reports.append(rep)
+        assert rep["solves"] == 8 and rep["new_plans"] == 0
+        for r in srv.finished:
+            assert torch.equal(r.vel, _alone(r, params, P.FP32)), r.rid
+        pairs = sum(1 for a in srv.finished for b in srv.finished
+                    if a.rid < b.rid and a.dev_start_ms < b.dev_end_ms and b.dev_start_ms < a.dev_end_ms)
+        if rep["max_inflight"] >= 2 and rep["max_on_device"] >= 2 and pairs >= 1:
+            overlapped = True
+            break
+    assert overlapped, reports
     srv.close()
 
 
