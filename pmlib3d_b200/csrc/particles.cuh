@@ -138,26 +138,61 @@ __global__ void k_place(const unsigned *__restrict__ key, const unsigned *__rest
 // sorted in place by one thread; larger bins go to an overflow list (ovf[0] =
 // count, ovf[1..] = bins) for k_fixup_big.  The sentinel bin is not needed in order.
 constexpr int FIX_SMALL = 32;
+// one bin [s, e) of the stable fix-up; bins of up to eight ids are sorted in
+// registers (all loads in flight together), larger ones in place
+__device__ __forceinline__ void fixup_bin(unsigned b, unsigned s, unsigned e, int *__restrict__ order,
+                                          unsigned *__restrict__ ovf) {
+  const unsigned k = e - s;
+  if (k < 2) return;
+  if (k > (unsigned)FIX_SMALL) {
+    const unsigned i = atomicAdd(&ovf[0], 1u);
+    ovf[1 + i] = b;
+    return;
+  }
+  int *o = order + s;
+  if (k <= 8) {
+    int v[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = (unsigned)i < k ? o[i] : 0x7fffffff;
+#pragma unroll
+    for (int i = 1; i < 8; i++)
+#pragma unroll
+      for (int j = i; j > 0; j--) {
+        const int a = v[j - 1], c = v[j];
+        v[j - 1] = min(a, c);
+        v[j] = max(a, c);
+      }
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+      if ((unsigned)i < k) o[i] = v[i];
+    return;
+  }
+  for (unsigned i = 1; i < k; i++) {
+    const int v = o[i];
+    unsigned j = i;
+    while (j > 0 && o[j - 1] > v) {
+      o[j] = o[j - 1];
+      j--;
+    }
+    o[j] = v;
+  }
+}
+// a thread takes four consecutive bins (one 16-byte load of their starts and the
+// next bin's start)
 __global__ void k_fixup_small(const unsigned *__restrict__ start, unsigned nbins, int *__restrict__ order,
                               unsigned *__restrict__ ovf) {
-  for (unsigned b = blockIdx.x * blockDim.x + threadIdx.x; b < nbins; b += gridDim.x * blockDim.x) {
-    const unsigned s = start[b], e = start[b + 1];
-    const unsigned k = e - s;
-    if (k < 2) continue;
-    if (k > (unsigned)FIX_SMALL) {
-      const unsigned i = atomicAdd(&ovf[0], 1u);
-      ovf[1 + i] = b;
-      continue;
-    }
-    int *o = order + s;
-    for (unsigned i = 1; i < k; i++) {
-      const int v = o[i];
-      unsigned j = i;
-      while (j > 0 && o[j - 1] > v) {
-        o[j] = o[j - 1];
-        j--;
-      }
-      o[j] = v;
+  const unsigned ngroups = (nbins + 3) / 4;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < ngroups; t += gridDim.x * blockDim.x) {
+    const unsigned b0 = 4 * t;
+    if (b0 + 4 <= nbins) {
+      const uint4 v = *reinterpret_cast<const uint4 *>(start + b0);
+      const unsigned e3 = start[b0 + 4];
+      fixup_bin(b0, v.x, v.y, order, ovf);
+      fixup_bin(b0 + 1, v.y, v.z, order, ovf);
+      fixup_bin(b0 + 2, v.z, v.w, order, ovf);
+      fixup_bin(b0 + 3, v.w, e3, order, ovf);
+    } else {
+      for (unsigned b = b0; b < nbins; b++) fixup_bin(b, start[b], start[b + 1], order, ovf);
     }
   }
 }
@@ -238,7 +273,7 @@ __global__ void __launch_bounds__(FIX_THREADS) k_fixup_big(const unsigned *__res
 
 // ------------------------------------------------------------------ scans (exclusive, u32)
 constexpr int SCAN_THREADS = 1024;
-constexpr int SCAN_PER_THREAD = 4;
+constexpr int SCAN_PER_THREAD = 16;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_PER_THREAD;
 
 __device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned *warp_sums, unsigned *total) {
@@ -269,15 +304,32 @@ __device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned *w
   return r;
 }
 
+// a thread's SCAN_PER_THREAD consecutive values (16-byte loads inside the array; the
+// arrays scanned here start on 16-byte boundaries)
+static_assert(SCAN_PER_THREAD % 4 == 0, "scan loads are 16-byte vectors");
+__device__ __forceinline__ void scan_load(const unsigned *__restrict__ in, size_t n, size_t base, unsigned *v) {
+  if (base + SCAN_PER_THREAD <= n) {
+#pragma unroll
+    for (int i = 0; i < SCAN_PER_THREAD; i += 4) {
+      const uint4 q = *reinterpret_cast<const uint4 *>(in + base + i);
+      v[i] = q.x; v[i + 1] = q.y; v[i + 2] = q.z; v[i + 3] = q.w;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < SCAN_PER_THREAD; i++) v[i] = (base + i < n) ? in[base + i] : 0u;
+  }
+}
+
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const unsigned *__restrict__ in, size_t n,
                                                               unsigned *__restrict__ part) {
   __shared__ unsigned ws[32];
   __shared__ unsigned tot;
   const size_t base = (size_t)blockIdx.x * SCAN_TILE + (size_t)threadIdx.x * SCAN_PER_THREAD;
+  unsigned v[SCAN_PER_THREAD];
+  scan_load(in, n, base, v);
   unsigned s = 0;
 #pragma unroll
-  for (int i = 0; i < SCAN_PER_THREAD; i++)
-    if (base + i < n) s += in[base + i];
+  for (int i = 0; i < SCAN_PER_THREAD; i++) s += v[i];
   block_exclusive_scan(s, ws, &tot);
   if (threadIdx.x == 0) part[blockIdx.x] = tot;
 }
@@ -306,17 +358,25 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(const unsigned *__r
   __shared__ unsigned tot;
   const size_t base = (size_t)blockIdx.x * SCAN_TILE + (size_t)threadIdx.x * SCAN_PER_THREAD;
   unsigned v[SCAN_PER_THREAD];
+  scan_load(in, n, base, v);
   unsigned s = 0;
 #pragma unroll
-  for (int i = 0; i < SCAN_PER_THREAD; i++) {
-    v[i] = (base + i < n) ? in[base + i] : 0u;
-    s += v[i];
-  }
+  for (int i = 0; i < SCAN_PER_THREAD; i++) s += v[i];
   unsigned off = block_exclusive_scan(s, ws, &tot) + part[blockIdx.x];
+  unsigned o[SCAN_PER_THREAD];
 #pragma unroll
   for (int i = 0; i < SCAN_PER_THREAD; i++) {
-    if (base + i < n) out[base + i] = off;
+    o[i] = off;
     off += v[i];
+  }
+  if (base + SCAN_PER_THREAD <= n) {
+#pragma unroll
+    for (int i = 0; i < SCAN_PER_THREAD; i += 4)
+      *reinterpret_cast<uint4 *>(out + base + i) = make_uint4(o[i], o[i + 1], o[i + 2], o[i + 3]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < SCAN_PER_THREAD; i++)
+      if (base + i < n) out[base + i] = o[i];
   }
 }
 

@@ -683,7 +683,7 @@ static int run_bin_sort(const pmgpu_topo *t, int order, const R *pos, int n, Par
     const int nblk = std::min((n + 255) / 256, 148 * 32);
     { KTimer kt_(KC_PLACE, st); k_place<<<nblk, 256, 0, st>>>(keys, ranks, n, s.start->as<unsigned>(), perm); }
     PM_LAUNCHED();
-    const int nbb = (int)std::min<unsigned>((g.nbins + 255) / 256, 148u * 32u);
+    const int nbb = (int)std::min<unsigned>(((g.nbins + 3) / 4 + 255) / 256, 148u * 32u);
     { KTimer kt_(KC_FIXUP, st); k_fixup_small<<<std::max(nbb, 1), 256, 0, st>>>(s.start->as<unsigned>(), g.nbins, perm, s.hist->as<unsigned>()); }
     PM_LAUNCHED();
     { KTimer kt_(KC_FIXUP, st); k_fixup_big<<<num_sms(), FIX_THREADS, 0, st>>>(s.start->as<unsigned>(), s.hist->as<unsigned>(), perm, s.key2->as<int>()); }
