@@ -84,45 +84,31 @@ __device__ __forceinline__ R cell_offset(R x, R xmin, R dx, long long b, R scale
 // cuboid, or which lie outside [xmin, xmax] across a periodic face (all weights
 // zeroed, :229-246), get the sentinel key nbins and are skipped by P2M (they still
 // take a slot, so the sorted order is a permutation of all particles).
-// rank = the particle's provisional slot within its bin: lanes of a warp that share
-// a key take consecutive slots in lane order, one atomic per key and warp.
+// rank = the particle's provisional slot within its bin (one atomic per particle; the
+// order within a bin is put right by the stable fix-up).
 template <typename R, int W>
 __global__ void k_bin(PartGeom<R> g, const R *__restrict__ pos, int n, unsigned *__restrict__ key,
                       unsigned *__restrict__ rank, unsigned *__restrict__ counts) {
   constexpr int off = Stencil<W>::off;
-  const int lane = threadIdx.x & 31;
   const int stride = gridDim.x * blockDim.x;
-  // the loop runs whole warps so that the warp-wide match below sees every lane
-  for (int p0 = blockIdx.x * blockDim.x; p0 < n; p0 += stride) {
-    const int p = p0 + (int)threadIdx.x;
-    const bool valid = p < n;
-    unsigned k = 0xFFFFFFFFu;
-    if (valid) {
-      bool ok = true;
-      long long bi[3];
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+    bool ok = true;
+    long long bi[3];
 #pragma unroll
-      for (int e = 0; e < 3; e++) {
-        const R x = pos[(size_t)3 * p + e];
-        const long long b = base_index(x, g.xmin[e], g.c1dx[e]);
-        const long long first = b - off, last = b - off + W - 1;
-        const int hi = g.lo[e] + g.ext[e] - 1;
-        if (!(last >= g.lo[e] && first <= hi)) ok = false;
-        if (g.bclo[e] != 0 && x < g.xmin[e]) ok = false;
-        if (g.bchi[e] != 0 && x > g.xmax[e]) ok = false;
-        bi[e] = b - g.blo[e];
-      }
-      k = g.nbins;
-      if (ok) k = (unsigned)(bi[0] + (long long)g.nb[0] * (bi[1] + (long long)g.nb[1] * bi[2]));
+    for (int e = 0; e < 3; e++) {
+      const R x = pos[(size_t)3 * p + e];
+      const long long b = base_index(x, g.xmin[e], g.c1dx[e]);
+      const long long first = b - off, last = b - off + W - 1;
+      const int hi = g.lo[e] + g.ext[e] - 1;
+      if (!(last >= g.lo[e] && first <= hi)) ok = false;
+      if (g.bclo[e] != 0 && x < g.xmin[e]) ok = false;
+      if (g.bchi[e] != 0 && x > g.xmax[e]) ok = false;
+      bi[e] = b - g.blo[e];
     }
-    const unsigned peers = __match_any_sync(0xffffffffu, k);
-    const int leader = __ffs(peers) - 1;
-    unsigned base = 0;
-    if (valid && lane == leader) base = atomicAdd(&counts[k], (unsigned)__popc(peers));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (valid) {
-      key[p] = k;
-      rank[p] = base + (unsigned)__popc(peers & ((1u << lane) - 1u));
-    }
+    unsigned k = g.nbins;
+    if (ok) k = (unsigned)(bi[0] + (long long)g.nb[0] * (bi[1] + (long long)g.nb[1] * bi[2]));
+    key[p] = k;
+    rank[p] = atomicAdd(&counts[k], 1u);
   }
 }
 
