@@ -46,6 +46,17 @@ using LinesKernel = void (*)(SolveGeom<R>, LineTiles, const typename cplx_t<R>::
 // (nullptr: none compiled); defined in passes_ct_*.cu
 LinesKernel<float> ct_lines_f32(const RegPlan &rp, int TK);
 LinesKernel<double> ct_lines_f64(const RegPlan &rp, int TK);
+// x passes (k_rxfwd / k_rxinv and their compile-time-plan instances)
+template <typename R>
+using RxfKernel = void (*)(SolveGeom<R>, const R *, typename cplx_t<R>::type *, int, int, int, FastDiv);
+template <typename R>
+using RxiKernel = void (*)(SolveGeom<R>, const typename cplx_t<R>::type *, R *, int, int, FastDiv);
+// the compile-time-plan x passes of 3-component fields for plan rp, rows per tile RB,
+// real row length P0 and spectrum pitch Hp (nullptr: none compiled); passes_ct_*.cu
+RxfKernel<float> ct_rxfwd_f32(const RegPlan &rp, int RB, int P0, int Hp);
+RxiKernel<float> ct_rxinv_f32(const RegPlan &rp, int RB, int P0, int Hp);
+RxfKernel<double> ct_rxfwd_f64(const RegPlan &rp, int RB, int P0, int Hp);
+RxiKernel<double> ct_rxinv_f64(const RegPlan &rp, int RB, int P0, int Hp);
 
 template <typename R, int NC>
 static int launch_lines(SolveGeom<R> &g, const typename cplx_t<R>::type *in, typename cplx_t<R>::type *out, int axis,
@@ -138,16 +149,25 @@ int fwd_xy(SolveGeom<R> &g, const R *in, typename cplx_t<R>::type *X, typename c
     const int RB = pick_rb_reg(g.N2, g.rx.n, g.H, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), false, reg_budget(sizeof(R)));
     if (RB > 0) {
       const size_t sm = rx_smem(g.N2, g.rx.n, g.H, g.P[0], g.Hp, NC, RB, sizeof(C), sizeof(R), false);
-      if (smem_attr((const void *)k_rxfwd<R, NC>, sm, caller)) return -1;
+      RxfKernel<R> kern = k_rxfwd<R, NC>;
+      if constexpr (NC == 3) {
+        if (g_fft_ct && !g.rx.bl) {
+          RxfKernel<R> ck;
+          if constexpr (sizeof(R) == 4) ck = ct_rxfwd_f32(g.rx, RB, g.P[0], (int)g.Hp);
+          else ck = ct_rxfwd_f64(g.rx, RB, g.P[0], (int)g.Hp);
+          if (ck) kern = ck;
+        }
+      }
+      if (smem_attr((const void *)kern, sm, caller)) return -1;
       const int rows = g.P[1] * g.P[2];
       const int ntiles = (rows + RB - 1) / RB;
       int per = 1;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rxfwd<R, NC>, RL_THREADS, sm) != cudaSuccess || per < 1)
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, RL_THREADS, sm) != cudaSuccess || per < 1)
         per = 1;
       const int grid = std::max(1, std::min(ntiles, per * num_sms()));
       { KTimer kt_(KC_XFWD, st);
-        k_rxfwd<R, NC><<<grid, RL_THREADS, sm, st>>>(g, in, X, RB, cs, vec16r ? 1 : 0,
-                                                     make_fastdiv((unsigned)(NC * RB / RVec<R>::G))); }
+        kern<<<grid, RL_THREADS, sm, st>>>(g, in, X, RB, cs, vec16r ? 1 : 0,
+                                           make_fastdiv((unsigned)(NC * RB / RVec<R>::G))); }
       PM_LAUNCHED();
       CKL(caller);
       const long long Hp = g.Hp;
@@ -217,14 +237,23 @@ int inv_yx(SolveGeom<R> &g, const pmgpu_topo *topo, typename cplx_t<R>::type *Y,
   const int RBr = g.rx_ok ? pick_rb_reg(g.N2, g.rx.n, g.H, g.P[0], g.Hp, NC, sizeof(C), sizeof(R), true, reg_budget(sizeof(R))) : 0;
   if (RBr > 0) {
     const size_t sm = rx_smem(g.N2, g.rx.n, g.H, g.P[0], g.Hp, NC, RBr, sizeof(C), sizeof(R), true);
-    if (smem_attr((const void *)k_rxinv<R, NC>, sm, caller)) return -1;
+    RxiKernel<R> kern = k_rxinv<R, NC>;
+    if constexpr (NC == 3) {
+      if (g_fft_ct && !g.rx.bl) {
+        RxiKernel<R> ck;
+        if constexpr (sizeof(R) == 4) ck = ct_rxinv_f32(g.rx, RBr, g.P[0], (int)g.Hp);
+        else ck = ct_rxinv_f64(g.rx, RBr, g.P[0], (int)g.Hp);
+        if (ck) kern = ck;
+      }
+    }
+    if (smem_attr((const void *)kern, sm, caller)) return -1;
     const int ntiles = (rows + RBr - 1) / RBr;
     int per = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rxinv<R, NC>, RL_THREADS, sm) != cudaSuccess || per < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, RL_THREADS, sm) != cudaSuccess || per < 1)
       per = 1;
     const int grid = std::max(1, std::min(ntiles, per * num_sms()));
     { KTimer kt_(KC_XINV, st);
-      k_rxinv<R, NC><<<grid, RL_THREADS, sm, st>>>(g, X, out, RBr, cs, make_fastdiv((unsigned)(NC * RBr / RVec<R>::G))); }
+      kern<<<grid, RL_THREADS, sm, st>>>(g, X, out, RBr, cs, make_fastdiv((unsigned)(NC * RBr / RVec<R>::G))); }
     PM_LAUNCHED();
     CKL(caller);
   } else {

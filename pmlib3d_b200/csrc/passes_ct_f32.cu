@@ -4,6 +4,7 @@
 // the radix orders the schedule tuner chooses between.  Other plans run the
 // run-time engine.
 #include "passes.cuh"
+#include "xpass_ct.cuh"
 
 namespace pmgpu {
 
@@ -19,6 +20,19 @@ LinesKernel<float> ct_lines_f32(const RegPlan &rp, int TK) {
 }
 
 #undef PMGPU_CT
+
+// x passes of the free-axis row length of 256 cells with four ghost layers (264 reals,
+// a 264-point packed transform) with the rows per tile the launcher picks
+RxfKernel<float> ct_rxfwd_f32(const RegPlan &rp, int RB, int P0, int Hp) {
+  if (ct_match<CtPlan<264, 12, 11, 2>>(rp) && RB == 7 && P0 == 264 && Hp == 272)
+    return k_rxfwd_ct<float, 3, 264, 12, 11, 2, 7, 264, 272>;
+  return nullptr;
+}
+RxiKernel<float> ct_rxinv_f32(const RegPlan &rp, int RB, int P0, int Hp) {
+  if (ct_match<CtPlan<264, 12, 11, 2>>(rp) && RB == 5 && P0 == 264 && Hp == 272)
+    return k_rxinv_ct<float, 3, 264, 12, 11, 2, 5, 264, 272>;
+  return nullptr;
+}
 
 int upload_cs_ct_f32(const void *t32, const void *t64) { return upload_cs_local(t32, t64); }
 

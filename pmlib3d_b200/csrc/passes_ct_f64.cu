@@ -1,6 +1,7 @@
 // passes_ct_f64.cu -- compile-time-plan y / z line passes for double fields of 3
 // components (see passes_ct_f32.cu).
 #include "passes.cuh"
+#include "xpass_ct.cuh"
 
 namespace pmgpu {
 
@@ -14,6 +15,19 @@ LinesKernel<double> ct_lines_f64(const RegPlan &rp, int TK) {
 }
 
 #undef PMGPU_CT
+
+// x passes of the free-axis row length of 256 cells with four ghost layers (264 reals,
+// a 264-point packed transform) with the rows per tile the launcher picks
+RxfKernel<double> ct_rxfwd_f64(const RegPlan &rp, int RB, int P0, int Hp) {
+  if (ct_match<CtPlan<264, 12, 11, 2>>(rp) && RB == 5 && P0 == 264 && Hp == 272)
+    return k_rxfwd_ct<double, 3, 264, 12, 11, 2, 5, 264, 272>;
+  return nullptr;
+}
+RxiKernel<double> ct_rxinv_f64(const RegPlan &rp, int RB, int P0, int Hp) {
+  if (ct_match<CtPlan<264, 12, 11, 2>>(rp) && RB == 4 && P0 == 264 && Hp == 272)
+    return k_rxinv_ct<double, 3, 264, 12, 11, 2, 4, 264, 272>;
+  return nullptr;
+}
 
 int upload_cs_ct_f64(const void *t32, const void *t64) { return upload_cs_local(t32, t64); }
 

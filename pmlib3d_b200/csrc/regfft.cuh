@@ -361,7 +361,7 @@ template <typename P, typename R, int LG, bool GFIRST, bool GLAST, int PEND, int
 __device__ __forceinline__ void rfft_fwd_ct(typename RVec<R>::V *buf, const typename cplx_t<R>::type *tw,
                                             const PhaseGlobal &gl) {
   if constexpr (p < PEND) {
-    const int nz = (GFIRST && p == 0) ? gl.rows_in : P::n;
+    const int nz = p == 0 ? gl.rows_in : P::n;  // phase 0: positions from rows_in on are zero
     rphase_ct<P, p, false, R, LG, GFIRST && p == 0, GLAST && p == P::np - 1>(buf, tw, gl, nz);
     __syncthreads();
     rfft_fwd_ct<P, R, LG, GFIRST, GLAST, PEND, p + 1>(buf, tw, gl);

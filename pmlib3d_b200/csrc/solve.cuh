@@ -374,10 +374,26 @@ __device__ __forceinline__ void z_fused_mid_r(const SolveGeom<R> &g, const RegPl
       if (pre && kx_i < g.H) Gv[k] = g.green[((size_t)min(zs[k], g.M[2] - zs[k]) * g.gM1 + iy) * g.H + kx_i];
     }
     C a[NC][RL];
+    // FP32, compile-time kx tile 8, three components and RL = 4: the four blocks of a
+    // warp sit a multiple of 16 complex apart, so the same position of every block
+    // falls in the same banks.  Threads of odd blocks walk their positions rotated
+    // by one (position j + 1 at step j), which puts the warp's two block parities 8
+    // complex apart: two wavefronts per access instead of four.  Only the order of
+    // the loads and stores changes.  (FP64 accesses need four wavefronts anyway.)
+    constexpr bool ROT = sizeof(R) == 4 && RL == 4 && TKC == 8 && NC == 3;
+    const int rot = ROT ? (beta & 1) : 0;
 #pragma unroll
     for (int c = 0; c < NC; c++) {
+      if constexpr (ROT) {
+        C tmp[RL];
 #pragma unroll
-      for (int j = 0; j < RL; j++) a[c][j] = base[j * L + c];
+        for (int j = 0; j < RL; j++) tmp[j] = base[((j + rot) & (RL - 1)) * L + c];
+#pragma unroll
+        for (int j = 0; j < RL; j++) a[c][j] = rot ? tmp[(j + RL - 1) & (RL - 1)] : tmp[j];
+      } else {
+#pragma unroll
+        for (int j = 0; j < RL; j++) a[c][j] = base[j * L + c];
+      }
       dft<RL, false>(a[c]);
     }
 #pragma unroll
@@ -392,8 +408,13 @@ __device__ __forceinline__ void z_fused_mid_r(const SolveGeom<R> &g, const RegPl
 #pragma unroll
     for (int c = 0; c < NC; c++) {
       dft<RL, true>(a[c]);
+      if constexpr (ROT) {
 #pragma unroll
-      for (int j = 0; j < RL; j++) base[j * L + c] = a[c][j];
+        for (int j = 0; j < RL; j++) base[((j + rot) & (RL - 1)) * L + c] = rot ? a[c][(j + 1) & (RL - 1)] : a[c][j];
+      } else {
+#pragma unroll
+        for (int j = 0; j < RL; j++) base[j * L + c] = a[c][j];
+      }
     }
   }
   __syncthreads();

@@ -1,11 +1,13 @@
 """Compile-time-plan line passes against the run-time register engine.
 
 The y / z passes of 3-component fields run kernels compiled for their plan (length,
-radices, kx tile) where one exists; they do the arithmetic of the run-time engine
+radices, kx tile) where one exists, and so do the x passes (plan of the packed
+half-length transform, rows per tile); they do the arithmetic of the run-time engine
 in the same order, so the solves agree to round-off (the compiler may fuse a
 different multiply and add of an expression in the two builds).  The grids have y
 and z lines of 528 points (256 cells, four ghost layers, free), the length of the
-256^3 step, and the schedules are set to the compiled plans.
+256^3 step, and the schedules are set to the compiled plans; the x-pass grid has 256
+free cells along x (264 reals a row, a 264-point packed transform).
 """
 import numpy as np
 import pytest
@@ -24,13 +26,16 @@ CASES = [
 ]
 
 
-def _solve(prec, sched, specialised, w, reproj):
+YZ_BOX = ((-0.0625, -1.0, -1.0), (0.0625, 1.0, 1.0))
+X_BOX = ((-1.0, -0.0625, -0.0625), (1.0, 0.0625, 0.0625))
+
+
+def _solve(prec, sched, specialised, w, reproj, box=YZ_BOX):
     old = P.fft_specialised(specialised)
     try:
         for axis, rad in sched.items():
             assert P.fft_set_schedule(528, prec, axis, rad, 8) == 0, P.last_error()
-        patch = P.make_patch((-0.0625, -1.0, -1.0), (0.0625, 1.0, 1.0), (1.0 / 128,) * 3,
-                             bound_cond=(0, 0, 0), nghost=4)
+        patch = P.make_patch(box[0], box[1], (1.0 / 128,) * 3, bound_cond=(0, 0, 0), nghost=4)
         ierr, topo = P.pmlib_topology_cuboid(patch, 3)
         assert ierr == 0
         params = P.make_params(order=6, kernel=1, radius=2.0, interp=3)
@@ -57,6 +62,22 @@ def test_specialised_equals_runtime_engine(prec, ysched, zsched, reproj):
     w = gaussian_field(topo, seed=5, noise=0.05)
     v1, w1, t1 = _solve(prec, sched, True, w, reproj)
     v0, w0, _ = _solve(prec, sched, False, w, reproj)
+    assert np.abs(v1).max() > 0
+    tol = 2e-6 if prec == P.FP32 else 1e-14
+    for a, b in ((v1, v0), (w1, w0)):
+        d = np.linalg.norm((a.astype(np.float64) - b).ravel()) / np.linalg.norm(b.astype(np.float64).ravel())
+        assert d < tol, d
+
+
+@pytest.mark.parametrize("prec", [P.FP32, P.FP64])
+@pytest.mark.parametrize("reproj", [False, True])
+def test_specialised_x_passes_equal_runtime_engine(prec, reproj):
+    patch = P.make_patch(X_BOX[0], X_BOX[1], (1.0 / 128,) * 3, bound_cond=(0, 0, 0), nghost=4)
+    ierr, topo = P.pmlib_topology_cuboid(patch, 3)
+    assert topo.ncell[0] == 256
+    w = gaussian_field(topo, seed=9, noise=0.05)
+    v1, w1, _ = _solve(prec, {}, True, w, reproj, box=X_BOX)
+    v0, w0, _ = _solve(prec, {}, False, w, reproj, box=X_BOX)
     assert np.abs(v1).max() > 0
     tol = 2e-6 if prec == P.FP32 else 1e-14
     for a, b in ((v1, v0), (w1, w0)):
