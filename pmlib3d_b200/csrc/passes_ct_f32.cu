@@ -1,8 +1,8 @@
-// passes_ct_f32.cu -- compile-time-plan y / z line passes for float fields of 3
-// components: the plans and kx tiles of the common grid lengths (the free-axis
-// lengths 2 (2^k + 8) of 2^k cells with four ghost layers, and powers of two), with
-// the radix orders the schedule tuner chooses between.  Other plans run the
-// run-time engine.
+// passes_ct_f32.cu -- compile-time-plan line passes for float fields of 3
+// components: y / z passes for the plans and kx tiles of the 528-point lines (256
+// cells with four ghost layers, free) with the radix orders and tiles the schedule
+// tuner chooses between, and x passes for the 264-real rows of the same grid.  Other
+// plans run the run-time engine.
 #include "passes.cuh"
 #include "xpass_ct.cuh"
 
@@ -16,6 +16,9 @@ LinesKernel<float> ct_lines_f32(const RegPlan &rp, int TK) {
   PMGPU_CT(528, 24, 22, 1, 8)
   PMGPU_CT(528, 22, 24, 1, 8)
   PMGPU_CT(528, 12, 11, 4, 8)
+  PMGPU_CT(528, 24, 22, 1, 4)
+  PMGPU_CT(528, 22, 24, 1, 4)
+  PMGPU_CT(528, 12, 11, 4, 4)
   return nullptr;
 }
 

@@ -1,4 +1,4 @@
-// passes_ct_f64.cu -- compile-time-plan y / z line passes for double fields of 3
+// passes_ct_f64.cu -- compile-time-plan line passes for double fields of 3
 // components (see passes_ct_f32.cu).
 #include "passes.cuh"
 #include "xpass_ct.cuh"
@@ -11,6 +11,8 @@ namespace pmgpu {
 LinesKernel<double> ct_lines_f64(const RegPlan &rp, int TK) {
   PMGPU_CT(528, 12, 11, 4, 8)
   PMGPU_CT(528, 8, 6, 11, 8)
+  PMGPU_CT(528, 12, 11, 4, 4)
+  PMGPU_CT(528, 8, 6, 11, 4)
   return nullptr;
 }
 

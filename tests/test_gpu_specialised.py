@@ -17,12 +17,14 @@ from tests.helpers import gaussian_field
 
 pytestmark = pytest.mark.gpu
 
-# (precision, y schedule, z schedule), tile 8
+# (precision, y schedule, z schedule, kx tile)
 CASES = [
-    (P.FP32, (24, 22), (12, 11, 4)),
-    (P.FP32, (24, 22), (22, 24)),
-    (P.FP64, (12, 11, 4), (12, 11, 4)),
-    (P.FP64, (12, 11, 4), (8, 6, 11)),
+    (P.FP32, (24, 22), (12, 11, 4), 8),
+    (P.FP32, (24, 22), (22, 24), 8),
+    (P.FP32, (22, 24), (12, 11, 4), 4),
+    (P.FP64, (12, 11, 4), (12, 11, 4), 8),
+    (P.FP64, (12, 11, 4), (8, 6, 11), 8),
+    (P.FP64, (12, 11, 4), (8, 6, 11), 4),
 ]
 
 
@@ -30,11 +32,11 @@ YZ_BOX = ((-0.0625, -1.0, -1.0), (0.0625, 1.0, 1.0))
 X_BOX = ((-1.0, -0.0625, -0.0625), (1.0, 0.0625, 0.0625))
 
 
-def _solve(prec, sched, specialised, w, reproj, box=YZ_BOX):
+def _solve(prec, sched, specialised, w, reproj, box=YZ_BOX, tile=8):
     old = P.fft_specialised(specialised)
     try:
         for axis, rad in sched.items():
-            assert P.fft_set_schedule(528, prec, axis, rad, 8) == 0, P.last_error()
+            assert P.fft_set_schedule(528, prec, axis, rad, tile) == 0, P.last_error()
         patch = P.make_patch(box[0], box[1], (1.0 / 128,) * 3, bound_cond=(0, 0, 0), nghost=4)
         ierr, topo = P.pmlib_topology_cuboid(patch, 3)
         assert ierr == 0
@@ -53,15 +55,15 @@ def _solve(prec, sched, specialised, w, reproj, box=YZ_BOX):
             P.fft_set_schedule(528, prec, axis, None)
 
 
-@pytest.mark.parametrize("prec,ysched,zsched", CASES)
+@pytest.mark.parametrize("prec,ysched,zsched,tile", CASES)
 @pytest.mark.parametrize("reproj", [False, True])
-def test_specialised_equals_runtime_engine(prec, ysched, zsched, reproj):
+def test_specialised_equals_runtime_engine(prec, ysched, zsched, tile, reproj):
     sched = {1: ysched, 2: zsched}
     patch = P.make_patch((-0.0625, -1.0, -1.0), (0.0625, 1.0, 1.0), (1.0 / 128,) * 3, bound_cond=(0, 0, 0), nghost=4)
     ierr, topo = P.pmlib_topology_cuboid(patch, 3)
     w = gaussian_field(topo, seed=5, noise=0.05)
-    v1, w1, t1 = _solve(prec, sched, True, w, reproj)
-    v0, w0, _ = _solve(prec, sched, False, w, reproj)
+    v1, w1, t1 = _solve(prec, sched, True, w, reproj, tile=tile)
+    v0, w0, _ = _solve(prec, sched, False, w, reproj, tile=tile)
     assert np.abs(v1).max() > 0
     tol = 2e-6 if prec == P.FP32 else 1e-14
     for a, b in ((v1, v0), (w1, w0)):
