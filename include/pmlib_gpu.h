@@ -242,11 +242,12 @@ int pmgpu_batch_fused(const pmgpu_batch *batch);
  * the same results to round-off; returns the previous setting. */
 int pmgpu_fft_engine(int engine);
 
-/* Lets the y / z line passes of 3-component fields run kernels compiled for their
- * plan (length, radices and kx tile known to the compiler) where one exists: 1 =
- * on (default), 0 = the run-time register engine only (no counterpart in the
- * reference).  The results are bit-identical either way; returns the previous
- * setting. */
+/* Lets the line passes of 3-component fields run kernels compiled for their plan
+ * where one exists (y / z: length, radices and kx tile; x: the packed transform's
+ * plan, rows per tile, row length and spectrum pitch known to the compiler): 1 = on
+ * (default), 0 = the run-time register engine only (no counterpart in the
+ * reference).  The arithmetic is the same either way (results agree to round-off);
+ * returns the previous setting. */
 int pmgpu_fft_specialised(int on);
 
 /* Global particle diagnostics accumulated in FP64 for FP32 or FP64 particle arrays
