@@ -956,7 +956,9 @@ __global__ void __launch_bounds__(M2P_THREADS) k_m2p_tile(PartGeom<R> g, const R
   constexpr int CX = M2P_TX + W - 1, CY = M2P_TY + W - 1, CZ = M2P_TZ + W - 1, NR = M2P_TY * M2P_TZ;
   constexpr int PLANE = CZ * CY * CX;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R *cells = reinterpret_cast<R *>(smem_raw);  // [3][CZ][CY][CX]
+  // components 0 and 1 as pairs [CZ][CY][CX][2], component 2 as a plane [CZ][CY][CX]:
+  // one 8-byte (FP64: 16-byte) and one 4-byte (8-byte) load a stencil point
+  R *cells = reinterpret_cast<R *>(smem_raw);
   __shared__ int rs[NR + 1], rg[NR];
   // tile origin in bins; org (<= 0) puts the tile edges on the first interior bin, so
   // that one particle per cell fills whole 32-bin rows (warp-aligned, no empty tiles)
@@ -998,7 +1000,7 @@ __global__ void __launch_bounds__(M2P_THREADS) k_m2p_tile(PartGeom<R> g, const R
   {
     constexpr int NE = (CX * 3 + 31) / 32;
     int so[NE], dof[NE];
-    bool ok[NE];
+    bool ok[NE], pair[NE];
 #pragma unroll
     for (int k = 0; k < NE; k++) {
       const int e = lane + 32 * k;
@@ -1006,12 +1008,13 @@ __global__ void __launch_bounds__(M2P_THREADS) k_m2p_tile(PartGeom<R> g, const R
       const int cx = cx0 + xx;
       ok[k] = e < CX * 3 && cx >= 0 && cx < g.ext[0];
       so[k] = cx * 3 + c;
-      dof[k] = e < CX * 3 ? c * PLANE + xx : -1;
+      pair[k] = c < 2;
+      dof[k] = e < CX * 3 ? (c < 2 ? 2 * xx + c : 2 * PLANE + xx) : -1;
     }
     for (int row = wid; row < CZ * CY; row += nw) {
       const int yy = row % CY, zz = row / CY;
       const int cy = cy0 + yy, cz = cz0 + zz;
-      R *dst = cells + (size_t)row * CX;
+      R *dst01 = cells + (size_t)2 * row * CX, *dst2 = cells + (size_t)row * CX;
       const bool rowin = cy >= 0 && cy < g.ext[1] && cz >= 0 && cz < g.ext[2];
       const R *src = f + (((size_t)(rowin ? cz : 0) * g.ext[1] + (rowin ? cy : 0)) * g.ext[0]) * 3;
       R v[NE];
@@ -1019,7 +1022,7 @@ __global__ void __launch_bounds__(M2P_THREADS) k_m2p_tile(PartGeom<R> g, const R
       for (int k = 0; k < NE; k++) v[k] = (rowin && ok[k]) ? __ldg(src + so[k]) : R(0);
 #pragma unroll
       for (int k = 0; k < NE; k++)
-        if (dof[k] >= 0) dst[dof[k]] = v[k];
+        if (dof[k] >= 0) (pair[k] ? dst01 : dst2)[dof[k]] = v[k];
     }
   }
   __syncthreads();
@@ -1049,20 +1052,24 @@ __global__ void __launch_bounds__(M2P_THREADS) k_m2p_tile(PartGeom<R> g, const R
       // first stencil cell relative to the tile: bin - tile origin
       tb[e] = b - g.blo[e] - (e == 0 ? x0 : e == 1 ? y0 : z0);
     }
-    const R *base = cells + (tb[2] * CY + tb[1]) * CX + tb[0];
+    typedef typename Pair2<R>::T P2;
+    const int c0i = (tb[2] * CY + tb[1]) * CX + tb[0];
+    const P2 *base01 = reinterpret_cast<const P2 *>(cells) + c0i;
+    const R *base2 = cells + 2 * PLANE + c0i;
     R a0 = R(0), a1 = R(0), a2 = R(0);
 #pragma unroll
     for (int sk = 0; sk < W; sk++)
 #pragma unroll
       for (int sj = 0; sj < W; sj++) {
         const R wjk = w[1][sj] * w[2][sk];
-        const R *row = base + (sk * CY + sj) * CX;
+        const int ro = (sk * CY + sj) * CX;
 #pragma unroll
         for (int si = 0; si < W; si++) {
           const R wt = w[0][si] * wjk;
-          a0 += wt * row[si];
-          a1 += wt * row[PLANE + si];
-          a2 += wt * row[2 * PLANE + si];
+          const P2 u01 = base01[ro + si];
+          a0 += wt * u01.x;
+          a1 += wt * u01.y;
+          a2 += wt * base2[ro + si];
         }
       }
     o[(size_t)3 * p + 0] = a0;
