@@ -402,7 +402,7 @@ template <typename R, int W> struct DepCfg;
 // ncw consumer warps, two producer groups of npg warps, staging capacity per buffer
 template <> struct DepCfg<float, 4> { static constexpr int ncw = 14, npg = 4, cap = 1152, ws = 4; };
 template <> struct DepCfg<float, 6> { static constexpr int ncw = 12, npg = 2, cap = 1024, ws = 8; };
-template <> struct DepCfg<double, 4> { static constexpr int ncw = 6, npg = 2, cap = 640, ws = 4; };
+template <> struct DepCfg<double, 4> { static constexpr int ncw = 8, npg = 2, cap = 704, ws = 4; };
 template <> struct DepCfg<double, 6> { static constexpr int ncw = 6, npg = 2, cap = 512, ws = 8; };
 
 template <typename R, int W> __host__ __device__ constexpr int dep_threads() {
