@@ -32,12 +32,12 @@ YZ_BOX = ((-0.0625, -1.0, -1.0), (0.0625, 1.0, 1.0))
 X_BOX = ((-1.0, -0.0625, -0.0625), (1.0, 0.0625, 0.0625))
 
 
-def _solve(prec, sched, specialised, w, reproj, box=YZ_BOX, tile=8):
+def _solve(prec, sched, specialised, w, reproj, box=YZ_BOX, tile=8, length=528, h=1.0 / 128, bc=(0, 0, 0)):
     old = P.fft_specialised(specialised)
     try:
         for axis, rad in sched.items():
-            assert P.fft_set_schedule(528, prec, axis, rad, tile) == 0, P.last_error()
-        patch = P.make_patch(box[0], box[1], (1.0 / 128,) * 3, bound_cond=(0, 0, 0), nghost=4)
+            assert P.fft_set_schedule(length, prec, axis, rad, tile) == 0, P.last_error()
+        patch = P.make_patch(box[0], box[1], (h,) * 3, bound_cond=bc, nghost=4)
         ierr, topo = P.pmlib_topology_cuboid(patch, 3)
         assert ierr == 0
         params = P.make_params(order=6, kernel=1, radius=2.0, interp=3)
@@ -52,7 +52,7 @@ def _solve(prec, sched, specialised, w, reproj, box=YZ_BOX, tile=8):
     finally:
         P.fft_specialised(old)
         for axis in sched:
-            P.fft_set_schedule(528, prec, axis, None)
+            P.fft_set_schedule(length, prec, axis, None)
 
 
 @pytest.mark.parametrize("prec,ysched,zsched,tile", CASES)
@@ -85,3 +85,27 @@ def test_specialised_x_passes_equal_runtime_engine(prec, reproj):
     for a, b in ((v1, v0), (w1, w0)):
         d = np.linalg.norm((a.astype(np.float64) - b).ravel()) / np.linalg.norm(b.astype(np.float64).ravel())
         assert d < tol, d
+
+
+# the periodic 512-point lines of the 512 x 512 x 256 ppf grid: y lines under a
+# compiled schedule, and x rows of 512 periodic cells (a 256-point packed transform)
+PPF_Y_BOX = ((-0.0625, -1.0, -0.0625), (0.0625, 1.0, 0.0625))
+PPF_X_BOX = ((-1.0, -0.0625, -0.0625), (1.0, 0.0625, 0.0625))
+
+
+@pytest.mark.parametrize("prec", [P.FP32, P.FP64])
+@pytest.mark.parametrize("case", ["y", "x"])
+def test_specialised_periodic_512_lines_equal_runtime_engine(prec, case):
+    h, bc = 1.0 / 256, (1, 1, 0)
+    box = PPF_Y_BOX if case == "y" else PPF_X_BOX
+    sched = {1: (8, 8, 8)} if case == "y" else {}
+    patch = P.make_patch(box[0], box[1], (h,) * 3, bound_cond=bc, nghost=4)
+    ierr, topo = P.pmlib_topology_cuboid(patch, 3)
+    assert topo.ncell[1 if case == "y" else 0] == 512
+    w = gaussian_field(topo, seed=11, noise=0.05)
+    v1, w1, _ = _solve(prec, sched, True, w, False, box=box, length=512, h=h, bc=bc)
+    v0, w0, _ = _solve(prec, sched, False, w, False, box=box, length=512, h=h, bc=bc)
+    assert np.abs(v1).max() > 0
+    tol = 2e-6 if prec == P.FP32 else 1e-14
+    d = np.linalg.norm((v1.astype(np.float64) - v0).ravel()) / np.linalg.norm(v0.astype(np.float64).ravel())
+    assert d < tol, d
