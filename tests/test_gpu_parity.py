@@ -314,6 +314,24 @@ def test_p2m_fp64(name, xmin, xmax, dx, bc, ng, interp):
     assert np.array_equal(mg, mg2)
 
 
+@pytest.mark.parametrize("nvar", [1, 2, 4])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_p2m_other_component_counts(nvar, precision):
+    """Fields of 1, 2 or 4 components deposit in groups of three and one."""
+    name, xmin, xmax, dx, bc, ng = CASES[1]
+    po, to, qo, pg, tg, qg = setup_pair(xmin, xmax, dx, bc, ng, interp=3)
+    pos, val3 = jittered_particles(to, seed=17, jitter=0.45, incl_ghost=True)
+    rng = np.random.default_rng(3)
+    val = np.ascontiguousarray(rng.standard_normal((pos.shape[0], nvar)) + np.tile(val3, 2)[:, :nvar])
+    to.npart = tg.npart = pos.shape[0]
+    mo = np.zeros(O.topo_shape(to, nvar))
+    assert O.interp_particle_mesh(to, 3, pos, val, mo) == 0
+    dt, tol = (np.float64, 1e-13) if precision == "fp64" else (np.float32, 1e-5)
+    mg = np.full(mo.shape, 7.0, dt)
+    assert P.pmlib_interp_particle_mesh(tg, qg, pos.astype(dt), val.astype(dt), mg, clear=True) == 0
+    assert rel_l2(mg, mo) < tol, rel_l2(mg, mo)
+
+
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_p2m_crowded_bins(precision):
     """Collisions: bins holding 2..32 particles (thread fix-up), 100 and 3000 (one
