@@ -29,11 +29,22 @@ __device__ __forceinline__ void rxf_tile_ct(const SolveGeom<R> &g, typename cplx
     const R *xr = Sr + (size_t)rr * P0 * NC;
     const int x0 = 2 * m, x1 = 2 * m + 1;
     const bool ok = row0 + rr < nrows;
+    if constexpr (NC == 3 && P0 % 2 == 0) {
+      // the six reals of points 2m and 2m+1 as three aligned pairs (rows of 3 P0
+      // reals start on even offsets): conflict-free within each half-warp
+      C v[3];
 #pragma unroll
-    for (int c = 0; c < NC; c++) {
-      const R a = ok ? xr[x0 * NC + c] : R(0);
-      const R b = (ok && x1 < P0) ? xr[x1 * NC + c] : R(0);
-      Bc[m * L + rr * NC + c] = mk(a, b);
+      for (int h = 0; h < 3; h++) v[h] = ok ? reinterpret_cast<const C *>(xr)[3 * m + h] : mk(R(0), R(0));
+      Bc[m * L + rr * NC + 0] = mk(v[0].x, v[1].y);
+      Bc[m * L + rr * NC + 1] = mk(v[0].y, v[2].x);
+      Bc[m * L + rr * NC + 2] = mk(v[1].x, v[2].y);
+    } else {
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        const R a = ok ? xr[x0 * NC + c] : R(0);
+        const R b = (ok && x1 < P0) ? xr[x1 * NC + c] : R(0);
+        Bc[m * L + rr * NC + c] = mk(a, b);
+      }
     }
   }
   __syncthreads();
