@@ -430,6 +430,9 @@ template <typename R, int W> __host__ __device__ constexpr size_t dep_slot_bytes
 template <typename R, int W> __host__ __device__ constexpr size_t deposit_smem() {
   return 2 * dep_buf_bytes<R, W>() + 4 * dep_slot_bytes<R, W>() + 16 * sizeof(int);
 }
+static_assert(deposit_smem<float, 4>() <= 227 * 1024 && deposit_smem<float, 6>() <= 227 * 1024 &&
+                  deposit_smem<double, 4>() <= 227 * 1024 && deposit_smem<double, 6>() <= 227 * 1024,
+              "the deposit's staging must fit one CTA's shared memory");
 
 // an int carried in a value slot (bit pattern)
 template <typename R> __device__ __forceinline__ R int_bits(int v);
