@@ -351,9 +351,10 @@ def run_served(P, torch, rates=(100.0, 300.0, 1000.0), count=60, budget_gb=24.0)
     """Served stream at swept Poisson arrival rates (FP32 form): solves/s, p50/p99."""
     from pmlib3d_b200 import serve as S
     par = P.make_params(order=6, kernel=1, radius=2.0, interp=3)
-    # warm-up: one stream of requests (its own seed) through a server of its own, so
-    # that the first measured rate does not pay the first use of kernels and tables
-    warm = S.request_stream(24, rate=1000.0, seed=9)
+    # warm-up: one stream of large requests (its own seed) through a server of its own,
+    # so that the first measured rate does not pay the first use of kernels and tables
+    # or the growth of the device's memory pool
+    warm = S.request_stream(48, rate=1000.0, seed=9, nmin=128, nmax=256)
     srv = S.Server(par, precision=P.FP32, slots=8, budget=int(budget_gb * 1e9))
     srv.run(warm)
     srv.close()
@@ -372,7 +373,7 @@ def run_served(P, torch, rates=(100.0, 300.0, 1000.0), count=60, budget_gb=24.0)
         torch.cuda.empty_cache()
     return {"workload": f"served: Poisson arrivals, cells per axis log-uniform 32-256, bc from {{fff, ppf, pff}}, "
                         f"Gaussian blob or ring along a random axis, FP32 form, {count} requests per rate "
-                        f"after a warm-up stream of 24, HBM budget {budget_gb:g} GB, 8 slots, Green's spectra "
+                        f"after a warm-up stream of 48 (128-256 cells a side), HBM budget {budget_gb:g} GB, 8 slots, Green's spectra "
                         f"cached per grid",
             "sweep": out}
 
