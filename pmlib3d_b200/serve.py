@@ -114,7 +114,10 @@ class Server:
         self.precision = precision
         self.nghost = nghost
         self.budget = int(budget)
-        self.slots = [_Slot(torch.cuda.Stream()) for _ in range(slots)]
+        # high-priority streams: the blocks of queued solves are dispatched before those
+        # of a plan set-up running at the same time (its FP64 Green's function and
+        # transform run at the default priority)
+        self.slots = [_Slot(torch.cuda.Stream(priority=-1)) for _ in range(slots)]
         self.ahead = ahead if ahead is not None else 2 * slots
         self.idle = OrderedDict()   # key -> list of idle plans (LRU order of keys)
         self.held = 0               # bytes of all live plans and of the admitted requests' buffers
