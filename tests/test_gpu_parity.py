@@ -1,5 +1,5 @@
 """GPU parity: every entry point of the C ABI against the CPU oracle on the same
-seeded inputs.  FP64 plain path: relative L2 <= 1e-12 (the bar of the north star;
+seeded inputs.  FP64 plain path: relative L2 <= 1e-12 (the FP64 drop-in's bar;
 the FFT summation order differs from the Glassman FFT, ~1e-15).  FP32 form:
 relative L2 <= 1e-5 against the FP64 oracle."""
 import copy
